@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Benchmark of the CGFD time-stepping path: Gcell-updates/s per RK4 step.
+
+Workload (default): the 400x400x200 Gaussian-hill model (hybrid curvilinear
+grid, vertical spacing 50->150 m, 3 perturbed layers, double-couple source,
+20-cell CFS-PML, 400 surface receivers) on one B200, FP32.  A "step" is one
+full RK4 time step (4 fused RHS+update stage kernels, source injection and the
+receiver record, replayed as a CUDA graph).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU runs are independent replicas (one model per GPU, no exchange);
+value is the sum over ranks of cells*K divided by the slowest rank's time.
+--impl reference runs the reference's own device runtime (src/calculate.cu,
+built from its sources into oracle/_ref/) on the same model.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "copara-cgfd3d_b200", "python"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "Gcell-updates/s per RK4 step"
+UNIT = "Gcell/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    p.add_argument("--kernel", choices=("fused", "simple"), default="fused")
+    p.add_argument("--config", choices=("hill400", "flat160"), default="hill400")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    return p.parse_args()
+
+
+def build_model(cfg, nt):
+    import models
+    if cfg == "hill400":
+        return models.config_c2(nt=nt)
+    return models.config_c1(nt=nt)
+
+
+def workload_name(cfg):
+    return {"hill400": "gaussian_hill_400x400x200_pml20",
+            "flat160": "flat_halfspace_160x160x80_pml12"}[cfg]
+
+
+def algorithmic_bytes_per_step(m, elem=4):
+    """Minimum HBM bytes of one RK4 step of the fused design: 144 state values
+    per cell (27+45+45+27 over the 4 stages: reads of W, FW, tW, writes of W,
+    tW, FW), the same again for each (cell, PML direction) pair (ADE
+    auxiliaries), and (3 media + m metric) coefficients per cell per stage
+    (m = 3 above ConIndex, 1 below, 0 for a trivial metric)."""
+    nxy = m.ni * m.nj
+    cells = m.cells
+    state = 144 * elem * cells
+    nab = m.nabs
+    pml_pairs = ((nab[0] + nab[1]) * m.nj * m.nk + (nab[2] + nab[3]) * m.ni * m.nk +
+                 (nab[4] + nab[5]) * m.ni * m.nj)
+    aux = 144 * elem * pml_pairs
+    zz = m.metric["zeta_z"][3:-3, 3:-3, 3:-3]
+    flat = bool(np.all(zz == 1.0) and np.all(m.metric["jac"][3:-3, 3:-3, 3:-3] == 1.0)
+                and np.all(m.metric["zeta_x"][3:-3, 3:-3, 3:-3] == 0.0))
+    if flat:
+        coef = 3 * 4 * 4 * cells
+    else:
+        n_curved = nxy * (m.nk + 3 - m.con_index)
+        coef = 4 * 4 * (6 * n_curved + 4 * (cells - n_curved))
+    return state + aux + coef
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(workload, kernel):
+    """Per-launch DRAM bytes of the stage kernel from the committed ncu
+    summary (profiles/stage_traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "stage_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    e = d.get(workload, {}).get(kernel)
+    return None if e is None else float(e["dram_bytes_per_launch"])
+
+
+def cpu_baseline(cfg, seconds):
+    """FP64 C++/OpenMP oracle (the CPU restatement of the reference path) on
+    the same model, for a bounded number of steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    m = build_model(cfg, nt=64)
+    o = pyoracle.OracleSolver(m.desc(), 0)
+    m.load(o)
+    o.step(1)  # warm caches, first touch
+    steps, t0 = 0, time.perf_counter()
+    while steps < 60:
+        o.step(1)
+        steps += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    el = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": m.cells * steps / el / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{workload_name(cfg)}, {steps} RK4 steps after 1 warm-up step, "
+                      f"FP64 oracle, {el:.1f} s"}
+
+
+def dist_init(n):
+    import torch
+    import torch.distributed as dist
+    if n <= 1:
+        return None, 0, 1, 0
+    rank = int(os.environ["RANK"])
+    world = int(os.environ["WORLD_SIZE"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    import datetime
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                            device_id=torch.device("cuda", local))
+    return dist, rank, world, local
+
+
+def allmax(dist, x):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        import torch
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def run_reference(args):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refio
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    if not refio.available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference parity driver oracle/_ref/ref_wavesim not built"}))
+        return
+    nt = args.warmup + args.steps + 2
+    m = build_model(args.config, nt)
+    r = refio.run(m, args.warmup + args.steps, timeout=3600)
+    secs = float(np.sum(r["step_secs"][args.warmup:args.warmup + args.steps]))
+    value = m.cells * args.steps / secs / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded model generator)", "impl": "reference",
+        "config": {"workload": workload_name(args.config), "cells": m.cells,
+                   "l2": "state >> L2 (126 MB), no flush needed"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"{workload_name(args.config)}, {args.steps} steps after "
+                                   f"{args.warmup} warm-up; the reference's own calculate.cu "
+                                   "(CUDA-only path) built from its sources, driven by one host "
+                                   "thread on the B200"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    dist, rank, world, local = dist_init(args.gpus)
+    import cgfd
+    kernel = cgfd.KERNEL_FUSED if args.kernel == "fused" else cgfd.KERNEL_SIMPLE
+    K, W = args.steps, args.warmup
+    K2 = min(K, 20)
+    nt = W + K + K2 + 2
+    m = build_model(args.config, nt)
+    s = cgfd.Solver(m.desc(kernel=kernel, device=local))
+    m.load(s)
+    s.prepare()
+    s.step(W)
+    s.sync()
+    barrier(dist)
+    with ClockSampler(local) as clk:
+        ms, _ = s.step_timed(K)
+    ms = allmax(dist, ms)
+    # mean duration of one stage kernel launch (stages issued individually)
+    _, stage_ms = s.step_timed(K2, per_stage=True)
+    stage_ms = allmax(dist, stage_ms)
+    nbad = s.check_finite()
+    s.close()
+    value = world * m.cells * K / (ms / 1e3) / 1e9
+
+    e2e = None
+    if not args.no_e2e:
+        barrier(dist)
+        t0 = time.perf_counter()
+        s2 = cgfd.Solver(m.desc(kernel=kernel, device=local))
+        m.load(s2)
+        s2.step(K)
+        seis = s2.seismograms()
+        s2.sync()
+        el = allmax(dist, time.perf_counter() - t0)
+        s2.close()
+        e2e = {"value": world * m.cells * K / el / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": int(m.upload_bytes() / K),
+               "d2h_bytes_per_step": int(seis.nbytes / m.nt),
+               "what": "cgfd_create + uploads of the model from host arrays + K steps + "
+                       "seismogram download, wall clock"}
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    bps = algorithmic_bytes_per_step(m)
+    achieved = bps / 4 / (stage_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = committed_traffic(workload_name(args.config), args.kernel)
+    n_src = 1 if (len(m.mnt_loc) + len(m.frc_loc)) else 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded model generator)",
+        "config": {"workload": workload_name(args.config), "cells": m.cells,
+                   "kernel": args.kernel, "replicas": world,
+                   "l2": "state >> L2 (126 MB), no flush needed",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                     "algorithmic_bytes_per_step": bps, "stage_kernel_ms": stage_ms},
+        "clocks": clk.summary(),
+        "gpu_launches": K * (4 + 4 * n_src + 1),
+        "nonfinite": nbad,
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.config, args.cpu_seconds)
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

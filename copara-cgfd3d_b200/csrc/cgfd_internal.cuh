@@ -1,0 +1,116 @@
+// cgfd_internal.cuh -- device data layout and kernel parameter blocks of the
+// B200 CGFD solver.
+//
+// HBM layout (all arrays 256-byte aligned, zero-initialised):
+//   * Every wavefield component is a 3-D array with x fastest:
+//         idx(ix, iy, iz) = (iz * nyi + iy) * px + ix
+//     ix = i_ref + 1 (valid x starts at XO = 4 so that a tile that starts at a
+//     valid cell starts on a 16-byte boundary), iy = j_ref, iz = k_ref.
+//     px (x pitch) is a multiple of 32 floats (128 B) and leaves >= 4 zero
+//     ghost columns on the right; nyi = nj+6, nzi = nk+6.  Ghost cells are
+//     never written, so the one-sided stencils read zeros there exactly like
+//     the reference's single-rank run (its ghost planes stay 0).
+//   * A field "set" is 9 consecutive components (Vx Vy Vz Txx Tyy Tzz Txy Txz
+//     Tyz) separated by fstride elements.  The solver keeps 4 sets: FW (step
+//     start), Wa and Wb (stage outputs, ping-pong because the stencil cannot
+//     run in place) and tW (RK accumulator).
+//   * ADE CFS-PML auxiliaries are compact per direction:
+//         X: (iz * nyi + iy) * nxa + xa      xa in [0, nabs0+nabs1)
+//         Y: (iz * nya + ya) * px  + ix      ya in [0, nabs2+nabs3)
+//         Z: (za * nyi + iy) * px  + ix      za in [0, nabs4+nabs5)
+//     each with 3 sets (FA step start, A stage value updated in place since
+//     the auxiliaries are read only at their own cell, tA accumulator).
+//   * Media are stored as (lambda+2mu, mu, 1/rho); the metric as zeta_x,
+//     zeta_y, zeta_z, jac; 1-D PML profiles APD, B, DB per axis in the same
+//     internal index space; the free-surface matrices matVx2Vz / matVy2Vz as
+//     18 planes of px*nyi.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+namespace cgfd {
+
+constexpr int LFD = 3;   // ghost width of the reference (LenFD)
+constexpr int XO = 4;    // internal x index of the first valid cell
+constexpr int NCOMP = 9;
+
+enum { VX = 0, VY, VZ, TXX, TYY, TZZ, TXY, TXZ, TYZ };
+
+// DRP/opt MacCormack one-sided operator (Zhang 2006; the reference's
+// src/typenew.h:52-56), Gottlieb 2-4 (typenew.h:69-71).
+#define CGFD_DA_1 (-0.30874f)
+#define CGFD_DA0 (-0.6326f)
+#define CGFD_DA1 (1.23300f)
+#define CGFD_DA2 (-0.3334f)
+#define CGFD_DA3 (0.04168f)
+#define CGFD_MA0 (-1.1666666666666667f)
+#define CGFD_MA1 (1.3333333333333333f)
+#define CGFD_MA2 (-0.16666666666666666f)
+
+struct Geom {
+  int ni, nj, nk;      // valid cells
+  int px, nyi, nzi;    // internal dims (px = x pitch)
+  int top;             // iz of the free surface (nk + 2)
+  int con;             // ConIndex (iz)
+  int nabs[6];
+  int nxa, nya, nza;   // auxiliary widths per direction
+  size_t plane;        // px * nyi
+  size_t fstride;      // elements between components of a set
+  size_t astride[3];   // elements between components of an aux set
+};
+
+__host__ __device__ inline size_t gidx(const Geom &g, int ix, int iy, int iz) {
+  return ((size_t)iz * g.nyi + iy) * g.px + ix;
+}
+
+// Arguments of one RK stage (RKite + Iteration*), for any kernel family.
+struct StageArgs {
+  Geom g;
+  int rk;              // 0..3
+  int X, Y, Z;         // +1 forward / -1 backward per axis
+  float h;             // steph
+  float adt, bdt;      // RK4A[rk]*dt (0 for rk 3), RK4B[rk]*dt
+  const float *in;     // stencil input set (FW for rk 0, else previous W)
+  const float *fw;     // FW (rk 1,2 read it)
+  float *out;          // output set: W (rk 0..2) or FW (rk 3)
+  float *tw;           // tW
+  const float *lam2mu, *mu, *irho;
+  const float *zx, *zy, *zz, *jac;
+  bool flat;           // metric is zeta=(0,0,1), jac=1 everywhere
+  const float *matv;   // 18 planes: matVx2Vz[0..8], matVy2Vz[0..8]
+  const float *apd[3], *b[3], *db[3];
+  // aux sets per direction: ain (FA for rk 0 else A), afw (FA), aout (A, or
+  // FA for rk 3), tA; null when that direction has no PML
+  const float *ain[3];
+  const float *afw[3];
+  float *aout[3];
+  float *ta[3];
+};
+
+// Point sources, applied after a stage as W_out += adt*S, tW += bdt*S
+// (the update is linear in the RHS, so this equals adding S to hW first).
+struct SourceArgs {
+  Geom g;
+  int nmnt, nfrc;
+  const int *mcell;    // internal linear index of each moment source
+  const float *mcoef;  // 6 per source: M / (h^3 J)
+  const float *mstf;   // nmnt * nstfm
+  int nstfm;
+  const int *fcell;
+  const float *fcoef;  // 3 per source: f / (h^3 J rho) (x2 on the surface)
+  const float *fstf;
+  int nstff;
+  int tinc;            // 0, 1, 1, 2 by stage
+  int tindex;          // >= 0: use it; < 0: 2*(*step)+tinc
+  const int *step;     // device step counter
+  float adt, bdt;
+  float *out, *tw;
+  int rk;
+};
+
+void launch_stage_simple(const StageArgs &a, void *stream);
+void launch_stage_fused(const StageArgs &a, void *stream);
+bool fused_supported(const Geom &g);
+
+}  // namespace cgfd

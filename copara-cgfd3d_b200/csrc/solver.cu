@@ -1,0 +1,943 @@
+// solver.cu -- C ABI (include/cgfd.h) of the B200 CGFD solver: device state,
+// uploads with layout conversion, the per-step CUDA graphs, sources,
+// receivers and diagnostics.
+//
+// Reference counterparts: class ChildProcs (src/typedata.h:114-217) and its
+// methods in src/calculate.cu (ctor 107-1005, ParH2D 2050-2228, VelCoeff
+// 1336-1353, RKite 1355-1600, wavesyn/abssyn 2956-3119, C2DPointPick/PWpick
+// 2678-2830), driven by the step loop of src/simulation.cc:252-711.
+#include "../../include/cgfd.h"
+#include "cgfd_internal.cuh"
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace cgfd;
+
+namespace {
+
+std::string g_last_create_error;
+
+// RK4 coefficients (src/calculate.cu:12-13).
+constexpr double RKA[3] = {0.5, 0.5, 1.0};
+constexpr double RKB[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+// F/B direction triples per step%4 and stage (src/simulation.cc:264-641).
+constexpr int DIRS[4][4][3] = {
+    {{1, 1, 1}, {-1, -1, -1}, {1, 1, 1}, {-1, -1, -1}},
+    {{1, 1, -1}, {-1, -1, 1}, {1, 1, -1}, {-1, -1, 1}},
+    {{-1, -1, -1}, {1, 1, 1}, {-1, -1, -1}, {1, 1, 1}},
+    {{-1, -1, 1}, {1, 1, -1}, {-1, -1, 1}, {1, 1, -1}}};
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// ------------------------------ kernels -----------------------------------
+
+// reference layout (i*ny+j)*nz+k  ->  internal layout (x fastest)
+__global__ void to_internal_kernel(const float *__restrict__ src, float *__restrict__ dst,
+                                   Geom g, int nx, int ny, int nz) {
+  const long n = (long)nx * ny * nz;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n;
+       q += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(q % nz);
+    const long r = q / nz;
+    const int j = (int)(r % ny);
+    const int i = (int)(r / ny);
+    dst[gidx(g, i + 1, j, k)] = src[q];
+  }
+}
+__global__ void to_reference_kernel(const float *__restrict__ src, float *__restrict__ dst,
+                                    Geom g, int nx, int ny, int nz) {
+  const long n = (long)nx * ny * nz;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n;
+       q += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(q % nz);
+    const long r = q / nz;
+    const int j = (int)(r % ny);
+    const int i = (int)(r / ny);
+    dst[q] = src[gidx(g, i + 1, j, k)];
+  }
+}
+
+// Point sources (LoadMoment/LoadForce, src/calculate.cu:6130-6255), applied
+// to the stage output; one thread walks the list so that repeated cells add
+// up in a fixed order.
+__global__ void inject_sources_kernel(SourceArgs s) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int t2 = (s.tindex >= 0) ? s.tindex : 2 * (*s.step) + s.tinc;
+  const size_t fs = s.g.fstride;
+  for (int q = 0; q < s.nmnt; ++q) {
+    const float stf = s.mstf[(size_t)q * s.nstfm + t2];
+    const int c = s.mcell[q];
+    for (int m = 0; m < 6; ++m) {
+      const float S = -s.mcoef[6 * q + m] * stf;
+      const size_t o = (size_t)(TXX + m) * fs + c;
+      if (s.rk == 3) {
+        s.out[o] += s.bdt * S;
+      } else {
+        s.out[o] += s.adt * S;
+        s.tw[o] += s.bdt * S;
+      }
+    }
+  }
+  for (int q = 0; q < s.nfrc; ++q) {
+    const float stf = s.fstf[(size_t)q * s.nstff + t2];
+    const int c = s.fcell[q];
+    for (int m = 0; m < 3; ++m) {
+      const float S = stf * s.fcoef[3 * q + m];
+      const size_t o = (size_t)(VX + m) * fs + c;
+      if (s.rk == 3) {
+        s.out[o] += s.bdt * S;
+      } else {
+        s.out[o] += s.adt * S;
+        s.tw[o] += s.bdt * S;
+      }
+    }
+  }
+}
+
+// Receiver recording (PWpick, src/calculate.cu:2780-2830) from FW after a
+// step, into seis[(c*nrecv + r)*nt + t]; then advances the step counter.
+__global__ void record_kernel(const float *__restrict__ fw, size_t fstride,
+                              const int *__restrict__ cells, int nrecv, int nt,
+                              float *__restrict__ seis, int *step) {
+  const int t = *step;
+  for (int q = threadIdx.x; q < 9 * nrecv; q += blockDim.x) {
+    const int c = q / nrecv, r = q % nrecv;
+    if (t < nt) seis[((size_t)c * nrecv + r) * nt + t] = fw[(size_t)c * fstride + cells[r]];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *step = t + 1;
+}
+
+__global__ void count_nonfinite_kernel(const float *__restrict__ v, size_t n,
+                                       unsigned long long *count) {
+  unsigned long long local = 0;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x)
+    if (!isfinite(v[q])) ++local;
+  for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
+}
+
+}  // namespace
+
+struct cgfd_solver {
+  cgfd_desc d{};
+  Geom g{};
+  cudaStream_t st = nullptr;
+  std::string err;
+  float *state = nullptr;  // 4 sets of 9 components: FW, Wa, Wb, tW
+  float *set[4] = {nullptr, nullptr, nullptr, nullptr};
+  int wcur = 0;            // set that holds "W" (last stage output)
+  float *media = nullptr;  // lam2mu, mu, irho
+  float *metric = nullptr; // zeta_x, zeta_y, zeta_z, jac
+  float *pml = nullptr;    // apd x y z, b x y z, db x y z
+  float *pmlp[9] = {};
+  float *aux[3] = {nullptr, nullptr, nullptr};  // per direction: FA, A, tA sets
+  float *matv = nullptr;
+  bool flat = false, have_metric = false, have_media = false, have_pml = false;
+  bool prepared = false;
+  // host copies needed by the FP64 free-surface matrices
+  std::vector<double> top_zeta;            // 3 * nx * ny (surface layer)
+  std::vector<double> top_alpha, top_beta, top_rho;  // nx * ny
+  std::vector<double> hb[3];               // B profiles
+  // sources
+  int nmnt = 0, nfrc = 0, nstfm = 0, nstff = 0;
+  std::vector<int> mloc, floc;
+  std::vector<float> m6, f3;
+  int *d_mcell = nullptr, *d_fcell = nullptr;
+  float *d_mcoef = nullptr, *d_fcoef = nullptr, *d_mstf = nullptr, *d_fstf = nullptr;
+  // receivers
+  int nrecv = 0;
+  int *d_rcell = nullptr;
+  float *d_seis = nullptr;
+  int *d_step = nullptr;
+  int steps = 0;
+  unsigned long long *d_count = nullptr;
+  // graphs (one per step%4 pattern)
+  cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool graphs_ok = false;
+};
+
+namespace {
+
+struct DevGuard {
+  int prev = -1;
+  explicit DevGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DevGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+int cuda_fail(cgfd_solver *h, cudaError_t e, const char *what) {
+  char buf[512];
+  std::snprintf(buf, sizeof(buf), "%s: %s (%d)", what, cudaGetErrorString(e), (int)e);
+  if (h) h->err = buf; else g_last_create_error = buf;
+  return CGFD_ERR_CUDA;
+}
+int arg_fail(cgfd_solver *h, const char *what) {
+  if (h) h->err = what; else g_last_create_error = what;
+  return CGFD_ERR_ARG;
+}
+
+#define CK(h, call)                                         \
+  do {                                                      \
+    cudaError_t e_ = (call);                                \
+    if (e_ != cudaSuccess) return cuda_fail((h), e_, #call); \
+  } while (0)
+
+void free_all(cgfd_solver *h) {
+  for (auto &gr : h->graph)
+    if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; }
+  void *ptrs[] = {h->state, h->media, h->metric, h->pml, h->aux[0], h->aux[1], h->aux[2],
+                  h->matv, h->d_mcell, h->d_fcell, h->d_mcoef, h->d_fcoef, h->d_mstf,
+                  h->d_fstf, h->d_rcell, h->d_seis, h->d_step, h->d_count};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (h->st) cudaStreamDestroy(h->st);
+}
+
+long ref_n(const cgfd_solver *h) {
+  return (long)(h->d.ni + 6) * (h->d.nj + 6) * (h->d.nk + 6);
+}
+
+// host float array (reference layout) -> internal array at dst
+int upload_ref(cgfd_solver *h, const float *host, float *dst) {
+  const long n = ref_n(h);
+  float *tmp = nullptr;
+  CK(h, cudaMalloc(&tmp, n * sizeof(float)));
+  cudaError_t e = cudaMemcpyAsync(tmp, host, n * sizeof(float), cudaMemcpyHostToDevice, h->st);
+  if (e == cudaSuccess) {
+    to_internal_kernel<<<592, 256, 0, h->st>>>(tmp, dst, h->g, h->d.ni + 6, h->d.nj + 6,
+                                                h->d.nk + 6);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return cuda_fail(h, e, "upload");
+  return CGFD_OK;
+}
+
+int download_ref(cgfd_solver *h, const float *src, float *host) {
+  const long n = ref_n(h);
+  float *tmp = nullptr;
+  CK(h, cudaMalloc(&tmp, n * sizeof(float)));
+  to_reference_kernel<<<592, 256, 0, h->st>>>(src, tmp, h->g, h->d.ni + 6, h->d.nj + 6,
+                                               h->d.nk + 6);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(host, tmp, n * sizeof(float), cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return cuda_fail(h, e, "download");
+  return CGFD_OK;
+}
+
+bool valid_loc(const cgfd_solver *h, const int *l) {
+  return l[0] >= LFD && l[0] < h->d.ni + LFD && l[1] >= LFD && l[1] < h->d.nj + LFD &&
+         l[2] >= LFD && l[2] < h->d.nk + LFD;
+}
+int cell_of(const cgfd_solver *h, const int *l) {
+  return (int)gidx(h->g, l[0] + 1, l[1], l[2]);
+}
+
+void invalidate(cgfd_solver *h) {
+  h->prepared = false;
+  h->graphs_ok = false;
+}
+
+// Free-surface velocity-gradient matrices in FP64 (VelPDcoeff under SimpleCar,
+// src/calculate.cu:3320-3428): for each surface column, with e3 = grad zeta,
+// A = C(e3,e3), B = C(e3,e1), C = C(e3,e2) of the isotropic stiffness, and
+// matVx2Vz = -A^-1 B * Bz/Bx, matVy2Vz = -A^-1 C * Bz/By.  A is inverted by
+// Gauss-Jordan without pivoting in the reference's order.
+void surface_matrices(const cgfd_solver *h, std::vector<float> &out) {
+  const int nx = h->d.ni + 6, ny = h->d.nj + 6, top = h->g.top;
+  const size_t plane = h->g.plane;
+  out.assign(18 * plane, 0.f);
+  for (int i = LFD; i < h->d.ni + LFD; ++i)
+    for (int j = LFD; j < h->d.nj + LFD; ++j) {
+      const size_t t2 = (size_t)i * ny + j;
+      const double rho = h->top_rho[t2], al = h->top_alpha[t2], be = h->top_beta[t2];
+      const double mu = rho * be * be, l2m = rho * al * al, la = l2m - 2.0 * mu;
+      const double e[3][3] = {{1, 0, 0}, {0, 1, 0},
+                              {h->top_zeta[t2], h->top_zeta[(size_t)nx * ny + t2],
+                               h->top_zeta[2 * (size_t)nx * ny + t2]}};
+      // stiffness contraction K(p,q)[r][s] for row direction e_p and column e_q
+      auto K = [&](const double *p, const double *q, double *m) {
+        for (int r = 0; r < 3; ++r)
+          for (int s = 0; s < 3; ++s) {
+            const double v = (r == s) ? (l2m * p[r] * q[r]) : (la * p[r] * q[s] + mu * p[s] * q[r]);
+            m[r * 3 + s] = v;
+          }
+        // shear terms on the diagonal: mu*(sum over the other two axes)
+        for (int r = 0; r < 3; ++r) {
+          double sh = 0;
+          for (int a = 0; a < 3; ++a)
+            if (a != r) sh += p[a] * q[a];
+          m[r * 3 + r] += mu * sh;
+        }
+      };
+      double A[9], B[9], C[9];
+      K(e[2], e[2], A);
+      K(e[2], e[0], B);
+      K(e[2], e[1], C);
+      for (int r = 0; r < 3; ++r) {  // Gauss-Jordan, no pivoting
+        double con = A[r * 3 + r];
+        A[r * 3 + r] = 1;
+        for (int s = 0; s < 3; ++s) A[r * 3 + s] /= con;
+        for (int s = 0; s < 3; ++s)
+          if (s != r) {
+            con = A[s * 3 + r];
+            A[s * 3 + r] = 0;
+            for (int q = 0; q < 3; ++q) A[s * 3 + q] -= A[r * 3 + q] * con;
+          }
+      }
+      const double bzx = h->hb[2][top] / h->hb[0][i], bzy = h->hb[2][top] / h->hb[1][j];
+      const size_t m2 = (size_t)j * h->g.px + (i + 1);
+      for (int r = 0; r < 3; ++r)
+        for (int s = 0; s < 3; ++s) {
+          double ab = 0, ac = 0;
+          for (int q = 0; q < 3; ++q) {
+            ab += A[r * 3 + q] * B[q * 3 + s];
+            ac += A[r * 3 + q] * C[q * 3 + s];
+          }
+          out[(size_t)(r * 3 + s) * plane + m2] = (float)(-1 * ab * bzx);
+          out[(size_t)(9 + r * 3 + s) * plane + m2] = (float)(-1 * ac * bzy);
+        }
+    }
+}
+
+StageArgs stage_args(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, int out_set) {
+  StageArgs a{};
+  a.g = h->g;
+  a.rk = rk;
+  a.X = X; a.Y = Y; a.Z = Z;
+  a.h = (float)h->d.steph;
+  a.adt = (rk < 3) ? (float)(RKA[rk] * h->d.stept) : 0.f;
+  a.bdt = (float)(RKB[rk] * h->d.stept);
+  a.in = h->set[in_set];
+  a.fw = h->set[0];
+  a.out = h->set[out_set];
+  a.tw = h->set[3];
+  const size_t fs = h->g.fstride;
+  a.lam2mu = h->media; a.mu = h->media + fs; a.irho = h->media + 2 * fs;
+  a.zx = h->metric; a.zy = h->metric + fs; a.zz = h->metric + 2 * fs; a.jac = h->metric + 3 * fs;
+  a.flat = h->flat;
+  a.matv = h->matv;
+  for (int q = 0; q < 3; ++q) {
+    a.apd[q] = h->pmlp[q]; a.b[q] = h->pmlp[3 + q]; a.db[q] = h->pmlp[6 + q];
+    if (h->aux[q]) {
+      const size_t ss = 9 * h->g.astride[q];
+      float *FA = h->aux[q], *A = h->aux[q] + ss, *TA = h->aux[q] + 2 * ss;
+      a.ain[q] = (rk == 0) ? FA : A;
+      a.afw[q] = FA;
+      a.aout[q] = (rk == 3) ? FA : A;
+      a.ta[q] = TA;
+    }
+  }
+  return a;
+}
+
+int launch_stage(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, int out_set,
+                 int tindex) {
+  StageArgs a = stage_args(h, rk, X, Y, Z, in_set, out_set);
+  if (h->d.kernel == CGFD_KERNEL_SIMPLE)
+    launch_stage_simple(a, h->st);
+  else
+    launch_stage_fused(a, h->st);
+  CK(h, cudaGetLastError());
+  if (h->nmnt + h->nfrc > 0) {
+    SourceArgs s{};
+    s.g = h->g;
+    s.nmnt = h->nmnt; s.nfrc = h->nfrc;
+    s.mcell = h->d_mcell; s.mcoef = h->d_mcoef; s.mstf = h->d_mstf; s.nstfm = h->nstfm;
+    s.fcell = h->d_fcell; s.fcoef = h->d_fcoef; s.fstf = h->d_fstf; s.nstff = h->nstff;
+    s.tinc = (rk == 0) ? 0 : (rk < 3 ? 1 : 2);
+    s.tindex = tindex;
+    s.step = h->d_step;
+    s.adt = a.adt; s.bdt = a.bdt;
+    s.out = a.out; s.tw = a.tw; s.rk = rk;
+    inject_sources_kernel<<<1, 32, 0, h->st>>>(s);
+    CK(h, cudaGetLastError());
+  }
+  return CGFD_OK;
+}
+
+// the four stages of one step of pattern p, reading tindex from the device
+// step counter, then the receiver record
+int enqueue_step(cgfd_solver *h, int p) {
+  static const int ins[4] = {0, 1, 2, 1}, outs[4] = {1, 2, 1, 0};
+  for (int rk = 0; rk < 4; ++rk) {
+    const int *dd = DIRS[p][rk];
+    int st = launch_stage(h, rk, dd[0], dd[1], dd[2], ins[rk], outs[rk], -1);
+    if (st) return st;
+  }
+  record_kernel<<<1, 256, 0, h->st>>>(h->set[0], h->g.fstride, h->d_rcell, h->nrecv,
+                                      h->d.nt, h->d_seis, h->d_step);
+  CK(h, cudaGetLastError());
+  return CGFD_OK;
+}
+
+int build_graphs(cgfd_solver *h) {
+  for (int p = 0; p < 4; ++p) {
+    if (h->graph[p]) { cudaGraphExecDestroy(h->graph[p]); h->graph[p] = nullptr; }
+    cudaGraph_t gr = nullptr;
+    CK(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    int st = enqueue_step(h, p);
+    cudaError_t e = cudaStreamEndCapture(h->st, &gr);
+    if (st) { if (gr) cudaGraphDestroy(gr); return st; }
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&h->graph[p], gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+  }
+  h->graphs_ok = true;
+  return CGFD_OK;
+}
+
+}  // namespace
+
+// --------------------------------- C ABI -----------------------------------
+extern "C" {
+
+int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
+  if (!d || !out) return arg_fail(nullptr, "null argument");
+  *out = nullptr;
+  if (d->ni < 1 || d->nj < 1 || d->nk < 4 || !(d->steph > 0) || !(d->stept > 0) || d->nt < 0)
+    return arg_fail(nullptr, "bad grid or step sizes");
+  if (d->hybrid_grid != 1) return arg_fail(nullptr, "only hybrid_grid=1 (SimpleCar) is supported");
+  for (int q = 0; q < 6; ++q)
+    if (d->nabs[q] < 0) return arg_fail(nullptr, "negative nabs");
+  if (d->nabs[5] != 0) return arg_fail(nullptr, "nabs[5] (top) must be 0: free surface");
+  if (d->nabs[0] + d->nabs[1] > d->ni || d->nabs[2] + d->nabs[3] > d->nj ||
+      d->nabs[4] + d->nabs[5] > d->nk)
+    return arg_fail(nullptr, "PML wider than the grid");
+  if (d->con_index < LFD || d->con_index > d->nk + LFD - 1)
+    return arg_fail(nullptr, "con_index must lie in [3, nk+2]");
+  if (d->storage != CGFD_STORE_F32) return arg_fail(nullptr, "storage type not supported");
+  if (d->kernel != CGFD_KERNEL_FUSED && d->kernel != CGFD_KERNEL_SIMPLE)
+    return arg_fail(nullptr, "unknown kernel family");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    g_last_create_error = "no CUDA device";
+    return CGFD_ERR_NODEVICE;
+  }
+  if (d->device < 0 || d->device >= ndev) return arg_fail(nullptr, "bad device ordinal");
+
+  cgfd_solver *h = new cgfd_solver();
+  h->d = *d;
+  Geom &g = h->g;
+  g.ni = d->ni; g.nj = d->nj; g.nk = d->nk;
+  g.px = (int)align_up((size_t)XO + d->ni + 4, 32);
+  g.nyi = d->nj + 6; g.nzi = d->nk + 6;
+  g.top = d->nk + LFD - 1;
+  g.con = d->con_index;
+  for (int q = 0; q < 6; ++q) g.nabs[q] = d->nabs[q];
+  g.nxa = d->nabs[0] + d->nabs[1];
+  g.nya = d->nabs[2] + d->nabs[3];
+  g.nza = d->nabs[4] + d->nabs[5];
+  g.plane = (size_t)g.px * g.nyi;
+  g.fstride = align_up(g.plane * g.nzi, 64);
+  g.astride[0] = align_up((size_t)g.nzi * g.nyi * g.nxa, 64);
+  g.astride[1] = align_up((size_t)g.nzi * g.nya * g.px, 64);
+  g.astride[2] = align_up((size_t)g.nza * g.nyi * g.px, 64);
+  if (d->kernel == CGFD_KERNEL_FUSED && !fused_supported(g)) {
+    delete h;
+    return arg_fail(nullptr, "fused kernel does not support this grid");
+  }
+
+  DevGuard guard(d->device);
+  int st = CGFD_OK;
+  auto alloc = [&](float **p, size_t n) -> int {
+    cudaError_t e2 = cudaMalloc(p, n * sizeof(float));
+    if (e2 != cudaSuccess) { cuda_fail(nullptr, e2, "cudaMalloc"); return CGFD_ERR_NOMEM; }
+    e2 = cudaMemset(*p, 0, n * sizeof(float));
+    if (e2 != cudaSuccess) { cuda_fail(nullptr, e2, "cudaMemset"); return CGFD_ERR_CUDA; }
+    return CGFD_OK;
+  };
+  const size_t fs = g.fstride;
+  if (!st) st = alloc(&h->state, 4 * 9 * fs);
+  if (!st) st = alloc(&h->media, 3 * fs);
+  if (!st) st = alloc(&h->metric, 4 * fs);
+  const size_t plen = align_up(g.px, 64) * 3 + align_up(g.nyi, 64) * 3 + align_up(g.nzi, 64) * 3;
+  if (!st) st = alloc(&h->pml, plen);
+  for (int q = 0; q < 3 && !st; ++q)
+    if ((q == 0 ? g.nxa : q == 1 ? g.nya : g.nza) > 0) st = alloc(&h->aux[q], 3 * 9 * g.astride[q]);
+  if (!st) st = alloc(&h->matv, 18 * g.plane);
+  if (!st) {
+    e = cudaMalloc(&h->d_step, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(h->d_step, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_count, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) st = cuda_fail(nullptr, e, "setup");
+  }
+  if (st) {
+    free_all(h);
+    delete h;
+    return st;
+  }
+  for (int q = 0; q < 4; ++q) h->set[q] = h->state + (size_t)q * 9 * fs;
+  {
+    float *p = h->pml;
+    const size_t lx = align_up(g.px, 64), ly = align_up(g.nyi, 64), lz = align_up(g.nzi, 64);
+    for (int t = 0; t < 3; ++t) {
+      h->pmlp[3 * t + 0] = p; p += lx;
+      h->pmlp[3 * t + 1] = p; p += ly;
+      h->pmlp[3 * t + 2] = p; p += lz;
+    }
+  }
+  h->wcur = 0;
+  *out = h;
+  return CGFD_OK;
+}
+
+int cgfd_destroy(cgfd_solver *h) {
+  if (!h) return CGFD_OK;
+  {
+    DevGuard guard(h->d.device);
+    if (h->st) cudaStreamSynchronize(h->st);
+    free_all(h);
+  }
+  delete h;
+  return CGFD_OK;
+}
+
+int cgfd_last_error(const cgfd_solver *h, char *buf, size_t len) {
+  if (!buf || !len) return CGFD_ERR_ARG;
+  std::snprintf(buf, len, "%s", h ? h->err.c_str() : g_last_create_error.c_str());
+  return CGFD_OK;
+}
+
+int cgfd_upload_metric(cgfd_solver *h, const double *zx, const double *zy, const double *zz,
+                       const double *jac) {
+  if (!h || !zx || !zy || !zz || !jac) return arg_fail(h, "null argument");
+  DevGuard guard(h->d.device);
+  const long n = ref_n(h);
+  const int nx = h->d.ni + 6, ny = h->d.nj + 6, nz = h->d.nk + 6;
+  std::vector<float> tmp(n);
+  const double *src[4] = {zx, zy, zz, jac};
+  bool flat = true;
+  for (int q = 0; q < 4; ++q) {
+    for (long t = 0; t < n; ++t) tmp[t] = (float)src[q][t];
+    int st = upload_ref(h, tmp.data(), h->metric + (size_t)q * h->g.fstride);
+    if (st) return st;
+  }
+  // Trivial metric (zeta = (0,0,1), J = 1) on every valid cell.  Metric values
+  // in ghost cells only ever multiply zero wavefield values or are replaced by
+  // the traction image, so they do not matter.
+  for (int i = LFD; i < h->d.ni + LFD && flat; ++i)
+    for (int j = LFD; j < h->d.nj + LFD && flat; ++j)
+      for (int k = LFD; k < h->d.nk + LFD && flat; ++k) {
+        const long t = ((long)i * ny + j) * nz + k;
+        if (zx[t] != 0.0 || zy[t] != 0.0 || zz[t] != 1.0 || jac[t] != 1.0) flat = false;
+      }
+  h->flat = flat;
+  h->top_zeta.assign(3 * (size_t)nx * ny, 0.0);
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      const long t = ((long)i * ny + j) * nz + h->g.top;
+      const size_t t2 = (size_t)i * ny + j;
+      h->top_zeta[t2] = zx[t];
+      h->top_zeta[(size_t)nx * ny + t2] = zy[t];
+      h->top_zeta[2 * (size_t)nx * ny + t2] = zz[t];
+    }
+  h->have_metric = true;
+  invalidate(h);
+  return CGFD_OK;
+}
+
+int cgfd_upload_media(cgfd_solver *h, const float *alpha, const float *beta, const float *rho) {
+  if (!h || !alpha || !beta || !rho) return arg_fail(h, "null argument");
+  DevGuard guard(h->d.device);
+  const long n = ref_n(h);
+  const int nx = h->d.ni + 6, ny = h->d.nj + 6, nz = h->d.nk + 6;
+  std::vector<float> l2m(n), mu(n), ir(n);
+  for (long t = 0; t < n; ++t) {
+    const double r = rho[t];
+    l2m[t] = (float)(r * (double)alpha[t] * alpha[t]);
+    mu[t] = (float)(r * (double)beta[t] * beta[t]);
+    ir[t] = r != 0.0 ? (float)(1.0 / r) : 0.f;
+  }
+  // the valid cells must have a positive density
+  for (int i = LFD; i < h->d.ni + LFD; ++i)
+    for (int j = LFD; j < h->d.nj + LFD; ++j)
+      for (int k = LFD; k < h->d.nk + LFD; ++k)
+        if (!(rho[((long)i * ny + j) * nz + k] > 0.f)) return arg_fail(h, "non-positive density");
+  int st = upload_ref(h, l2m.data(), h->media);
+  if (!st) st = upload_ref(h, mu.data(), h->media + h->g.fstride);
+  if (!st) st = upload_ref(h, ir.data(), h->media + 2 * h->g.fstride);
+  if (st) return st;
+  h->top_alpha.assign((size_t)nx * ny, 0.0);
+  h->top_beta.assign((size_t)nx * ny, 0.0);
+  h->top_rho.assign((size_t)nx * ny, 0.0);
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      const long t = ((long)i * ny + j) * nz + h->g.top;
+      h->top_alpha[(size_t)i * ny + j] = alpha[t];
+      h->top_beta[(size_t)i * ny + j] = beta[t];
+      h->top_rho[(size_t)i * ny + j] = rho[t];
+    }
+  h->have_media = true;
+  invalidate(h);
+  return CGFD_OK;
+}
+
+int cgfd_upload_pml(cgfd_solver *h, const double *apdx, const double *apdy, const double *apdz,
+                    const double *bx, const double *by, const double *bz, const double *dbx,
+                    const double *dby, const double *dbz) {
+  if (!h || !apdx || !apdy || !apdz || !bx || !by || !bz || !dbx || !dby || !dbz)
+    return arg_fail(h, "null argument");
+  DevGuard guard(h->d.device);
+  const int n3[3] = {h->d.ni + 6, h->d.nj + 6, h->d.nk + 6};
+  const int len[3] = {h->g.px, h->g.nyi, h->g.nzi};
+  const int off[3] = {1, 0, 0};  // internal index = reference index + off
+  const double *src[9] = {apdx, apdy, apdz, bx, by, bz, dbx, dby, dbz};
+  for (int q = 0; q < 9; ++q) {
+    const int ax = q % 3;
+    // B defaults to 1 (no stretching) outside the reference range
+    std::vector<float> v(len[ax], q / 3 == 1 ? 1.f : 0.f);
+    for (int t = 0; t < n3[ax]; ++t) {
+      if (q / 3 == 1 && !(src[q][t] > 0.0)) return arg_fail(h, "PML B must be positive");
+      v[t + off[ax]] = (float)src[q][t];
+    }
+    CK(h, cudaMemcpy(h->pmlp[q], v.data(), len[ax] * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  for (int ax = 0; ax < 3; ++ax) h->hb[ax].assign(src[3 + ax], src[3 + ax] + n3[ax]);
+  h->have_pml = true;
+  invalidate(h);
+  return CGFD_OK;
+}
+
+static int upload_points(cgfd_solver *h, int n, const int *loc, int ncoef, const float *coef,
+                         int nstf, const float *stf, std::vector<int> &hloc,
+                         std::vector<float> &hcoef, int *&dcell, float *&dstf, int &cnt,
+                         int &cnstf) {
+  if (n < 0 || (n > 0 && (!loc || !coef || !stf || nstf < 1))) return arg_fail(h, "bad sources");
+  for (int q = 0; q < n; ++q)
+    if (!valid_loc(h, loc + 3 * q)) return arg_fail(h, "source outside the valid grid");
+  DevGuard guard(h->d.device);
+  if (dcell) { cudaFree(dcell); dcell = nullptr; }
+  if (dstf) { cudaFree(dstf); dstf = nullptr; }
+  hloc.assign(loc, loc + 3 * n);
+  hcoef.assign(coef, coef + (size_t)ncoef * n);
+  cnt = n;
+  cnstf = nstf;
+  if (n > 0) {
+    std::vector<int> cells(n);
+    for (int q = 0; q < n; ++q) cells[q] = cell_of(h, loc + 3 * q);
+    CK(h, cudaMalloc(&dcell, n * sizeof(int)));
+    CK(h, cudaMemcpy(dcell, cells.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(h, cudaMalloc(&dstf, (size_t)n * nstf * sizeof(float)));
+    CK(h, cudaMemcpy(dstf, stf, (size_t)n * nstf * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  invalidate(h);
+  return CGFD_OK;
+}
+
+int cgfd_upload_moments(cgfd_solver *h, int n, const int *loc, const float *m6, int nstf,
+                        const float *stf) {
+  if (!h) return arg_fail(h, "null handle");
+  return upload_points(h, n, loc, 6, m6, nstf, stf, h->mloc, h->m6, h->d_mcell, h->d_mstf,
+                       h->nmnt, h->nstfm);
+}
+
+int cgfd_upload_forces(cgfd_solver *h, int n, const int *loc, const float *f3, int nstf,
+                       const float *stf) {
+  if (!h) return arg_fail(h, "null handle");
+  return upload_points(h, n, loc, 3, f3, nstf, stf, h->floc, h->f3, h->d_fcell, h->d_fstf,
+                       h->nfrc, h->nstff);
+}
+
+int cgfd_set_receivers(cgfd_solver *h, int n, const int *loc) {
+  if (!h || n < 0 || (n > 0 && !loc)) return arg_fail(h, "bad receivers");
+  for (int q = 0; q < n; ++q)
+    if (!valid_loc(h, loc + 3 * q)) return arg_fail(h, "receiver outside the valid grid");
+  DevGuard guard(h->d.device);
+  if (h->d_rcell) { cudaFree(h->d_rcell); h->d_rcell = nullptr; }
+  if (h->d_seis) { cudaFree(h->d_seis); h->d_seis = nullptr; }
+  h->nrecv = n;
+  if (n > 0) {
+    std::vector<int> cells(n);
+    for (int q = 0; q < n; ++q) cells[q] = cell_of(h, loc + 3 * q);
+    CK(h, cudaMalloc(&h->d_rcell, n * sizeof(int)));
+    CK(h, cudaMemcpy(h->d_rcell, cells.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    const size_t ns = (size_t)9 * n * (h->d.nt > 0 ? h->d.nt : 1);
+    CK(h, cudaMalloc(&h->d_seis, ns * sizeof(float)));
+    CK(h, cudaMemset(h->d_seis, 0, ns * sizeof(float)));
+  }
+  invalidate(h);
+  return CGFD_OK;
+}
+
+int cgfd_prepare(cgfd_solver *h) {
+  if (!h) return arg_fail(h, "null handle");
+  if (!(h->have_metric && h->have_media && h->have_pml)) {
+    h->err = "metric, media and PML must be uploaded before stepping";
+    return CGFD_ERR_STATE;
+  }
+  if (h->prepared && h->graphs_ok) return CGFD_OK;
+  DevGuard guard(h->d.device);
+  std::vector<float> mv;
+  surface_matrices(h, mv);
+  CK(h, cudaMemcpy(h->matv, mv.data(), mv.size() * sizeof(float), cudaMemcpyHostToDevice));
+  // source coefficients from the device copies of jac and 1/rho
+  const double h3 = h->d.steph * h->d.steph * h->d.steph;
+  auto cell_value = [&](const float *base, int cell, float *v) {
+    return cudaMemcpy(v, base + cell, sizeof(float), cudaMemcpyDeviceToHost);
+  };
+  const size_t fs = h->g.fstride;
+  if (h->d_mcoef) { cudaFree(h->d_mcoef); h->d_mcoef = nullptr; }
+  if (h->d_fcoef) { cudaFree(h->d_fcoef); h->d_fcoef = nullptr; }
+  if (h->nmnt) {
+    std::vector<float> c(6 * h->nmnt);
+    for (int q = 0; q < h->nmnt; ++q) {
+      float jac = 1.f;
+      CK(h, cell_value(h->metric + 3 * fs, cell_of(h, &h->mloc[3 * q]), &jac));
+      const double A = 1.0 / (h3 * jac);
+      for (int m = 0; m < 6; ++m) c[6 * q + m] = (float)(h->m6[6 * q + m] * A);
+    }
+    CK(h, cudaMalloc(&h->d_mcoef, c.size() * sizeof(float)));
+    CK(h, cudaMemcpy(h->d_mcoef, c.data(), c.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if (h->nfrc) {
+    std::vector<float> c(3 * h->nfrc);
+    for (int q = 0; q < h->nfrc; ++q) {
+      const int cell = cell_of(h, &h->floc[3 * q]);
+      float jac = 1.f, irho = 1.f;
+      CK(h, cell_value(h->metric + 3 * fs, cell, &jac));
+      CK(h, cell_value(h->media + 2 * fs, cell, &irho));
+      double A = irho / (h3 * jac);
+      if (h->floc[3 * q + 2] == h->g.top) A *= 2.0;
+      for (int m = 0; m < 3; ++m) c[3 * q + m] = (float)(h->f3[3 * q + m] * A);
+    }
+    CK(h, cudaMalloc(&h->d_fcoef, c.size() * sizeof(float)));
+    CK(h, cudaMemcpy(h->d_fcoef, c.data(), c.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  h->prepared = true;
+  int st = build_graphs(h);
+  if (st) return st;
+  return CGFD_OK;
+}
+
+int cgfd_step(cgfd_solver *h, int n_steps) {
+  if (!h || n_steps < 0) return arg_fail(h, "bad arguments");
+  int st = cgfd_prepare(h);
+  if (st) return st;
+  const int last = h->steps + n_steps - 1;
+  if (n_steps > 0) {
+    if (h->nrecv && last >= h->d.nt) return arg_fail(h, "more steps than the seismogram buffer (nt)");
+    if ((h->nmnt && 2 * last + 2 >= h->nstfm) || (h->nfrc && 2 * last + 2 >= h->nstff))
+      return arg_fail(h, "source time function too short for the requested steps");
+  }
+  DevGuard guard(h->d.device);
+  CK(h, cudaMemcpyAsync(h->d_step, &h->steps, sizeof(int), cudaMemcpyHostToDevice, h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  for (int s = 0; s < n_steps; ++s) {
+    CK(h, cudaGraphLaunch(h->graph[h->steps % 4], h->st));
+    h->steps++;
+  }
+  h->wcur = 0;
+  return CGFD_OK;
+}
+
+int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms) {
+  if (!h || n_steps < 1 || !ms) return arg_fail(h, "bad arguments");
+  int st = cgfd_prepare(h);
+  if (st) return st;
+  const int last = h->steps + n_steps - 1;
+  if (h->nrecv && last >= h->d.nt) return arg_fail(h, "more steps than the seismogram buffer (nt)");
+  if ((h->nmnt && 2 * last + 2 >= h->nstfm) || (h->nfrc && 2 * last + 2 >= h->nstff))
+    return arg_fail(h, "source time function too short for the requested steps");
+  DevGuard guard(h->d.device);
+  CK(h, cudaMemcpyAsync(h->d_step, &h->steps, sizeof(int), cudaMemcpyHostToDevice, h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  cudaEvent_t e0, e1;
+  CK(h, cudaEventCreate(&e0));
+  CK(h, cudaEventCreate(&e1));
+  std::vector<cudaEvent_t> ev;
+  if (stage_ms) {
+    ev.resize(8 * (size_t)n_steps);
+    for (auto &e : ev) CK(h, cudaEventCreate(&e));
+  }
+  CK(h, cudaEventRecord(e0, h->st));
+  static const int ins[4] = {0, 1, 2, 1}, outs[4] = {1, 2, 1, 0};
+  for (int s = 0; s < n_steps; ++s) {
+    const int p = h->steps % 4;
+    if (!stage_ms) {
+      CK(h, cudaGraphLaunch(h->graph[p], h->st));
+    } else {
+      for (int rk = 0; rk < 4; ++rk) {
+        const int *dd = DIRS[p][rk];
+        StageArgs a = stage_args(h, rk, dd[0], dd[1], dd[2], ins[rk], outs[rk]);
+        CK(h, cudaEventRecord(ev[8 * (size_t)s + 2 * rk], h->st));
+        if (h->d.kernel == CGFD_KERNEL_SIMPLE) launch_stage_simple(a, h->st);
+        else launch_stage_fused(a, h->st);
+        CK(h, cudaGetLastError());
+        CK(h, cudaEventRecord(ev[8 * (size_t)s + 2 * rk + 1], h->st));
+        // sources exactly as in the graph
+        if (h->nmnt + h->nfrc > 0) {
+          SourceArgs sa{};
+          sa.g = h->g;
+          sa.nmnt = h->nmnt; sa.nfrc = h->nfrc;
+          sa.mcell = h->d_mcell; sa.mcoef = h->d_mcoef; sa.mstf = h->d_mstf; sa.nstfm = h->nstfm;
+          sa.fcell = h->d_fcell; sa.fcoef = h->d_fcoef; sa.fstf = h->d_fstf; sa.nstff = h->nstff;
+          sa.tinc = (rk == 0) ? 0 : (rk < 3 ? 1 : 2);
+          sa.tindex = -1;
+          sa.step = h->d_step;
+          sa.adt = a.adt; sa.bdt = a.bdt;
+          sa.out = a.out; sa.tw = a.tw; sa.rk = rk;
+          inject_sources_kernel<<<1, 32, 0, h->st>>>(sa);
+          CK(h, cudaGetLastError());
+        }
+      }
+      record_kernel<<<1, 256, 0, h->st>>>(h->set[0], h->g.fstride, h->d_rcell, h->nrecv,
+                                          h->d.nt, h->d_seis, h->d_step);
+      CK(h, cudaGetLastError());
+    }
+    h->steps++;
+  }
+  CK(h, cudaEventRecord(e1, h->st));
+  CK(h, cudaEventSynchronize(e1));
+  CK(h, cudaEventElapsedTime(ms, e0, e1));
+  if (stage_ms) {
+    double sum = 0;
+    for (size_t q = 0; q < ev.size(); q += 2) {
+      float t = 0;
+      CK(h, cudaEventElapsedTime(&t, ev[q], ev[q + 1]));
+      sum += t;
+    }
+    *stage_ms = (float)(sum / (ev.size() / 2));
+    for (auto &e : ev) cudaEventDestroy(e);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->wcur = 0;
+  return CGFD_OK;
+}
+
+int cgfd_rk_stage(cgfd_solver *h, int rk, int curr_t, int X, int Y, int Z) {
+  if (!h) return arg_fail(h, "null handle");
+  if (rk < 0 || rk > 3 || (X != 1 && X != -1) || (Y != 1 && Y != -1) || (Z != 1 && Z != -1) ||
+      curr_t < 0)
+    return arg_fail(h, "bad stage arguments");
+  int st = cgfd_prepare(h);
+  if (st) return st;
+  const int tinc = (rk == 0) ? 0 : (rk < 3 ? 1 : 2);
+  const int tindex = 2 * curr_t + tinc;
+  if ((h->nmnt && tindex >= h->nstfm) || (h->nfrc && tindex >= h->nstff))
+    return arg_fail(h, "source time function too short for this step");
+  DevGuard guard(h->d.device);
+  // input: FW for rk 0, else the last stage output; output: the other W set
+  const int in = (rk == 0) ? 0 : h->wcur;
+  int out;
+  if (rk == 3) out = 0;
+  else out = (in == 1) ? 2 : 1;
+  if (rk == 3 && in == 0) return arg_fail(h, "stage 3 needs a previous stage output");
+  st = launch_stage(h, rk, X, Y, Z, in, out, tindex);
+  if (st) return st;
+  h->wcur = out;
+  return CGFD_OK;
+}
+
+int cgfd_sync(cgfd_solver *h, double timeout_s) {
+  if (!h) return arg_fail(h, "null handle");
+  DevGuard guard(h->d.device);
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    cudaError_t e = cudaStreamQuery(h->st);
+    if (e == cudaSuccess) return CGFD_OK;
+    if (e != cudaErrorNotReady) return cuda_fail(h, e, "cudaStreamQuery");
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (timeout_s >= 0 && el > timeout_s) {
+      h->err = "timeout waiting for the device";
+      return CGFD_ERR_TIMEOUT;
+    }
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+}
+
+int cgfd_steps_done(const cgfd_solver *h, int *n) {
+  if (!h || !n) return CGFD_ERR_ARG;
+  *n = h->steps;
+  return CGFD_OK;
+}
+
+int cgfd_get_seismograms(cgfd_solver *h, float *out, int *nt_done) {
+  if (!h) return arg_fail(h, "null handle");
+  DevGuard guard(h->d.device);
+  CK(h, cudaStreamSynchronize(h->st));
+  if (nt_done) *nt_done = h->steps < h->d.nt ? h->steps : h->d.nt;
+  if (h->nrecv && out)
+    CK(h, cudaMemcpy(out, h->d_seis, (size_t)9 * h->nrecv * h->d.nt * sizeof(float),
+                     cudaMemcpyDeviceToHost));
+  return CGFD_OK;
+}
+
+static float *set_ptr(cgfd_solver *h, int set, int comp) {
+  if (comp < 0 || comp > 8) return nullptr;
+  int s;
+  if (set == CGFD_SET_FW) s = 0;
+  else if (set == CGFD_SET_W) s = h->wcur;
+  else if (set == CGFD_SET_TW) s = 3;
+  else return nullptr;
+  return h->set[s] + (size_t)comp * h->g.fstride;
+}
+
+int cgfd_get_field(cgfd_solver *h, int set, int comp, float *out) {
+  if (!h || !out) return arg_fail(h, "null argument");
+  float *p = set_ptr(h, set, comp);
+  if (!p) return arg_fail(h, "bad set or component");
+  DevGuard guard(h->d.device);
+  CK(h, cudaStreamSynchronize(h->st));
+  return download_ref(h, p, out);
+}
+
+int cgfd_set_field(cgfd_solver *h, int set, int comp, const float *in) {
+  if (!h || !in) return arg_fail(h, "null argument");
+  float *p = set_ptr(h, set, comp);
+  if (!p) return arg_fail(h, "bad set or component");
+  DevGuard guard(h->d.device);
+  CK(h, cudaStreamSynchronize(h->st));
+  // only valid cells are taken; ghosts stay zero
+  const long n = ref_n(h);
+  const int nx = h->d.ni + 6, ny = h->d.nj + 6, nz = h->d.nk + 6;
+  std::vector<float> v(n, 0.f);
+  for (int i = LFD; i < nx - LFD; ++i)
+    for (int j = LFD; j < ny - LFD; ++j)
+      for (int k = LFD; k < nz - LFD; ++k) {
+        const long t = ((long)i * ny + j) * nz + k;
+        v[t] = in[t];
+      }
+  return upload_ref(h, v.data(), p);
+}
+
+int cgfd_check_finite(cgfd_solver *h, long long *n_bad) {
+  if (!h) return arg_fail(h, "null handle");
+  DevGuard guard(h->d.device);
+  CK(h, cudaMemsetAsync(h->d_count, 0, sizeof(unsigned long long), h->st));
+  count_nonfinite_kernel<<<592, 256, 0, h->st>>>(h->set[0], 9 * h->g.fstride, h->d_count);
+  CK(h, cudaGetLastError());
+  unsigned long long c = 0;
+  CK(h, cudaMemcpyAsync(&c, h->d_count, sizeof(c), cudaMemcpyDeviceToHost, h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  if (n_bad) *n_bad = (long long)c;
+  if (c) {
+    h->err = "non-finite values in the wavefield";
+    return CGFD_ERR_NONFINITE;
+  }
+  return CGFD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,279 @@
+"""ctypes binding of libcgfd.so, the B200 CGFD solver (include/cgfd.h).
+
+The binding is a thin host-side mirror of the reference's device runtime,
+class ChildProcs (src/typedata.h:114-217): create the solver from a
+description, upload metric / media / PML factors / sources / receivers
+(ParH2D, src/calculate.cu:2050-2228), step (the RKite loop of
+src/simulation.cc:252-711) and read seismograms (PWpick/PWgather).
+
+Every call goes to the CUDA library; there is no Python or CPU fallback.  If
+the library is missing the import fails with the build command to run.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libcgfd.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing; build it with `make -C {os.path.dirname(_HERE)}`")
+_lib = C.CDLL(LIB_PATH)
+
+OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_TIMEOUT, ERR_NONFINITE, ERR_NODEVICE = range(8)
+STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
+KERNEL_FUSED, KERNEL_SIMPLE = 0, 1
+SET_FW, SET_W, SET_TW = 0, 1, 2
+COMPONENTS = ("Vx", "Vy", "Vz", "Txx", "Tyy", "Tzz", "Txy", "Txz", "Tyz")
+STF_TYPES = {"Gauss": 0, "gauss": 1, "Ricker": 2, "ricker": 3, "Bell": 4,
+             "bell": 5, "BELL": 6, "Step": 7}
+
+
+class Desc(C.Structure):
+    _fields_ = [("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int),
+                ("steph", C.c_double), ("stept", C.c_double), ("nt", C.c_int),
+                ("con_index", C.c_int), ("hybrid_grid", C.c_int),
+                ("nabs", C.c_int * 6), ("storage", C.c_int), ("device", C.c_int),
+                ("kernel", C.c_int)]
+
+
+_P = C.c_void_p
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+
+_SIGS = {
+    "cgfd_create": (C.c_int, [C.POINTER(Desc), C.POINTER(_P)]),
+    "cgfd_destroy": (C.c_int, [_P]),
+    "cgfd_last_error": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
+    "cgfd_upload_metric": (C.c_int, [_P, _dp, _dp, _dp, _dp]),
+    "cgfd_upload_media": (C.c_int, [_P, _fp, _fp, _fp]),
+    "cgfd_upload_pml": (C.c_int, [_P] + [_dp] * 9),
+    "cgfd_upload_moments": (C.c_int, [_P, C.c_int, _ip, _fp, C.c_int, _fp]),
+    "cgfd_upload_forces": (C.c_int, [_P, C.c_int, _ip, _fp, C.c_int, _fp]),
+    "cgfd_set_receivers": (C.c_int, [_P, C.c_int, _ip]),
+    "cgfd_prepare": (C.c_int, [_P]),
+    "cgfd_step": (C.c_int, [_P, C.c_int]),
+    "cgfd_step_timed": (C.c_int, [_P, C.c_int, _fp, _fp]),
+    "cgfd_rk_stage": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "cgfd_sync": (C.c_int, [_P, C.c_double]),
+    "cgfd_steps_done": (C.c_int, [_P, _ip]),
+    "cgfd_get_seismograms": (C.c_int, [_P, _fp, _ip]),
+    "cgfd_get_field": (C.c_int, [_P, C.c_int, C.c_int, _fp]),
+    "cgfd_set_field": (C.c_int, [_P, C.c_int, C.c_int, _fp]),
+    "cgfd_check_finite": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
+    "cgfd_metric_from_coords": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double,
+                                          _dp, _dp, _dp, C.POINTER(_dp)]),
+    "cgfd_cfs_factors": (C.c_int, [C.c_int, C.c_int, C.c_int, _ip, _dp, _dp, _dp,
+                                   _dp, _dp, _dp] + [_dp] * 9),
+    "cgfd_stf": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
+                           C.c_double, _fp]),
+    "cgfd_angle2moment": (C.c_int, [C.c_double, C.c_double, C.c_double, _dp]),
+}
+for _name, (_res, _args) in _SIGS.items():
+    _f = getattr(_lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+EXPORTED = tuple(_SIGS)
+
+
+class CgfdError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"cgfd status {status}: {msg}")
+        self.status = status
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _f(a):
+    return a.ctypes.data_as(_fp)
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip)
+
+
+def _as(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def last_error(handle=None) -> str:
+    buf = C.create_string_buffer(1024)
+    _lib.cgfd_last_error(handle, buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def make_desc(ni, nj, nk, steph, stept, nt, con_index, nabs, storage=STORE_F32,
+              device=0, kernel=KERNEL_FUSED, hybrid_grid=1) -> Desc:
+    d = Desc()
+    d.ni, d.nj, d.nk = ni, nj, nk
+    d.steph, d.stept, d.nt = steph, stept, nt
+    d.con_index, d.hybrid_grid = con_index, hybrid_grid
+    for q in range(6):
+        d.nabs[q] = int(nabs[q])
+    d.storage, d.device, d.kernel = storage, device, kernel
+    return d
+
+
+class Solver:
+    """One solver on one GPU (mirrors ChildProcs)."""
+
+    def __init__(self, desc: Desc):
+        h = _P()
+        st = _lib.cgfd_create(C.byref(desc), C.byref(h))
+        if st:
+            raise CgfdError(st, last_error(None))
+        self._h = h
+        self.desc = desc
+        self.shape = (desc.ni + 6, desc.nj + 6, desc.nk + 6)
+        self.nrecv = 0
+
+    def _chk(self, st):
+        if st:
+            raise CgfdError(st, last_error(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.cgfd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def upload_metric(self, zeta_x, zeta_y, zeta_z, jac):
+        arrs = [_as(a, np.float64).reshape(-1) for a in (zeta_x, zeta_y, zeta_z, jac)]
+        self._chk(_lib.cgfd_upload_metric(self._h, *[_d(a) for a in arrs]))
+
+    def upload_media(self, alpha, beta, rho):
+        arrs = [_as(a, np.float32).reshape(-1) for a in (alpha, beta, rho)]
+        self._chk(_lib.cgfd_upload_media(self._h, *[_f(a) for a in arrs]))
+
+    def upload_pml(self, apd, b, db):
+        arrs = [_as(a, np.float64) for a in (*apd, *b, *db)]
+        self._chk(_lib.cgfd_upload_pml(self._h, *[_d(a) for a in arrs]))
+
+    def upload_moments(self, loc, m6, stf):
+        loc = _as(loc, np.int32).reshape(-1, 3)
+        m6 = _as(m6, np.float32).reshape(-1, 6)
+        stf = _as(stf, np.float32).reshape(len(loc), -1)
+        self._chk(_lib.cgfd_upload_moments(self._h, len(loc), _i(loc), _f(m6),
+                                           stf.shape[1], _f(stf)))
+
+    def upload_forces(self, loc, f3, stf):
+        loc = _as(loc, np.int32).reshape(-1, 3)
+        f3 = _as(f3, np.float32).reshape(-1, 3)
+        stf = _as(stf, np.float32).reshape(len(loc), -1)
+        self._chk(_lib.cgfd_upload_forces(self._h, len(loc), _i(loc), _f(f3),
+                                          stf.shape[1], _f(stf)))
+
+    def set_receivers(self, loc):
+        loc = _as(loc, np.int32).reshape(-1, 3)
+        self._chk(_lib.cgfd_set_receivers(self._h, len(loc), _i(loc)))
+        self.nrecv = len(loc)
+
+    def prepare(self):
+        self._chk(_lib.cgfd_prepare(self._h))
+
+    def step(self, n=1):
+        self._chk(_lib.cgfd_step(self._h, int(n)))
+
+    def step_timed(self, n, per_stage=False):
+        """Runs n steps; returns (device ms for the n steps, mean ms of one
+        stage kernel or None).  per_stage issues the stages without graphs."""
+        ms = C.c_float()
+        sms = C.c_float()
+        self._chk(_lib.cgfd_step_timed(self._h, int(n), C.byref(ms),
+                                       C.byref(sms) if per_stage else None))
+        return ms.value, (sms.value if per_stage else None)
+
+    def rk_stage(self, rk, curr_t, x, y, z):
+        self._chk(_lib.cgfd_rk_stage(self._h, rk, curr_t, x, y, z))
+
+    def sync(self, timeout_s=600.0):
+        self._chk(_lib.cgfd_sync(self._h, float(timeout_s)))
+
+    def steps_done(self) -> int:
+        n = C.c_int()
+        self._chk(_lib.cgfd_steps_done(self._h, C.byref(n)))
+        return n.value
+
+    def seismograms(self) -> np.ndarray:
+        """(9, nrecv, nt) float32, as HPW."""
+        out = np.zeros((9, max(self.nrecv, 0), self.desc.nt), np.float32)
+        n = C.c_int()
+        self._chk(_lib.cgfd_get_seismograms(self._h, _f(out), C.byref(n)))
+        return out
+
+    def get_field(self, comp, fset=SET_FW) -> np.ndarray:
+        out = np.zeros(self.shape, np.float32)
+        self._chk(_lib.cgfd_get_field(self._h, fset, comp, _f(out)))
+        return out
+
+    def set_field(self, comp, values, fset=SET_FW):
+        v = _as(values, np.float32).reshape(self.shape)
+        self._chk(_lib.cgfd_set_field(self._h, fset, comp, _f(v)))
+
+    def check_finite(self) -> int:
+        n = C.c_longlong()
+        st = _lib.cgfd_check_finite(self._h, C.byref(n))
+        if st not in (OK, ERR_NONFINITE):
+            self._chk(st)
+        return n.value
+
+
+# ------------------------- host pre-processing ------------------------------
+
+def metric_from_coords(ni, nj, nk, steph, x, y, z):
+    """gridmesh::calmetric: returns dict of 10 full arrays (FP64)."""
+    shape = (ni + 6, nj + 6, nk + 6)
+    xs = [_as(a, np.float64).reshape(shape) for a in (x, y, z)]
+    names = ("xi_x", "xi_y", "xi_z", "eta_x", "eta_y", "eta_z",
+             "zeta_x", "zeta_y", "zeta_z", "jac")
+    outs = [np.zeros(shape, np.float64) for _ in names]
+    ptrs = (_dp * 10)(*[_d(o) for o in outs])
+    st = _lib.cgfd_metric_from_coords(ni, nj, nk, steph, *[_d(a) for a in xs], ptrs)
+    if st:
+        raise CgfdError(st, "metric_from_coords")
+    return dict(zip(names, outs))
+
+
+def cfs_factors(ni, nj, nk, nabs, velabs, bmax, amax, dlx, dly, dlz):
+    """absorb::CalCFSfactors: returns (apd, b, db), each a tuple of 3 arrays."""
+    nabs = _as(nabs, np.int32)
+    v, bm, am = (_as(a, np.float64) for a in (velabs, bmax, amax))
+    dl = [_as(a, np.float64) for a in (dlx, dly, dlz)]
+    n3 = (ni + 6, nj + 6, nk + 6)
+    outs = [np.zeros(n3[q % 3], np.float64) for q in range(9)]
+    st = _lib.cgfd_cfs_factors(ni, nj, nk, _i(nabs), _d(v), _d(bm), _d(am),
+                               *[_d(a) for a in dl], *[_d(o) for o in outs])
+    if st:
+        raise CgfdError(st, "cfs_factors")
+    return tuple(outs[0:3]), tuple(outs[3:6]), tuple(outs[6:9])
+
+
+def stf(kind, start, t0, f0, n, dt) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    st = _lib.cgfd_stf(STF_TYPES[kind] if isinstance(kind, str) else int(kind),
+                       start, t0, f0, n, dt, _f(out))
+    if st:
+        raise CgfdError(st, "stf")
+    return out
+
+
+def angle2moment(strike, dip, rake) -> np.ndarray:
+    m = np.zeros(6, np.float64)
+    _lib.cgfd_angle2moment(strike, dip, rake, _d(m))
+    return m

@@ -1,0 +1,217 @@
+/*
+ * cgfd.h -- C ABI of the B200 (sm_100a) time-stepping solver for the
+ * collocated-grid curvilinear finite-difference (CGFD) elastic-wave method.
+ *
+ * This is the drop-in boundary for the device runtime of CoPara-CGFD3D,
+ * i.e. for `class ChildProcs` (src/typedata.h:114-217, implemented in
+ * src/calculate.cu).  Every entry point below names the reference interface
+ * it replaces.  All functions return an int status (cgfd_status); nothing
+ * throws or aborts across this boundary (the reference's CC()/Kcheck() call
+ * cudaDeviceReset()+MPI_Abort, src/calculate.cu:17-41).  One solver handle
+ * drives one GPU and must be used from one host thread at a time.
+ *
+ * Index conventions are the reference's (src/simulation.cc:798-835):
+ *   full arrays are nx*ny*nz with nx=ni+6, ny=nj+6, nz=nk+6 (LenFD=3 ghost
+ *   cells per side), flattened as  g = (i*ny + j)*nz + k  (z fastest);
+ *   valid cells have i in [3, ni+3), j in [3, nj+3), k in [3, nk+3);
+ *   k grows upwards and k = nk+2 is the free surface.
+ * Source and receiver locations are (i,j,k) triples in that index space,
+ * exactly like locx/locy/locz of the reference (Cstart = 0, one rank).
+ * Field component order is the reference's wfield order
+ * (src/typenew.h:265-270): Vx Vy Vz Txx Tyy Tzz Txy Txz Tyz.
+ */
+#ifndef CGFD_H
+#define CGFD_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CGFD_ABI_VERSION 1
+
+typedef enum cgfd_status {
+    CGFD_OK            = 0,
+    CGFD_ERR_ARG       = 1,  /* bad argument, size or index                    */
+    CGFD_ERR_CUDA      = 2,  /* CUDA runtime error (text in cgfd_last_error)    */
+    CGFD_ERR_STATE     = 3,  /* call out of order (e.g. step before upload)     */
+    CGFD_ERR_NOMEM     = 4,  /* device or host allocation failed                */
+    CGFD_ERR_TIMEOUT   = 5,  /* a bounded wait on the device ran out            */
+    CGFD_ERR_NONFINITE = 6,  /* NaN or Inf found in the wavefield               */
+    CGFD_ERR_NODEVICE  = 7   /* no usable CUDA device                           */
+} cgfd_status;
+
+/* Storage type of the 9 wavefields and the RK registers.  Arithmetic is FP32
+ * in every case; 16-bit storage keeps one power-of-two scale per field. */
+typedef enum cgfd_storage {
+    CGFD_STORE_F32  = 0,
+    CGFD_STORE_F16  = 1,
+    CGFD_STORE_BF16 = 2
+} cgfd_storage;
+
+/* Kernel family used for the RK stages. */
+typedef enum cgfd_kernel {
+    CGFD_KERNEL_FUSED  = 0,  /* z-marching tiled kernel (default)            */
+    CGFD_KERNEL_SIMPLE = 1   /* one thread per cell, no tiling (cross-check) */
+} cgfd_kernel;
+
+/* Field sets that cgfd_get_field / cgfd_set_field address. */
+typedef enum cgfd_set {
+    CGFD_SET_FW = 0,  /* wavefield at the start of the next step (FW)       */
+    CGFD_SET_W  = 1,  /* output of the last RK stage that ran (W)           */
+    CGFD_SET_TW = 2   /* RK accumulator (tW)                                */
+} cgfd_set;
+
+/* Solver description; fills the role of the ChildProcs constructor arguments
+ * (src/calculate.cu:107-111) and of the cindx struct (src/typenew.h:134-141). */
+typedef struct cgfd_desc {
+    int    ni, nj, nk;   /* valid cells in x, y, z                               */
+    double steph;        /* grid spacing h (m); x and y spacing equal h (SimpleCar) */
+    double stept;        /* time step (s)                                         */
+    int    nt;           /* steps the seismogram buffer holds                     */
+    int    con_index;    /* ConIndex: cells with k >= con_index use the full zeta
+                            metric, cells below use zeta_z only; 3..nk+2          */
+    int    hybrid_grid;  /* HyGrid; must be 1 (default SimpleCar build)           */
+    int    nabs[6];      /* CFS-PML widths X1 X2 Y1 Y2 Z1 Z2; Z2 must be 0 (free surface on top) */
+    int    storage;      /* cgfd_storage                                          */
+    int    device;       /* CUDA device ordinal                                   */
+    int    kernel;       /* cgfd_kernel                                           */
+} cgfd_desc;
+
+typedef struct cgfd_solver cgfd_solver;
+
+/* Replaces ChildProcs::ChildProcs + device allocation (src/calculate.cu:107-1005).
+ * Allocates and zeroes all device state; does not read any file. */
+int cgfd_create(const cgfd_desc *desc, cgfd_solver **out);
+
+/* Replaces ChildProcs::~ChildProcs (src/calculate.cu:1007-1334). NULL is a no-op. */
+int cgfd_destroy(cgfd_solver *h);
+
+/* Copies the text of the last error of h (or of the last failed cgfd_create
+ * when h is NULL) into buf.  Replaces the reference's printf diagnostics. */
+int cgfd_last_error(const cgfd_solver *h, char *buf, size_t len);
+
+/* Grid metric, FP64, full arrays (nx*ny*nz, reference layout).  Replaces the
+ * H_drv buffers + ParH2D (src/typedata.h:148, src/calculate.cu:2050-2115).
+ * Under SimpleCar only zeta_{x,y,z} and the Jacobian are used on the device. */
+int cgfd_upload_metric(cgfd_solver *h, const double *zeta_x, const double *zeta_y,
+                       const double *zeta_z, const double *jac);
+
+/* Media: P velocity (alpha), S velocity (beta), density (rho); full arrays.
+ * Replaces H_mpa + ParH2D (src/typedata.h:149, src/calculate.cu:2105-2113). */
+int cgfd_upload_media(cgfd_solver *h, const float *alpha, const float *beta,
+                      const float *rho);
+
+/* ADE CFS-PML factors (1-D profiles of length nx, ny, nz): APD = alpha + d/beta,
+ * B = beta, DB = d/beta.  Replaces H_apr + ParH2D (src/calculate.cu:2157-2180);
+ * the factors come from absorb::CalCFSfactors (src/absorb.cpp:346-805) or from
+ * cgfd_cfs_factors below. */
+int cgfd_upload_pml(cgfd_solver *h,
+                    const double *apd_x, const double *apd_y, const double *apd_z,
+                    const double *b_x,   const double *b_y,   const double *b_z,
+                    const double *db_x,  const double *db_y,  const double *db_z);
+
+/* Moment-tensor point sources: loc = 3n ints (i,j,k), m6 = 6n floats
+ * (mxx myy mzz mxy mxz myz), stf = n*nstf floats sampled every stept/2
+ * (nstf >= 2*nt+1).  Replaces H_mnt + ParH2D (src/calculate.cu:2133-2152)
+ * and is injected like LoadMoment (src/calculate.cu:6193-6255). */
+int cgfd_upload_moments(cgfd_solver *h, int n, const int *loc, const float *m6,
+                        int nstf, const float *stf);
+
+/* Single-force point sources: loc = 3n, f3 = 3n (fx fy fz), stf as above.
+ * Replaces H_frc + ParH2D and LoadForce (src/calculate.cu:6130-6191). */
+int cgfd_upload_forces(cgfd_solver *h, int n, const int *loc, const float *f3,
+                       int nstf, const float *stf);
+
+/* Receivers (3n ints).  Replaces Hpt + C2DPointPick (src/calculate.cu:2678-2746). */
+int cgfd_set_receivers(cgfd_solver *h, int n, const int *loc);
+
+/* Builds the free-surface velocity-gradient matrices in FP64 (the work of
+ * VelPDcoeff, src/calculate.cu:3320-3428, called through ChildProcs::VelCoeff,
+ * src/calculate.cu:1336-1353) and the per-step CUDA graphs.  Called by
+ * cgfd_step on first use; may be called explicitly. */
+int cgfd_prepare(cgfd_solver *h);
+
+/* Advances n_steps full RK4 steps with the reference's direction schedule
+ * (src/simulation.cc:252-700) and records the receivers after each step
+ * (PWpick, src/calculate.cu:2780-2830).  Asynchronous on the solver stream. */
+int cgfd_step(cgfd_solver *h, int n_steps);
+
+/* cgfd_step with device timing: *ms receives the CUDA-event time of the
+ * n_steps on the solver stream.  When stage_ms is not NULL the steps are
+ * issued stage by stage instead of as graphs and *stage_ms receives the mean
+ * device time of one RK-stage kernel launch.  No reference counterpart (the
+ * reference prints wall-clock progress, src/simulation.cc:710-716). */
+int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms);
+
+/* One RK stage exactly as ChildProcs::RKite(RKindex, currT, Xvec, Yvec, Zvec)
+ * (src/calculate.cu:1355-1600) followed by the synchronisation the driver does
+ * around it (wavesyn/abssyn, src/calculate.cu:2956-3119).  After rk_index 3 the
+ * step state FW holds the new wavefield.  Receivers are not recorded. */
+int cgfd_rk_stage(cgfd_solver *h, int rk_index, int curr_t, int xvec, int yvec,
+                  int zvec);
+
+/* Waits (bounded by timeout_s seconds) for all queued work of h. */
+int cgfd_sync(cgfd_solver *h, double timeout_s);
+
+/* Number of steps recorded so far. */
+int cgfd_steps_done(const cgfd_solver *h, int *n);
+
+/* Seismograms: out = 9 * nrecv * nt floats, laid out like HPW
+ * (component-major, then receiver, then time: out[(c*nrecv + r)*nt + t]),
+ * recorded from FW after each step.  Replaces PWgather/HPW
+ * (src/calculate.cu:2748-2778). */
+int cgfd_get_seismograms(cgfd_solver *h, float *out, int *nt_done);
+
+/* Full-array (reference layout) copy of one component of a field set. */
+int cgfd_get_field(cgfd_solver *h, int set, int comp, float *out);
+int cgfd_set_field(cgfd_solver *h, int set, int comp, const float *in);
+
+/* Counts NaN/Inf values of FW on the device; *n_bad receives the count.
+ * Returns CGFD_ERR_NONFINITE when the count is not zero. */
+int cgfd_check_finite(cgfd_solver *h, long long *n_bad);
+
+/* ---------------- host pre-processing helpers (FP64) ---------------------- */
+
+/* Grid metric from node coordinates (full arrays, reference layout), by
+ * 2-point central differences and cross products, then mirrored into the
+ * ghost cells: gridmesh::calmetric (src/gridmesh.cpp:1476-1627).
+ * out[0..9] = xi_x xi_y xi_z eta_x eta_y eta_z zeta_x zeta_y zeta_z jac. */
+int cgfd_metric_from_coords(int ni, int nj, int nk, double steph,
+                            const double *x, const double *y, const double *z,
+                            double *const out[10]);
+
+/* ADE CFS-PML profiles: absorb::CalCFSfactors (src/absorb.cpp:346-805).
+ * dlx[i] (dly[j], dlz[k]) is steph/|grad xi| at (i, nj1, nk1)
+ * (resp. |grad eta| at (ni1, j, nk1), |grad zeta| at (ni1, nj1, k)). */
+int cgfd_cfs_factors(int ni, int nj, int nk, const int nabs[6],
+                     const double velabs[6], const double bmax[6],
+                     const double amax[6], const double *dlx,
+                     const double *dly, const double *dlz,
+                     double *apd_x, double *apd_y, double *apd_z,
+                     double *b_x, double *b_y, double *b_z,
+                     double *db_x, double *db_y, double *db_z);
+
+/* Source-time-function types (src/mathfunc.cpp:481-608). */
+typedef enum cgfd_stf_type {
+    CGFD_STF_GAUSS = 0, CGFD_STF_GAUSS_D = 1, CGFD_STF_RICKER = 2,
+    CGFD_STF_RICKER_D = 3, CGFD_STF_BELL = 4, CGFD_STF_BELL_D = 5,
+    CGFD_STF_BELL_I = 6, CGFD_STF_STEP = 7
+} cgfd_stf_type;
+
+/* Samples an STF n times at spacing dt starting at -start, as
+ * source::cal_stf_moment (src/source.cpp:102-131); the reference calls it with
+ * dt = stept/2 and n = 2*(nt+1) (src/source.cpp:408,775). */
+int cgfd_stf(int type, double start, double t0, double f0, int n, double dt,
+             float *out);
+
+/* Strike/dip/rake (degrees) to a unit moment tensor (mxx myy mzz mxy mxz myz):
+ * source::angle2moment (src/source.cpp:134-155). */
+int cgfd_angle2moment(double strike, double dip, double rake, double m6[6]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CGFD_H */

@@ -1,0 +1,69 @@
+"""The C ABI: every entry point include/cgfd.h declares is exported by
+libcgfd.so, argument errors come back as status codes (no GPU needed), and
+the product library does not depend on the oracle."""
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "cgfd.h")
+
+
+def declared():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"^int\s+(cgfd_\w+)\s*\(", src, re.M)))
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    assert "cgfd_create" in names and "cgfd_step" in names and len(names) >= 20
+
+
+def test_library_exports_every_declared_symbol():
+    import cgfd
+    out = subprocess.run(["nm", "-D", "--defined-only", cgfd.LIB_PATH],
+                         capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\bT\s+(cgfd_\w+)", out))
+    missing = [n for n in declared() if n not in exported]
+    assert not missing, missing
+    for n in declared():
+        assert hasattr(cgfd._lib, n)
+
+
+def test_binding_covers_every_declared_symbol():
+    import cgfd
+    assert sorted(cgfd.EXPORTED) == declared()
+
+
+def test_product_library_has_no_oracle_dependency():
+    import cgfd
+    out = subprocess.run(["nm", "-D", cgfd.LIB_PATH], capture_output=True, text=True).stdout
+    assert "orc_" not in out
+    ldd = subprocess.run(["ldd", cgfd.LIB_PATH], capture_output=True, text=True).stdout
+    assert "oracle" not in ldd
+
+
+@pytest.mark.parametrize("field,value", [
+    ("ni", 0), ("nk", 2), ("steph", 0.0), ("stept", -1.0), ("hybrid_grid", 0),
+    ("con_index", 2), ("con_index", 40), ("storage", 9), ("kernel", 7)])
+def test_create_rejects_bad_descriptions(field, value):
+    import cgfd
+    d = cgfd.make_desc(20, 20, 20, 100.0, 0.005, 10, 10, (4, 4, 4, 4, 4, 0))
+    setattr(d, field, value)
+    with pytest.raises(cgfd.CgfdError) as e:
+        cgfd.Solver(d)
+    assert e.value.status == cgfd.ERR_ARG
+    assert cgfd.last_error(None)
+
+
+def test_create_rejects_pml_on_top_and_oversized_pml():
+    import cgfd
+    d = cgfd.make_desc(20, 20, 20, 100.0, 0.005, 10, 10, (4, 4, 4, 4, 4, 2))
+    with pytest.raises(cgfd.CgfdError) as e:
+        cgfd.Solver(d)
+    assert e.value.status == cgfd.ERR_ARG and "free surface" in cgfd.last_error(None)
+    d = cgfd.make_desc(20, 20, 20, 100.0, 0.005, 10, 10, (12, 12, 4, 4, 4, 0))
+    with pytest.raises(cgfd.CgfdError):
+        cgfd.Solver(d)

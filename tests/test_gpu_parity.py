@@ -1,0 +1,99 @@
+"""GPU parity: the B200 solver against the FP64 CPU oracle and against the
+reference's own CUDA device runtime (oracle/_ref/ref_wavesim, built from the
+reference's src/calculate.cu) on the same inputs.
+
+Tolerances: seismograms and fields within 1e-5 relative L2 of the reference
+(the parity bar for FP32 arithmetic), and within 1e-5 of the FP64 oracle for
+these short runs.
+"""
+import numpy as np
+import pytest
+
+import cases
+import cgfd
+import refio
+from helpers import rel_l2, valid
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _cmp(a, b, tol, what):
+    for c in range(9):
+        if np.linalg.norm(b[c]) == 0:
+            assert np.linalg.norm(a[c]) == 0, (what, c)
+            continue
+        e = rel_l2(a[c], b[c])
+        assert e < tol, f"{what} component {cgfd.COMPONENTS[c]}: rel L2 {e:.3e}"
+
+
+def _kernels():
+    return [cgfd.KERNEL_SIMPLE, cgfd.KERNEL_FUSED]
+
+
+def _skip_if_unsupported(kernel, m):
+    try:
+        cgfd.Solver(m.desc(kernel=kernel)).close()
+    except cgfd.CgfdError as e:
+        if kernel == cgfd.KERNEL_FUSED and "fused kernel does not support" in str(e):
+            pytest.skip("fused kernel not built for this grid")
+        raise
+
+
+@pytest.mark.parametrize("kernel", _kernels(), ids=["simple", "fused"])
+@pytest.mark.parametrize("name", list(cases.CASES))
+def test_product_matches_fp64_oracle(name, kernel):
+    m, nsteps, nstages, init = cases.build(name)
+    _skip_if_unsupported(kernel, m)
+    ps, pfw, pw = cases.run_product(m, nsteps, nstages, init, kernel=kernel)
+    os_, ofw, ow = cases.run_oracle(m, nsteps, nstages, init)
+    if nsteps:
+        _cmp(ps, os_, TOL, "seismogram")
+    _cmp(valid(pw), valid(ow), TOL, "W")
+    if nstages < 4:
+        _cmp(valid(pfw), valid(ofw), TOL, "FW")
+
+
+@pytest.mark.parametrize("name", list(cases.CASES))
+def test_reference_matches_fp64_oracle(name):
+    """Pins the oracle to the reference's own CUDA path."""
+    m, nsteps, nstages, init = cases.build(name)
+    r = refio.run(m, nsteps, init, nstages)
+    os_, ofw, ow = cases.run_oracle(m, nsteps, nstages, init)
+    if nsteps:
+        _cmp(r["seis"], os_, TOL, "seismogram")
+    _cmp(valid(r["w"]), valid(ow), TOL, "W")
+    if nstages < 4:
+        _cmp(valid(r["fw"]), valid(ofw), TOL, "FW")
+
+
+@pytest.mark.parametrize("kernel", _kernels(), ids=["simple", "fused"])
+@pytest.mark.parametrize("name", list(cases.CASES))
+def test_product_matches_reference(name, kernel):
+    m, nsteps, nstages, init = cases.build(name)
+    _skip_if_unsupported(kernel, m)
+    r = refio.run(m, nsteps, init, nstages)
+    ps, pfw, pw = cases.run_product(m, nsteps, nstages, init, kernel=kernel)
+    if nsteps:
+        _cmp(ps, r["seis"], TOL, "seismogram")
+    _cmp(valid(pw), valid(r["w"]), TOL, "W")
+    if nstages < 4:
+        _cmp(valid(pfw), valid(r["fw"]), TOL, "FW")
+
+
+@pytest.mark.parametrize("kernel", _kernels(), ids=["simple", "fused"])
+def test_flat_halfspace_160x160x80_500_steps_matches_reference(kernel):
+    """The 160x160x80 flat half-space model, full 500 steps, 25 receivers."""
+    import models
+    m = models.config_c1()
+    _skip_if_unsupported(kernel, m)
+    r = refio.run(m, m.nt)
+    s = cgfd.Solver(m.desc(kernel=kernel))
+    m.load(s)
+    s.step(m.nt)
+    ps = s.seismograms()
+    s.close()
+    for c in range(9):
+        e = rel_l2(ps[c], r["seis"][c])
+        assert e < TOL, f"{cgfd.COMPONENTS[c]} rel L2 {e:.3e}"

@@ -1,0 +1,51 @@
+"""The CPU oracle against golden vectors produced by the reference's own CUDA
+device runtime on a B200 (tests/golden/make_golden.py).  This pins the
+oracle: seismograms and stage outputs within 1e-5 relative L2 (the reference
+computes in FP32, the oracle in FP64)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from helpers import rel_l2
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL = 1e-5
+
+
+def _golden_names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def test_golden_set_is_complete():
+    assert set(_golden_names()) == set(cases.CASES), "regenerate tests/golden (make_golden.py)"
+
+
+@pytest.mark.parametrize("name", sorted(cases.CASES))
+def test_oracle_matches_reference_golden(name):
+    path = os.path.join(GOLDEN, f"{name}.npz")
+    if not os.path.exists(path):
+        pytest.fail(f"missing golden file {path}")
+    g = np.load(path)
+    m, nsteps, nstages, init = cases.build(name)
+    assert str(g["digest"]) == cases.model_digest(m, init), "inputs changed since the golden run"
+    seis, fw, w = cases.run_oracle(m, nsteps, nstages, init)
+    if nsteps:
+        for c in range(9):
+            e = rel_l2(seis[c], g["seis"][c])
+            assert e < TOL, (c, e)
+    if nstages:
+        wv = w[:, 3:-3, 3:-3, 3:-3]
+        for c in range(9):
+            e = rel_l2(wv[c], g["w"][c])
+            assert e < TOL, (c, e)
+
+
+def test_oracle_fp32_and_fp64_agree():
+    m, nsteps, nstages, init = cases.build("hill_60")
+    a = cases.run_oracle(m, nsteps, nstages, init, prec=0)[0]
+    b = cases.run_oracle(m, nsteps, nstages, init, prec=1)[0]
+    for c in range(9):
+        assert rel_l2(b[c], a[c]) < 1e-5
