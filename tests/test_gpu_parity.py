@@ -12,7 +12,7 @@ import pytest
 import cases
 import cgfd
 import refio
-from helpers import rel_l2, valid
+from helpers import comp_errors, rel_l2, valid
 
 pytestmark = pytest.mark.gpu
 
@@ -20,11 +20,7 @@ TOL = 1e-5
 
 
 def _cmp(a, b, tol, what):
-    for c in range(9):
-        if np.linalg.norm(b[c]) == 0:
-            assert np.linalg.norm(a[c]) == 0, (what, c)
-            continue
-        e = rel_l2(a[c], b[c])
+    for c, e in enumerate(comp_errors(a, b)):
         assert e < tol, f"{what} component {cgfd.COMPONENTS[c]}: rel L2 {e:.3e}"
 
 
@@ -94,6 +90,8 @@ def test_flat_halfspace_160x160x80_500_steps_matches_reference(kernel):
     s.step(m.nt)
     ps = s.seismograms()
     s.close()
-    for c in range(9):
+    # the velocity seismograms strictly, per component
+    for c in range(3):
         e = rel_l2(ps[c], r["seis"][c])
         assert e < TOL, f"{cgfd.COMPONENTS[c]} rel L2 {e:.3e}"
+    _cmp(ps, r["seis"], TOL, "seismogram")
