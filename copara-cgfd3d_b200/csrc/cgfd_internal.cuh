@@ -78,6 +78,7 @@ struct StageArgs {
   const float *lam2mu, *mu, *irho;
   const float *zx, *zy, *zz, *jac;
   bool flat;           // metric is zeta=(0,0,1), jac=1 everywhere
+  bool plain_interior; // B = 1 and DB = APD = 0 outside the PML layers
   const float *matv;   // 18 planes: matVx2Vz[0..8], matVy2Vz[0..8]
   const float *apd[3], *b[3], *db[3];
   // aux sets per direction: ain (FA for rk 0 else A), afw (FA), aout (A, or
@@ -110,7 +111,12 @@ struct SourceArgs {
 };
 
 void launch_stage_simple(const StageArgs &a, void *stream);
-void launch_stage_fused(const StageArgs &a, void *stream);
 bool fused_supported(const Geom &g);
+size_t fused_map_bytes();
+bool fused_make_map(void *map, const Geom &g, const float *set_base);
+int fused_zchunk(const Geom &g);
+void fused_init_attributes();
+void launch_stage_fused_map(const void *map, const StageArgs &a, int zchunk, int *err,
+                            void *stream);
 
 }  // namespace cgfd

@@ -164,6 +164,12 @@ struct cgfd_solver {
   // graphs (one per step%4 pattern)
   cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
   bool graphs_ok = false;
+  // fused kernel: one TMA tensor map per stencil-input set (FW, Wa, Wb),
+  // z-chunk length, device error flag (bounded waits that expired)
+  alignas(64) unsigned char tmaps[3][128];
+  int zchunk = 0;
+  int *d_err = nullptr;
+  bool plain_interior = true;
 };
 
 namespace {
@@ -201,7 +207,7 @@ void free_all(cgfd_solver *h) {
     if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; }
   void *ptrs[] = {h->state, h->media, h->metric, h->pml, h->aux[0], h->aux[1], h->aux[2],
                   h->matv, h->d_mcell, h->d_fcell, h->d_mcoef, h->d_fcoef, h->d_mstf,
-                  h->d_fstf, h->d_rcell, h->d_seis, h->d_step, h->d_count};
+                  h->d_fstf, h->d_rcell, h->d_seis, h->d_step, h->d_count, h->d_err};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->st) cudaStreamDestroy(h->st);
@@ -334,6 +340,7 @@ StageArgs stage_args(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, in
   a.lam2mu = h->media; a.mu = h->media + fs; a.irho = h->media + 2 * fs;
   a.zx = h->metric; a.zy = h->metric + fs; a.zz = h->metric + 2 * fs; a.jac = h->metric + 3 * fs;
   a.flat = h->flat;
+  a.plain_interior = h->plain_interior;
   a.matv = h->matv;
   for (int q = 0; q < 3; ++q) {
     a.apd[q] = h->pmlp[q]; a.b[q] = h->pmlp[3 + q]; a.db[q] = h->pmlp[6 + q];
@@ -355,7 +362,7 @@ int launch_stage(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, int ou
   if (h->d.kernel == CGFD_KERNEL_SIMPLE)
     launch_stage_simple(a, h->st);
   else
-    launch_stage_fused(a, h->st);
+    launch_stage_fused_map(h->tmaps[in_set], a, h->zchunk, h->d_err, h->st);
   CK(h, cudaGetLastError());
   if (h->nmnt + h->nfrc > 0) {
     SourceArgs s{};
@@ -480,6 +487,8 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
     e = cudaMalloc(&h->d_step, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->d_step, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&h->d_count, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(h->d_err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
     if (e != cudaSuccess) st = cuda_fail(nullptr, e, "setup");
   }
@@ -489,6 +498,22 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
     return st;
   }
   for (int q = 0; q < 4; ++q) h->set[q] = h->state + (size_t)q * 9 * fs;
+  if (d->kernel == CGFD_KERNEL_FUSED) {
+    if (fused_map_bytes() > sizeof(h->tmaps[0])) {
+      free_all(h);
+      delete h;
+      return arg_fail(nullptr, "tensor map size mismatch");
+    }
+    for (int q = 0; q < 3; ++q)
+      if (!fused_make_map(h->tmaps[q], g, h->set[q])) {
+        free_all(h);
+        delete h;
+        g_last_create_error = "cuTensorMapEncodeTiled failed";
+        return CGFD_ERR_CUDA;
+      }
+    h->zchunk = fused_zchunk(g);
+    fused_init_attributes();
+  }
   {
     float *p = h->pml;
     const size_t lx = align_up(g.px, 64), ly = align_up(g.nyi, 64), lz = align_up(g.nzi, 64);
@@ -615,6 +640,14 @@ int cgfd_upload_pml(cgfd_solver *h, const double *apdx, const double *apdy, cons
     CK(h, cudaMemcpy(h->pmlp[q], v.data(), len[ax] * sizeof(float), cudaMemcpyHostToDevice));
   }
   for (int ax = 0; ax < 3; ++ax) h->hb[ax].assign(src[3 + ax], src[3 + ax] + n3[ax]);
+  // outside the layers the factors must be B = 1, DB = APD = 0 for the
+  // kernels' interior path; otherwise every cell takes the general path
+  bool plain = true;
+  const int nv[3] = {h->d.ni, h->d.nj, h->d.nk};
+  for (int ax = 0; ax < 3; ++ax)
+    for (int t = 3 + h->d.nabs[2 * ax]; t < 3 + nv[ax] - h->d.nabs[2 * ax + 1]; ++t)
+      if (src[3 + ax][t] != 1.0 || src[6 + ax][t] != 0.0 || src[ax][t] != 0.0) plain = false;
+  h->plain_interior = plain;
   h->have_pml = true;
   invalidate(h);
   return CGFD_OK;
@@ -783,7 +816,7 @@ int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms) {
         StageArgs a = stage_args(h, rk, dd[0], dd[1], dd[2], ins[rk], outs[rk]);
         CK(h, cudaEventRecord(ev[8 * (size_t)s + 2 * rk], h->st));
         if (h->d.kernel == CGFD_KERNEL_SIMPLE) launch_stage_simple(a, h->st);
-        else launch_stage_fused(a, h->st);
+        else launch_stage_fused_map(h->tmaps[ins[rk]], a, h->zchunk, h->d_err, h->st);
         CK(h, cudaGetLastError());
         CK(h, cudaEventRecord(ev[8 * (size_t)s + 2 * rk + 1], h->st));
         // sources exactly as in the graph
@@ -857,7 +890,15 @@ int cgfd_sync(cgfd_solver *h, double timeout_s) {
   const auto t0 = std::chrono::steady_clock::now();
   for (;;) {
     cudaError_t e = cudaStreamQuery(h->st);
-    if (e == cudaSuccess) return CGFD_OK;
+    if (e == cudaSuccess) {
+      int flag = 0;
+      CK(h, cudaMemcpy(&flag, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+      if (flag) {
+        h->err = "a bounded wait inside a stage kernel expired";
+        return CGFD_ERR_TIMEOUT;
+      }
+      return CGFD_OK;
+    }
     if (e != cudaErrorNotReady) return cuda_fail(h, e, "cudaStreamQuery");
     const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (timeout_s >= 0 && el > timeout_s) {

@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(TX *TY, 3)
   const int pmax = z1 - 1 + LEAD;  // last plane the chunk reads
   const size_t fs = g.fstride;
 
+  int issued = z0 - 1;  // last plane whose load thread 0 has issued
   if (tid == 0) {
     abort_flag = 0;
     for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);
@@ -119,6 +120,7 @@ __global__ void __launch_bounds__(TX *TY, 3)
       const int s = p % NSLOT;
       mbar_expect_tx(&bars[s], SLOT_BYTES);
       tma_load(ring + (size_t)s * SLOT, &tmap, bx0, by0, p, &bars[s]);
+      issued = p;
     }
   }
   __syncthreads();
@@ -143,12 +145,14 @@ __global__ void __launch_bounds__(TX *TY, 3)
     if (active) push(a.in, fs, gidx(g, ix, iy, p));
     else push(ring, 0, 0);  // keeps the window shape; values unused
   }
-  bool ok = true;
+  // A wait that expires sets the CTA-wide abort flag; the flag is read only
+  // after a __syncthreads, so every thread leaves the march together.
   for (int p = z0; p < z0 + LEAD; ++p) {
     const int s = p % NSLOT;
-    if (!mbar_wait(&bars[s], (p / NSLOT) & 1)) { ok = false; break; }
-    push(ring + (size_t)s * SLOT, PLANE, sc);
+    if (mbar_wait(&bars[s], ((p - z0) / NSLOT) & 1)) push(ring + (size_t)s * SLOT, PLANE, sc);
+    else abort_flag = 1;
   }
+  __syncthreads();
 
   // per-column constants
   const float rx = (float)X / a.h, ry = (float)Y / a.h, rz = (float)Z / a.h;
@@ -159,20 +163,23 @@ __global__ void __launch_bounds__(TX *TY, 3)
   const float Bx = a.b[0][ix], By = a.b[1][iy];
   const float iBx = 1.f / Bx, iBy = 1.f / By;
   const float APDx = a.apd[0][ix], DBx = a.db[0][ix], APDy = a.apd[1][iy], DBy = a.db[1][iy];
-  // tile-uniform: no x/y PML anywhere in this tile
+  // tile-uniform: no x/y PML anywhere in this tile (and B = 1, DB = APD = 0
+  // outside the layers, which the solver checks at upload)
   const bool tile_xy_interior =
-      (bx0 >= g.nabs[0]) && (bx0 + TX <= g.ni - g.nabs[1]) && (by0 >= g.nabs[2]) &&
-      (by0 + TY <= g.nj - g.nabs[3]);
+      a.plain_interior && (bx0 >= g.nabs[0]) && (bx0 + TX <= g.ni - g.nabs[1]) &&
+      (by0 >= g.nabs[2]) && (by0 + TY <= g.nj - g.nabs[3]);
 
-  for (int iz = z0; iz < z1 && ok; ++iz) {
+  for (int iz = z0; iz < z1 && !abort_flag; ++iz) {
     // bring plane iz+LEAD into the windows
+    bool got;
     {
       const int p = iz + LEAD, s = p % NSLOT;
-      if (!mbar_wait(&bars[s], (p / NSLOT) & 1)) { ok = false; break; }
-      push(ring + (size_t)s * SLOT, PLANE, sc);
+      got = mbar_wait(&bars[s], ((p - z0) / NSLOT) & 1);
+      if (got) push(ring + (size_t)s * SLOT, PLANE, sc);
+      else abort_flag = 1;
     }
     const float *P = ring + (size_t)(iz % NSLOT) * SLOT;  // plane iz with halo
-    if (active) {
+    if (active && got) {
       const int k = iz - LFD;
       const size_t cidx = gidx(g, ix, iy, iz);
       auto xs = [&](int c, int d) { return P[c * PLANE + sc + X * d]; };
@@ -395,23 +402,22 @@ __global__ void __launch_bounds__(TX *TY, 3)
     }
     // slot of plane iz is free: refill it with plane iz+NSLOT
     __syncthreads();
+    if (abort_flag) break;
     if (tid == 0 && iz + NSLOT <= pmax) {
       const int p = iz + NSLOT, s = p % NSLOT;
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_expect_tx(&bars[s], SLOT_BYTES);
       tma_load(ring + (size_t)s * SLOT, &tmap, bx0, by0, p, &bars[s]);
+      issued = p;
     }
-  }
-  if (!ok) {
-    atomicExch(&abort_flag, 1);
-    if (err) atomicExch(err, 1);
   }
   __syncthreads();
   if (abort_flag && tid == 0) {
-    // drain: wait (bounded) for every copy this CTA issued
-    const int last_issued = min(pmax, z1 - 1 + NSLOT);
-    for (int p = max(z0, last_issued - NSLOT + 1); p <= last_issued; ++p)
-      mbar_wait(&bars[p % NSLOT], (p / NSLOT) & 1);
+    if (err) atomicExch(err, 1);
+    // drain: wait (bounded) for the copies still possibly in flight (at most
+    // one per slot) before the CTA's shared memory goes away
+    for (int p = max(z0, issued - NSLOT + 1); p <= issued; ++p)
+      mbar_wait(&bars[p % NSLOT], ((p - z0) / NSLOT) & 1);
   }
 }
 
@@ -448,11 +454,6 @@ bool make_map(CUtensorMap *m, const Geom &g, const float *base) {
 template <int X, int Y, int Z, int KIND>
 void launch_t(const CUtensorMap &m, const StageArgs &a, int zchunk, int *err, cudaStream_t s) {
   auto k = stage_fused_kernel<X, Y, Z, KIND>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
-    attr = true;
-  }
   const int nzc = (a.g.nk + zchunk - 1) / zchunk;
   dim3 grid((a.g.ni + TX - 1) / TX, (a.g.nj + TY - 1) / TY, nzc);
   k<<<grid, dim3(TX, TY, 1), SMEM_BYTES, s>>>(m, a, zchunk, err);
@@ -507,6 +508,23 @@ void launch_stage_fused_map(const void *map, const StageArgs &a, int zchunk, int
   else launch_dirs<2>(m, a, zchunk, err, s);
 }
 
-void launch_stage_fused(const StageArgs &, void *) {}
+void fused_init_attributes() {
+  auto set = [](const void *f) {
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
+  };
+#define CGFD_ATTR(K)                                                                       \
+  set((const void *)stage_fused_kernel<-1, -1, -1, K>);                                   \
+  set((const void *)stage_fused_kernel<-1, -1, 1, K>);                                    \
+  set((const void *)stage_fused_kernel<-1, 1, -1, K>);                                    \
+  set((const void *)stage_fused_kernel<-1, 1, 1, K>);                                     \
+  set((const void *)stage_fused_kernel<1, -1, -1, K>);                                    \
+  set((const void *)stage_fused_kernel<1, -1, 1, K>);                                     \
+  set((const void *)stage_fused_kernel<1, 1, -1, K>);                                     \
+  set((const void *)stage_fused_kernel<1, 1, 1, K>);
+  CGFD_ATTR(0)
+  CGFD_ATTR(1)
+  CGFD_ATTR(2)
+#undef CGFD_ATTR
+}
 
 }  // namespace cgfd
