@@ -166,7 +166,7 @@ struct cgfd_solver {
   bool graphs_ok = false;
   // fused kernel: one TMA tensor map per stencil-input set (FW, Wa, Wb),
   // z-chunk length, device error flag (bounded waits that expired)
-  alignas(64) unsigned char tmaps[3][128];
+  alignas(64) unsigned char tmaps[3][256];
   int zchunk = 0;
   int *d_err = nullptr;
   bool plain_interior = true;
