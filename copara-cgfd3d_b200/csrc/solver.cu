@@ -894,8 +894,9 @@ int cgfd_sync(cgfd_solver *h, double timeout_s) {
       int flag = 0;
       CK(h, cudaMemcpy(&flag, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
       if (flag) {
-        h->err = "a bounded wait inside a stage kernel expired";
-        return CGFD_ERR_TIMEOUT;
+        h->err = flag == 2 ? "stage kernel alignment self-check failed (no copy issued)"
+                           : "a bounded wait inside a stage kernel expired";
+        return flag == 2 ? CGFD_ERR_CUDA : CGFD_ERR_TIMEOUT;
       }
       return CGFD_OK;
     }

@@ -52,10 +52,16 @@ template <> struct PartInfo<PART_VEL> {  // stresses are staged
 template <> struct PartInfo<PART_STR> {  // velocities are staged
   static constexpr int NC = 3, C0 = VX;
 };
+// bytes one TMA box delivers, and the slot stride: a tensor copy needs a
+// 128-byte aligned shared-memory destination, so slots are padded to 128 B
 template <int PART>
-__host__ __device__ constexpr uint32_t slot_bytes() { return (uint32_t)(PLANE * PartInfo<PART>::NC * 4); }
+__host__ __device__ constexpr uint32_t box_bytes() { return (uint32_t)(PLANE * PartInfo<PART>::NC * 4); }
 template <int PART>
-__host__ __device__ constexpr size_t smem_bytes() { return (size_t)NSLOT * slot_bytes<PART>() + 128; }
+__host__ __device__ constexpr uint32_t slot_bytes() { return (box_bytes<PART>() + 127u) / 128u * 128u; }
+// ring + barriers, plus 128 B of slack to align the ring base
+template <int PART>
+__host__ __device__ constexpr size_t smem_bytes() { return (size_t)NSLOT * slot_bytes<PART>() + 128 + 128; }
+static_assert(slot_bytes<0>() % 128 == 0 && slot_bytes<1>() % 128 == 0, "slot alignment");
 
 __device__ __forceinline__ uint32_t su32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -419,11 +425,13 @@ __global__ void __launch_bounds__(TX *TY, 4)
     stage_part_kernel(const __grid_constant__ CUtensorMap tmap, const StageArgs a, int zchunk,
                       int *err) {
   constexpr int NC = PartInfo<PART>::NC, C0 = PartInfo<PART>::C0;
-  constexpr int SLOTF = PLANE * NC;
-  constexpr uint32_t SB = slot_bytes<PART>();
+  constexpr uint32_t SB = slot_bytes<PART>(), BB = box_bytes<PART>();
+  constexpr int SLOTF = SB / 4;  // float stride between slots
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  float *ring = reinterpret_cast<float *>(smem_raw);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + (size_t)NSLOT * SB);
+  // align the ring on the shared-window address itself
+  unsigned char *base = smem_raw + ((128u - (su32(smem_raw) & 127u)) & 127u);
+  float *ring = reinterpret_cast<float *>(base);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(base + (size_t)NSLOT * SB);
   __shared__ int abort_flag;
 
   const Geom &g = a.g;
@@ -444,16 +452,26 @@ __global__ void __launch_bounds__(TX *TY, 4)
   int issued = z0 - 1;  // last plane whose load thread 0 has issued
   if (tid == 0) {
     abort_flag = 0;
-    for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    for (int p = z0; p < z0 + NSLOT && p <= pmax; ++p) {
-      const int s = p % NSLOT;
-      mbar_expect_tx(&bars[s], SB);
-      tma_load(ring + (size_t)s * SLOTF, &tmap, bx0, by0, p, C0, &bars[s]);
-      issued = p;
+    // self-check before any copy is issued: 128-byte aligned slot
+    // destinations, 8-byte aligned barriers, 16-byte aligned box origin
+    bool aligned = ((su32(bars) & 7u) == 0) && ((bx0 * 4) % 16 == 0);
+    for (int s = 0; s < NSLOT; ++s) aligned = aligned && ((su32(ring + (size_t)s * SLOTF) & 127u) == 0);
+    if (!aligned) {
+      abort_flag = 1;
+      if (err) atomicExch(err, 2);
+    } else {
+      for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      for (int p = z0; p < z0 + NSLOT && p <= pmax; ++p) {
+        const int s = p % NSLOT;
+        mbar_expect_tx(&bars[s], BB);
+        tma_load(ring + (size_t)s * SLOTF, &tmap, bx0, by0, p, C0, &bars[s]);
+        issued = p;
+      }
     }
   }
   __syncthreads();
+  if (abort_flag) return;  // nothing was issued
 
   // register windows: w[c][0..4] = planes iz-LAG .. iz+LEAD at this column
   float w[NC][5];
@@ -530,7 +548,7 @@ __global__ void __launch_bounds__(TX *TY, 4)
     if (tid == 0 && iz + NSLOT <= pmax) {
       const int p = iz + NSLOT, s = p % NSLOT;
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_expect_tx(&bars[s], SB);
+      mbar_expect_tx(&bars[s], BB);
       tma_load(ring + (size_t)s * SLOTF, &tmap, bx0, by0, p, C0, &bars[s]);
       issued = p;
     }
