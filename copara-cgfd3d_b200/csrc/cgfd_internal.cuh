@@ -112,11 +112,14 @@ struct SourceArgs {
 
 void launch_stage_simple(const StageArgs &a, void *stream);
 bool fused_supported(const Geom &g);
-size_t fused_map_bytes();
-bool fused_make_map(void *map, const Geom &g, const float *set_base);
-int fused_zchunk(const Geom &g);
-void fused_init_attributes();
-void launch_stage_fused_map(const void *map, const StageArgs &a, int zchunk, int *err,
-                            void *stream);
+// Tensor maps and launch shape of the fused kernels for one solver's buffers
+// (sets = FW, Wa, Wb, tW).  nullptr when a tensor map cannot be encoded.
+void *fused_create_plan(const Geom &g, float *const sets[4], const float *media,
+                        const float *metric);
+void fused_destroy_plan(void *plan);
+// Both kernels (velocity, stress) of one RK stage; in_set is 0 (FW), 1 or 2.
+void launch_stage_fused(const void *plan, const StageArgs &a, int in_set, int *err,
+                        void *stream);
+int fused_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str);
 
 }  // namespace cgfd

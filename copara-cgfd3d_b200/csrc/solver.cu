@@ -164,10 +164,9 @@ struct cgfd_solver {
   // graphs (one per step%4 pattern)
   cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
   bool graphs_ok = false;
-  // fused kernel: one TMA tensor map per stencil-input set (FW, Wa, Wb),
-  // z-chunk length, device error flag (bounded waits that expired)
-  alignas(64) unsigned char tmaps[3][256];
-  int zchunk = 0;
+  // fused kernels: tensor maps and launch shape; device error flag (bounded
+  // waits that expired, alignment self-check)
+  void *plan = nullptr;
   int *d_err = nullptr;
   bool plain_interior = true;
 };
@@ -203,6 +202,7 @@ int arg_fail(cgfd_solver *h, const char *what) {
   } while (0)
 
 void free_all(cgfd_solver *h) {
+  if (h->plan) { fused_destroy_plan(h->plan); h->plan = nullptr; }
   for (auto &gr : h->graph)
     if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; }
   void *ptrs[] = {h->state, h->media, h->metric, h->pml, h->aux[0], h->aux[1], h->aux[2],
@@ -362,7 +362,7 @@ int launch_stage(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, int ou
   if (h->d.kernel == CGFD_KERNEL_SIMPLE)
     launch_stage_simple(a, h->st);
   else
-    launch_stage_fused_map(h->tmaps[in_set], a, h->zchunk, h->d_err, h->st);
+    launch_stage_fused(h->plan, a, in_set, h->d_err, h->st);
   CK(h, cudaGetLastError());
   if (h->nmnt + h->nfrc > 0) {
     SourceArgs s{};
@@ -499,20 +499,13 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
   }
   for (int q = 0; q < 4; ++q) h->set[q] = h->state + (size_t)q * 9 * fs;
   if (d->kernel == CGFD_KERNEL_FUSED) {
-    if (fused_map_bytes() > sizeof(h->tmaps[0])) {
+    h->plan = fused_create_plan(g, h->set, h->media, h->metric);
+    if (!h->plan) {
       free_all(h);
       delete h;
-      return arg_fail(nullptr, "tensor map size mismatch");
+      g_last_create_error = "cuTensorMapEncodeTiled failed";
+      return CGFD_ERR_CUDA;
     }
-    for (int q = 0; q < 3; ++q)
-      if (!fused_make_map(h->tmaps[q], g, h->set[q])) {
-        free_all(h);
-        delete h;
-        g_last_create_error = "cuTensorMapEncodeTiled failed";
-        return CGFD_ERR_CUDA;
-      }
-    h->zchunk = fused_zchunk(g);
-    fused_init_attributes();
   }
   {
     float *p = h->pml;
@@ -816,7 +809,7 @@ int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms) {
         StageArgs a = stage_args(h, rk, dd[0], dd[1], dd[2], ins[rk], outs[rk]);
         CK(h, cudaEventRecord(ev[8 * (size_t)s + 2 * rk], h->st));
         if (h->d.kernel == CGFD_KERNEL_SIMPLE) launch_stage_simple(a, h->st);
-        else launch_stage_fused_map(h->tmaps[ins[rk]], a, h->zchunk, h->d_err, h->st);
+        else launch_stage_fused(h->plan, a, ins[rk], h->d_err, h->st);
         CK(h, cudaGetLastError());
         CK(h, cudaEventRecord(ev[8 * (size_t)s + 2 * rk + 1], h->st));
         // sources exactly as in the graph

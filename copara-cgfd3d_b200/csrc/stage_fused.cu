@@ -5,19 +5,23 @@
 // stress part only velocity derivatives, so each kernel stages only the
 // components it differentiates and carries half the register state.
 //
-// Each CTA owns a 32 x 4 tile of (x, y) columns and marches upwards through a
-// chunk of z-planes.  Per plane, the differentiated components of the stage
-// input arrive with an x/y halo by TMA (cp.async.bulk.tensor, one 4-D box
-// {40 x, 10 y, 1 z, NC components} per plane, no multicast) into a ring of 5
-// shared-memory slots, one mbarrier per slot, so the loads of the next planes
-// overlap the arithmetic on the current one.  The one-sided DRP stencils reach
-// -1..+3 or -3..+1 cells; the box covers -4..+4 in x (x origin 16-byte
-// aligned) and -3..+3 in y.  z stencils run from per-thread register windows
-// of 5 planes per component.  The RK update (Iteration*), the CFS-PML
-// auxiliaries and the free-surface work (VLOW operators, surface matrices,
-// traction image) are fused into the same pass: a stage reads W_in once from
-// HBM for its stencils plus FW / tW / aux and the coefficients, and writes
-// W_out / tW / aux.  There are no derivative or hW arrays.
+// Work is a set of items (a 32 x 4 tile of (x, y) columns times a chunk of
+// z-planes); a persistent grid of CTAs walks the items, and each CTA marches
+// upwards through its chunk.  Every plane the march needs arrives by TMA
+// (cp.async.bulk.tensor, no multicast) into one slot of a 5-slot shared-memory
+// ring, on one mbarrier per slot:
+//   * the differentiated components of the stage input with an x/y halo (one
+//     4-D box {40 x, 10 y, 1 z, NC components}; the one-sided DRP stencils
+//     reach -1..+3 or -3..+1 cells, the box covers -4..+4 in x so that its x
+//     origin is 16-byte aligned, and -3..+3 in y);
+//   * the pointwise operands of the same plane without halo (FW and/or tW
+//     components for the RK update, the media coefficients, the metric).
+// Loads run 5 planes ahead of the arithmetic, so no warp waits on a plain
+// global load during the march; results are written with coalesced stores.
+// z stencils run from per-thread register windows of 5 planes per component.
+// The RK update (Iteration*), the CFS-PML auxiliaries and the free-surface
+// work (VLOW operators, surface matrices, traction image) are fused into the
+// same pass; there are no derivative or hW arrays.
 //
 // Per cell the arithmetic is that of the reference's CalDiffmix + CalWavemix
 // + CalTIMGmix + Iteration* (src/calculate.cu:4121-4621, 5668-5897,
@@ -26,7 +30,8 @@
 // Every wait on an mbarrier is bounded (about 2 s of %globaltimer).  On
 // expiry the CTA leaves the march together (the flag is read after a
 // barrier), records an error code in *err, waits (bounded) for its own copies
-// still in flight and returns; the host then reports CGFD_ERR_TIMEOUT.
+// still in flight and returns; the host then reports CGFD_ERR_TIMEOUT.  Before
+// issuing any copy the CTA checks the alignment of its slots and barriers.
 #include "cgfd_internal.cuh"
 
 #include <cuda.h>
@@ -34,34 +39,55 @@
 #include <cudaTypedefs.h>
 
 #include <cstdint>
+#include <new>
 
 namespace cgfd {
 namespace {
 
-constexpr int TX = 32, TY = 4;                 // threads per CTA tile
-constexpr int BOXX = TX + 8, BOXY = TY + 6;    // TMA box (x starts 4 left, y 3 below)
+constexpr int TX = 32, TY = 4, TT = TX * TY;   // threads per CTA tile
+constexpr int BOXX = TX + 8, BOXY = TY + 6;    // halo box (x starts 4 left, y 3 below)
 constexpr int NSLOT = 5;
-constexpr int PLANE = BOXX * BOXY;             // floats per component per plane
+constexpr int PLANE = BOXX * BOXY;             // floats per component per halo plane
 constexpr unsigned long long WAIT_NS = 2000000000ull;
 enum { PART_VEL = 0, PART_STR = 1 };
 
+// NC: staged (differentiated) components, C0: first of them in a set;
+// NS: components the part updates (V: 3, T: 6), S0 their first index;
+// NCOEF: media coefficients it reads, COEF0 the first (lam2mu, mu, irho).
 template <int PART> struct PartInfo;
-template <> struct PartInfo<PART_VEL> {  // stresses are staged
-  static constexpr int NC = 6, C0 = TXX;
+template <> struct PartInfo<PART_VEL> {
+  static constexpr int NC = 6, C0 = TXX, NS = 3, S0 = VX, NCOEF = 1, COEF0 = 2;
 };
-template <> struct PartInfo<PART_STR> {  // velocities are staged
-  static constexpr int NC = 3, C0 = VX;
+template <> struct PartInfo<PART_STR> {
+  static constexpr int NC = 3, C0 = VX, NS = 6, S0 = TXX, NCOEF = 2, COEF0 = 0;
 };
-// bytes one TMA box delivers, and the slot stride: a tensor copy needs a
-// 128-byte aligned shared-memory destination, so slots are padded to 128 B
-template <int PART>
-__host__ __device__ constexpr uint32_t box_bytes() { return (uint32_t)(PLANE * PartInfo<PART>::NC * 4); }
-template <int PART>
-__host__ __device__ constexpr uint32_t slot_bytes() { return (box_bytes<PART>() + 127u) / 128u * 128u; }
-// ring + barriers, plus 128 B of slack to align the ring base
-template <int PART>
-__host__ __device__ constexpr size_t smem_bytes() { return (size_t)NSLOT * slot_bytes<PART>() + 128 + 128; }
-static_assert(slot_bytes<0>() % 128 == 0 && slot_bytes<1>() % 128 == 0, "slot alignment");
+
+// Slot layout (floats): halo [NC][BOXY][BOXX], then pointwise tiles of TT
+// floats: u0 [NS] (FW, or tW in the final stage), u1 [NS] (tW in the inner
+// stages), coef [NCOEF], met [3] (zeta_x, zeta_y, zeta_z).  A tensor copy
+// needs a 128-byte aligned shared-memory destination: every region starts on
+// 128 B (TT floats = 512 B) and the slot stride is a multiple of 128 B.
+template <int PART> struct Slot {
+  static constexpr int NC = PartInfo<PART>::NC, NS = PartInfo<PART>::NS;
+  static constexpr uint32_t HALO_B = (uint32_t)(PLANE * NC * 4);
+  static constexpr uint32_t HALO_F = (HALO_B + 127u) / 128u * 32u;  // floats, padded
+  static constexpr uint32_t U0 = HALO_F, U1 = U0 + NS * TT, COEF = U1 + NS * TT;
+  static constexpr uint32_t MET = COEF + PartInfo<PART>::NCOEF * TT;
+  static constexpr uint32_t FLOATS = MET + 3 * TT;
+  static constexpr uint32_t BYTES = FLOATS * 4;
+  static constexpr size_t SMEM = (size_t)NSLOT * BYTES + 128 + 128;  // + barriers, align slack
+};
+static_assert(Slot<PART_VEL>::BYTES % 128 == 0 && Slot<PART_STR>::BYTES % 128 == 0, "slots");
+static_assert((Slot<PART_VEL>::U0 * 4) % 128 == 0 && (Slot<PART_STR>::U0 * 4) % 128 == 0, "u0");
+
+// Tensor maps of one stage launch.
+struct StageMaps {
+  CUtensorMap halo;  // stage input, box {40, 10, 1, NC}
+  CUtensorMap u0;    // FW (or tW), box {32, 4, 1, NS}
+  CUtensorMap u1;    // tW, box {32, 4, 1, NS}
+  CUtensorMap coef;  // media, box {32, 4, 1, NCOEF}
+  CUtensorMap met;   // metric, box {32, 4, 1, 3}
+};
 
 __device__ __forceinline__ uint32_t su32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -110,18 +136,33 @@ __device__ __forceinline__ float drp5(float m1, float c0, float p1, float p2, fl
   return (CGFD_DA_1 * m1 + CGFD_DA0 * c0 + CGFD_DA1 * p1 + CGFD_DA2 * p2 + CGFD_DA3 * p3) * r;
 }
 
-// RK update of one value (Iteration*): KIND 0 first stage, 1 inner, 2 final
+// RK update of one value (Iteration*): KIND 0 first stage (u0 = FW),
+// 1 inner (u0 = FW, u1 = tW), 2 final (u0 = tW)
 template <int KIND>
-__device__ __forceinline__ void rk_put(float *out, float *tw, const float *fw, size_t o, float fwv,
-                                       float hh, float adt, float bdt) {
+__device__ __forceinline__ void rk_store(float *out, float *tw, size_t o, float u0, float u1,
+                                         float hh, float adt, float bdt) {
   if (KIND == 0) {
-    out[o] = fwv + adt * hh;
-    tw[o] = fwv + bdt * hh;
+    out[o] = u0 + adt * hh;
+    tw[o] = u0 + bdt * hh;
   } else if (KIND == 1) {
-    out[o] = fw[o] + adt * hh;
-    tw[o] = tw[o] + bdt * hh;
+    out[o] = u0 + adt * hh;
+    tw[o] = u1 + bdt * hh;
   } else {
-    out[o] = tw[o] + bdt * hh;
+    out[o] = u0 + bdt * hh;
+  }
+}
+// same for the ADE auxiliaries, which are read straight from global memory
+template <int KIND>
+__device__ __forceinline__ void rk_aux(const StageArgs &a, int d, size_t o, float hh) {
+  if (KIND == 0) {
+    const float f = a.ain[d][o];
+    a.aout[d][o] = f + a.adt * hh;
+    a.ta[d][o] = f + a.bdt * hh;
+  } else if (KIND == 1) {
+    a.aout[d][o] = a.afw[d][o] + a.adt * hh;
+    a.ta[d][o] = a.ta[d][o] + a.bdt * hh;
+  } else {
+    a.aout[d][o] = a.ta[d][o] + a.bdt * hh;
   }
 }
 
@@ -134,14 +175,23 @@ struct Cell {
   size_t px, py, pz;  // aux indices
 };
 
+// Pointwise operands of the current plane in shared memory.
+struct Pw {
+  const float *u0, *u1, *coef, *met;  // already offset to this thread's column
+  __device__ float U0(int q) const { return u0[q * TT]; }
+  __device__ float U1(int q) const { return u1[q * TT]; }
+  __device__ float C(int q) const { return coef[q * TT]; }
+  __device__ float M(int q) const { return met[q * TT]; }
+};
+
 // -------------------------- velocity part ---------------------------------
 // dV/dt = (1/rho) (d_xi sigma_x + d_eta sigma_y + zeta . d_zeta sigma), each
 // directional part divided by its CFS beta; ADE auxiliaries for V; traction
 // image for the top 3 layers.
 template <int X, int Y, int Z, int KIND, int LAG>
 __device__ __forceinline__ void vel_cell(const StageArgs &a, const Cell &e, const float *P,
-                                         int sc, const float (&w)[6][5], float rx, float ry,
-                                         float rz) {
+                                         int sc, const Pw &pw, const float (&w)[6][5],
+                                         float rx, float ry, float rz) {
   const Geom &g = a.g;
   const size_t fs = g.fstride;
   // staged components: 0 Txx 1 Tyy 2 Tzz 3 Txy 4 Txz 5 Tyz
@@ -152,12 +202,12 @@ __device__ __forceinline__ void vel_cell(const StageArgs &a, const Cell &e, cons
   auto dy = [&](int s) { return drp5(ys(s, -1), ys(s, 0), ys(s, 1), ys(s, 2), ys(s, 3), ry); };
   auto dz = [&](int s) { return drp5(zs(s, -1), zs(s, 0), zs(s, 1), zs(s, 2), zs(s, 3), rz); };
 
-  const float irho = a.irho[e.c];
+  const float irho = pw.C(0);
   float ztx = 0.f, zty = 0.f, ztz = 1.f;
   const bool curved = e.iz >= g.con && !a.flat;
   if (!a.flat) {
-    ztz = a.zz[e.c];
-    if (curved) { ztx = a.zx[e.c]; zty = a.zy[e.c]; }
+    ztz = pw.M(2);
+    if (curved) { ztx = pw.M(0); zty = pw.M(1); }
   }
   float dxi[3], det[3], dzt[3];
   dxi[0] = dx(0) * irho;  // DxTxx
@@ -266,24 +316,17 @@ __device__ __forceinline__ void vel_cell(const StageArgs &a, const Cell &e, cons
         hw[q] = hv;
       }
     }
-    auto aux = [&](int d, size_t p, const float *hh) {
-      const size_t as = g.astride[d];
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const size_t o = q * as + p;
-        rk_put<KIND>(a.aout[d], a.ta[d], a.afw[d], o, KIND == 0 ? a.ain[d][o] : 0.f, hh[q],
-                     a.adt, a.bdt);
-      }
-    };
-    if (e.xpml) aux(0, e.px, hax);
-    if (e.ypml) aux(1, e.py, hay);
-    if (e.zpml) aux(2, e.pz, haz);
+    for (int q = 0; q < 3; ++q) {
+      if (e.xpml) rk_aux<KIND>(a, 0, q * g.astride[0] + e.px, hax[q]);
+      if (e.ypml) rk_aux<KIND>(a, 1, q * g.astride[1] + e.py, hay[q]);
+      if (e.zpml) rk_aux<KIND>(a, 2, q * g.astride[2] + e.pz, haz[q]);
+    }
   }
 #pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    const size_t o = (size_t)(VX + q) * fs + e.c;
-    rk_put<KIND>(a.out, a.tw, a.fw, o, KIND == 0 ? a.in[o] : 0.f, hw[q], a.adt, a.bdt);
-  }
+  for (int q = 0; q < 3; ++q)
+    rk_store<KIND>(a.out, a.tw, (size_t)(VX + q) * fs + e.c, pw.U0(q),
+                   KIND == 1 ? pw.U1(q) : 0.f, hw[q], a.adt, a.bdt);
 }
 
 // --------------------------- stress part ----------------------------------
@@ -292,8 +335,8 @@ __device__ __forceinline__ void vel_cell(const StageArgs &a, const Cell &e, cons
 // next two layers use the 2-point and Gottlieb 2-4 operators (VLOW).
 template <int X, int Y, int Z, int KIND, int LAG>
 __device__ __forceinline__ void str_cell(const StageArgs &a, const Cell &e, const float *P,
-                                         int sc, const float (&w)[3][5], float rx, float ry,
-                                         float rz) {
+                                         int sc, const Pw &pw, const float (&w)[3][5],
+                                         float rx, float ry, float rz) {
   const Geom &g = a.g;
   const size_t fs = g.fstride;
   auto xs = [&](int s, int d) { return P[s * PLANE + sc + X * d]; };
@@ -329,12 +372,12 @@ __device__ __forceinline__ void str_cell(const StageArgs &a, const Cell &e, cons
     DzVx = dz(0); DzVy = dz(1); DzVz = dz(2);
   }
 
-  const float lam2mu = a.lam2mu[e.c], miu = a.mu[e.c];
+  const float lam2mu = pw.C(0), miu = pw.C(1);
   const float lambda = lam2mu - 2.f * miu;
   float ztx = 0.f, zty = 0.f, ztz = 1.f;
   if (!a.flat) {
-    ztz = a.zz[e.c];
-    if (e.iz >= g.con) { ztx = a.zx[e.c]; zty = a.zy[e.c]; }
+    ztz = pw.M(2);
+    if (e.iz >= g.con) { ztx = pw.M(0); zty = pw.M(1); }
   }
   // components in the set order Txx Tyy Tzz Txy Txz Tyz (index q = comp - 3)
   float dxi[6], det[6], dzt[6];
@@ -399,167 +442,188 @@ __device__ __forceinline__ void str_cell(const StageArgs &a, const Cell &e, cons
         haz[q] = dzt[q] * DB - APD * av;
       }
     }
-    auto aux = [&](int d, size_t p, const float *hh) {
-      const size_t as = g.astride[d];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        const size_t o = (3 + q) * as + p;
-        rk_put<KIND>(a.aout[d], a.ta[d], a.afw[d], o, KIND == 0 ? a.ain[d][o] : 0.f, hh[q],
-                     a.adt, a.bdt);
-      }
-    };
-    if (e.xpml) aux(0, e.px, hax);
-    if (e.ypml) aux(1, e.py, hay);
-    if (e.zpml) aux(2, e.pz, haz);
+    for (int q = 0; q < 6; ++q) {
+      if (e.xpml) rk_aux<KIND>(a, 0, (3 + q) * g.astride[0] + e.px, hax[q]);
+      if (e.ypml) rk_aux<KIND>(a, 1, (3 + q) * g.astride[1] + e.py, hay[q]);
+      if (e.zpml) rk_aux<KIND>(a, 2, (3 + q) * g.astride[2] + e.pz, haz[q]);
+    }
   }
 #pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    const size_t o = (size_t)(TXX + q) * fs + e.c;
-    rk_put<KIND>(a.out, a.tw, a.fw, o, KIND == 0 ? a.in[o] : 0.f, hw[q], a.adt, a.bdt);
-  }
+  for (int q = 0; q < 6; ++q)
+    rk_store<KIND>(a.out, a.tw, (size_t)(TXX + q) * fs + e.c, pw.U0(q),
+                   KIND == 1 ? pw.U1(q) : 0.f, hw[q], a.adt, a.bdt);
 }
 
 // ------------------------------ the march ---------------------------------
+// items: tile index fastest, so the CTAs resident at one time work on
+// neighbouring tiles of the same z-chunk and share halo rows in L2
 template <int PART, int X, int Y, int Z, int KIND>
-__global__ void __launch_bounds__(TX *TY, 4)
-    stage_part_kernel(const __grid_constant__ CUtensorMap tmap, const StageArgs a, int zchunk,
-                      int *err) {
+__global__ void __launch_bounds__(TT, 3)
+    stage_part_kernel(const __grid_constant__ StageMaps maps, const StageArgs a, int zchunk,
+                      int ntx, int ntiles, int nitems, int *err) {
+  using S = Slot<PART>;
   constexpr int NC = PartInfo<PART>::NC, C0 = PartInfo<PART>::C0;
-  constexpr uint32_t SB = slot_bytes<PART>(), BB = box_bytes<PART>();
-  constexpr int SLOTF = SB / 4;  // float stride between slots
+  constexpr int NS = PartInfo<PART>::NS, S0 = PartInfo<PART>::S0;
+  constexpr int NCOEF = PartInfo<PART>::NCOEF, COEF0 = PartInfo<PART>::COEF0;
+  constexpr int LEAD = (Z > 0) ? 3 : 1, LAG = (Z > 0) ? 1 : 3;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // align the ring on the shared-window address itself
   unsigned char *base = smem_raw + ((128u - (su32(smem_raw) & 127u)) & 127u);
   float *ring = reinterpret_cast<float *>(base);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(base + (size_t)NSLOT * SB);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(base + (size_t)NSLOT * S::BYTES);
   __shared__ int abort_flag;
 
   const Geom &g = a.g;
-  constexpr int LEAD = (Z > 0) ? 3 : 1, LAG = (Z > 0) ? 1 : 3;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int bx0 = blockIdx.x * TX, by0 = blockIdx.y * TY;
-  Cell e;
-  e.i = bx0 + tx;
-  e.j = by0 + ty;
-  const bool active = (e.i < g.ni) && (e.j < g.nj);
-  e.ix = e.i + XO;
-  e.iy = e.j + LFD;
-  const int z0 = LFD + blockIdx.z * zchunk;
-  const int z1 = min(z0 + zchunk, g.nk + LFD);
-  const int pmax = z1 - 1 + LEAD;  // last plane the chunk reads
   const size_t fs = g.fstride;
+  const bool flat = a.flat;
+  // bytes one plane delivers: halo always, pointwise only for computed planes
+  const uint32_t pw_bytes = (uint32_t)(TT * 4) *
+      (NS * (KIND == 1 ? 2 : 1) + NCOEF + (flat ? 0 : 3));
 
-  int issued = z0 - 1;  // last plane whose load thread 0 has issued
   if (tid == 0) {
     abort_flag = 0;
-    // self-check before any copy is issued: 128-byte aligned slot
-    // destinations, 8-byte aligned barriers, 16-byte aligned box origin
-    bool aligned = ((su32(bars) & 7u) == 0) && ((bx0 * 4) % 16 == 0);
-    for (int s = 0; s < NSLOT; ++s) aligned = aligned && ((su32(ring + (size_t)s * SLOTF) & 127u) == 0);
+    bool aligned = ((su32(bars) & 7u) == 0);
+    for (int s = 0; s < NSLOT; ++s)
+      aligned = aligned && ((su32(ring + (size_t)s * S::FLOATS) & 127u) == 0);
     if (!aligned) {
       abort_flag = 1;
       if (err) atomicExch(err, 2);
     } else {
       for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-      for (int p = z0; p < z0 + NSLOT && p <= pmax; ++p) {
-        const int s = p % NSLOT;
-        mbar_expect_tx(&bars[s], BB);
-        tma_load(ring + (size_t)s * SLOTF, &tmap, bx0, by0, p, C0, &bars[s]);
-        issued = p;
-      }
     }
   }
   __syncthreads();
   if (abort_flag) return;  // nothing was issued
 
-  // register windows: w[c][0..4] = planes iz-LAG .. iz+LEAD at this column
-  float w[NC][5];
-#pragma unroll
-  for (int c = 0; c < NC; ++c)
-#pragma unroll
-    for (int q = 0; q < 5; ++q) w[c][q] = 0.f;
-  auto push = [&](const float *src, size_t stride, size_t off) {
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-#pragma unroll
-      for (int q = 0; q < 4; ++q) w[c][q] = w[c][q + 1];
-      w[c][4] = src[c * stride + off];
-    }
-  };
-  const int sc = (ty + 3) * BOXX + (tx + 4);  // this column inside a slot plane
-  // planes below the chunk come straight from global memory (centre only)
-  for (int p = z0 - LAG; p < z0; ++p) {
-    if (active) push(a.in + (size_t)C0 * fs, fs, gidx(g, e.ix, e.iy, p));
-    else push(ring, 0, 0);  // keeps the window shape; values unused
-  }
-  // A wait that expires sets the CTA-wide abort flag; the flag is read only
-  // after a __syncthreads, so every thread leaves the march together.
-  for (int p = z0; p < z0 + LEAD; ++p) {
-    const int s = p % NSLOT;
-    if (mbar_wait(&bars[s], ((p - z0) / NSLOT) & 1)) push(ring + (size_t)s * SLOTF, PLANE, sc);
-    else abort_flag = 1;
-  }
-  __syncthreads();
-
+  uint32_t ph = 0;    // parity of the next wait, per slot (same in every thread)
+  uint32_t pend = 0;  // thread 0: slots with a copy not yet waited for
   const float rx = (float)X / a.h, ry = (float)Y / a.h, rz = (float)Z / a.h;
-  e.xpml = active && (e.i < g.nabs[0] || e.i >= g.ni - g.nabs[1]);
-  e.ypml = active && (e.j < g.nabs[2] || e.j >= g.nj - g.nabs[3]);
-  const int xa = (e.i < g.nabs[0]) ? e.i : e.i - (g.ni - g.nabs[1]) + g.nabs[0];
-  const int ya = (e.j < g.nabs[2]) ? e.j : e.j - (g.nj - g.nabs[3]) + g.nabs[2];
-  e.iBx = 1.f / a.b[0][e.ix];
-  e.iBy = 1.f / a.b[1][e.iy];
-  // tile-uniform: no x/y PML anywhere in this tile (and B = 1, DB = APD = 0
-  // outside the layers, which the solver checks at upload)
-  const bool tile_xy_interior =
-      a.plain_interior && (bx0 >= g.nabs[0]) && (bx0 + TX <= g.ni - g.nabs[1]) &&
-      (by0 >= g.nabs[2]) && (by0 + TY <= g.nj - g.nabs[3]);
+  const int sc = (ty + 3) * BOXX + (tx + 4);  // this column inside a halo plane
 
-  for (int iz = z0; iz < z1 && !abort_flag; ++iz) {
-    bool got;
-    {  // bring plane iz+LEAD into the windows
-      const int p = iz + LEAD, s = p % NSLOT;
-      got = mbar_wait(&bars[s], ((p - z0) / NSLOT) & 1);
-      if (got) push(ring + (size_t)s * SLOTF, PLANE, sc);
+  for (int item = blockIdx.x; item < nitems && !abort_flag; item += gridDim.x) {
+    const int tile = item % ntiles, cz = item / ntiles;
+    const int bx0 = (tile % ntx) * TX, by0 = (tile / ntx) * TY;
+    const int z0 = LFD + cz * zchunk;
+    const int z1 = min(z0 + zchunk, g.nk + LFD);
+    const int pmax = z1 - 1 + LEAD;  // last plane the chunk reads
+    auto issue = [&](int p) {        // thread 0 only
+      const int s = (p - z0) % NSLOT;
+      float *slot = ring + (size_t)s * S::FLOATS;
+      const bool compute = p < z1;
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(&bars[s], S::HALO_B + (compute ? pw_bytes : 0u));
+      tma_load(slot, &maps.halo, bx0, by0, p, C0, &bars[s]);
+      if (compute) {
+        const int cx = XO + bx0, cy = LFD + by0;
+        tma_load(slot + S::U0, &maps.u0, cx, cy, p, S0, &bars[s]);
+        if (KIND == 1) tma_load(slot + S::U1, &maps.u1, cx, cy, p, S0, &bars[s]);
+        tma_load(slot + S::COEF, &maps.coef, cx, cy, p, COEF0, &bars[s]);
+        if (!flat) tma_load(slot + S::MET, &maps.met, cx, cy, p, 0, &bars[s]);
+      }
+      pend |= 1u << s;
+    };
+    auto wait = [&](int p) -> bool {  // every thread, in plane order
+      const int s = (p - z0) % NSLOT;
+      const bool ok = mbar_wait(&bars[s], (ph >> s) & 1u);
+      if (ok) {  // an expired wait leaves the copy pending for the drain
+        ph ^= 1u << s;
+        if (tid == 0) pend &= ~(1u << s);
+      }
+      return ok;
+    };
+    if (tid == 0)
+      for (int p = z0; p < z0 + NSLOT && p <= pmax; ++p) issue(p);
+
+    Cell e;
+    e.i = bx0 + tx;
+    e.j = by0 + ty;
+    const bool active = (e.i < g.ni) && (e.j < g.nj);
+    e.ix = e.i + XO;
+    e.iy = e.j + LFD;
+    e.xpml = active && (e.i < g.nabs[0] || e.i >= g.ni - g.nabs[1]);
+    e.ypml = active && (e.j < g.nabs[2] || e.j >= g.nj - g.nabs[3]);
+    const int xa = (e.i < g.nabs[0]) ? e.i : e.i - (g.ni - g.nabs[1]) + g.nabs[0];
+    const int ya = (e.j < g.nabs[2]) ? e.j : e.j - (g.nj - g.nabs[3]) + g.nabs[2];
+    e.iBx = 1.f / a.b[0][e.ix];
+    e.iBy = 1.f / a.b[1][e.iy];
+    // tile-uniform: no x/y PML anywhere in this tile (and B = 1, DB = APD = 0
+    // outside the layers, which the solver checks at upload)
+    const bool tile_xy_interior =
+        a.plain_interior && (bx0 >= g.nabs[0]) && (bx0 + TX <= g.ni - g.nabs[1]) &&
+        (by0 >= g.nabs[2]) && (by0 + TY <= g.nj - g.nabs[3]);
+
+    // register windows: w[c][0..4] = planes iz-LAG .. iz+LEAD at this column
+    float w[NC][5];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int q = 0; q < 5; ++q) w[c][q] = 0.f;
+    auto push = [&](const float *src, size_t stride, size_t off) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) w[c][q] = w[c][q + 1];
+        w[c][4] = src[c * stride + off];
+      }
+    };
+    // planes below the chunk come straight from global memory (centre only)
+    for (int p = z0 - LAG; p < z0; ++p) {
+      if (active) push(a.in + (size_t)C0 * fs, fs, gidx(g, e.ix, e.iy, p));
+      else push(ring, 0, 0);  // keeps the window shape; values unused
+    }
+    // A wait that expires sets the CTA-wide abort flag; the flag is read only
+    // after a __syncthreads, so every thread leaves the march together.
+    for (int p = z0; p < z0 + LEAD; ++p) {
+      if (wait(p)) push(ring + (size_t)((p - z0) % NSLOT) * S::FLOATS, PLANE, sc);
       else abort_flag = 1;
     }
-    if (active && got) {
-      const float *P = ring + (size_t)(iz % NSLOT) * SLOTF;  // plane iz with halo
-      e.iz = iz;
-      e.k = iz - LFD;
-      e.c = gidx(g, e.ix, e.iy, iz);
-      e.top = (iz == g.top);
-      e.near_top = iz >= g.top - 2;
-      e.zpml = (e.k < g.nabs[4]) || (e.k >= g.nk - g.nabs[5]);
-      e.interior = tile_xy_interior && !e.zpml && !e.near_top;
-      e.iBz = 1.f / a.b[2][iz];
-      e.px = ((size_t)iz * g.nyi + e.iy) * g.nxa + xa;
-      e.py = ((size_t)iz * g.nya + ya) * g.px + e.ix;
-      const int za = (e.k < g.nabs[4]) ? e.k : e.k - (g.nk - g.nabs[5]) + g.nabs[4];
-      e.pz = ((size_t)za * g.nyi + e.iy) * g.px + e.ix;
-      if constexpr (PART == PART_VEL)
-        vel_cell<X, Y, Z, KIND, LAG>(a, e, P, sc, w, rx, ry, rz);
-      else
-        str_cell<X, Y, Z, KIND, LAG>(a, e, P, sc, w, rx, ry, rz);
-    }
-    // the slot of plane iz is free: refill it with plane iz+NSLOT
     __syncthreads();
-    if (abort_flag) break;
-    if (tid == 0 && iz + NSLOT <= pmax) {
-      const int p = iz + NSLOT, s = p % NSLOT;
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_expect_tx(&bars[s], BB);
-      tma_load(ring + (size_t)s * SLOTF, &tmap, bx0, by0, p, C0, &bars[s]);
-      issued = p;
+
+    for (int iz = z0; iz < z1 && !abort_flag; ++iz) {
+      bool got;
+      {  // bring plane iz+LEAD into the windows
+        const int p = iz + LEAD;
+        got = wait(p);
+        if (got) push(ring + (size_t)((p - z0) % NSLOT) * S::FLOATS, PLANE, sc);
+        else abort_flag = 1;
+      }
+      if (active && got) {
+        const float *slot = ring + (size_t)((iz - z0) % NSLOT) * S::FLOATS;
+        const int tc = ty * TX + tx;
+        Pw pw{slot + S::U0 + tc, slot + S::U1 + tc, slot + S::COEF + tc, slot + S::MET + tc};
+        e.iz = iz;
+        e.k = iz - LFD;
+        e.c = gidx(g, e.ix, e.iy, iz);
+        e.top = (iz == g.top);
+        e.near_top = iz >= g.top - 2;
+        e.zpml = (e.k < g.nabs[4]) || (e.k >= g.nk - g.nabs[5]);
+        e.interior = tile_xy_interior && !e.zpml && !e.near_top;
+        e.iBz = 1.f / a.b[2][iz];
+        e.px = ((size_t)iz * g.nyi + e.iy) * g.nxa + xa;
+        e.py = ((size_t)iz * g.nya + ya) * g.px + e.ix;
+        const int za = (e.k < g.nabs[4]) ? e.k : e.k - (g.nk - g.nabs[5]) + g.nabs[4];
+        e.pz = ((size_t)za * g.nyi + e.iy) * g.px + e.ix;
+        if constexpr (PART == PART_VEL)
+          vel_cell<X, Y, Z, KIND, LAG>(a, e, slot, sc, pw, w, rx, ry, rz);
+        else
+          str_cell<X, Y, Z, KIND, LAG>(a, e, slot, sc, pw, w, rx, ry, rz);
+      }
+      // the slot of plane iz is free: refill it with plane iz+NSLOT
+      __syncthreads();
+      if (abort_flag) break;
+      if (tid == 0 && iz + NSLOT <= pmax) issue(iz + NSLOT);
     }
+    __syncthreads();  // all reads of the ring done before the next item reuses it
   }
-  __syncthreads();
   if (abort_flag && tid == 0) {
     if (err) atomicExch(err, 1);
-    // drain: wait (bounded) for the copies still possibly in flight (at most
-    // one per slot) before the CTA's shared memory goes away
-    for (int p = max(z0, issued - NSLOT + 1); p <= issued; ++p)
-      mbar_wait(&bars[p % NSLOT], ((p - z0) / NSLOT) & 1);
+    // drain: wait (bounded) for copies still in flight before the CTA's
+    // shared memory goes away
+    for (int s = 0; s < NSLOT; ++s)
+      if (pend & (1u << s)) mbar_wait(&bars[s], (ph >> s) & 1u);
   }
 }
 
@@ -578,15 +642,17 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// 4-D map over one field set: {x: px, y: nyi, z: nzi, component: 9}, box of
-// nc components
-bool make_map(CUtensorMap *m, const Geom &g, const float *base, int nc) {
+// 4-D map over ncomp arrays of the internal layout: {x: px, y: nyi, z: nzi,
+// component}, with a box of {bx, by, 1, bc}
+bool make_map(CUtensorMap *m, const Geom &g, const float *base, int ncomp, int bx, int by,
+              int bc) {
   auto fn = encode_fn();
   if (!fn) return false;
-  cuuint64_t dims[4] = {(cuuint64_t)g.px, (cuuint64_t)g.nyi, (cuuint64_t)g.nzi, 9};
+  cuuint64_t dims[4] = {(cuuint64_t)g.px, (cuuint64_t)g.nyi, (cuuint64_t)g.nzi,
+                        (cuuint64_t)ncomp};
   cuuint64_t strides[3] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.plane * 4,
                            (cuuint64_t)g.fstride * 4};
-  cuuint32_t box[4] = {BOXX, BOXY, 1, (cuuint32_t)nc};
+  cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)bc};
   cuuint32_t es[4] = {1, 1, 1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)base, dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -594,41 +660,40 @@ bool make_map(CUtensorMap *m, const Geom &g, const float *base, int nc) {
   return r == CUDA_SUCCESS;
 }
 
+struct Plan {
+  // per field set (FW, Wa, Wb, tW): halo boxes for the two parts and the
+  // pointwise boxes of V (3) and T (6) components
+  CUtensorMap haloV[4], haloS[4], ctrV[4], ctrT[4];
+  CUtensorMap coefV, coefS, met;
+  int zchunk, ntx, ntiles, nitems, grid[2];
+};
+
 template <int PART, int X, int Y, int Z, int KIND>
-void launch_t(const CUtensorMap &m, const StageArgs &a, int zchunk, int *err, cudaStream_t s) {
-  const int nzc = (a.g.nk + zchunk - 1) / zchunk;
-  dim3 grid((a.g.ni + TX - 1) / TX, (a.g.nj + TY - 1) / TY, nzc);
-  stage_part_kernel<PART, X, Y, Z, KIND>
-      <<<grid, dim3(TX, TY, 1), smem_bytes<PART>(), s>>>(m, a, zchunk, err);
+void launch_t(const Plan &pl, const StageMaps &m, const StageArgs &a, int *err, cudaStream_t s) {
+  stage_part_kernel<PART, X, Y, Z, KIND><<<pl.grid[PART], dim3(TX, TY, 1), Slot<PART>::SMEM, s>>>(
+      m, a, pl.zchunk, pl.ntx, pl.ntiles, pl.nitems, err);
 }
 
 template <int PART, int KIND>
-void launch_dirs(const CUtensorMap &m, const StageArgs &a, int zc, int *err, cudaStream_t s) {
+void launch_dirs(const Plan &pl, const StageMaps &m, const StageArgs &a, int *err,
+                 cudaStream_t s) {
   const int code = (a.X > 0 ? 4 : 0) + (a.Y > 0 ? 2 : 0) + (a.Z > 0 ? 1 : 0);
   switch (code) {
-    case 0: launch_t<PART, -1, -1, -1, KIND>(m, a, zc, err, s); break;
-    case 1: launch_t<PART, -1, -1, 1, KIND>(m, a, zc, err, s); break;
-    case 2: launch_t<PART, -1, 1, -1, KIND>(m, a, zc, err, s); break;
-    case 3: launch_t<PART, -1, 1, 1, KIND>(m, a, zc, err, s); break;
-    case 4: launch_t<PART, 1, -1, -1, KIND>(m, a, zc, err, s); break;
-    case 5: launch_t<PART, 1, -1, 1, KIND>(m, a, zc, err, s); break;
-    case 6: launch_t<PART, 1, 1, -1, KIND>(m, a, zc, err, s); break;
-    default: launch_t<PART, 1, 1, 1, KIND>(m, a, zc, err, s); break;
+    case 0: launch_t<PART, -1, -1, -1, KIND>(pl, m, a, err, s); break;
+    case 1: launch_t<PART, -1, -1, 1, KIND>(pl, m, a, err, s); break;
+    case 2: launch_t<PART, -1, 1, -1, KIND>(pl, m, a, err, s); break;
+    case 3: launch_t<PART, -1, 1, 1, KIND>(pl, m, a, err, s); break;
+    case 4: launch_t<PART, 1, -1, -1, KIND>(pl, m, a, err, s); break;
+    case 5: launch_t<PART, 1, -1, 1, KIND>(pl, m, a, err, s); break;
+    case 6: launch_t<PART, 1, 1, -1, KIND>(pl, m, a, err, s); break;
+    default: launch_t<PART, 1, 1, 1, KIND>(pl, m, a, err, s); break;
   }
-}
-
-template <int PART>
-void launch_part(const CUtensorMap &m, const StageArgs &a, int zc, int *err, cudaStream_t s) {
-  if (a.rk == 0) launch_dirs<PART, 0>(m, a, zc, err, s);
-  else if (a.rk < 3) launch_dirs<PART, 1>(m, a, zc, err, s);
-  else launch_dirs<PART, 2>(m, a, zc, err, s);
 }
 
 template <int PART, int KIND>
 void set_attrs() {
   auto set = [](const void *f) {
-    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem_bytes<PART>());
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Slot<PART>::SMEM);
   };
   set((const void *)stage_part_kernel<PART, -1, -1, -1, KIND>);
   set((const void *)stage_part_kernel<PART, -1, -1, 1, KIND>);
@@ -640,44 +705,108 @@ void set_attrs() {
   set((const void *)stage_part_kernel<PART, 1, 1, 1, KIND>);
 }
 
+template <int PART>
+int resident_ctas() {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per, stage_part_kernel<PART, 1, 1, 1, 1>, TT, Slot<PART>::SMEM);
+  if (per < 1) per = 1;
+  if (sms < 1) sms = 1;
+  return per * sms;
+}
+
 }  // namespace
 
 bool fused_supported(const Geom &g) {
-  // the tile's TMA box starts on a 16-byte boundary (XO = 4 floats, px a
-  // multiple of 32) and the grid is at least one chunk deep
+  // tile boxes start on 16-byte boundaries (XO = 4 floats, px a multiple of
+  // 32) and the grid is at least one plane deep beyond the stencil reach
   return (XO % 4) == 0 && g.px % 32 == 0 && g.nk >= 4;
 }
 
-size_t fused_map_bytes() { return 2 * sizeof(CUtensorMap); }
-
-bool fused_make_map(void *map, const Geom &g, const float *set_base) {
-  CUtensorMap *m = reinterpret_cast<CUtensorMap *>(map);
-  return make_map(&m[0], g, set_base, PartInfo<PART_VEL>::NC) &&
-         make_map(&m[1], g, set_base, PartInfo<PART_STR>::NC);
+void *fused_create_plan(const Geom &g, float *const sets[4], const float *media,
+                        const float *metric) {
+  static bool attrs = false;
+  if (!attrs) {
+    set_attrs<PART_VEL, 0>(); set_attrs<PART_VEL, 1>(); set_attrs<PART_VEL, 2>();
+    set_attrs<PART_STR, 0>(); set_attrs<PART_STR, 1>(); set_attrs<PART_STR, 2>();
+    attrs = true;
+  }
+  Plan *pl = new (std::nothrow) Plan();
+  if (!pl) return nullptr;
+  bool ok = true;
+  for (int q = 0; q < 4; ++q) {
+    ok = ok && make_map(&pl->haloV[q], g, sets[q], 9, BOXX, BOXY, PartInfo<PART_VEL>::NC);
+    ok = ok && make_map(&pl->haloS[q], g, sets[q], 9, BOXX, BOXY, PartInfo<PART_STR>::NC);
+    ok = ok && make_map(&pl->ctrV[q], g, sets[q], 9, TX, TY, PartInfo<PART_VEL>::NS);
+    ok = ok && make_map(&pl->ctrT[q], g, sets[q], 9, TX, TY, PartInfo<PART_STR>::NS);
+  }
+  ok = ok && make_map(&pl->coefV, g, media, 3, TX, TY, PartInfo<PART_VEL>::NCOEF);
+  ok = ok && make_map(&pl->coefS, g, media, 3, TX, TY, PartInfo<PART_STR>::NCOEF);
+  ok = ok && make_map(&pl->met, g, metric, 4, TX, TY, 3);
+  if (!ok) {
+    delete pl;
+    return nullptr;
+  }
+  pl->ntx = (g.ni + TX - 1) / TX;
+  pl->ntiles = pl->ntx * ((g.nj + TY - 1) / TY);
+  const int G = resident_ctas<PART_VEL>() < resident_ctas<PART_STR>() ? resident_ctas<PART_VEL>()
+                                                                     : resident_ctas<PART_STR>();
+  // z-chunk length: minimise (rounds of work over the resident CTAs) x
+  // (chunk length + start-up planes)
+  double best = 1e30;
+  int bestzc = g.nk;
+  for (int nzc = 1; nzc <= (g.nk + 7) / 8; ++nzc) {
+    const int zc = (g.nk + nzc - 1) / nzc;
+    const long items = (long)pl->ntiles * ((g.nk + zc - 1) / zc);
+    const long rounds = (items + G - 1) / G;
+    const double cost = (double)rounds * (zc + 6);
+    if (cost < best - 1e-9) { best = cost; bestzc = zc; }
+  }
+  pl->zchunk = bestzc;
+  pl->nitems = pl->ntiles * ((g.nk + bestzc - 1) / bestzc);
+  pl->grid[0] = pl->nitems < resident_ctas<PART_VEL>() ? pl->nitems : resident_ctas<PART_VEL>();
+  pl->grid[1] = pl->nitems < resident_ctas<PART_STR>() ? pl->nitems : resident_ctas<PART_STR>();
+  return pl;
 }
 
-int fused_zchunk(const Geom &g) {
-  // enough CTAs for ~4 per SM on 148 SMs, chunks of at least 16 planes
-  const long tiles = (long)((g.ni + TX - 1) / TX) * ((g.nj + TY - 1) / TY);
-  int nzc = (int)((4L * 148 + tiles - 1) / tiles);
-  nzc = nzc < 1 ? 1 : nzc;
-  int zc = (g.nk + nzc - 1) / nzc;
-  if (zc < 16) zc = 16;
-  if (zc > g.nk) zc = g.nk;
-  return zc;
-}
+void fused_destroy_plan(void *plan) { delete reinterpret_cast<Plan *>(plan); }
 
-void fused_init_attributes() {
-  set_attrs<PART_VEL, 0>(); set_attrs<PART_VEL, 1>(); set_attrs<PART_VEL, 2>();
-  set_attrs<PART_STR, 0>(); set_attrs<PART_STR, 1>(); set_attrs<PART_STR, 2>();
-}
-
-void launch_stage_fused_map(const void *map, const StageArgs &a, int zchunk, int *err,
-                            void *stream) {
-  const CUtensorMap *m = reinterpret_cast<const CUtensorMap *>(map);
+void launch_stage_fused(const void *plan, const StageArgs &a, int in_set, int *err,
+                        void *stream) {
+  const Plan &pl = *reinterpret_cast<const Plan *>(plan);
   cudaStream_t s = (cudaStream_t)stream;
-  launch_part<PART_VEL>(m[0], a, zchunk, err, s);
-  launch_part<PART_STR>(m[1], a, zchunk, err, s);
+  const int kind = a.rk == 0 ? 0 : (a.rk < 3 ? 1 : 2);
+  StageMaps mv, ms;
+  mv.halo = pl.haloV[in_set];
+  mv.u0 = kind == 2 ? pl.ctrV[3] : pl.ctrV[0];
+  mv.u1 = pl.ctrV[3];
+  mv.coef = pl.coefV;
+  mv.met = pl.met;
+  ms.halo = pl.haloS[in_set];
+  ms.u0 = kind == 2 ? pl.ctrT[3] : pl.ctrT[0];
+  ms.u1 = pl.ctrT[3];
+  ms.coef = pl.coefS;
+  ms.met = pl.met;
+  if (kind == 0) {
+    launch_dirs<PART_VEL, 0>(pl, mv, a, err, s);
+    launch_dirs<PART_STR, 0>(pl, ms, a, err, s);
+  } else if (kind == 1) {
+    launch_dirs<PART_VEL, 1>(pl, mv, a, err, s);
+    launch_dirs<PART_STR, 1>(pl, ms, a, err, s);
+  } else {
+    launch_dirs<PART_VEL, 2>(pl, mv, a, err, s);
+    launch_dirs<PART_STR, 2>(pl, ms, a, err, s);
+  }
+}
+
+int fused_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str) {
+  const Plan &pl = *reinterpret_cast<const Plan *>(plan);
+  if (zchunk) *zchunk = pl.zchunk;
+  if (grid_vel) *grid_vel = pl.grid[0];
+  if (grid_str) *grid_str = pl.grid[1];
+  return pl.nitems;
 }
 
 }  // namespace cgfd

@@ -95,3 +95,23 @@ def test_flat_halfspace_160x160x80_500_steps_matches_reference(kernel):
         e = rel_l2(ps[c], r["seis"][c])
         assert e < TOL, f"{cgfd.COMPONENTS[c]} rel L2 {e:.3e}"
     _cmp(ps, r["seis"], TOL, "seismogram")
+
+
+def test_fused_matches_simple_kernel_on_hill_400x400x200():
+    """Full-size property check on the 400x400x200 hill model: 8 steps of the
+    tiled kernels (many work items per persistent CTA) against the untiled
+    per-cell kernel, seismograms and the final wavefield."""
+    import models
+    m = models.config_c2(nt=8)
+    out = {}
+    for kern in (cgfd.KERNEL_FUSED, cgfd.KERNEL_SIMPLE):
+        s = cgfd.Solver(m.desc(kernel=kern))
+        m.load(s)
+        s.step(8)
+        fw = np.stack([s.get_field(c)[::3, ::3, 3:-3] for c in range(9)])
+        out[kern] = (s.seismograms(), fw)
+        s.close()
+    for c, e in enumerate(comp_errors(out[cgfd.KERNEL_FUSED][1], out[cgfd.KERNEL_SIMPLE][1])):
+        assert e < 1e-5, (cgfd.COMPONENTS[c], e)
+    for c, e in enumerate(comp_errors(out[cgfd.KERNEL_FUSED][0], out[cgfd.KERNEL_SIMPLE][0])):
+        assert e < 1e-5, (cgfd.COMPONENTS[c], e)
