@@ -154,20 +154,48 @@ __device__ __forceinline__ void rk_store(float *out, float *tw, size_t o, float 
     out[o] = u0 + bdt * hh;
   }
 }
-// same for the ADE auxiliaries, which are read straight from global memory
-template <int KIND>
-__device__ __forceinline__ void rk_aux(const StageArgs &a, int d, size_t o, float hh) {
-  if (KIND == 0) {
-    const float f = a.ain[d][o];
-    a.aout[d][o] = f + a.adt * hh;
-    a.ta[d][o] = f + a.bdt * hh;
-  } else if (KIND == 1) {
-    a.aout[d][o] = a.afw[d][o] + a.adt * hh;
-    a.ta[d][o] = a.ta[d][o] + a.bdt * hh;
-  } else {
-    a.aout[d][o] = a.ta[d][o] + a.bdt * hh;
+// ADE auxiliaries of one cell and direction: every load first (all in flight
+// together, issued before the stencil arithmetic), the stores at the end.
+// ai = stage input (FA in the first stage, A after), af = FA, at = tA.
+template <int KIND, int N>
+struct Aux {
+  float ai[N], af[N], at[N];
+  __device__ __forceinline__ void load(const StageArgs &a, int d, size_t p, int c0) {
+    const size_t as = a.g.astride[d];
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      const size_t o = (c0 + q) * as + p;
+      ai[q] = a.ain[d][o];
+    }
   }
-}
+  // RK operands (FA, tA), loaded together right before the stores
+  __device__ __forceinline__ void load_rk(const StageArgs &a, int d, size_t p, int c0) {
+    const size_t as = a.g.astride[d];
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      const size_t o = (c0 + q) * as + p;
+      if (KIND == 1) af[q] = a.afw[d][o];
+      if (KIND != 0) at[q] = a.ta[d][o];
+    }
+  }
+  __device__ __forceinline__ void store(const StageArgs &a, int d, size_t p, int c0,
+                                        const float *hh) const {
+    const size_t as = a.g.astride[d];
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      const size_t o = (c0 + q) * as + p;
+      if (KIND == 0) {
+        a.aout[d][o] = ai[q] + a.adt * hh[q];
+        a.ta[d][o] = ai[q] + a.bdt * hh[q];
+      } else if (KIND == 1) {
+        a.aout[d][o] = af[q] + a.adt * hh[q];
+        a.ta[d][o] = at[q] + a.bdt * hh[q];
+      } else {
+        a.aout[d][o] = at[q] + a.bdt * hh[q];
+      }
+    }
+  }
+};
 
 // Per-cell context shared by the two parts.
 struct Cell {
@@ -182,6 +210,7 @@ struct Cell {
 struct Edge {
   float iBz;
   size_t px, py, pz;  // aux indices
+  __device__ Edge() : iBz(1.f), px(0), py(0), pz(0) {}
   __device__ Edge(const StageArgs &a, const Cell &e) {
     const Geom &g = a.g;
     iBz = 1.f / a.b[2][e.iz];
@@ -219,6 +248,16 @@ __device__ __forceinline__ void vel_cell(const StageArgs &a, const Cell &e, cons
   auto dy = [&](int s) { return drp5(ys(s, -1), ys(s, 0), ys(s, 1), ys(s, 2), ys(s, 3), ry); };
   auto dz = [&](int s) { return drp5(zs(s, -1), zs(s, 0), zs(s, 1), zs(s, 2), zs(s, 3), rz); };
 
+  // boundary cells: issue every auxiliary load before the stencil arithmetic
+  const bool bnd = !e.interior;
+  Edge ed;
+  Aux<KIND, 3> ax, ay, az;
+  if (bnd) {
+    ed = Edge(a, e);
+    if (e.xpml) ax.load(a, 0, ed.px, 0);
+    if (e.ypml) ay.load(a, 1, ed.py, 0);
+    if (e.zpml) az.load(a, 2, ed.pz, 0);
+  }
   const float irho = pw.C(0);
   float ztx = 0.f, zty = 0.f, ztz = 1.f;
   const bool curved = e.iz >= g.con && !a.flat;
@@ -249,7 +288,6 @@ __device__ __forceinline__ void vel_cell(const StageArgs &a, const Cell &e, cons
 #pragma unroll
     for (int q = 0; q < 3; ++q) hw[q] = dxi[q] + det[q] + dzt[q];
   } else {
-    const Edge ed(a, e);
 #pragma unroll
     for (int q = 0; q < 3; ++q) hw[q] = dxi[q] * e.iBx + det[q] * e.iBy + dzt[q] * ed.iBz;
     float hax[3], hay[3], haz[3];
@@ -257,27 +295,24 @@ __device__ __forceinline__ void vel_cell(const StageArgs &a, const Cell &e, cons
       const float APD = a.apd[0][e.ix], DB = a.db[0][e.ix];
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
-        const float av = a.ain[0][q * g.astride[0] + ed.px];
-        hw[q] -= av * e.iBx;
-        hax[q] = dxi[q] * DB - APD * av;
+        hw[q] -= ax.ai[q] * e.iBx;
+        hax[q] = dxi[q] * DB - APD * ax.ai[q];
       }
     }
     if (e.ypml) {
       const float APD = a.apd[1][e.iy], DB = a.db[1][e.iy];
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
-        const float av = a.ain[1][q * g.astride[1] + ed.py];
-        hw[q] -= av * e.iBy;
-        hay[q] = det[q] * DB - APD * av;
+        hw[q] -= ay.ai[q] * e.iBy;
+        hay[q] = det[q] * DB - APD * ay.ai[q];
       }
     }
     if (e.zpml) {
       const float APD = a.apd[2][e.iz], DB = a.db[2][e.iz];
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
-        const float av = a.ain[2][q * g.astride[2] + ed.pz];
-        hw[q] -= av * ed.iBz;
-        haz[q] = dzt[q] * DB - APD * av;
+        hw[q] -= az.ai[q] * ed.iBz;
+        haz[q] = dzt[q] * DB - APD * az.ai[q];
       }
     }
     if (e.near_top) {
@@ -322,24 +357,22 @@ __device__ __forceinline__ void vel_cell(const StageArgs &a, const Cell &e, cons
         const float DzT = rhojac * drp5(vz[3 - Z], vz[3], vz[3 + Z], vz[3 + 2 * Z], vz[3 + 3 * Z], rz);
         float hv = DxT * e.iBx + DyT * e.iBy + DzT;
         if (e.xpml) {
-          const float av = a.ain[0][q * g.astride[0] + ed.px];
-          hv -= av * e.iBx;
-          hax[q] = a.db[0][e.ix] * DxT - a.apd[0][e.ix] * av;
+          hv -= ax.ai[q] * e.iBx;
+          hax[q] = a.db[0][e.ix] * DxT - a.apd[0][e.ix] * ax.ai[q];
         }
         if (e.ypml) {
-          const float av = a.ain[1][q * g.astride[1] + ed.py];
-          hv -= av * e.iBy;
-          hay[q] = a.db[1][e.iy] * DyT - a.apd[1][e.iy] * av;
+          hv -= ay.ai[q] * e.iBy;
+          hay[q] = a.db[1][e.iy] * DyT - a.apd[1][e.iy] * ay.ai[q];
         }
         hw[q] = hv;
       }
     }
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      if (e.xpml) rk_aux<KIND>(a, 0, q * g.astride[0] + ed.px, hax[q]);
-      if (e.ypml) rk_aux<KIND>(a, 1, q * g.astride[1] + ed.py, hay[q]);
-      if (e.zpml) rk_aux<KIND>(a, 2, q * g.astride[2] + ed.pz, haz[q]);
-    }
+    if (e.xpml) ax.load_rk(a, 0, ed.px, 0);
+    if (e.ypml) ay.load_rk(a, 1, ed.py, 0);
+    if (e.zpml) az.load_rk(a, 2, ed.pz, 0);
+    if (e.xpml) ax.store(a, 0, ed.px, 0, hax);
+    if (e.ypml) ay.store(a, 1, ed.py, 0, hay);
+    if (e.zpml) az.store(a, 2, ed.pz, 0, haz);
   }
 #pragma unroll
   for (int q = 0; q < 3; ++q)
@@ -364,6 +397,16 @@ __device__ __forceinline__ void str_cell(const StageArgs &a, const Cell &e, cons
   auto dy = [&](int s) { return drp5(ys(s, -1), ys(s, 0), ys(s, 1), ys(s, 2), ys(s, 3), ry); };
   auto dz = [&](int s) { return drp5(zs(s, -1), zs(s, 0), zs(s, 1), zs(s, 2), zs(s, 3), rz); };
 
+  // boundary cells: issue every auxiliary load before the stencil arithmetic
+  const bool bnd = !e.interior;
+  Edge ed;
+  Aux<KIND, 6> ax, ay, az;
+  if (bnd) {
+    ed = Edge(a, e);
+    if (e.xpml) ax.load(a, 0, ed.px, 3);
+    if (e.ypml) ay.load(a, 1, ed.py, 3);
+    if (e.zpml) az.load(a, 2, ed.pz, 3);
+  }
   const float DxVx = dx(0), DxVy = dx(1), DxVz = dx(2);
   const float DyVx = dy(0), DyVy = dy(1), DyVz = dy(2);
   float DzVx, DzVy, DzVz;
@@ -414,7 +457,6 @@ __device__ __forceinline__ void str_cell(const StageArgs &a, const Cell &e, cons
 #pragma unroll
     for (int q = 0; q < 6; ++q) hw[q] = dxi[q] + det[q] + dzt[q];
   } else {
-    const Edge ed(a, e);
 #pragma unroll
     for (int q = 0; q < 6; ++q) hw[q] = dxi[q] * e.iBx + det[q] * e.iBy + dzt[q] * ed.iBz;
     float hax[6], hay[6], haz[6];
@@ -432,9 +474,8 @@ __device__ __forceinline__ void str_cell(const StageArgs &a, const Cell &e, cons
       const float APD = a.apd[0][e.ix], DB = a.db[0][e.ix];
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        const float av = a.ain[0][(3 + q) * g.astride[0] + ed.px];
-        hw[q] -= av * e.iBx;
-        hax[q] = dxi[q] * DB - APD * av;
+        hw[q] -= ax.ai[q] * e.iBx;
+        hax[q] = dxi[q] * DB - APD * ax.ai[q];
       }
       if (e.top)
         surf(cx[0] * DxVx + cx[1] * DxVy + cx[2] * DxVz, cx[3] * DxVx + cx[4] * DxVy + cx[5] * DxVz,
@@ -444,9 +485,8 @@ __device__ __forceinline__ void str_cell(const StageArgs &a, const Cell &e, cons
       const float APD = a.apd[1][e.iy], DB = a.db[1][e.iy];
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        const float av = a.ain[1][(3 + q) * g.astride[1] + ed.py];
-        hw[q] -= av * e.iBy;
-        hay[q] = det[q] * DB - APD * av;
+        hw[q] -= ay.ai[q] * e.iBy;
+        hay[q] = det[q] * DB - APD * ay.ai[q];
       }
       if (e.top)
         surf(cy[0] * DyVx + cy[1] * DyVy + cy[2] * DyVz, cy[3] * DyVx + cy[4] * DyVy + cy[5] * DyVz,
@@ -456,17 +496,16 @@ __device__ __forceinline__ void str_cell(const StageArgs &a, const Cell &e, cons
       const float APD = a.apd[2][e.iz], DB = a.db[2][e.iz];
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        const float av = a.ain[2][(3 + q) * g.astride[2] + ed.pz];
-        hw[q] -= av * ed.iBz;
-        haz[q] = dzt[q] * DB - APD * av;
+        hw[q] -= az.ai[q] * ed.iBz;
+        haz[q] = dzt[q] * DB - APD * az.ai[q];
       }
     }
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      if (e.xpml) rk_aux<KIND>(a, 0, (3 + q) * g.astride[0] + ed.px, hax[q]);
-      if (e.ypml) rk_aux<KIND>(a, 1, (3 + q) * g.astride[1] + ed.py, hay[q]);
-      if (e.zpml) rk_aux<KIND>(a, 2, (3 + q) * g.astride[2] + ed.pz, haz[q]);
-    }
+    if (e.xpml) ax.load_rk(a, 0, ed.px, 3);
+    if (e.ypml) ay.load_rk(a, 1, ed.py, 3);
+    if (e.zpml) az.load_rk(a, 2, ed.pz, 3);
+    if (e.xpml) ax.store(a, 0, ed.px, 3, hax);
+    if (e.ypml) ay.store(a, 1, ed.py, 3, hay);
+    if (e.zpml) az.store(a, 2, ed.pz, 3, haz);
   }
 #pragma unroll
   for (int q = 0; q < 6; ++q)
