@@ -308,7 +308,7 @@ def main():
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_step": bps, "stage_kernel_ms": stage_ms},
         "clocks": clk.summary(),
-        "gpu_launches": K * (4 * (2 if args.kernel == "fused" else 1) + 4 * n_src + 1),
+        "gpu_launches": K * (4 * (3 if args.kernel == "fused" else 1) + 4 * n_src + 1),
         "nonfinite": nbad,
     }
     if e2e:

@@ -111,6 +111,8 @@ struct SourceArgs {
 };
 
 void launch_stage_simple(const StageArgs &a, void *stream);
+// traction-image velocity update of the top 3 layers (after the fused kernels)
+void launch_timg(const StageArgs &a, void *stream);
 bool fused_supported(const Geom &g);
 // Tensor maps and launch shape of the fused kernels for one solver's buffers
 // (sets = FW, Wa, Wb, tW).  nullptr when a tensor map cannot be encoded.

@@ -127,6 +127,7 @@ void launch_stage_fused(const void *plan, const StageArgs &a, int in_set, int *e
     launch_v2(pl, mv, a, err, s);
     launch_s2(pl, ms, a, err, s);
   }
+  launch_timg(a, s);
 }
 
 int fused_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str) {

@@ -232,8 +232,8 @@ struct Pw {
 
 // -------------------------- velocity part ---------------------------------
 // dV/dt = (1/rho) (d_xi sigma_x + d_eta sigma_y + zeta . d_zeta sigma), each
-// directional part divided by its CFS beta; ADE auxiliaries for V; traction
-// image for the top 3 layers.
+// directional part divided by its CFS beta; ADE auxiliaries for V.  The top 3
+// layers take the traction image instead (timg.cu).
 template <int X, int Y, int Z, int KIND, int LAG>
 __device__ __forceinline__ void vel_cell(const StageArgs &a, const Cell &e, const float *P,
                                          int sc, const Pw &pw, const float (&w)[6][5],
@@ -315,64 +315,16 @@ __device__ __forceinline__ void vel_cell(const StageArgs &a, const Cell &e, cons
         haz[q] = dzt[q] * DB - APD * az.ai[q];
       }
     }
-    if (e.near_top) {
-      // traction image (CalTIMGmix): conservative momentum equation with the
-      // normal traction J zeta.sigma odd about the surface; the z vector is
-      // read from global memory since it reaches 3 planes to either side
-      const int s = g.top - e.iz;
-      const float rhojac = a.flat ? irho : irho / a.jac[e.c];
-      const long sy = g.px, sz = (long)g.plane;
-      constexpr int TS[3][2] = {{0, 3}, {3, 1}, {4, 5}};  // staged (x, y) stress per V
-      constexpr int TC[3][3] = {{TXX, TXY, TXZ}, {TXY, TYY, TYZ}, {TXZ, TYZ, TZZ}};
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        float vx[5], vy[5], vz[7];
-#pragma unroll
-        for (int d = -1; d <= 3; ++d) {
-          float jx = 1.f, jy = 1.f;
-          if (!a.flat) {
-            jx = a.jac[(long)e.c + X * d];
-            jy = a.jac[(long)e.c + Y * d * sy];
-          }
-          vx[d + 1] = jx * xs(TS[q][0], d);
-          vy[d + 1] = jy * ys(TS[q][1], d);
-        }
-#pragma unroll
-        for (int n = 0; n < 7; ++n) {
-          const long gz = (long)e.c + (n - 3) * sz;
-          const float t1 = a.in[TC[q][0] * fs + gz], t2 = a.in[TC[q][1] * fs + gz],
-                      t3 = a.in[TC[q][2] * fs + gz];
-          vz[n] = a.flat ? t3 : a.jac[gz] * (a.zx[gz] * t1 + a.zy[gz] * t2 + a.zz[gz] * t3);
-        }
-        // the surface is s layers up (vector index 3+s): zero there, odd above
-        if (s == 0) {
-          vz[3] = 0.f; vz[4] = -vz[2]; vz[5] = -vz[1]; vz[6] = -vz[0];
-        } else if (s == 1) {
-          vz[4] = 0.f; vz[5] = -vz[3]; vz[6] = -vz[2];
-        } else {
-          vz[5] = 0.f; vz[6] = -vz[4];
-        }
-        const float DxT = rhojac * drp5(vx[0], vx[1], vx[2], vx[3], vx[4], rx);
-        const float DyT = rhojac * drp5(vy[0], vy[1], vy[2], vy[3], vy[4], ry);
-        const float DzT = rhojac * drp5(vz[3 - Z], vz[3], vz[3 + Z], vz[3 + 2 * Z], vz[3 + 3 * Z], rz);
-        float hv = DxT * e.iBx + DyT * e.iBy + DzT;
-        if (e.xpml) {
-          hv -= ax.ai[q] * e.iBx;
-          hax[q] = a.db[0][e.ix] * DxT - a.apd[0][e.ix] * ax.ai[q];
-        }
-        if (e.ypml) {
-          hv -= ay.ai[q] * e.iBy;
-          hay[q] = a.db[1][e.iy] * DyT - a.apd[1][e.iy] * ay.ai[q];
-        }
-        hw[q] = hv;
-      }
-    }
-    if (e.xpml) ax.load_rk(a, 0, ed.px, 0);
-    if (e.ypml) ay.load_rk(a, 1, ed.py, 0);
+    // the top 3 layers' velocities (and their x/y auxiliaries) come from the
+    // traction-image kernel (timg.cu); only the z auxiliaries are kept here
+    const bool xy = !e.near_top;
+    if (e.xpml && xy) ax.load_rk(a, 0, ed.px, 0);
+    if (e.ypml && xy) ay.load_rk(a, 1, ed.py, 0);
     if (e.zpml) az.load_rk(a, 2, ed.pz, 0);
-    if (e.xpml) ax.store(a, 0, ed.px, 0, hax);
-    if (e.ypml) ay.store(a, 1, ed.py, 0, hay);
+    if (e.xpml && xy) ax.store(a, 0, ed.px, 0, hax);
+    if (e.ypml && xy) ay.store(a, 1, ed.py, 0, hay);
     if (e.zpml) az.store(a, 2, ed.pz, 0, haz);
+    if (!xy) return;
   }
 #pragma unroll
   for (int q = 0; q < 3; ++q)
@@ -640,48 +592,37 @@ __global__ void __launch_bounds__(TT, 3)
     }
     __syncthreads();
 
-    // The march is unrolled by the ring size: plane iz lives in slot
-    // (iz - z0) % NSLOT, so every slot offset and every rotation of the
-    // register windows is a compile-time constant.
+    // plane iz lives in slot (iz - z0) % NSLOT
     const int tc = ty * TX + tx;
-    const size_t cbase = gidx(g, e.ix, e.iy, z0);
     const int zlo = LFD + g.nabs[4], zhi = g.nk + LFD - g.nabs[5];  // z interior [zlo, zhi)
-    bool stop = false;
-    for (int zb = z0; zb < z1 && !stop; zb += NSLOT) {
-#pragma unroll
-      for (int u = 0; u < NSLOT; ++u) {
-        const int iz = zb + u;
-        if (iz < z1 && !stop) {
-          {  // bring plane iz+LEAD into the windows
-            const int p = iz + LEAD;
-            const bool got = wait(p);
-            if (got) push(ring + (size_t)((u + LEAD) % NSLOT) * S::FLOATS, PLANE, sc);
-            else abort_flag = 1;
-            if (active && got) {
-              const float *slot = ring + (size_t)u * S::FLOATS;
-              Pw pw{slot + S::U0 + tc, slot + S::U1 + tc, slot + S::COEF + tc, slot + S::MET + tc};
-              e.iz = iz;
-              e.k = iz - LFD;
-              e.c = cbase + (size_t)(iz - z0) * g.plane;
-              e.top = (iz == g.top);
-              e.near_top = iz >= g.top - 2;
-              e.zpml = (iz < zlo) || (iz >= zhi);
-              e.interior = tile_xy_interior && !e.zpml && !e.near_top;
-              if constexpr (PART == PART_VEL)
-                vel_cell<X, Y, Z, KIND, LAG>(a, e, slot, sc, pw, w, rx, ry, rz);
-              else
-                str_cell<X, Y, Z, KIND, LAG>(a, e, slot, sc, pw, w, rx, ry, rz);
-            }
-          }
-          // the slot of plane iz is free: refill it with plane iz+NSLOT
-          __syncthreads();
-          if (abort_flag) {
-            stop = true;
-          } else if (tid == 0 && iz + NSLOT <= pmax) {
-            issue(iz + NSLOT);
-          }
-        }
+    size_t cidx = gidx(g, e.ix, e.iy, z0);
+    int slot_c = 0, slot_n = LEAD % NSLOT;  // slots of plane iz and of plane iz+LEAD
+    for (int iz = z0; iz < z1; ++iz) {
+      const bool got = wait(iz + LEAD);
+      if (got) push(ring + (size_t)slot_n * S::FLOATS, PLANE, sc);
+      else abort_flag = 1;
+      if (active && got) {
+        const float *slot = ring + (size_t)slot_c * S::FLOATS;
+        Pw pw{slot + S::U0 + tc, slot + S::U1 + tc, slot + S::COEF + tc, slot + S::MET + tc};
+        e.iz = iz;
+        e.k = iz - LFD;
+        e.c = cidx;
+        e.top = (iz == g.top);
+        e.near_top = iz >= g.top - 2;
+        e.zpml = (iz < zlo) || (iz >= zhi);
+        e.interior = tile_xy_interior && !e.zpml && !e.near_top;
+        if constexpr (PART == PART_VEL)
+          vel_cell<X, Y, Z, KIND, LAG>(a, e, slot, sc, pw, w, rx, ry, rz);
+        else
+          str_cell<X, Y, Z, KIND, LAG>(a, e, slot, sc, pw, w, rx, ry, rz);
       }
+      // the slot of plane iz is free: refill it with plane iz+NSLOT
+      __syncthreads();
+      if (abort_flag) break;
+      if (tid == 0 && iz + NSLOT <= pmax) issue(iz + NSLOT);
+      cidx += g.plane;
+      slot_c = (slot_c + 1 == NSLOT) ? 0 : slot_c + 1;
+      slot_n = (slot_n + 1 == NSLOT) ? 0 : slot_n + 1;
     }
     __syncthreads();  // all reads of the ring done before the next item reuses it
   }

@@ -1,0 +1,129 @@
+// timg.cu -- traction-image velocity update of the top 3 layers, for the
+// fused stage kernels (which skip those cells).
+//
+// Same arithmetic as the reference's CalTIMGmix (src/calculate.cu:5668-5897):
+// on the 3 layers below and at the free surface, dV/dt comes from the
+// conservative momentum equation
+//     dV/dt = (1 / (rho J)) [ d_xi(J sigma.grad xi) + d_eta(J sigma.grad eta)
+//                             + d_zeta(J sigma.grad zeta) ],
+// with J sigma.grad zeta (the traction on zeta planes) set to zero on the
+// surface layer and mirrored oddly above it.  Under SimpleCar grad xi and
+// grad eta are the unit x and y vectors.  The x/y CFS-PML auxiliaries of V
+// take their traction-image form; the RK update (Iteration*) is applied here
+// for those cells.  A plain per-cell kernel: it touches 3 planes only.
+#include "cgfd_internal.cuh"
+
+#include <cuda_runtime.h>
+
+namespace cgfd {
+namespace {
+
+__device__ __forceinline__ float drp5(float m1, float c0, float p1, float p2, float p3, float r) {
+  return (CGFD_DA_1 * m1 + CGFD_DA0 * c0 + CGFD_DA1 * p1 + CGFD_DA2 * p2 + CGFD_DA3 * p3) * r;
+}
+
+__global__ void __launch_bounds__(128) timg_kernel(StageArgs a) {
+  const Geom &g = a.g;
+  const int i = blockIdx.x * 32 + threadIdx.x;
+  const int j = blockIdx.y * 4 + threadIdx.y;
+  const int iz = g.top - 2 + blockIdx.z;
+  if (i >= g.ni || j >= g.nj) return;
+  const int ix = i + XO, iy = j + LFD;
+  const long c = (long)gidx(g, ix, iy, iz);
+  const size_t fs = g.fstride;
+  const long sy = g.px, sz = (long)g.plane;
+  const int s = g.top - iz;  // the surface lies s layers above
+  const float rx = a.X / a.h, ry = a.Y / a.h, rz = a.Z / a.h;
+  const float irho = a.irho[c];
+  const float rhojac = a.flat ? irho : irho / a.jac[c];
+  const float iBx = 1.f / a.b[0][ix], iBy = 1.f / a.b[1][iy];
+  const bool xpml = i < g.nabs[0] || i >= g.ni - g.nabs[1];
+  const bool ypml = j < g.nabs[2] || j >= g.nj - g.nabs[3];
+  const int xa = (i < g.nabs[0]) ? i : i - (g.ni - g.nabs[1]) + g.nabs[0];
+  const int ya = (j < g.nabs[2]) ? j : j - (g.nj - g.nabs[3]) + g.nabs[2];
+  const size_t px = ((size_t)iz * g.nyi + iy) * g.nxa + xa;
+  const size_t py = ((size_t)iz * g.nya + ya) * g.px + ix;
+  const int kind = a.rk == 0 ? 0 : (a.rk < 3 ? 1 : 2);
+  constexpr int TC[3][3] = {{TXX, TXY, TXZ}, {TXY, TYY, TYZ}, {TXZ, TYZ, TZZ}};
+  const float *in = a.in;
+
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const float *T1 = in + TC[q][0] * fs, *T2 = in + TC[q][1] * fs, *T3 = in + TC[q][2] * fs;
+    float vx[5], vy[5], vz[7];
+#pragma unroll
+    for (int d = -1; d <= 3; ++d) {
+      const long gx = c + a.X * d, gy = c + a.Y * d * sy;
+      vx[d + 1] = (a.flat ? 1.f : a.jac[gx]) * T1[gx];
+      vy[d + 1] = (a.flat ? 1.f : a.jac[gy]) * T2[gy];
+    }
+#pragma unroll
+    for (int n = 0; n < 7; ++n) {
+      const long gz = c + (n - 3) * sz;
+      vz[n] = a.flat ? T3[gz]
+                     : a.jac[gz] * (a.zx[gz] * T1[gz] + a.zy[gz] * T2[gz] + a.zz[gz] * T3[gz]);
+    }
+    if (s == 0) {
+      vz[3] = 0.f; vz[4] = -vz[2]; vz[5] = -vz[1]; vz[6] = -vz[0];
+    } else if (s == 1) {
+      vz[4] = 0.f; vz[5] = -vz[3]; vz[6] = -vz[2];
+    } else {
+      vz[5] = 0.f; vz[6] = -vz[4];
+    }
+    const float DxT = rhojac * drp5(vx[0], vx[1], vx[2], vx[3], vx[4], rx);
+    const float DyT = rhojac * drp5(vy[0], vy[1], vy[2], vy[3], vy[4], ry);
+    const float DzT = a.Z > 0 ? rhojac * drp5(vz[2], vz[3], vz[4], vz[5], vz[6], rz)
+                              : rhojac * drp5(vz[4], vz[3], vz[2], vz[1], vz[0], rz);
+    float hv = DxT * iBx + DyT * iBy + DzT;
+    // auxiliaries: X then Y, each read before it is written (own cell only)
+    auto aux = [&](int d, size_t p, float h) {
+      const size_t o = q * g.astride[d] + p;
+      const float ai = a.ain[d][o];
+      if (kind == 0) {
+        a.aout[d][o] = ai + a.adt * h;
+        a.ta[d][o] = ai + a.bdt * h;
+      } else if (kind == 1) {
+        const float f = a.afw[d][o], t = a.ta[d][o];
+        a.aout[d][o] = f + a.adt * h;
+        a.ta[d][o] = t + a.bdt * h;
+      } else {
+        a.aout[d][o] = a.ta[d][o] + a.bdt * h;
+      }
+    };
+    float hax = 0.f, hay = 0.f;
+    if (xpml) {
+      const float ai = a.ain[0][q * g.astride[0] + px];
+      hv -= ai * iBx;
+      hax = a.db[0][ix] * DxT - a.apd[0][ix] * ai;
+    }
+    if (ypml) {
+      const float ai = a.ain[1][q * g.astride[1] + py];
+      hv -= ai * iBy;
+      hay = a.db[1][iy] * DyT - a.apd[1][iy] * ai;
+    }
+    if (xpml) aux(0, px, hax);
+    if (ypml) aux(1, py, hay);
+    const size_t o = (size_t)(VX + q) * fs + c;
+    if (kind == 0) {
+      const float u0 = in[o];
+      a.out[o] = u0 + a.adt * hv;
+      a.tw[o] = u0 + a.bdt * hv;
+    } else if (kind == 1) {
+      const float u0 = a.fw[o], u1 = a.tw[o];
+      a.out[o] = u0 + a.adt * hv;
+      a.tw[o] = u1 + a.bdt * hv;
+    } else {
+      a.out[o] = a.tw[o] + a.bdt * hv;
+    }
+  }
+}
+
+}  // namespace
+
+void launch_timg(const StageArgs &a, void *stream) {
+  dim3 block(32, 4, 1);
+  dim3 grid((a.g.ni + 31) / 32, (a.g.nj + 3) / 4, 3);
+  timg_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(a);
+}
+
+}  // namespace cgfd
