@@ -111,6 +111,8 @@ struct SourceArgs {
 };
 
 void launch_stage_simple(const StageArgs &a, void *stream);
+// text returned by cgfd_last_error(NULL, ...)
+void set_global_error(const char *msg);
 // traction-image velocity update of the top 3 layers (after the fused kernels)
 void launch_timg(const StageArgs &a, void *stream);
 bool fused_supported(const Geom &g);

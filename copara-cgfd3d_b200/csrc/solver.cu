@@ -8,6 +8,7 @@
 // 2678-2830), driven by the step loop of src/simulation.cc:252-711.
 #include "../../include/cgfd.h"
 #include "cgfd_internal.cuh"
+#include "nonfinite.cuh"
 
 #include <cuda_runtime.h>
 
@@ -20,6 +21,7 @@
 #include <vector>
 
 using namespace cgfd;
+using namespace cgfd::nf;
 
 namespace {
 
@@ -116,16 +118,6 @@ __global__ void record_kernel(const float *__restrict__ fw, size_t fstride,
   if (threadIdx.x == 0) *step = t + 1;
 }
 
-__global__ void count_nonfinite_kernel(const float *__restrict__ v, size_t n,
-                                       unsigned long long *count) {
-  unsigned long long local = 0;
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
-       q += (size_t)gridDim.x * blockDim.x)
-    if (!isfinite(v[q])) ++local;
-  for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
-  if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
-}
-
 }  // namespace
 
 struct cgfd_solver {
@@ -160,7 +152,8 @@ struct cgfd_solver {
   float *d_seis = nullptr;
   int *d_step = nullptr;
   int steps = 0;
-  unsigned long long *d_count = nullptr;
+  unsigned long long *d_partials = nullptr;  // non-finite count scratch
+  int nf_blocks = 0;
   // graphs (one per step%4 pattern)
   cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
   bool graphs_ok = false;
@@ -170,6 +163,12 @@ struct cgfd_solver {
   int *d_err = nullptr;
   bool plain_interior = true;
 };
+
+namespace {
+
+}  // namespace
+
+void cgfd::set_global_error(const char *msg) { g_last_create_error = msg; }
 
 namespace {
 
@@ -207,7 +206,7 @@ void free_all(cgfd_solver *h) {
     if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; }
   void *ptrs[] = {h->state, h->media, h->metric, h->pml, h->aux[0], h->aux[1], h->aux[2],
                   h->matv, h->d_mcell, h->d_fcell, h->d_mcoef, h->d_fcoef, h->d_mstf,
-                  h->d_fstf, h->d_rcell, h->d_seis, h->d_step, h->d_count, h->d_err};
+                  h->d_fstf, h->d_rcell, h->d_seis, h->d_step, h->d_partials, h->d_err};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->st) cudaStreamDestroy(h->st);
@@ -486,7 +485,9 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
   if (!st) {
     e = cudaMalloc(&h->d_step, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->d_step, 0, sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&h->d_count, sizeof(unsigned long long));
+    h->nf_blocks = (int)nonfinite_blocks(9 * g.fstride);
+    if (e == cudaSuccess)
+      e = cudaMalloc(&h->d_partials, (h->nf_blocks + 1) * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&h->d_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->d_err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
@@ -961,11 +962,14 @@ int cgfd_set_field(cgfd_solver *h, int set, int comp, const float *in) {
 int cgfd_check_finite(cgfd_solver *h, long long *n_bad) {
   if (!h) return arg_fail(h, "null handle");
   DevGuard guard(h->d.device);
-  CK(h, cudaMemsetAsync(h->d_count, 0, sizeof(unsigned long long), h->st));
-  count_nonfinite_kernel<<<592, 256, 0, h->st>>>(h->set[0], 9 * h->g.fstride, h->d_count);
+  nonfinite_partial_kernel<<<h->nf_blocks, NF_THREADS, 0, h->st>>>(h->set[0], 9 * h->g.fstride,
+                                                                   h->d_partials);
+  CK(h, cudaGetLastError());
+  nonfinite_sum_kernel<<<1, NF_THREADS, 0, h->st>>>(h->d_partials, h->nf_blocks);
   CK(h, cudaGetLastError());
   unsigned long long c = 0;
-  CK(h, cudaMemcpyAsync(&c, h->d_count, sizeof(c), cudaMemcpyDeviceToHost, h->st));
+  CK(h, cudaMemcpyAsync(&c, h->d_partials + h->nf_blocks, sizeof(c), cudaMemcpyDeviceToHost,
+                        h->st));
   CK(h, cudaStreamSynchronize(h->st));
   if (n_bad) *n_bad = (long long)c;
   if (c) {
