@@ -66,6 +66,8 @@ _SIGS = {
     "cgfd_get_field": (C.c_int, [_P, C.c_int, C.c_int, _fp]),
     "cgfd_set_field": (C.c_int, [_P, C.c_int, C.c_int, _fp]),
     "cgfd_check_finite": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
+    "cgfd_count_nonfinite_noalloc": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_longlong),
+                                               C.c_void_p]),
     "cgfd_metric_from_coords": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double,
                                           _dp, _dp, _dp, C.POINTER(_dp)]),
     "cgfd_cfs_factors": (C.c_int, [C.c_int, C.c_int, C.c_int, _ip, _dp, _dp, _dp,
@@ -232,6 +234,21 @@ class Solver:
         if st not in (OK, ERR_NONFINITE):
             self._chk(st)
         return n.value
+
+
+NOALLOC_MAX_VALUES = 16384 * 8192
+
+
+def count_nonfinite_noalloc(device_ptr: int, n: int, stream: int = 0) -> int:
+    """NaN/Inf count of n floats at a device address, without any device
+    allocation (cgfd_count_nonfinite_noalloc).  Raises CgfdError on argument
+    or CUDA errors; returns the count otherwise."""
+    out = C.c_longlong()
+    st = _lib.cgfd_count_nonfinite_noalloc(C.c_void_p(device_ptr), n, C.byref(out),
+                                           C.c_void_p(stream) if stream else None)
+    if st not in (OK, ERR_NONFINITE):
+        raise CgfdError(st, last_error(None))
+    return out.value
 
 
 # ------------------------- host pre-processing ------------------------------

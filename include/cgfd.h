@@ -172,6 +172,22 @@ int cgfd_set_field(cgfd_solver *h, int set, int comp, const float *in);
  * Returns CGFD_ERR_NONFINITE when the count is not zero. */
 int cgfd_check_finite(cgfd_solver *h, long long *n_bad);
 
+/* NaN/Inf count of any float array on the device (d_values, n values), the
+ * same count cgfd_check_finite makes for a solver's wavefield, for callers
+ * that cannot call cudaMalloc when they run the check: a host application
+ * whose pool owns all device memory, a real-time loop that must not take the
+ * allocator's synchronisation, code borrowing another framework's buffers.
+ * No reference counterpart (the reference has no NaN/Inf check).
+ * It allocates nothing: its scratch is a fixed array in the library's device
+ * image, so n is limited to 134,217,728 values per call (larger n returns
+ * CGFD_ERR_ARG).  The first call on a device looks that array up (set-up)
+ * and should come before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller.
+ * Runs on `stream` (a cudaStream_t, NULL = default stream) and waits for it;
+ * returns CGFD_ERR_NONFINITE when *n_bad is not zero. */
+int cgfd_count_nonfinite_noalloc(const float *d_values, size_t n, long long *n_bad,
+                                 void *stream);
+
 /* ---------------- host pre-processing helpers (FP64) ---------------------- */
 
 /* Grid metric from node coordinates (full arrays, reference layout), by
