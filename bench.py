@@ -40,7 +40,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--kernel", choices=("fused", "simple"), default="fused")
-    p.add_argument("--config", choices=("hill400", "flat160"), default="hill400")
+    p.add_argument("--config", choices=("hill400", "flat160", "hill256"), default="hill400")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -51,12 +51,15 @@ def build_model(cfg, nt):
     import models
     if cfg == "hill400":
         return models.config_c2(nt=nt)
+    if cfg == "hill256":
+        return models.hill_256(nt=nt)
     return models.config_c1(nt=nt)
 
 
 def workload_name(cfg):
     return {"hill400": "gaussian_hill_400x400x200_pml20",
-            "flat160": "flat_halfspace_160x160x80_pml12"}[cfg]
+            "flat160": "flat_halfspace_160x160x80_pml12",
+            "hill256": "gaussian_hill_256x256x128_pml20"}[cfg]
 
 
 def algorithmic_bytes_per_step(m, elem=4):

@@ -277,6 +277,13 @@ def config_c2(nt=2000) -> Model:
     return gaussian_hill(nt=nt, name="gaussian_hill_400x400x200")
 
 
+def hill_256(nt=40, nabs=(20, 20, 20, 20, 20, 0)) -> Model:
+    """The 400x400x200 hill model's generator at 256x256x128 (8.4 M cells,
+    about 2 GB on the device): the profiling case for the stage kernels."""
+    return gaussian_hill(ni=256, nj=256, nk=128, nt=nt, n_side=5, rcv_spacing=1000.0,
+                         nabs=nabs, name="gaussian_hill_256x256x128")
+
+
 def small_flat(nt=40, ni=28, nj=24, nk=20, **kw) -> Model:
     kw.setdefault("nabs", (5, 5, 5, 5, 5, 0))
     return flat_halfspace(ni=ni, nj=nj, nk=nk, h=100.0, dt=0.008, nt=nt,
