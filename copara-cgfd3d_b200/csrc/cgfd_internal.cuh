@@ -4,8 +4,10 @@
 // HBM layout (all arrays 256-byte aligned, zero-initialised):
 //   * Every wavefield component is a 3-D array with x fastest:
 //         idx(ix, iy, iz) = (iz * nyi + iy) * px + ix
-//     ix = i_ref + 1 (valid x starts at XO = 4 so that a tile that starts at a
-//     valid cell starts on a 16-byte boundary), iy = j_ref, iz = k_ref.
+//     ix = i_ref + XSH with XSH = XO - 3: the first valid cell sits at
+//     XO = 32, so a tile of cells that starts at a valid cell starts on a
+//     128-byte line and every warp's 128-byte row of stores covers whole
+//     32-byte sectors (no partial-sector writes); iy = j_ref, iz = k_ref.
 //     px (x pitch) is a multiple of 32 floats (128 B) and leaves >= 4 zero
 //     ghost columns on the right; nyi = nj+6, nzi = nk+6.  Ghost cells are
 //     never written, so the one-sided stencils read zeros there exactly like
@@ -32,7 +34,11 @@
 namespace cgfd {
 
 constexpr int LFD = 3;   // ghost width of the reference (LenFD)
-constexpr int XO = 4;    // internal x index of the first valid cell
+#ifndef CGFD_XO
+#define CGFD_XO 32
+#endif
+constexpr int XO = CGFD_XO;  // internal x index of the first valid cell
+constexpr int XSH = XO - LFD;  // internal x index = reference x index + XSH
 constexpr int NCOMP = 9;
 
 enum { VX = 0, VY, VZ, TXX, TYY, TZZ, TXY, TXZ, TYZ };

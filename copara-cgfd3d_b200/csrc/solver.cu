@@ -51,7 +51,7 @@ __global__ void to_internal_kernel(const float *__restrict__ src, float *__restr
     const long r = q / nz;
     const int j = (int)(r % ny);
     const int i = (int)(r / ny);
-    dst[gidx(g, i + 1, j, k)] = src[q];
+    dst[gidx(g, i + XSH, j, k)] = src[q];
   }
 }
 __global__ void to_reference_kernel(const float *__restrict__ src, float *__restrict__ dst,
@@ -63,7 +63,7 @@ __global__ void to_reference_kernel(const float *__restrict__ src, float *__rest
     const long r = q / nz;
     const int j = (int)(r % ny);
     const int i = (int)(r / ny);
-    dst[q] = src[gidx(g, i + 1, j, k)];
+    dst[q] = src[gidx(g, i + XSH, j, k)];
   }
 }
 
@@ -253,7 +253,7 @@ bool valid_loc(const cgfd_solver *h, const int *l) {
          l[2] >= LFD && l[2] < h->d.nk + LFD;
 }
 int cell_of(const cgfd_solver *h, const int *l) {
-  return (int)gidx(h->g, l[0] + 1, l[1], l[2]);
+  return (int)gidx(h->g, l[0] + XSH, l[1], l[2]);
 }
 
 void invalidate(cgfd_solver *h) {
@@ -309,7 +309,7 @@ void surface_matrices(const cgfd_solver *h, std::vector<float> &out) {
           }
       }
       const double bzx = h->hb[2][top] / h->hb[0][i], bzy = h->hb[2][top] / h->hb[1][j];
-      const size_t m2 = (size_t)j * h->g.px + (i + 1);
+      const size_t m2 = (size_t)j * h->g.px + (i + XSH);
       for (int r = 0; r < 3; ++r)
         for (int s = 0; s < 3; ++s) {
           double ab = 0, ac = 0;
@@ -621,7 +621,7 @@ int cgfd_upload_pml(cgfd_solver *h, const double *apdx, const double *apdy, cons
   DevGuard guard(h->d.device);
   const int n3[3] = {h->d.ni + 6, h->d.nj + 6, h->d.nk + 6};
   const int len[3] = {h->g.px, h->g.nyi, h->g.nzi};
-  const int off[3] = {1, 0, 0};  // internal index = reference index + off
+  const int off[3] = {XSH, 0, 0};  // internal index = reference index + off
   const double *src[9] = {apdx, apdy, apdz, bx, by, bz, dbx, dby, dbz};
   for (int q = 0; q < 9; ++q) {
     const int ax = q % 3;

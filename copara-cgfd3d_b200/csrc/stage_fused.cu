@@ -10,6 +10,10 @@ namespace cgfd {
 namespace fused {
 namespace {
 
+#ifndef CGFD_L2_PROMO
+#define CGFD_L2_PROMO CU_TENSOR_MAP_L2_PROMOTION_L2_128B
+#endif
+constexpr CUtensorMapL2promotion L2_PROMO = CGFD_L2_PROMO;
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -38,7 +42,7 @@ bool make_map(CUtensorMap *m, const Geom &g, const float *base, int ncomp, int b
   cuuint32_t es[4] = {1, 1, 1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)base, dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                  L2_PROMO, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
 

@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(TT, 3)
       const bool compute = p < z1;
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_expect_tx(&bars[s], S::HALO_B + (compute ? pw_bytes : 0u));
-      tma_load(slot, &maps.halo, bx0, by0, p, C0, &bars[s]);
+      tma_load(slot, &maps.halo, bx0 + XO - 4, by0, p, C0, &bars[s]);
       if (compute) {
         const int cx = XO + bx0, cy = LFD + by0;
         tma_load(slot + S::U0, &maps.u0, cx, cy, p, S0, &bars[s]);
