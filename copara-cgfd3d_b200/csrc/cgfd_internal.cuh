@@ -17,7 +17,10 @@
 //     start), Wa and Wb (stage outputs, ping-pong because the stencil cannot
 //     run in place) and tW (RK accumulator).
 //   * ADE CFS-PML auxiliaries are compact per direction:
-//         X: (iz * nyi + iy) * nxa + xa      xa in [0, nabs0+nabs1)
+//         X: (iz * nyi + iy) * nxa + xa      xa = i (left layer) or
+//            i - (ni - nabs1) + xaoff (right layer); xaoff >= nabs0 is chosen
+//            congruent to ni - nabs1 modulo 4 so that xa and i agree modulo
+//            4 (aligned pair and tile accesses) and nxa is a multiple of 4
 //         Y: (iz * nya + ya) * px  + ix      ya in [0, nabs2+nabs3)
 //         Z: (za * nyi + iy) * px  + ix      za in [0, nabs4+nabs5)
 //     each with 3 sets (FA step start, A stage value updated in place since
@@ -60,7 +63,8 @@ struct Geom {
   int top;             // iz of the free surface (nk + 2)
   int con;             // ConIndex (iz)
   int nabs[6];
-  int nxa, nya, nza;   // auxiliary widths per direction
+  int nxa, nya, nza;   // auxiliary widths per direction (nxa: row pitch)
+  int xaoff;           // X auxiliaries: xa of the first right-hand PML column
   size_t plane;        // px * nyi
   size_t fstride;      // elements between components of a set
   size_t astride[3];   // elements between components of an aux set
@@ -131,5 +135,14 @@ void fused_destroy_plan(void *plan);
 void launch_stage_fused(const void *plan, const StageArgs &a, int in_set, int *err,
                         void *stream);
 int fused_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str);
+// The paired kernels (two x-adjacent cells per thread, stage_pair.cu); aux
+// holds the three directions' auxiliary arrays (null: no PML there).
+bool pair_supported(const Geom &g);
+void *pair_create_plan(const Geom &g, float *const sets[4], const float *media,
+                       const float *metric, float *const aux[3]);
+void pair_destroy_plan(void *plan);
+void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *err,
+                       void *stream);
+int pair_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str);
 
 }  // namespace cgfd

@@ -201,7 +201,11 @@ int arg_fail(cgfd_solver *h, const char *what) {
   } while (0)
 
 void free_all(cgfd_solver *h) {
-  if (h->plan) { fused_destroy_plan(h->plan); h->plan = nullptr; }
+  if (h->plan) {
+    if (h->d.kernel == CGFD_KERNEL_PAIR) pair_destroy_plan(h->plan);
+    else fused_destroy_plan(h->plan);
+    h->plan = nullptr;
+  }
   for (auto &gr : h->graph)
     if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; }
   void *ptrs[] = {h->state, h->media, h->metric, h->pml, h->aux[0], h->aux[1], h->aux[2],
@@ -355,13 +359,20 @@ StageArgs stage_args(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, in
   return a;
 }
 
+// the stage kernels of the solver's kernel family
+void dispatch_stage(cgfd_solver *h, const StageArgs &a, int in_set) {
+  if (h->d.kernel == CGFD_KERNEL_SIMPLE)
+    launch_stage_simple(a, h->st);
+  else if (h->d.kernel == CGFD_KERNEL_PAIR)
+    launch_stage_pair(h->plan, a, in_set, h->d_err, h->st);
+  else
+    launch_stage_fused(h->plan, a, in_set, h->d_err, h->st);
+}
+
 int launch_stage(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, int out_set,
                  int tindex) {
   StageArgs a = stage_args(h, rk, X, Y, Z, in_set, out_set);
-  if (h->d.kernel == CGFD_KERNEL_SIMPLE)
-    launch_stage_simple(a, h->st);
-  else
-    launch_stage_fused(h->plan, a, in_set, h->d_err, h->st);
+  dispatch_stage(h, a, in_set);
   CK(h, cudaGetLastError());
   if (h->nmnt + h->nfrc > 0) {
     SourceArgs s{};
@@ -432,7 +443,8 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
   if (d->con_index < LFD || d->con_index > d->nk + LFD - 1)
     return arg_fail(nullptr, "con_index must lie in [3, nk+2]");
   if (d->storage != CGFD_STORE_F32) return arg_fail(nullptr, "storage type not supported");
-  if (d->kernel != CGFD_KERNEL_FUSED && d->kernel != CGFD_KERNEL_SIMPLE)
+  if (d->kernel != CGFD_KERNEL_FUSED && d->kernel != CGFD_KERNEL_SIMPLE &&
+      d->kernel != CGFD_KERNEL_PAIR)
     return arg_fail(nullptr, "unknown kernel family");
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -451,7 +463,13 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
   g.top = d->nk + LFD - 1;
   g.con = d->con_index;
   for (int q = 0; q < 6; ++q) g.nabs[q] = d->nabs[q];
-  g.nxa = d->nabs[0] + d->nabs[1];
+  if (d->nabs[0] + d->nabs[1] > 0) {
+    g.xaoff = d->nabs[0] + ((d->ni - d->nabs[1] - d->nabs[0]) % 4 + 4) % 4;
+    g.nxa = (int)align_up((size_t)(g.xaoff + d->nabs[1]), 4);
+  } else {
+    g.xaoff = 0;
+    g.nxa = 0;
+  }
   g.nya = d->nabs[2] + d->nabs[3];
   g.nza = d->nabs[4] + d->nabs[5];
   g.plane = (size_t)g.px * g.nyi;
@@ -459,9 +477,10 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
   g.astride[0] = align_up((size_t)g.nzi * g.nyi * g.nxa, 64);
   g.astride[1] = align_up((size_t)g.nzi * g.nya * g.px, 64);
   g.astride[2] = align_up((size_t)g.nza * g.nyi * g.px, 64);
-  if (d->kernel == CGFD_KERNEL_FUSED && !fused_supported(g)) {
+  if ((d->kernel == CGFD_KERNEL_FUSED && !fused_supported(g)) ||
+      (d->kernel == CGFD_KERNEL_PAIR && !pair_supported(g))) {
     delete h;
-    return arg_fail(nullptr, "fused kernel does not support this grid");
+    return arg_fail(nullptr, "tiled kernel does not support this grid");
   }
 
   DevGuard guard(d->device);
@@ -499,8 +518,10 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
     return st;
   }
   for (int q = 0; q < 4; ++q) h->set[q] = h->state + (size_t)q * 9 * fs;
-  if (d->kernel == CGFD_KERNEL_FUSED) {
-    h->plan = fused_create_plan(g, h->set, h->media, h->metric);
+  if (d->kernel == CGFD_KERNEL_FUSED || d->kernel == CGFD_KERNEL_PAIR) {
+    h->plan = (d->kernel == CGFD_KERNEL_PAIR)
+                  ? pair_create_plan(g, h->set, h->media, h->metric, h->aux)
+                  : fused_create_plan(g, h->set, h->media, h->metric);
     if (!h->plan) {
       free_all(h);
       delete h;
@@ -809,8 +830,7 @@ int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms) {
         const int *dd = DIRS[p][rk];
         StageArgs a = stage_args(h, rk, dd[0], dd[1], dd[2], ins[rk], outs[rk]);
         CK(h, cudaEventRecord(ev[8 * (size_t)s + 2 * rk], h->st));
-        if (h->d.kernel == CGFD_KERNEL_SIMPLE) launch_stage_simple(a, h->st);
-        else launch_stage_fused(h->plan, a, ins[rk], h->d_err, h->st);
+        dispatch_stage(h, a, ins[rk]);
         CK(h, cudaGetLastError());
         CK(h, cudaEventRecord(ev[8 * (size_t)s + 2 * rk + 1], h->st));
         // sources exactly as in the graph

@@ -36,6 +36,7 @@
 #pragma once
 
 #include "cgfd_internal.cuh"
+#include "ptx_util.cuh"
 
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -46,12 +47,12 @@
 
 namespace cgfd {
 namespace fused {
+using namespace ptx;
 
 constexpr int TX = 32, TY = 4, TT = TX * TY;   // threads per CTA tile
 constexpr int BOXX = TX + 8, BOXY = TY + 6;    // halo box (x starts 4 left, y 3 below)
 constexpr int NSLOT = 5;
 constexpr int PLANE = BOXX * BOXY;             // floats per component per halo plane
-constexpr unsigned long long WAIT_NS = 2000000000ull;
 enum { PART_VEL = 0, PART_STR = 1 };
 
 // NC: staged (differentiated) components, C0: first of them in a set;
@@ -91,49 +92,6 @@ struct StageMaps {
   CUtensorMap coef;  // media, box {32, 4, 1, NCOEF}
   CUtensorMap met;   // metric, box {32, 4, 1, 3}
 };
-
-__device__ __forceinline__ uint32_t su32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t n) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(n) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(su32(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ unsigned long long gtime() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-  return t;
-}
-// bounded wait; false on expiry
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
-  if (mbar_try_wait(b, parity)) return true;
-  const unsigned long long t0 = gtime();
-  while (!mbar_try_wait(b, parity))
-    if (gtime() - t0 > WAIT_NS) return false;
-  return true;
-}
-__device__ __forceinline__ void tma_load(float *dst, const CUtensorMap *map, int x, int y, int z,
-                                         int c, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(su32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(z), "r"(c), "r"(su32(bar))
-      : "memory");
-}
 
 __device__ __forceinline__ float drp5(float m1, float c0, float p1, float p2, float p3, float r) {
   return (CGFD_DA_1 * m1 + CGFD_DA0 * c0 + CGFD_DA1 * p1 + CGFD_DA2 * p2 + CGFD_DA3 * p3) * r;
@@ -502,7 +460,7 @@ __global__ void __launch_bounds__(TT, 3)
       if (err) atomicExch(err, 2);
     } else {
       for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      fence_mbar_init();
     }
   }
   __syncthreads();
@@ -523,7 +481,7 @@ __global__ void __launch_bounds__(TT, 3)
       const int s = (p - z0) % NSLOT;
       float *slot = ring + (size_t)s * S::FLOATS;
       const bool compute = p < z1;
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      fence_proxy_async();
       mbar_expect_tx(&bars[s], S::HALO_B + (compute ? pw_bytes : 0u));
       tma_load(slot, &maps.halo, bx0 + XO - 4, by0, p, C0, &bars[s]);
       if (compute) {
@@ -555,7 +513,7 @@ __global__ void __launch_bounds__(TT, 3)
     e.iy = e.j + LFD;
     e.xpml = active && (e.i < g.nabs[0] || e.i >= g.ni - g.nabs[1]);
     e.ypml = active && (e.j < g.nabs[2] || e.j >= g.nj - g.nabs[3]);
-    e.xa = (e.i < g.nabs[0]) ? e.i : e.i - (g.ni - g.nabs[1]) + g.nabs[0];
+    e.xa = (e.i < g.nabs[0]) ? e.i : e.i - (g.ni - g.nabs[1]) + g.xaoff;
     e.ya = (e.j < g.nabs[2]) ? e.j : e.j - (g.nj - g.nabs[3]) + g.nabs[2];
     e.iBx = 1.f / a.b[0][e.ix];
     e.iBy = 1.f / a.b[1][e.iy];

@@ -1,0 +1,856 @@
+// stage_pair_impl.cuh -- z-marching RK stage kernels for sm_100a with two
+// x-adjacent cells per thread (templates; instantiated by pair_*.cu).
+//
+// One RK stage is two kernels, split along the velocity-stress structure of
+// the equations: the velocity part differentiates only the six stresses and
+// the stress part only the three velocities.  A CTA of 32 x 4 threads owns a
+// tile of 64 x 4 (x, y) columns, each thread the cell pair (2t, 2t+1) of its
+// row, and marches through a chunk of z-planes; a persistent grid of CTAs
+// (two per SM) walks the (tile, z-chunk) items.
+//
+// Pairs make every per-cell quantity a float2: the stencil and RHS
+// arithmetic runs as packed FFMA2 / FMUL2 / FADD2 (one instruction for both
+// cells), and the shared-memory reads, the pointwise operands and the
+// global stores are 64-bit accesses.  Only the x-derivative assembles some of
+// its operand pairs from neighbouring pairs.
+//
+// The march runs against the long reach of the z-stencil: a forward stencil
+// (reach -1..+3) marches downwards, a backward one (reach -3..+1) upwards, so
+// the stencil always needs one plane ahead and three behind.  Each plane
+// arrives by TMA (cp.async.bulk.tensor, no multicast) into one slot of a
+// 4-slot shared-memory ring, on one mbarrier per slot:
+//   * the differentiated components with an x/y halo, one 4-D box
+//     {72 x, 10 y, 1 z, NC components} (x from -4, y from -3);
+//   * the pointwise operands of the plane, boxes {64, 4, 1, n}: the RK
+//     registers (FW and/or tW), the media coefficients and the metric.
+// A plane is needed one iteration after it lands (its centre enters the
+// per-thread register window of five planes) and in the next one (x/y
+// stencils, pointwise operands); two further planes are in flight.
+//
+// The per-cell arithmetic is that of the reference's CalDiffmix + CalWavemix
+// + Iteration* (src/calculate.cu:4121-4621, 6330-6734); the top three layers'
+// velocities come from the traction-image kernel (timg.cu) and point sources
+// from a separate tiny kernel (solver.cu).  CFS-PML auxiliaries are read and
+// written with 64-bit global accesses (prefetched into L2 by tensor prefetch
+// when the plane's slot is issued).
+//
+// Every mbarrier wait is bounded (about 2 s of %globaltimer).  On expiry the
+// CTA leaves the march together (the flag is read after a barrier), records
+// an error code in *err, waits (bounded) for its own copies still in flight
+// and returns; the host then reports CGFD_ERR_TIMEOUT.  Before issuing any
+// copy the CTA checks the alignment of its slots and barriers (error code 2).
+#pragma once
+
+#include "cgfd_internal.cuh"
+#include "ptx_util.cuh"
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+
+namespace cgfd {
+namespace pair {
+using namespace ptx;
+
+constexpr int TX = 32, TY = 4, TT = TX * TY;  // threads per CTA
+constexpr int CX = 2 * TX;                    // cells per tile row
+constexpr int HX = CX + 8, HY = TY + 6;       // halo box (x from -4, y from -3)
+constexpr int HPL = HX * HY;                  // floats per component per halo plane
+constexpr int PWT = CX * TY;                  // floats per pointwise tile
+constexpr int NSLOT = 4;
+enum { PART_VEL = 0, PART_STR = 1 };
+
+// NC: staged (differentiated) components, C0: first of them in a set;
+// NS: components the part updates (V: 3, T: 6), S0 their first index;
+// NCOEF: media coefficients it reads, COEF0 the first (lam2mu, mu, irho).
+template <int PART> struct PartInfo;
+template <> struct PartInfo<PART_VEL> {
+  static constexpr int NC = 6, C0 = TXX, NS = 3, S0 = VX, NCOEF = 1, COEF0 = 2;
+};
+template <> struct PartInfo<PART_STR> {
+  static constexpr int NC = 3, C0 = VX, NS = 6, S0 = TXX, NCOEF = 2, COEF0 = 0;
+};
+
+// Slot layout (floats): halo [NC][HY][HX], then pointwise tiles of PWT
+// floats: u0 [NS] (FW, or tW in the final stage), u1 [NS] (tW in the inner
+// stages), coef [NCOEF], met [3] (zeta_x, zeta_y, zeta_z).  Every region
+// starts on 128 B (a tensor copy's shared-memory destination must) and the
+// slot stride is a multiple of 128 B.
+template <int PART> struct Slot {
+  static constexpr int NC = PartInfo<PART>::NC, NS = PartInfo<PART>::NS;
+  static constexpr uint32_t HALO_B = (uint32_t)(HPL * NC * 4);
+  static constexpr uint32_t HALO_F = (HALO_B + 127u) / 128u * 32u;  // floats, padded
+  static constexpr uint32_t U0 = HALO_F, U1 = U0 + NS * PWT, COEF = U1 + NS * PWT;
+  static constexpr uint32_t MET = COEF + PartInfo<PART>::NCOEF * PWT;
+  static constexpr uint32_t FLOATS = MET + 3 * PWT;
+  static constexpr uint32_t BYTES = FLOATS * 4;
+  static constexpr size_t SMEM = (size_t)NSLOT * BYTES + 128 + 128;  // + barriers, align slack
+};
+static_assert(Slot<PART_VEL>::BYTES % 128 == 0 && Slot<PART_STR>::BYTES % 128 == 0, "slots");
+// two CTAs per SM: 228 KB of shared memory per SM, 1 KB of it reserved per CTA
+static_assert(2 * (Slot<PART_VEL>::SMEM + 1024) <= 233472, "two velocity CTAs per SM");
+static_assert(2 * (Slot<PART_STR>::SMEM + 1024) <= 233472, "two stress CTAs per SM");
+
+// Tensor maps of one launch.  halo/u0/u1/coef/met feed the ring; the aux
+// maps (per direction: stage input, FA, tA) only drive L2 prefetches.
+struct Maps {
+  CUtensorMap halo;  // stage input, box {72, 10, 1, NC}
+  CUtensorMap u0;    // FW (or tW), box {64, 4, 1, NS}
+  CUtensorMap u1;    // tW, box {64, 4, 1, NS}
+  CUtensorMap coef;  // media, box {64, 4, 1, NCOEF}
+  CUtensorMap met;   // metric, box {64, 4, 1, 3}
+  CUtensorMap aux[3][3];  // [direction][ain, afw, ta], box {64, 4, 1, NS}
+};
+
+struct Work {
+  int zchunk, ntx, ntiles, nitems;
+  int has_aux[3];     // direction has a PML (aux maps valid)
+};
+
+// ---------------------------- float2 helpers ------------------------------
+typedef float2 f2;
+__device__ __forceinline__ f2 F2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ f2 S2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ f2 add2(f2 a, f2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ f2 neg2(f2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ f2 lds2(const float *p) { return *reinterpret_cast<const f2 *>(p); }
+
+// DRP/opt MacCormack 5-point operator on a pair, in the forward form
+// (m1 = p - s, c0 = p, p1..p3 = p + s..3s for the marching sign s; r = s/h)
+__device__ __forceinline__ f2 drp2(f2 m1, f2 c0, f2 p1, f2 p2, f2 p3, float r) {
+  f2 t = mul2(S2(CGFD_DA_1), m1);
+  t = fma2(S2(CGFD_DA0), c0, t);
+  t = fma2(S2(CGFD_DA1), p1, t);
+  t = fma2(S2(CGFD_DA2), p2, t);
+  t = fma2(S2(CGFD_DA3), p3, t);
+  return mul2(t, S2(r));
+}
+
+// x-derivative of the pair (halo columns cb, cb+1 of row R) with the centre
+// pair C already in registers; r = X/h
+template <int X>
+__device__ __forceinline__ f2 dx_pair(const float *R, int cb, f2 C, float r) {
+  if constexpr (X > 0) {
+    const f2 La = lds2(R + cb - 2), Lb = lds2(R + cb + 2), Lc = lds2(R + cb + 4);
+    return drp2(F2(La.y, C.x), C, F2(C.y, Lb.x), Lb, F2(Lb.y, Lc.x), r);
+  } else {
+    const f2 Lz = lds2(R + cb - 4), La = lds2(R + cb - 2), Lb = lds2(R + cb + 2);
+    return drp2(F2(C.y, Lb.x), C, F2(La.y, C.x), La, F2(Lz.y, La.x), r);
+  }
+}
+// y-derivative of the pair from the component's halo plane P (row ry of
+// this thread, column cb), centre pair C in registers; r = Y/h
+template <int Y>
+__device__ __forceinline__ f2 dy_pair(const float *P, int ry, int cb, f2 C, float r) {
+  const f2 m1 = lds2(P + (ry - Y) * HX + cb), p1 = lds2(P + (ry + Y) * HX + cb);
+  const f2 p2 = lds2(P + (ry + 2 * Y) * HX + cb), p3 = lds2(P + (ry + 3 * Y) * HX + cb);
+  return drp2(m1, C, p1, p2, p3, r);
+}
+
+// masked pair access: bit 0 = first cell, bit 1 = second; p1 is the second
+// cell's address (p0 + 1 wherever both bits can be set)
+__device__ __forceinline__ f2 ld2(const float *p0, const float *p1, int m) {
+  if (m == 3) return *reinterpret_cast<const f2 *>(p0);
+  f2 r = F2(0.f, 0.f);
+  if (m & 1) r.x = *p0;
+  if (m & 2) r.y = *p1;
+  return r;
+}
+__device__ __forceinline__ void st2(float *p0, float *p1, int m, f2 v) {
+  if (m == 3) {
+    *reinterpret_cast<f2 *>(p0) = v;
+  } else {
+    if (m & 1) *p0 = v.x;
+    if (m & 2) *p1 = v.y;
+  }
+}
+
+// RK update of one pair (Iteration*): KIND 0 first stage (u0 = FW),
+// 1 inner (u0 = FW, u1 = tW), 2 final (u0 = tW)
+template <int KIND>
+__device__ __forceinline__ void rk_store2(float *out, float *tw, int m, f2 u0, f2 u1, f2 hh,
+                                          float adt, float bdt) {
+  if (KIND == 0) {
+    st2(out, out + 1, m, fma2(S2(adt), hh, u0));
+    st2(tw, tw + 1, m, fma2(S2(bdt), hh, u0));
+  } else if (KIND == 1) {
+    st2(out, out + 1, m, fma2(S2(adt), hh, u0));
+    st2(tw, tw + 1, m, fma2(S2(bdt), hh, u1));
+  } else {
+    st2(out, out + 1, m, fma2(S2(bdt), hh, u0));
+  }
+}
+
+// ADE auxiliaries of one pair and direction: the stage input ai (FA in the
+// first stage, A after) is loaded early (it enters the RHS); the RK update
+// then reads FA / tA set by set right before writing A (FA in the final
+// stage) and tA, so that only one set's values are live at a time.
+// o0/o1: the cells' indices, m: the cells' mask.
+template <int KIND, int N>
+struct Aux2 {
+  f2 ai[N];
+  __device__ __forceinline__ void load(const StageArgs &a, int d, size_t o0, size_t o1, int m,
+                                       int c0) {
+    const size_t as = a.g.astride[d];
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      const float *b = a.ain[d] + (c0 + q) * as;
+      ai[q] = ld2(b + o0, b + o1, m);
+    }
+  }
+  __device__ __forceinline__ void update(const StageArgs &a, int d, size_t o0, size_t o1, int m,
+                                         int c0, const f2 *hh) const {
+    const size_t as = a.g.astride[d];
+    if (KIND == 0) {
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        float *po = a.aout[d] + (c0 + q) * as, *pt = a.ta[d] + (c0 + q) * as;
+        st2(po + o0, po + o1, m, fma2(S2(a.adt), hh[q], ai[q]));
+        st2(pt + o0, pt + o1, m, fma2(S2(a.bdt), hh[q], ai[q]));
+      }
+    } else if (KIND == 1) {
+      f2 u[N];
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        const float *b = a.afw[d] + (c0 + q) * as;
+        u[q] = ld2(b + o0, b + o1, m);
+      }
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        float *po = a.aout[d] + (c0 + q) * as;
+        st2(po + o0, po + o1, m, fma2(S2(a.adt), hh[q], u[q]));
+      }
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        const float *b = a.ta[d] + (c0 + q) * as;
+        u[q] = ld2(b + o0, b + o1, m);
+      }
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        float *pt = a.ta[d] + (c0 + q) * as;
+        st2(pt + o0, pt + o1, m, fma2(S2(a.bdt), hh[q], u[q]));
+      }
+    } else {
+      f2 u[N];
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        const float *b = a.ta[d] + (c0 + q) * as;
+        u[q] = ld2(b + o0, b + o1, m);
+      }
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        float *po = a.aout[d] + (c0 + q) * as;
+        st2(po + o0, po + o1, m, fma2(S2(a.bdt), hh[q], u[q]));
+      }
+    }
+  }
+};
+
+// Per-pair context of one item (tile column pair), shared by the two parts.
+struct Pair {
+  int i, j, ix, iy;   // first cell (valid and internal indices)
+  int m;              // cells inside the grid (bit mask)
+  int mx;             // cells inside an x layer (bit mask)
+  bool ypml;          // the row is inside a y layer
+  int xa0, xa1, ya;   // auxiliary x indices of the two cells, y index of the row
+  f2 iBx, apdx, dbx, bbx;  // x profiles of the two cells (1/B, APD, DB, B)
+  float iBy, apdy, dby, bby;
+};
+
+// Per-plane quantities of the general (boundary) path.
+struct Plane {
+  int iz, k;
+  size_t c;           // linear index of the first cell
+  bool zpml, top, near_top, curved, lean;
+};
+
+// Pointwise operands of this thread's pair in the current slot.
+struct Pw2 {
+  const float *u0, *u1, *coef, *met;
+  __device__ f2 U0(int q) const { return lds2(u0 + q * PWT); }
+  __device__ f2 U1(int q) const { return lds2(u1 + q * PWT); }
+  __device__ f2 C(int q) const { return lds2(coef + q * PWT); }
+  __device__ f2 M(int q) const { return lds2(met + q * PWT); }
+};
+
+// auxiliary indices of the pair on a plane (X: per cell; Y, Z: the pair is
+// contiguous)
+struct AuxIdx {
+  size_t x0, x1, y, z;
+  float iBz, apdz, dbz;
+  __device__ AuxIdx() : x0(0), x1(0), y(0), z(0), iBz(1.f), apdz(0.f), dbz(0.f) {}
+  __device__ AuxIdx(const StageArgs &a, const Pair &e, const Plane &pl) {
+    const Geom &g = a.g;
+    iBz = 1.f / a.b[2][pl.iz];
+    apdz = a.apd[2][pl.iz];
+    dbz = a.db[2][pl.iz];
+    const size_t rx = ((size_t)pl.iz * g.nyi + e.iy) * g.nxa;
+    x0 = rx + e.xa0;
+    x1 = rx + e.xa1;
+    y = ((size_t)pl.iz * g.nya + e.ya) * g.px + e.ix;
+    const int za = (pl.k < g.nabs[4]) ? pl.k : pl.k - (g.nk - g.nabs[5]) + g.nabs[4];
+    z = ((size_t)za * g.nyi + e.iy) * g.px + e.ix;
+  }
+};
+
+// -------------------------- velocity part ---------------------------------
+// dV/dt = (1/rho) (d_xi sigma_x + d_eta sigma_y + zeta . d_zeta sigma), each
+// directional part divided by its CFS beta; ADE auxiliaries for V.  The top 3
+// layers' velocities come from the traction-image kernel (timg.cu); only
+// their z auxiliaries are updated here.
+// w[s][q]: staged component s on plane iz + (3 - q) * Z (q = 3: this plane).
+template <int X, int Y, int Z, int KIND>
+__device__ __forceinline__ void vel_pair(const StageArgs &a, const Pair &e, const Plane &pl,
+                                         const float *H, int ry, int cb, const Pw2 &pw,
+                                         const f2 (&w)[6][5], float rx, float rys, float rz) {
+  const size_t fs = a.g.fstride;
+  auto dx = [&](int s) { return dx_pair<X>(H + s * HPL + ry * HX, cb, w[s][3], rx); };
+  auto dy = [&](int s) { return dy_pair<Y>(H + s * HPL, ry, cb, w[s][3], rys); };
+  auto dz = [&](int s) { return drp2(w[s][4], w[s][3], w[s][2], w[s][1], w[s][0], rz); };
+
+  if (pl.lean) {
+    const f2 irho = pw.C(0);
+    f2 ztz = S2(1.f);
+    if (!a.flat) ztz = pw.M(2);
+    f2 hw[3];
+    if (pl.curved) {
+      const f2 ztx = pw.M(0), zty = pw.M(1);
+      const f2 DzTxx = dz(0), DzTyy = dz(1), DzTzz = dz(2);
+      const f2 DzTxy = dz(3), DzTxz = dz(4), DzTyz = dz(5);
+      const f2 z0 = mul2(fma2(ztz, DzTxz, fma2(zty, DzTxy, mul2(ztx, DzTxx))), irho);
+      const f2 z1 = mul2(fma2(ztz, DzTyz, fma2(zty, DzTyy, mul2(ztx, DzTxy))), irho);
+      const f2 z2 = mul2(fma2(ztz, DzTzz, fma2(zty, DzTyz, mul2(ztx, DzTxz))), irho);
+      hw[0] = add2(add2(mul2(dx(0), irho), mul2(dy(3), irho)), z0);
+      hw[1] = add2(add2(mul2(dx(3), irho), mul2(dy(1), irho)), z1);
+      hw[2] = add2(add2(mul2(dx(4), irho), mul2(dy(5), irho)), z2);
+    } else {
+      hw[0] = add2(add2(mul2(dx(0), irho), mul2(dy(3), irho)), mul2(mul2(ztz, dz(4)), irho));
+      hw[1] = add2(add2(mul2(dx(3), irho), mul2(dy(1), irho)), mul2(mul2(ztz, dz(5)), irho));
+      hw[2] = add2(add2(mul2(dx(4), irho), mul2(dy(5), irho)), mul2(mul2(ztz, dz(2)), irho));
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+      rk_store2<KIND>(a.out + (VX + q) * fs + pl.c, a.tw + (VX + q) * fs + pl.c, 3, pw.U0(q),
+                      KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], a.adt, a.bdt);
+    return;
+  }
+
+  // general path: issue every auxiliary load before the stencil arithmetic
+  const AuxIdx ix(a, e, pl);
+  const int mx = e.mx, my = e.ypml ? e.m : 0, mz = pl.zpml ? e.m : 0;
+  Aux2<KIND, 3> ax, ay, az;
+  if (mx) ax.load(a, 0, ix.x0, ix.x1, mx, 0);
+  if (my) ay.load(a, 1, ix.y, ix.y + 1, my, 0);
+  if (mz) az.load(a, 2, ix.z, ix.z + 1, mz, 0);
+  const f2 irho = pw.C(0);
+  f2 ztx = S2(0.f), zty = S2(0.f), ztz = S2(1.f);
+  if (!a.flat) {
+    ztz = pw.M(2);
+    if (pl.curved) { ztx = pw.M(0); zty = pw.M(1); }
+  }
+  f2 dxi[3], det[3], dzt[3];
+  dxi[0] = mul2(dx(0), irho);  // DxTxx
+  dxi[1] = mul2(dx(3), irho);  // DxTxy
+  dxi[2] = mul2(dx(4), irho);  // DxTxz
+  det[0] = mul2(dy(3), irho);  // DyTxy
+  det[1] = mul2(dy(1), irho);  // DyTyy
+  det[2] = mul2(dy(5), irho);  // DyTyz
+  const f2 DzTzz = dz(2), DzTxz = dz(4), DzTyz = dz(5);
+  if (pl.curved) {
+    const f2 DzTxx = dz(0), DzTyy = dz(1), DzTxy = dz(3);
+    dzt[0] = mul2(fma2(ztz, DzTxz, fma2(zty, DzTxy, mul2(ztx, DzTxx))), irho);
+    dzt[1] = mul2(fma2(ztz, DzTyz, fma2(zty, DzTyy, mul2(ztx, DzTxy))), irho);
+    dzt[2] = mul2(fma2(ztz, DzTzz, fma2(zty, DzTyz, mul2(ztx, DzTxz))), irho);
+  } else {
+    dzt[0] = mul2(mul2(ztz, DzTxz), irho);
+    dzt[1] = mul2(mul2(ztz, DzTyz), irho);
+    dzt[2] = mul2(mul2(ztz, DzTzz), irho);
+  }
+  const f2 iBy = S2(e.iBy), iBz = S2(ix.iBz);
+  f2 hw[3], hax[3], hay[3], haz[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) hw[q] = fma2(dzt[q], iBz, fma2(det[q], iBy, mul2(dxi[q], e.iBx)));
+  if (mx) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      hw[q] = fma2(neg2(ax.ai[q]), e.iBx, hw[q]);
+      hax[q] = fma2(neg2(e.apdx), ax.ai[q], mul2(dxi[q], e.dbx));
+    }
+  }
+  if (my) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      hw[q] = fma2(neg2(ay.ai[q]), iBy, hw[q]);
+      hay[q] = fma2(neg2(S2(e.apdy)), ay.ai[q], mul2(det[q], S2(e.dby)));
+    }
+  }
+  if (mz) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      hw[q] = fma2(neg2(az.ai[q]), iBz, hw[q]);
+      haz[q] = fma2(neg2(S2(ix.apdz)), az.ai[q], mul2(dzt[q], S2(ix.dbz)));
+    }
+  }
+  // the top 3 layers' velocities (and their x/y auxiliaries) come from the
+  // traction-image kernel; only the z auxiliaries are kept here
+  const bool xy = !pl.near_top;
+  const int mxs = xy ? mx : 0, mys = xy ? my : 0;
+  if (mxs) ax.update(a, 0, ix.x0, ix.x1, mxs, 0, hax);
+  if (mys) ay.update(a, 1, ix.y, ix.y + 1, mys, 0, hay);
+  if (mz) az.update(a, 2, ix.z, ix.z + 1, mz, 0, haz);
+  if (!xy) return;
+#pragma unroll
+  for (int q = 0; q < 3; ++q)
+    rk_store2<KIND>(a.out + (VX + q) * fs + pl.c, a.tw + (VX + q) * fs + pl.c, e.m, pw.U0(q),
+                    KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], a.adt, a.bdt);
+}
+
+// --------------------------- stress part ----------------------------------
+// dsigma/dt from Hooke's law with the velocity gradient in curvilinear form;
+// the surface-layer d/dzeta of V comes from the traction-free matrices, the
+// next two layers use the 2-point and Gottlieb 2-4 operators (VLOW).
+// w[s][q]: velocity component s on plane iz + (3 - q) * Z.
+
+// row r (0, 3, 6) of a surface matrix (9 planes from mv) times (u, v, t)
+__device__ __forceinline__ f2 mat_row(const float *mv, size_t plane, int r, f2 u, f2 v, f2 t) {
+  return fma2(lds2(mv + (r + 2) * plane), t,
+              fma2(lds2(mv + (r + 1) * plane), v, mul2(lds2(mv + r * plane), u)));
+}
+
+template <int X, int Y, int Z, int KIND>
+__device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, const Plane &pl,
+                                         const float *H, int ry, int cb, const Pw2 &pw,
+                                         const f2 (&w)[3][5], float rx, float rys, float rz) {
+  const Geom &g = a.g;
+  const size_t fs = g.fstride;
+  auto dx = [&](int s) { return dx_pair<X>(H + s * HPL + ry * HX, cb, w[s][3], rx); };
+  auto dy = [&](int s) { return dy_pair<Y>(H + s * HPL, ry, cb, w[s][3], rys); };
+  auto dz = [&](int s) { return drp2(w[s][4], w[s][3], w[s][2], w[s][1], w[s][0], rz); };
+
+  // general path: issue every stage-input auxiliary load before the stencil
+  const bool gen = !pl.lean;
+  int mx = 0, my = 0, mz = 0;
+  AuxIdx ix;
+  Aux2<KIND, 6> ax, ay, az;
+  if (gen) {
+    ix = AuxIdx(a, e, pl);
+    mx = e.mx;
+    my = e.ypml ? e.m : 0;
+    mz = pl.zpml ? e.m : 0;
+    if (mx) ax.load(a, 0, ix.x0, ix.x1, mx, 3);
+    if (my) ay.load(a, 1, ix.y, ix.y + 1, my, 3);
+    if (mz) az.load(a, 2, ix.z, ix.z + 1, mz, 3);
+  }
+  const f2 DxVx = dx(0), DxVy = dx(1), DxVz = dx(2);
+  const f2 DyVx = dy(0), DyVy = dy(1), DyVz = dy(2);
+  f2 DzVx, DzVy, DzVz;
+  // surface matrices of this pair (matVx2Vz: planes 0..8, matVy2Vz: 9..17)
+  const float *mv = a.matv + (size_t)e.iy * g.px + e.ix;
+  if (pl.top) {
+    DzVx = add2(mat_row(mv + 9 * g.plane, g.plane, 0, DyVx, DyVy, DyVz),
+                mat_row(mv, g.plane, 0, DxVx, DxVy, DxVz));
+    DzVy = add2(mat_row(mv + 9 * g.plane, g.plane, 3, DyVx, DyVy, DyVz),
+                mat_row(mv, g.plane, 3, DxVx, DxVy, DxVz));
+    DzVz = add2(mat_row(mv + 9 * g.plane, g.plane, 6, DyVx, DyVy, DyVz),
+                mat_row(mv, g.plane, 6, DxVx, DxVy, DxVz));
+  } else if (pl.iz == g.top - 1) {  // 2-point (M22)
+    DzVx = mul2(add2(w[0][2], neg2(w[0][3])), S2(rz));
+    DzVy = mul2(add2(w[1][2], neg2(w[1][3])), S2(rz));
+    DzVz = mul2(add2(w[2][2], neg2(w[2][3])), S2(rz));
+  } else if (pl.iz == g.top - 2) {  // Gottlieb 2-4 (M24)
+    auto m24 = [&](int s) {
+      return mul2(fma2(S2(CGFD_MA2), w[s][1], fma2(S2(CGFD_MA1), w[s][2],
+                                                  mul2(S2(CGFD_MA0), w[s][3]))), S2(rz));
+    };
+    DzVx = m24(0);
+    DzVy = m24(1);
+    DzVz = m24(2);
+  } else {
+    DzVx = dz(0);
+    DzVy = dz(1);
+    DzVz = dz(2);
+  }
+
+  const f2 lam2mu = pw.C(0), miu = pw.C(1);
+  const f2 lambda = fma2(S2(-2.f), miu, lam2mu);
+  f2 ztx = S2(0.f), zty = S2(0.f), ztz = S2(1.f);
+  if (!a.flat) {
+    ztz = pw.M(2);
+    if (pl.curved) { ztx = pw.M(0); zty = pw.M(1); }
+  }
+  // components in the set order Txx Tyy Tzz Txy Txz Tyz (index q = comp - 3)
+  f2 dxi[6], det[6], dzt[6];
+  {
+    const f2 tx2 = mul2(ztx, DzVx), ty2 = mul2(zty, DzVy), tz2 = mul2(ztz, DzVz);
+    dxi[0] = mul2(lam2mu, DxVx); det[0] = mul2(lambda, DyVy);
+    dzt[0] = fma2(lambda, tz2, fma2(lambda, ty2, mul2(lam2mu, tx2)));
+    dxi[1] = mul2(lambda, DxVx); det[1] = mul2(lam2mu, DyVy);
+    dzt[1] = fma2(lambda, tz2, fma2(lam2mu, ty2, mul2(lambda, tx2)));
+    dxi[2] = mul2(lambda, DxVx); det[2] = mul2(lambda, DyVy);
+    dzt[2] = fma2(lam2mu, tz2, fma2(lambda, ty2, mul2(lambda, tx2)));
+    dxi[3] = mul2(DxVy, miu); det[3] = mul2(DyVx, miu);
+    dzt[3] = mul2(fma2(ztx, DzVy, mul2(zty, DzVx)), miu);
+    dxi[4] = mul2(DxVz, miu); det[4] = S2(0.f);
+    dzt[4] = mul2(fma2(ztx, DzVz, mul2(ztz, DzVx)), miu);
+    dxi[5] = S2(0.f); det[5] = mul2(DyVz, miu);
+    dzt[5] = mul2(fma2(zty, DzVz, mul2(ztz, DzVy)), miu);
+  }
+
+  f2 hw[6];
+  if (!gen) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) hw[q] = add2(add2(dxi[q], det[q]), dzt[q]);
+  } else {
+    const f2 iBy = S2(e.iBy), iBz = S2(ix.iBz);
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+      hw[q] = fma2(dzt[q], iBz, fma2(det[q], iBy, mul2(dxi[q], e.iBx)));
+    if (mx) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) hw[q] = fma2(neg2(ax.ai[q]), e.iBx, hw[q]);
+    }
+    if (my) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) hw[q] = fma2(neg2(ay.ai[q]), iBy, hw[q]);
+    }
+    if (mz) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) hw[q] = fma2(neg2(az.ai[q]), iBz, hw[q]);
+    }
+    // surface layer: the ADE auxiliaries also take the xi (eta) part of the
+    // surface-matrix d/dzeta of V (src/calculate.cu:4479-4491, 4527-4538)
+    auto surf = [&](f2 z1v, f2 z2v, f2 z3v, f2 f, f2 *out) {
+      const f2 a1 = mul2(ztx, z1v), a2 = mul2(zty, z2v), a3 = mul2(ztz, z3v);
+      out[0] = fma2(f, fma2(lambda, a3, fma2(lambda, a2, mul2(lam2mu, a1))), out[0]);
+      out[1] = fma2(f, fma2(lambda, a3, fma2(lam2mu, a2, mul2(lambda, a1))), out[1]);
+      out[2] = fma2(f, fma2(lam2mu, a3, fma2(lambda, a2, mul2(lambda, a1))), out[2]);
+      out[3] = fma2(f, mul2(fma2(ztx, z2v, mul2(zty, z1v)), miu), out[3]);
+      out[4] = fma2(f, mul2(fma2(ztx, z3v, mul2(ztz, z1v)), miu), out[4]);
+      out[5] = fma2(f, mul2(fma2(zty, z3v, mul2(ztz, z2v)), miu), out[5]);
+    };
+    // one direction at a time: auxiliary RHS, then its RK update
+    f2 ha[6];
+    if (mx) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) ha[q] = fma2(neg2(e.apdx), ax.ai[q], mul2(dxi[q], e.dbx));
+      if (pl.top)
+        surf(mat_row(mv, g.plane, 0, DxVx, DxVy, DxVz), mat_row(mv, g.plane, 3, DxVx, DxVy, DxVz),
+             mat_row(mv, g.plane, 6, DxVx, DxVy, DxVz), mul2(e.dbx, e.bbx), ha);
+      ax.update(a, 0, ix.x0, ix.x1, mx, 3, ha);
+    }
+    if (my) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q)
+        ha[q] = fma2(neg2(S2(e.apdy)), ay.ai[q], mul2(det[q], S2(e.dby)));
+      if (pl.top) {
+        const float *my2 = mv + 9 * g.plane;
+        surf(mat_row(my2, g.plane, 0, DyVx, DyVy, DyVz), mat_row(my2, g.plane, 3, DyVx, DyVy, DyVz),
+             mat_row(my2, g.plane, 6, DyVx, DyVy, DyVz), S2(e.dby * e.bby), ha);
+      }
+      ay.update(a, 1, ix.y, ix.y + 1, my, 3, ha);
+    }
+    if (mz) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q)
+        ha[q] = fma2(neg2(S2(ix.apdz)), az.ai[q], mul2(dzt[q], S2(ix.dbz)));
+      az.update(a, 2, ix.z, ix.z + 1, mz, 3, ha);
+    }
+  }
+  const int m = gen ? e.m : 3;
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+    rk_store2<KIND>(a.out + (TXX + q) * fs + pl.c, a.tw + (TXX + q) * fs + pl.c, m, pw.U0(q),
+                    KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], a.adt, a.bdt);
+}
+
+// ------------------------------ the march ---------------------------------
+// items: tile index fastest, so the CTAs resident at one time work on
+// neighbouring tiles of the same z-chunk and share halo rows in L2
+template <int PART, int X, int Y, int Z, int KIND>
+__global__ void __launch_bounds__(TT, 2)
+    pair_kernel(const __grid_constant__ Maps maps, const StageArgs a, const Work wk, int *err) {
+  using S = Slot<PART>;
+  constexpr int NC = PartInfo<PART>::NC, C0 = PartInfo<PART>::C0;
+  constexpr int NS = PartInfo<PART>::NS, S0 = PartInfo<PART>::S0;
+  constexpr int NCOEF = PartInfo<PART>::NCOEF, COEF0 = PartInfo<PART>::COEF0;
+  constexpr int DIR = (Z > 0) ? -1 : 1;  // march direction in z
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // align the ring on the shared-window address itself
+  unsigned char *base = smem_raw + ((128u - (su32(smem_raw) & 127u)) & 127u);
+  float *ring = reinterpret_cast<float *>(base);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(base + (size_t)NSLOT * S::BYTES);
+  __shared__ int abort_flag;
+
+  const Geom &g = a.g;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const size_t fs = g.fstride;
+  const bool flat = a.flat;
+  // bytes one plane delivers: halo always, pointwise only for computed planes
+  const uint32_t pw_bytes = (uint32_t)(PWT * 4) *
+      (NS * (KIND == 1 ? 2 : 1) + NCOEF + (flat ? 0 : 3));
+
+  if (tid == 0) {
+    abort_flag = 0;
+    bool aligned = ((su32(bars) & 7u) == 0);
+    for (int s = 0; s < NSLOT; ++s)
+      aligned = aligned && ((su32(ring + (size_t)s * S::FLOATS) & 127u) == 0);
+    if (!aligned) {
+      abort_flag = 1;
+      if (err) atomicExch(err, 2);
+    } else {
+      for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);
+      fence_mbar_init();
+    }
+  }
+  __syncthreads();
+  if (abort_flag) return;  // nothing was issued
+
+  uint32_t ph = 0;    // parity of the next wait, per slot (same in every thread)
+  uint32_t pend = 0;  // thread 0: slots with a copy not yet waited for
+  const float rx = (float)X / a.h, rys = (float)Y / a.h, rz = (float)Z / a.h;
+  const int ry = ty + 3, cb = 4 + 2 * tx;
+  const int sc = ry * HX + cb;       // this pair inside a halo plane
+  const int tc = ty * CX + 2 * tx;   // this pair inside a pointwise tile
+  const int zlo = LFD + g.nabs[4], zhi = g.nk + LFD - g.nabs[5];  // z interior [zlo, zhi)
+  const int kinda = (KIND == 1) ? 3 : (KIND == 2 ? 2 : 1);        // aux sets read
+
+  for (int item = blockIdx.x; item < wk.nitems && !abort_flag; item += gridDim.x) {
+    const int tile = item % wk.ntiles, cz = item / wk.ntiles;
+    const int i0 = (tile % wk.ntx) * CX, j0 = (tile / wk.ntx) * TY;
+    const int z0 = LFD + cz * wk.zchunk;
+    const int z1 = min(z0 + wk.zchunk, g.nk + LFD);
+    const int n = z1 - z0;                  // planes computed
+    const int zf = (DIR > 0) ? z0 : z1 - 1;  // first plane in march order
+    // tile-uniform PML presence (for the L2 prefetches)
+    const bool tx_pml = wk.has_aux[0] && (i0 < g.nabs[0] || i0 + CX > g.ni - g.nabs[1]);
+    const bool ty_pml = wk.has_aux[1] && (j0 < g.nabs[2] || j0 + TY > g.nj - g.nabs[3]);
+    const int xa_t = (i0 < g.nabs[0]) ? i0 : i0 - (g.ni - g.nabs[1]) + g.xaoff;
+    const int ya_t = (j0 < g.nabs[2]) ? j0 : j0 - (g.nj - g.nabs[3]) + g.nabs[2];
+    // march index q: plane zf + DIR*q in slot q & 3; q = n is read for the
+    // window only (no pointwise operands)
+    auto issue = [&](int q) {  // thread 0 only
+      const int s = q & (NSLOT - 1);
+      float *slot = ring + (size_t)s * S::FLOATS;
+      const int p = zf + DIR * q;
+      const bool compute = q < n;
+      fence_proxy_async();
+      mbar_expect_tx(&bars[s], S::HALO_B + (compute ? pw_bytes : 0u));
+      tma_load(slot, &maps.halo, XO + i0 - 4, j0, p, C0, &bars[s]);
+      if (compute) {
+        const int cx = XO + i0, cy = LFD + j0;
+        tma_load(slot + S::U0, &maps.u0, cx, cy, p, S0, &bars[s]);
+        if (KIND == 1) tma_load(slot + S::U1, &maps.u1, cx, cy, p, S0, &bars[s]);
+        tma_load(slot + S::COEF, &maps.coef, cx, cy, p, COEF0, &bars[s]);
+        if (!flat) tma_load(slot + S::MET, &maps.met, cx, cy, p, 0, &bars[s]);
+        const int c0 = (PART == PART_VEL) ? 0 : 3;
+        const bool zp = wk.has_aux[2] && (p < zlo || p >= zhi);
+        const int za = (p - LFD < g.nabs[4]) ? p - LFD : p - LFD - (g.nk - g.nabs[5]) + g.nabs[4];
+        for (int t = 0; t < kinda; ++t) {
+          const int set = (KIND == 2 && t == 1) ? 2 : t;  // final stage: ain, ta
+          if (tx_pml) tma_prefetch(&maps.aux[0][set], xa_t, cy, p, c0);
+          if (ty_pml) tma_prefetch(&maps.aux[1][set], cx, ya_t, p, c0);
+          if (zp) tma_prefetch(&maps.aux[2][set], cx, cy, za, c0);
+        }
+      }
+      pend |= 1u << s;
+    };
+    auto wait = [&](int q) -> bool {  // every thread, in march order
+      const int s = q & (NSLOT - 1);
+      const bool ok = mbar_wait(&bars[s], (ph >> s) & 1u);
+      if (ok) {  // an expired wait leaves the copy pending for the drain
+        ph ^= 1u << s;
+        if (tid == 0) pend &= ~(1u << s);
+      }
+      return ok;
+    };
+    if (tid == 0)
+      for (int q = 0; q < NSLOT && q <= n; ++q) issue(q);
+
+    Pair e;
+    e.i = i0 + 2 * tx;
+    e.j = j0 + ty;
+    e.ix = e.i + XO;
+    e.iy = e.j + LFD;
+    const bool rowok = e.j < g.nj;
+    e.m = (rowok && e.i < g.ni ? 1 : 0) | (rowok && e.i + 1 < g.ni ? 2 : 0);
+    auto inx = [&](int i) { return i < g.nabs[0] || i >= g.ni - g.nabs[1]; };
+    e.mx = ((e.m & 1) && inx(e.i) ? 1 : 0) | ((e.m & 2) && inx(e.i + 1) ? 2 : 0);
+    e.ypml = e.m && (e.j < g.nabs[2] || e.j >= g.nj - g.nabs[3]);
+    // xa1 = xa0 + 1 whenever both cells are in a layer (xaoff), and xa0 is
+    // even then, so the pair is one aligned 64-bit access
+    auto xa = [&](int i) { return (i < g.nabs[0]) ? i : i - (g.ni - g.nabs[1]) + g.xaoff; };
+    e.xa0 = xa(e.i);
+    e.xa1 = xa(e.i + 1);
+    e.ya = (e.j < g.nabs[2]) ? e.j : e.j - (g.nj - g.nabs[3]) + g.nabs[2];
+    e.iBx = S2(1.f); e.apdx = S2(0.f); e.dbx = S2(0.f); e.bbx = S2(1.f);
+    e.iBy = 1.f; e.apdy = 0.f; e.dby = 0.f; e.bby = 1.f;
+    if (e.m & 1) {
+      e.bbx.x = a.b[0][e.ix]; e.iBx.x = 1.f / e.bbx.x;
+      e.apdx.x = a.apd[0][e.ix]; e.dbx.x = a.db[0][e.ix];
+    }
+    if (e.m & 2) {
+      e.bbx.y = a.b[0][e.ix + 1]; e.iBx.y = 1.f / e.bbx.y;
+      e.apdx.y = a.apd[0][e.ix + 1]; e.dbx.y = a.db[0][e.ix + 1];
+    }
+    if (e.m) {
+      e.bby = a.b[1][e.iy]; e.iBy = 1.f / e.bby;
+      e.apdy = a.apd[1][e.iy]; e.dby = a.db[1][e.iy];
+    }
+    // tile-uniform: no x/y PML anywhere in this tile (and B = 1, DB = APD = 0
+    // outside the layers, which the solver checks at upload)
+    const bool tile_int = a.plain_interior && (i0 >= g.nabs[0]) &&
+                          (i0 + CX <= g.ni - g.nabs[1]) && (j0 >= g.nabs[2]) &&
+                          (j0 + TY <= g.nj - g.nabs[3]);
+
+    // register window: w[c][q] = plane (current) + DIR * (q - 3)
+    f2 w[NC][5];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int q = 0; q < 5; ++q) w[c][q] = S2(0.f);
+    auto push_smem = [&](const float *plane) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) w[c][q] = w[c][q + 1];
+        w[c][4] = lds2(plane + c * HPL + sc);
+      }
+    };
+    // the three planes behind the chunk come straight from global memory
+    for (int k = 3; k >= 1; --k) {
+      const size_t o = gidx(g, e.ix, e.iy, zf - DIR * k);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) w[c][q] = w[c][q + 1];
+        const float *src = a.in + (size_t)(C0 + c) * fs + o;
+        w[c][4] = e.m ? ld2(src, src + 1, e.m) : S2(0.f);
+      }
+    }
+    // A wait that expires sets the CTA-wide abort flag; the flag is read only
+    // after a __syncthreads, so every thread leaves the march together.
+    if (wait(0)) push_smem(ring);
+    else abort_flag = 1;
+    __syncthreads();
+
+    size_t c = gidx(g, e.ix, e.iy, zf);
+    for (int q = 0; q < n; ++q) {
+      const bool got = wait(q + 1);
+      if (got) push_smem(ring + (size_t)((q + 1) & (NSLOT - 1)) * S::FLOATS);
+      else abort_flag = 1;
+      if (e.m && got) {
+        const float *slot = ring + (size_t)(q & (NSLOT - 1)) * S::FLOATS;
+        Plane pl;
+        pl.iz = zf + DIR * q;
+        pl.k = pl.iz - LFD;
+        pl.c = c;
+        pl.top = (pl.iz == g.top);
+        pl.near_top = pl.iz >= g.top - 2;
+        pl.zpml = (pl.iz < zlo) || (pl.iz >= zhi);
+        pl.curved = pl.iz >= g.con && !flat;
+        pl.lean = tile_int && !pl.zpml && !pl.near_top;
+        const Pw2 pw{slot + S::U0 + tc, slot + S::U1 + tc, slot + S::COEF + tc,
+                     slot + S::MET + tc};
+        if constexpr (PART == PART_VEL)
+          vel_pair<X, Y, Z, KIND>(a, e, pl, slot, ry, cb, pw, w, rx, rys, rz);
+        else
+          str_pair<X, Y, Z, KIND>(a, e, pl, slot, ry, cb, pw, w, rx, rys, rz);
+      }
+      // the slot of plane q is free: refill it with plane q + NSLOT
+      __syncthreads();
+      if (abort_flag) break;
+      if (tid == 0 && q + NSLOT <= n) issue(q + NSLOT);
+      c += (DIR > 0) ? g.plane : (size_t)0 - g.plane;
+    }
+    __syncthreads();  // all reads of the ring done before the next item reuses it
+  }
+  if (abort_flag && tid == 0) {
+    if (err) atomicExch(err, 1);
+    // drain: wait (bounded) for copies still in flight before the CTA's
+    // shared memory goes away
+    for (int s = 0; s < NSLOT; ++s)
+      if (pend & (1u << s)) mbar_wait(&bars[s], (ph >> s) & 1u);
+  }
+}
+
+// Tensor maps and launch shape of one solver (host side, stage_pair.cu).
+struct Plan {
+  // per field set (FW, Wa, Wb, tW): halo boxes of the two parts and the
+  // pointwise boxes of V (3) and T (6) components
+  CUtensorMap haloV[4], haloS[4], ctrV[4], ctrT[4];
+  CUtensorMap coefV, coefS, met;
+  // auxiliaries: [direction][FA, A, tA], boxes of V (3) and T (6) components
+  CUtensorMap auxV[3][3], auxT[3][3];
+  Work wk;
+  int grid[2];
+};
+
+template <int PART, int X, int Y, int Z, int KIND>
+void launch_t(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
+  pair_kernel<PART, X, Y, Z, KIND><<<pl.grid[PART], dim3(TX, TY, 1), Slot<PART>::SMEM, s>>>(
+      m, a, pl.wk, err);
+}
+
+template <int PART, int KIND>
+void launch_dirs(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
+  const int code = (a.X > 0 ? 4 : 0) + (a.Y > 0 ? 2 : 0) + (a.Z > 0 ? 1 : 0);
+  switch (code) {
+    case 0: launch_t<PART, -1, -1, -1, KIND>(pl, m, a, err, s); break;
+    case 1: launch_t<PART, -1, -1, 1, KIND>(pl, m, a, err, s); break;
+    case 2: launch_t<PART, -1, 1, -1, KIND>(pl, m, a, err, s); break;
+    case 3: launch_t<PART, -1, 1, 1, KIND>(pl, m, a, err, s); break;
+    case 4: launch_t<PART, 1, -1, -1, KIND>(pl, m, a, err, s); break;
+    case 5: launch_t<PART, 1, -1, 1, KIND>(pl, m, a, err, s); break;
+    case 6: launch_t<PART, 1, 1, -1, KIND>(pl, m, a, err, s); break;
+    default: launch_t<PART, 1, 1, 1, KIND>(pl, m, a, err, s); break;
+  }
+}
+
+template <int PART, int KIND>
+void set_attrs() {
+  auto set = [](const void *f) {
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Slot<PART>::SMEM);
+  };
+  set((const void *)pair_kernel<PART, -1, -1, -1, KIND>);
+  set((const void *)pair_kernel<PART, -1, -1, 1, KIND>);
+  set((const void *)pair_kernel<PART, -1, 1, -1, KIND>);
+  set((const void *)pair_kernel<PART, -1, 1, 1, KIND>);
+  set((const void *)pair_kernel<PART, 1, -1, -1, KIND>);
+  set((const void *)pair_kernel<PART, 1, -1, 1, KIND>);
+  set((const void *)pair_kernel<PART, 1, 1, -1, KIND>);
+  set((const void *)pair_kernel<PART, 1, 1, 1, KIND>);
+}
+
+template <int PART>
+int resident_ctas() {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pair_kernel<PART, 1, 1, 1, 1>, TT,
+                                                Slot<PART>::SMEM);
+  if (per < 1) per = 1;
+  if (sms < 1) sms = 1;
+  return per * sms;
+}
+
+// per-(part, kind) entry points, one translation unit each (pair_*.cu)
+#define CGFD_PAIR_DECL(P, K)                                                          \
+  void launch_##P##K(const Plan &pl, const Maps &m, const StageArgs &a, int *err,   \
+                     cudaStream_t s);                                                \
+  void attrs_##P##K();
+CGFD_PAIR_DECL(v, 0)
+CGFD_PAIR_DECL(v, 1)
+CGFD_PAIR_DECL(v, 2)
+CGFD_PAIR_DECL(s, 0)
+CGFD_PAIR_DECL(s, 1)
+CGFD_PAIR_DECL(s, 2)
+#undef CGFD_PAIR_DECL
+int resident_vel();
+int resident_str();
+
+}  // namespace pair
+}  // namespace cgfd

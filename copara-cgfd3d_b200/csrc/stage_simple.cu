@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(128) stage_simple_kernel(StageArgs a) {
   const int *nabs = g.nabs;
   long px_ = -1, py_ = -1, pz_ = -1;
   if (i < nabs[0] || i >= g.ni - nabs[1]) {
-    const int xa = (i < nabs[0]) ? i : i - (g.ni - nabs[1]) + nabs[0];
+    const int xa = (i < nabs[0]) ? i : i - (g.ni - nabs[1]) + g.xaoff;
     px_ = ((long)iz * g.nyi + iy) * g.nxa + xa;
   }
   if (j < nabs[2] || j >= g.nj - nabs[3]) {

@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(128) timg_kernel(StageArgs a) {
   const float iBx = 1.f / a.b[0][ix], iBy = 1.f / a.b[1][iy];
   const bool xpml = i < g.nabs[0] || i >= g.ni - g.nabs[1];
   const bool ypml = j < g.nabs[2] || j >= g.nj - g.nabs[3];
-  const int xa = (i < g.nabs[0]) ? i : i - (g.ni - g.nabs[1]) + g.nabs[0];
+  const int xa = (i < g.nabs[0]) ? i : i - (g.ni - g.nabs[1]) + g.xaoff;
   const int ya = (j < g.nabs[2]) ? j : j - (g.nj - g.nabs[3]) + g.nabs[2];
   const size_t px = ((size_t)iz * g.nyi + iy) * g.nxa + xa;
   const size_t py = ((size_t)iz * g.nya + ya) * g.px + ix;

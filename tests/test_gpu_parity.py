@@ -24,20 +24,20 @@ def _cmp(a, b, tol, what):
         assert e < tol, f"{what} component {cgfd.COMPONENTS[c]}: rel L2 {e:.3e}"
 
 
-def _kernels():
-    return [cgfd.KERNEL_SIMPLE, cgfd.KERNEL_FUSED]
+KERNELS = [cgfd.KERNEL_SIMPLE, cgfd.KERNEL_FUSED, cgfd.KERNEL_PAIR]
+KIDS = ["simple", "fused", "pair"]
 
 
 def _skip_if_unsupported(kernel, m):
     try:
         cgfd.Solver(m.desc(kernel=kernel)).close()
     except cgfd.CgfdError as e:
-        if kernel == cgfd.KERNEL_FUSED and "fused kernel does not support" in str(e):
-            pytest.skip("fused kernel not built for this grid")
+        if kernel != cgfd.KERNEL_SIMPLE and "kernel does not support" in str(e):
+            pytest.skip("tiled kernel not built for this grid")
         raise
 
 
-@pytest.mark.parametrize("kernel", _kernels(), ids=["simple", "fused"])
+@pytest.mark.parametrize("kernel", KERNELS, ids=KIDS)
 @pytest.mark.parametrize("name", list(cases.CASES))
 def test_product_matches_fp64_oracle(name, kernel):
     m, nsteps, nstages, init = cases.build(name)
@@ -64,7 +64,7 @@ def test_reference_matches_fp64_oracle(name):
         _cmp(valid(r["fw"]), valid(ofw), TOL, "FW")
 
 
-@pytest.mark.parametrize("kernel", _kernels(), ids=["simple", "fused"])
+@pytest.mark.parametrize("kernel", KERNELS, ids=KIDS)
 @pytest.mark.parametrize("name", list(cases.CASES))
 def test_product_matches_reference(name, kernel):
     m, nsteps, nstages, init = cases.build(name)
@@ -78,7 +78,7 @@ def test_product_matches_reference(name, kernel):
         _cmp(valid(pfw), valid(r["fw"]), TOL, "FW")
 
 
-@pytest.mark.parametrize("kernel", _kernels(), ids=["simple", "fused"])
+@pytest.mark.parametrize("kernel", KERNELS, ids=KIDS)
 def test_flat_halfspace_160x160x80_500_steps_matches_reference(kernel):
     """The 160x160x80 flat half-space model, full 500 steps, 25 receivers."""
     import models
@@ -97,21 +97,23 @@ def test_flat_halfspace_160x160x80_500_steps_matches_reference(kernel):
     _cmp(ps, r["seis"], TOL, "seismogram")
 
 
-def test_fused_matches_simple_kernel_on_hill_400x400x200():
+def test_tiled_kernels_match_simple_kernel_on_hill_400x400x200():
     """Full-size property check on the 400x400x200 hill model: 8 steps of the
     tiled kernels (many work items per persistent CTA) against the untiled
     per-cell kernel, seismograms and the final wavefield."""
     import models
     m = models.config_c2(nt=8)
     out = {}
-    for kern in (cgfd.KERNEL_FUSED, cgfd.KERNEL_SIMPLE):
+    for kern in KERNELS:
         s = cgfd.Solver(m.desc(kernel=kern))
         m.load(s)
         s.step(8)
         fw = np.stack([s.get_field(c)[::3, ::3, 3:-3] for c in range(9)])
         out[kern] = (s.seismograms(), fw)
         s.close()
-    for c, e in enumerate(comp_errors(out[cgfd.KERNEL_FUSED][1], out[cgfd.KERNEL_SIMPLE][1])):
-        assert e < 1e-5, (cgfd.COMPONENTS[c], e)
-    for c, e in enumerate(comp_errors(out[cgfd.KERNEL_FUSED][0], out[cgfd.KERNEL_SIMPLE][0])):
-        assert e < 1e-5, (cgfd.COMPONENTS[c], e)
+    ref = out[cgfd.KERNEL_SIMPLE]
+    for kern in (cgfd.KERNEL_FUSED, cgfd.KERNEL_PAIR):
+        for c, e in enumerate(comp_errors(out[kern][1], ref[1])):
+            assert e < 1e-5, (kern, cgfd.COMPONENTS[c], e)
+        for c, e in enumerate(comp_errors(out[kern][0], ref[0])):
+            assert e < 1e-5, (kern, cgfd.COMPONENTS[c], e)
