@@ -39,7 +39,7 @@ def parse():
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    p.add_argument("--kernel", choices=("fused", "simple"), default="fused")
+    p.add_argument("--kernel", choices=("fused", "simple", "scalar"), default="fused")
     p.add_argument("--config", choices=("hill400", "flat160", "hill256"), default="hill400")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -252,7 +252,8 @@ def main():
         return
     dist, rank, world, local = dist_init(args.gpus)
     import cgfd
-    kernel = cgfd.KERNEL_FUSED if args.kernel == "fused" else cgfd.KERNEL_SIMPLE
+    kernel = {"fused": cgfd.KERNEL_FUSED, "simple": cgfd.KERNEL_SIMPLE,
+              "scalar": cgfd.KERNEL_SCALAR}[args.kernel]
     K, W = args.steps, args.warmup
     K2 = min(K, 20)
     nt = W + K + K2 + 2
@@ -311,7 +312,7 @@ def main():
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_step": bps, "stage_kernel_ms": stage_ms},
         "clocks": clk.summary(),
-        "gpu_launches": K * (4 * (3 if args.kernel == "fused" else 1) + 4 * n_src + 1),
+        "gpu_launches": K * (4 * (1 if args.kernel == "simple" else 3) + 4 * n_src + 1),
         "nonfinite": nbad,
     }
     if e2e:

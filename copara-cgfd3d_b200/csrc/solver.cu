@@ -202,7 +202,7 @@ int arg_fail(cgfd_solver *h, const char *what) {
 
 void free_all(cgfd_solver *h) {
   if (h->plan) {
-    if (h->d.kernel == CGFD_KERNEL_PAIR) pair_destroy_plan(h->plan);
+    if (h->d.kernel == CGFD_KERNEL_FUSED) pair_destroy_plan(h->plan);
     else fused_destroy_plan(h->plan);
     h->plan = nullptr;
   }
@@ -363,7 +363,7 @@ StageArgs stage_args(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, in
 void dispatch_stage(cgfd_solver *h, const StageArgs &a, int in_set) {
   if (h->d.kernel == CGFD_KERNEL_SIMPLE)
     launch_stage_simple(a, h->st);
-  else if (h->d.kernel == CGFD_KERNEL_PAIR)
+  else if (h->d.kernel == CGFD_KERNEL_FUSED)
     launch_stage_pair(h->plan, a, in_set, h->d_err, h->st);
   else
     launch_stage_fused(h->plan, a, in_set, h->d_err, h->st);
@@ -444,7 +444,7 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
     return arg_fail(nullptr, "con_index must lie in [3, nk+2]");
   if (d->storage != CGFD_STORE_F32) return arg_fail(nullptr, "storage type not supported");
   if (d->kernel != CGFD_KERNEL_FUSED && d->kernel != CGFD_KERNEL_SIMPLE &&
-      d->kernel != CGFD_KERNEL_PAIR)
+      d->kernel != CGFD_KERNEL_SCALAR)
     return arg_fail(nullptr, "unknown kernel family");
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -477,8 +477,8 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
   g.astride[0] = align_up((size_t)g.nzi * g.nyi * g.nxa, 64);
   g.astride[1] = align_up((size_t)g.nzi * g.nya * g.px, 64);
   g.astride[2] = align_up((size_t)g.nza * g.nyi * g.px, 64);
-  if ((d->kernel == CGFD_KERNEL_FUSED && !fused_supported(g)) ||
-      (d->kernel == CGFD_KERNEL_PAIR && !pair_supported(g))) {
+  if ((d->kernel == CGFD_KERNEL_SCALAR && !fused_supported(g)) ||
+      (d->kernel == CGFD_KERNEL_FUSED && !pair_supported(g))) {
     delete h;
     return arg_fail(nullptr, "tiled kernel does not support this grid");
   }
@@ -518,8 +518,8 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
     return st;
   }
   for (int q = 0; q < 4; ++q) h->set[q] = h->state + (size_t)q * 9 * fs;
-  if (d->kernel == CGFD_KERNEL_FUSED || d->kernel == CGFD_KERNEL_PAIR) {
-    h->plan = (d->kernel == CGFD_KERNEL_PAIR)
+  if (d->kernel == CGFD_KERNEL_FUSED || d->kernel == CGFD_KERNEL_SCALAR) {
+    h->plan = (d->kernel == CGFD_KERNEL_FUSED)
                   ? pair_create_plan(g, h->set, h->media, h->metric, h->aux)
                   : fused_create_plan(g, h->set, h->media, h->metric);
     if (!h->plan) {

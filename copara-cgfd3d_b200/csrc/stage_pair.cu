@@ -4,7 +4,9 @@
 // pair_{v,s}{0,1,2}.cu.
 #include "stage_pair_impl.cuh"
 
+#include <algorithm>
 #include <new>
+#include <vector>
 
 namespace cgfd {
 namespace pair {
@@ -60,9 +62,19 @@ bool aux_map(CUtensorMap *m, const Geom &g, int d, const float *base, int bc) {
 
 using namespace pair;
 
+#ifndef CGFD_PAIR_ITEMS_PER_CTA
+#define CGFD_PAIR_ITEMS_PER_CTA 6
+#endif
+#ifndef CGFD_PAIR_MIN_CHUNK
+#define CGFD_PAIR_MIN_CHUNK 16
+#endif
+// work list shape: about this many items per resident CTA, z-chunks of at
+// least this many planes
+constexpr int ITEMS_PER_CTA = CGFD_PAIR_ITEMS_PER_CTA, MIN_CHUNK = CGFD_PAIR_MIN_CHUNK;
+
 bool pair_supported(const Geom &g) {
   // tile boxes start on 16-byte boundaries (XO and i0 multiples of 4, px of
-  // 32) and the grid is at least one plane deep beyond the stencil reach
+  // 32) and every z-chunk has at least 4 planes
   return (XO % 4) == 0 && XO >= 4 && g.px % 32 == 0 && g.nk >= 4;
 }
 
@@ -100,30 +112,87 @@ void *pair_create_plan(const Geom &g, float *const sets[4], const float *media,
     delete pl;
     return nullptr;
   }
-  Work &wk = pl->wk;
-  wk.ntx = (g.ni + CX - 1) / CX;
-  wk.ntiles = wk.ntx * ((g.nj + TY - 1) / TY);
+  // work items: the bottom PML layer as a z-chunk of its own, the rest in
+  // pieces long enough to amortise the four window planes read around each
+  // chunk and numerous enough to balance
+  // x tiles start at the grid's first column (a tile whose PML columns share
+  // it with interior columns costs about as much per plane as a tile of PML
+  // columns alone: the boundary path is latency-bound per plane)
+  const int xorg = 0;
+  const int ntx = (g.ni - xorg + CX - 1) / CX, nty = (g.nj + TY - 1) / TY;
+  const int ntiles = ntx * nty;
   const int rv = resident_vel(), rs = resident_str();
   const int G = rv < rs ? rv : rs;
-  // z-chunk length: minimise (rounds of work over the resident CTAs) x
-  // (chunk length + the four window planes read around it)
-  double best = 1e30;
-  int bestzc = g.nk;
-  for (int nzc = 1; nzc <= (g.nk + 7) / 8; ++nzc) {
-    const int zc = (g.nk + nzc - 1) / nzc;
-    const long items = (long)wk.ntiles * ((g.nk + zc - 1) / zc);
-    const long rounds = (items + G - 1) / G;
-    const double cost = (double)rounds * (zc + 4);
-    if (cost < best - 1e-9) { best = cost; bestzc = zc; }
+  // (every chunk has at least 4 planes: the kernel's initial issue of four
+  // entries relies on it)
+  std::vector<int> zb{LFD};
+  const int zlo = LFD + g.nabs[4], ztop = g.nk + LFD;
+  if (g.nabs[4] >= 8 && ztop - zlo >= 8) zb.push_back(zlo);
+  const int zr = zb.back(), rest = ztop - zr;
+  int pieces = 1;
+  while ((long)ntiles * ((long)zb.size() - 1 + pieces) < (long)ITEMS_PER_CTA * G &&
+         rest / (pieces + 1) >= MIN_CHUNK)
+    ++pieces;
+  for (int q = 1; q <= pieces; ++q) zb.push_back(zr + (int)((long)rest * q / pieces));
+  for (size_t c = 0; c + 1 < zb.size(); ++c)
+    if (zb[c + 1] - zb[c] < 4) {
+      delete pl;
+      return nullptr;
+    }
+  pl->zchunk = (rest + pieces - 1) / pieces;
+  // order: the most expensive first (estimated cost: planes x sum over the
+  // tile's valid columns of (1 + number of PML directions)), so the cheap
+  // items fill the tail; equal costs keep the (z-chunk, tile) order, so
+  // neighbouring tiles of a class run together and share halo rows in L2
+  struct It { int4 v; double cost; };
+  std::vector<It> items;
+  for (size_t c = 0; c + 1 < zb.size(); ++c) {
+    const bool zp = zb[c] < zlo;
+    for (int t = 0; t < ntiles; ++t) {
+      const int i0 = xorg + (t % ntx) * CX, j0 = (t / ntx) * TY;
+      double w = 0;
+      for (int j = j0; j < j0 + TY && j < g.nj; ++j) {
+        const bool yp = j < g.nabs[2] || j >= g.nj - g.nabs[3];
+        for (int i = i0 < 0 ? 0 : i0; i < i0 + CX && i < g.ni; ++i) {
+          const bool xp = i < g.nabs[0] || i >= g.ni - g.nabs[1];
+          w += 1 + (xp ? 1 : 0) + (yp ? 1 : 0) + (zp ? 1 : 0);
+        }
+      }
+      items.push_back({make_int4(i0, j0, zb[c], zb[c + 1]), w * (zb[c + 1] - zb[c])});
+    }
   }
-  wk.zchunk = bestzc;
-  wk.nitems = wk.ntiles * ((g.nk + bestzc - 1) / bestzc);
+  std::stable_sort(items.begin(), items.end(),
+                   [](const It &x, const It &y) { return x.cost > y.cost; });
+  std::vector<int4> hv(items.size());
+  for (size_t q = 0; q < items.size(); ++q) hv[q] = items[q].v;
+  Work &wk = pl->wk;
+  wk.nitems = (int)hv.size();
+  int4 *d_items = nullptr;
+  int *d_counter = nullptr;
+  if (cudaMalloc(&d_items, hv.size() * sizeof(int4)) != cudaSuccess ||
+      cudaMemcpy(d_items, hv.data(), hv.size() * sizeof(int4), cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMalloc(&d_counter, 2 * sizeof(int)) != cudaSuccess ||
+      cudaMemset(d_counter, 0, 2 * sizeof(int)) != cudaSuccess) {
+    cudaFree(d_items);
+    cudaFree(d_counter);
+    delete pl;
+    return nullptr;
+  }
+  wk.items = d_items;
+  wk.counter = d_counter;
   pl->grid[0] = wk.nitems < rv ? wk.nitems : rv;
   pl->grid[1] = wk.nitems < rs ? wk.nitems : rs;
   return pl;
 }
 
-void pair_destroy_plan(void *plan) { delete reinterpret_cast<Plan *>(plan); }
+void pair_destroy_plan(void *plan) {
+  Plan *pl = reinterpret_cast<Plan *>(plan);
+  if (!pl) return;
+  cudaFree((void *)pl->wk.items);
+  cudaFree(pl->wk.counter);
+  delete pl;
+}
 
 void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *err,
                        void *stream) {
@@ -147,6 +216,8 @@ void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *er
     mv.aux[d][0] = pl.auxV[d][in]; mv.aux[d][1] = pl.auxV[d][0]; mv.aux[d][2] = pl.auxV[d][2];
     ms.aux[d][0] = pl.auxT[d][in]; ms.aux[d][1] = pl.auxT[d][0]; ms.aux[d][2] = pl.auxT[d][2];
   }
+  // both parts' item counters restart at zero
+  cudaMemsetAsync(pl.wk.counter, 0, 2 * sizeof(int), s);
   if (kind == 0) {
     launch_v0(pl, mv, a, err, s);
     launch_s0(pl, ms, a, err, s);
@@ -162,7 +233,7 @@ void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *er
 
 int pair_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str) {
   const Plan &pl = *reinterpret_cast<const Plan *>(plan);
-  if (zchunk) *zchunk = pl.wk.zchunk;
+  if (zchunk) *zchunk = pl.zchunk;
   if (grid_vel) *grid_vel = pl.grid[0];
   if (grid_str) *grid_str = pl.grid[1];
   return pl.wk.nitems;

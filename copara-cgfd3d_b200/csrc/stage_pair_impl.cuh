@@ -61,6 +61,10 @@ constexpr int HPL = HX * HY;                  // floats per component per halo p
 constexpr int PWT = CX * TY;                  // floats per pointwise tile
 constexpr int NSLOT = 4;
 enum { PART_VEL = 0, PART_STR = 1 };
+#ifndef CGFD_PAIR_UNROLL
+#define CGFD_PAIR_UNROLL 1
+#endif
+constexpr int MARCH_UNROLL = CGFD_PAIR_UNROLL;  // unroll factor of the march loop
 
 // NC: staged (differentiated) components, C0: first of them in a set;
 // NS: components the part updates (V: 3, T: 6), S0 their first index;
@@ -104,8 +108,14 @@ struct Maps {
   CUtensorMap aux[3][3];  // [direction][ain, afw, ta], box {64, 4, 1, NS}
 };
 
+// Work list of a launch: items {i0, j0, z0, z1} (tile origin and z range),
+// ordered by decreasing estimated cost; CTAs take them in order from an
+// atomic counter (reset before every launch), so expensive PML items start
+// first and the cheap interior items fill the tail.
 struct Work {
-  int zchunk, ntx, ntiles, nitems;
+  const int4 *items;
+  int *counter;       // [0]: velocity launch, [1]: stress launch
+  int nitems;
   int has_aux[3];     // direction has a PML (aux maps valid)
 };
 
@@ -187,8 +197,8 @@ __device__ __forceinline__ void rk_store2(float *out, float *tw, int m, f2 u0, f
 
 // ADE auxiliaries of one pair and direction: the stage input ai (FA in the
 // first stage, A after) is loaded early (it enters the RHS); the RK update
-// then reads FA / tA set by set right before writing A (FA in the final
-// stage) and tA, so that only one set's values are live at a time.
+// then reads FA and tA of one direction together right before writing A (FA
+// in the final stage) and tA, so that only one direction's values are live.
 // o0/o1: the cells' indices, m: the cells' mask.
 template <int KIND, int N>
 struct Aux2 {
@@ -213,26 +223,21 @@ struct Aux2 {
         st2(pt + o0, pt + o1, m, fma2(S2(a.bdt), hh[q], ai[q]));
       }
     } else if (KIND == 1) {
-      f2 u[N];
+      // FA and tA together: one memory round trip per direction
+      f2 u[N], v[N];
 #pragma unroll
       for (int q = 0; q < N; ++q) {
         const float *b = a.afw[d] + (c0 + q) * as;
+        const float *t = a.ta[d] + (c0 + q) * as;
         u[q] = ld2(b + o0, b + o1, m);
+        v[q] = ld2(t + o0, t + o1, m);
       }
 #pragma unroll
       for (int q = 0; q < N; ++q) {
         float *po = a.aout[d] + (c0 + q) * as;
-        st2(po + o0, po + o1, m, fma2(S2(a.adt), hh[q], u[q]));
-      }
-#pragma unroll
-      for (int q = 0; q < N; ++q) {
-        const float *b = a.ta[d] + (c0 + q) * as;
-        u[q] = ld2(b + o0, b + o1, m);
-      }
-#pragma unroll
-      for (int q = 0; q < N; ++q) {
         float *pt = a.ta[d] + (c0 + q) * as;
-        st2(pt + o0, pt + o1, m, fma2(S2(a.bdt), hh[q], u[q]));
+        st2(po + o0, po + o1, m, fma2(S2(a.adt), hh[q], u[q]));
+        st2(pt + o0, pt + o1, m, fma2(S2(a.bdt), hh[q], v[q]));
       }
     } else {
       f2 u[N];
@@ -580,9 +585,9 @@ __global__ void __launch_bounds__(TT, 2)
   constexpr int DIR = (Z > 0) ? -1 : 1;  // march direction in z
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // align the ring on the shared-window address itself
-  unsigned char *base = smem_raw + ((128u - (su32(smem_raw) & 127u)) & 127u);
-  float *ring = reinterpret_cast<float *>(base);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(base + (size_t)NSLOT * S::BYTES);
+  unsigned char *sbase = smem_raw + ((128u - (su32(smem_raw) & 127u)) & 127u);
+  float *ring = reinterpret_cast<float *>(sbase);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sbase + (size_t)NSLOT * S::BYTES);
   __shared__ int abort_flag;
 
   const Geom &g = a.g;
@@ -618,48 +623,61 @@ __global__ void __launch_bounds__(TT, 2)
   const int zlo = LFD + g.nabs[4], zhi = g.nk + LFD - g.nabs[5];  // z interior [zlo, zhi)
   const int kinda = (KIND == 1) ? 3 : (KIND == 2 ? 2 : 1);        // aux sets read
 
-  for (int item = blockIdx.x; item < wk.nitems && !abort_flag; item += gridDim.x) {
-    const int tile = item % wk.ntiles, cz = item / wk.ntiles;
-    const int i0 = (tile % wk.ntx) * CX, j0 = (tile / wk.ntx) * TY;
-    const int z0 = LFD + cz * wk.zchunk;
-    const int z1 = min(z0 + wk.zchunk, g.nk + LFD);
-    const int n = z1 - z0;                  // planes computed
-    const int zf = (DIR > 0) ? z0 : z1 - 1;  // first plane in march order
-    // tile-uniform PML presence (for the L2 prefetches)
-    const bool tx_pml = wk.has_aux[0] && (i0 < g.nabs[0] || i0 + CX > g.ni - g.nabs[1]);
-    const bool ty_pml = wk.has_aux[1] && (j0 < g.nabs[2] || j0 + TY > g.nj - g.nabs[3]);
-    const int xa_t = (i0 < g.nabs[0]) ? i0 : i0 - (g.ni - g.nabs[1]) + g.xaoff;
-    const int ya_t = (j0 < g.nabs[2]) ? j0 : j0 - (g.nj - g.nabs[3]) + g.nabs[2];
-    // march index q: plane zf + DIR*q in slot q & 3; q = n is read for the
-    // window only (no pointwise operands)
-    auto issue = [&](int q) {  // thread 0 only
-      const int s = q & (NSLOT - 1);
-      float *slot = ring + (size_t)s * S::FLOATS;
-      const int p = zf + DIR * q;
-      const bool compute = q < n;
-      fence_proxy_async();
-      mbar_expect_tx(&bars[s], S::HALO_B + (compute ? pw_bytes : 0u));
-      tma_load(slot, &maps.halo, XO + i0 - 4, j0, p, C0, &bars[s]);
-      if (compute) {
-        const int cx = XO + i0, cy = LFD + j0;
-        tma_load(slot + S::U0, &maps.u0, cx, cy, p, S0, &bars[s]);
-        if (KIND == 1) tma_load(slot + S::U1, &maps.u1, cx, cy, p, S0, &bars[s]);
-        tma_load(slot + S::COEF, &maps.coef, cx, cy, p, COEF0, &bars[s]);
-        if (!flat) tma_load(slot + S::MET, &maps.met, cx, cy, p, 0, &bars[s]);
-        const int c0 = (PART == PART_VEL) ? 0 : 3;
-        const bool zp = wk.has_aux[2] && (p < zlo || p >= zhi);
+  // Item entries q = 0..n (plane zf + DIR*q; entry n is read for the window
+  // only) go to ring slot (base + q) & 3, base counting the entries of the
+  // CTA's earlier items; thread 0 issues, every thread waits, in order.
+  auto issue = [&](const int4 it, int q, int s) {  // thread 0 only
+    float *slot = ring + (size_t)s * S::FLOATS;
+    const int i0 = it.x, j0 = it.y, n = it.w - it.z;
+    const int p = ((DIR > 0) ? it.z : it.w - 1) + DIR * q;
+    const bool compute = q < n;
+    fence_proxy_async();
+    mbar_expect_tx(&bars[s], S::HALO_B + (compute ? pw_bytes : 0u));
+    tma_load(slot, &maps.halo, XO + i0 - 4, j0, p, C0, &bars[s]);
+    if (compute) {
+      const int cx = XO + i0, cy = LFD + j0;
+      tma_load(slot + S::U0, &maps.u0, cx, cy, p, S0, &bars[s]);
+      if (KIND == 1) tma_load(slot + S::U1, &maps.u1, cx, cy, p, S0, &bars[s]);
+      tma_load(slot + S::COEF, &maps.coef, cx, cy, p, COEF0, &bars[s]);
+      if (!flat) tma_load(slot + S::MET, &maps.met, cx, cy, p, 0, &bars[s]);
+      // the plane's PML auxiliaries into L2 (tile- and plane-uniform presence)
+      const bool xp = wk.has_aux[0] && (i0 < g.nabs[0] || i0 + CX > g.ni - g.nabs[1]);
+      const bool yp = wk.has_aux[1] && (j0 < g.nabs[2] || j0 + TY > g.nj - g.nabs[3]);
+      const bool zp = wk.has_aux[2] && (p < zlo || p >= zhi);
+      if (xp || yp || zp) {
+        const int xa_t = (i0 < g.nabs[0]) ? max(i0, 0) : i0 - (g.ni - g.nabs[1]) + g.xaoff;
+        const int ya_t = (j0 < g.nabs[2]) ? j0 : j0 - (g.nj - g.nabs[3]) + g.nabs[2];
         const int za = (p - LFD < g.nabs[4]) ? p - LFD : p - LFD - (g.nk - g.nabs[5]) + g.nabs[4];
+        const int c0 = (PART == PART_VEL) ? 0 : 3;
+        const int cxp = max(cx, 0);  // prefetch boxes start inside the arrays
         for (int t = 0; t < kinda; ++t) {
           const int set = (KIND == 2 && t == 1) ? 2 : t;  // final stage: ain, ta
-          if (tx_pml) tma_prefetch(&maps.aux[0][set], xa_t, cy, p, c0);
-          if (ty_pml) tma_prefetch(&maps.aux[1][set], cx, ya_t, p, c0);
-          if (zp) tma_prefetch(&maps.aux[2][set], cx, cy, za, c0);
+          if (xp) tma_prefetch(&maps.aux[0][set], xa_t, cy, p, c0);
+          if (yp) tma_prefetch(&maps.aux[1][set], cxp, ya_t, p, c0);
+          if (zp) tma_prefetch(&maps.aux[2][set], cxp, cy, za, c0);
         }
       }
-      pend |= 1u << s;
-    };
+    }
+    pend |= 1u << s;
+  };
+
+  __shared__ int s_next;
+  int base = 0;  // stream position of the current item's entry 0
+  for (;;) {
+    // the next item, taken only when this CTA is free (a CTA never holds a
+    // claim on work while it is still busy)
+    if (tid == 0) s_next = atomicAdd(wk.counter + PART, 1);
+    __syncthreads();
+    const int cur = s_next;
+    if (cur >= wk.nitems || abort_flag) break;  // CTA-uniform
+    const int4 it = wk.items[cur];
+    const int i0 = it.x, j0 = it.y, z0 = it.z, z1 = it.w;
+    const int n = z1 - z0;                  // planes computed (>= 4)
+    const int zf = (DIR > 0) ? z0 : z1 - 1;  // first plane in march order
+    if (tid == 0)
+      for (int q = 0; q < NSLOT; ++q) issue(it, q, (base + q) & (NSLOT - 1));
     auto wait = [&](int q) -> bool {  // every thread, in march order
-      const int s = q & (NSLOT - 1);
+      const int s = (base + q) & (NSLOT - 1);
       const bool ok = mbar_wait(&bars[s], (ph >> s) & 1u);
       if (ok) {  // an expired wait leaves the copy pending for the drain
         ph ^= 1u << s;
@@ -667,16 +685,14 @@ __global__ void __launch_bounds__(TT, 2)
       }
       return ok;
     };
-    if (tid == 0)
-      for (int q = 0; q < NSLOT && q <= n; ++q) issue(q);
 
     Pair e;
     e.i = i0 + 2 * tx;
     e.j = j0 + ty;
     e.ix = e.i + XO;
     e.iy = e.j + LFD;
-    const bool rowok = e.j < g.nj;
-    e.m = (rowok && e.i < g.ni ? 1 : 0) | (rowok && e.i + 1 < g.ni ? 2 : 0);
+    const bool rowok = e.j < g.nj;  // (tile origins may lie left of the grid)
+    e.m = (rowok && e.i >= 0 && e.i < g.ni ? 1 : 0) | (rowok && e.i + 1 >= 0 && e.i + 1 < g.ni ? 2 : 0);
     auto inx = [&](int i) { return i < g.nabs[0] || i >= g.ni - g.nabs[1]; };
     e.mx = ((e.m & 1) && inx(e.i) ? 1 : 0) | ((e.m & 2) && inx(e.i + 1) ? 2 : 0);
     e.ypml = e.m && (e.j < g.nabs[2] || e.j >= g.nj - g.nabs[3]);
@@ -733,17 +749,18 @@ __global__ void __launch_bounds__(TT, 2)
     }
     // A wait that expires sets the CTA-wide abort flag; the flag is read only
     // after a __syncthreads, so every thread leaves the march together.
-    if (wait(0)) push_smem(ring);
+    if (wait(0)) push_smem(ring + (size_t)(base & (NSLOT - 1)) * S::FLOATS);
     else abort_flag = 1;
     __syncthreads();
 
     size_t c = gidx(g, e.ix, e.iy, zf);
+#pragma unroll MARCH_UNROLL
     for (int q = 0; q < n; ++q) {
       const bool got = wait(q + 1);
-      if (got) push_smem(ring + (size_t)((q + 1) & (NSLOT - 1)) * S::FLOATS);
+      if (got) push_smem(ring + (size_t)((base + q + 1) & (NSLOT - 1)) * S::FLOATS);
       else abort_flag = 1;
       if (e.m && got) {
-        const float *slot = ring + (size_t)(q & (NSLOT - 1)) * S::FLOATS;
+        const float *slot = ring + (size_t)((base + q) & (NSLOT - 1)) * S::FLOATS;
         Plane pl;
         pl.iz = zf + DIR * q;
         pl.k = pl.iz - LFD;
@@ -760,13 +777,15 @@ __global__ void __launch_bounds__(TT, 2)
         else
           str_pair<X, Y, Z, KIND>(a, e, pl, slot, ry, cb, pw, w, rx, rys, rz);
       }
-      // the slot of plane q is free: refill it with plane q + NSLOT
+      // the slot of entry q is free: refill it with stream position
+      // base + q + NSLOT (this item's entry q + 4, or the next item's)
       __syncthreads();
       if (abort_flag) break;
-      if (tid == 0 && q + NSLOT <= n) issue(q + NSLOT);
+      if (tid == 0 && q + NSLOT <= n) issue(it, q + NSLOT, (base + q) & (NSLOT - 1));
       c += (DIR > 0) ? g.plane : (size_t)0 - g.plane;
     }
     __syncthreads();  // all reads of the ring done before the next item reuses it
+    base += n + 1;
   }
   if (abort_flag && tid == 0) {
     if (err) atomicExch(err, 1);
@@ -786,6 +805,7 @@ struct Plan {
   // auxiliaries: [direction][FA, A, tA], boxes of V (3) and T (6) components
   CUtensorMap auxV[3][3], auxT[3][3];
   Work wk;
+  int zchunk;   // planes of the interior z-chunks
   int grid[2];
 };
 

@@ -26,7 +26,7 @@ _lib = C.CDLL(LIB_PATH)
 
 OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_TIMEOUT, ERR_NONFINITE, ERR_NODEVICE = range(8)
 STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
-KERNEL_FUSED, KERNEL_SIMPLE, KERNEL_PAIR = 0, 1, 2
+KERNEL_FUSED, KERNEL_SIMPLE, KERNEL_SCALAR = 0, 1, 2
 SET_FW, SET_W, SET_TW = 0, 1, 2
 COMPONENTS = ("Vx", "Vy", "Vz", "Txx", "Tyy", "Tzz", "Txy", "Txz", "Tyz")
 STF_TYPES = {"Gauss": 0, "gauss": 1, "Ricker": 2, "ricker": 3, "Bell": 4,

@@ -52,9 +52,11 @@ typedef enum cgfd_storage {
 
 /* Kernel family used for the RK stages. */
 typedef enum cgfd_kernel {
-    CGFD_KERNEL_FUSED  = 0,  /* z-marching tiled kernel (default)            */
+    CGFD_KERNEL_FUSED  = 0,  /* z-marching tiled kernel, two x-adjacent cells
+                                per thread (default)                       */
     CGFD_KERNEL_SIMPLE = 1,  /* one thread per cell, no tiling (cross-check) */
-    CGFD_KERNEL_PAIR   = 2   /* z-marching, two x-adjacent cells per thread  */
+    CGFD_KERNEL_SCALAR = 2   /* z-marching tiled kernel, one cell per thread
+                                (cross-check of the tiled structure)       */
 } cgfd_kernel;
 
 /* Field sets that cgfd_get_field / cgfd_set_field address. */

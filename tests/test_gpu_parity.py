@@ -24,8 +24,8 @@ def _cmp(a, b, tol, what):
         assert e < tol, f"{what} component {cgfd.COMPONENTS[c]}: rel L2 {e:.3e}"
 
 
-KERNELS = [cgfd.KERNEL_SIMPLE, cgfd.KERNEL_FUSED, cgfd.KERNEL_PAIR]
-KIDS = ["simple", "fused", "pair"]
+KERNELS = [cgfd.KERNEL_SIMPLE, cgfd.KERNEL_FUSED, cgfd.KERNEL_SCALAR]
+KIDS = ["simple", "fused", "scalar"]
 
 
 def _skip_if_unsupported(kernel, m):
@@ -112,7 +112,7 @@ def test_tiled_kernels_match_simple_kernel_on_hill_400x400x200():
         out[kern] = (s.seismograms(), fw)
         s.close()
     ref = out[cgfd.KERNEL_SIMPLE]
-    for kern in (cgfd.KERNEL_FUSED, cgfd.KERNEL_PAIR):
+    for kern in (cgfd.KERNEL_FUSED, cgfd.KERNEL_SCALAR):
         for c, e in enumerate(comp_errors(out[kern][1], ref[1])):
             assert e < 1e-5, (kern, cgfd.COMPONENTS[c], e)
         for c, e in enumerate(comp_errors(out[kern][0], ref[0])):
