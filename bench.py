@@ -41,6 +41,8 @@ def parse():
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--kernel", choices=("fused", "simple", "scalar"), default="fused")
     p.add_argument("--config", choices=("hill400", "flat160", "hill256"), default="hill400")
+    p.add_argument("--storage", choices=("f32", "f16", "bf16"), default="f32",
+                   help="storage type of the field sets (arithmetic is FP32)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -65,16 +67,17 @@ def workload_name(cfg):
 def algorithmic_bytes_per_step(m, elem=4):
     """Minimum HBM bytes of one RK4 step of the fused design: 144 state values
     per cell (27+45+45+27 over the 4 stages: reads of W, FW, tW, writes of W,
-    tW, FW), the same again for each (cell, PML direction) pair (ADE
-    auxiliaries), and (3 media + m metric) coefficients per cell per stage
-    (m = 3 above ConIndex, 1 below, 0 for a trivial metric)."""
+    tW, FW) of elem bytes each, the same again for each (cell, PML direction)
+    pair (ADE auxiliaries, FP32), and (3 media + m metric) FP32 coefficients
+    per cell per stage (m = 3 above ConIndex, 1 below, 0 for a trivial
+    metric)."""
     nxy = m.ni * m.nj
     cells = m.cells
     state = 144 * elem * cells
     nab = m.nabs
     pml_pairs = ((nab[0] + nab[1]) * m.nj * m.nk + (nab[2] + nab[3]) * m.ni * m.nk +
                  (nab[4] + nab[5]) * m.ni * m.nj)
-    aux = 144 * elem * pml_pairs
+    aux = 144 * 4 * pml_pairs
     zz = m.metric["zeta_z"][3:-3, 3:-3, 3:-3]
     flat = bool(np.all(zz == 1.0) and np.all(m.metric["jac"][3:-3, 3:-3, 3:-3] == 1.0)
                 and np.all(m.metric["zeta_x"][3:-3, 3:-3, 3:-3] == 0.0))
@@ -258,7 +261,8 @@ def main():
     K2 = min(K, 20)
     nt = W + K + K2 + 2
     m = build_model(args.config, nt)
-    s = cgfd.Solver(m.desc(kernel=kernel, device=local))
+    storage = {"f32": cgfd.STORE_F32, "f16": cgfd.STORE_F16, "bf16": cgfd.STORE_BF16}[args.storage]
+    s = cgfd.Solver(m.desc(kernel=kernel, device=local, storage=storage))
     m.load(s)
     s.prepare()
     s.step(W)
@@ -278,7 +282,7 @@ def main():
     if not args.no_e2e:
         barrier(dist)
         t0 = time.perf_counter()
-        s2 = cgfd.Solver(m.desc(kernel=kernel, device=local))
+        s2 = cgfd.Solver(m.desc(kernel=kernel, device=local, storage=storage))
         m.load(s2)
         s2.step(K)
         seis = s2.seismograms()
@@ -294,17 +298,19 @@ def main():
         if dist is not None:
             dist.destroy_process_group()
         return
-    bps = algorithmic_bytes_per_step(m)
+    bps = algorithmic_bytes_per_step(m, 4 if args.storage == "f32" else 2)
     achieved = bps / 4 / (stage_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    traffic = committed_traffic(workload_name(args.config), args.kernel)
+    traffic = committed_traffic(workload_name(args.config),
+                                args.kernel if args.storage == "f32" else
+                                f"{args.kernel}_{args.storage}")
     n_src = 1 if (len(m.mnt_loc) + len(m.frc_loc)) else 0
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
         "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded model generator)",
         "config": {"workload": workload_name(args.config), "cells": m.cells,
-                   "kernel": args.kernel, "replicas": world,
+                   "kernel": args.kernel, "storage": args.storage, "replicas": world,
                    "l2": "state >> L2 (126 MB), no flush needed",
                    "parallelism": "replicas" if world > 1 else "single"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

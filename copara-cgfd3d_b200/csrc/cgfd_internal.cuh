@@ -34,6 +34,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "elem.cuh"
+
 namespace cgfd {
 
 constexpr int LFD = 3;   // ghost width of the reference (LenFD)
@@ -81,10 +83,14 @@ struct StageArgs {
   int X, Y, Z;         // +1 forward / -1 backward per axis
   float h;             // steph
   float adt, bdt;      // RK4A[rk]*dt (0 for rk 3), RK4B[rk]*dt
-  const float *in;     // stencil input set (FW for rk 0, else previous W)
-  const float *fw;     // FW (rk 1,2 read it)
-  float *out;          // output set: W (rk 0..2) or FW (rk 3)
-  float *tw;           // tW
+  // field sets, of the storage element type elem (ELEM_F32 / F16 / BF16)
+  const void *in;      // stencil input set (FW for rk 0, else previous W)
+  const void *fw;      // FW (rk 1,2 read it)
+  void *out;           // output set: W (rk 0..2) or FW (rk 3)
+  void *tw;            // tW
+  int elem;
+  float sc[NCOMP];     // value of one stored unit per component (2^k)
+  float isc[NCOMP];    // its inverse (stored units per value)
   const float *lam2mu, *mu, *irho;
   const float *zx, *zy, *zz, *jac;
   bool flat;           // metric is zeta=(0,0,1), jac=1 everywhere
@@ -116,7 +122,9 @@ struct SourceArgs {
   int tindex;          // >= 0: use it; < 0: 2*(*step)+tinc
   const int *step;     // device step counter
   float adt, bdt;
-  float *out, *tw;
+  void *out, *tw;      // field sets of element type elem
+  int elem;
+  float isc[NCOMP];
   int rk;
 };
 
@@ -138,7 +146,7 @@ int fused_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str)
 // The paired kernels (two x-adjacent cells per thread, stage_pair.cu); aux
 // holds the three directions' auxiliary arrays (null: no PML there).
 bool pair_supported(const Geom &g);
-void *pair_create_plan(const Geom &g, float *const sets[4], const float *media,
+void *pair_create_plan(const Geom &g, int elem, void *const sets[4], const float *media,
                        const float *metric, float *const aux[3]);
 void pair_destroy_plan(void *plan);
 void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *err,

@@ -1,4 +1,4 @@
-// nonfinite.cuh -- count of NaN / Inf values in a float array, in two passes
+// nonfinite.cuh -- count of NaN / Inf values in a float (or 16-bit) array, in two passes
 // over a scratch array of per-block partial counts:
 //   nonfinite_partial_kernel: block b counts values [b*NF_CHUNK, (b+1)*NF_CHUNK)
 //                             and writes partials[b];
@@ -42,6 +42,22 @@ static __global__ void __launch_bounds__(NF_THREADS)
   for (int q = 0; q < NF_ITEMS; ++q) {
     const size_t o = base + (size_t)q * NF_THREADS + threadIdx.x;
     if (o < n && !isfinite(v[o])) ++local;
+  }
+  const unsigned long long t = nf_block_sum(local);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+// the same for 16-bit storage: a value is NaN or Inf when all its exponent
+// bits (emask: 0x7C00 for IEEE half, 0x7F80 for bfloat16) are set
+static __global__ void __launch_bounds__(NF_THREADS)
+    nonfinite16_partial_kernel(const uint16_t *__restrict__ v, size_t n, uint16_t emask,
+                               unsigned long long *__restrict__ partials) {
+  const size_t base = (size_t)blockIdx.x * NF_CHUNK;
+  unsigned long long local = 0;
+#pragma unroll 4
+  for (int q = 0; q < NF_ITEMS; ++q) {
+    const size_t o = base + (size_t)q * NF_THREADS + threadIdx.x;
+    if (o < n && (v[o] & emask) == emask) ++local;
   }
   const unsigned long long t = nf_block_sum(local);
   if (threadIdx.x == 0) partials[blockIdx.x] = t;

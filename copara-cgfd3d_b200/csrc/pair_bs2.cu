@@ -1,0 +1,15 @@
+// pair_bs2.cu -- instantiates the paired stress kernels of RK stage kind
+// 2 (final stage) with BF16 storage for the 8 stencil directions.
+#include "stage_pair_impl.cuh"
+
+namespace cgfd {
+namespace pair {
+
+void launch_bs2(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
+  launch_dirs<__nv_bfloat16, PART_STR, 2>(pl, m, a, err, s);
+}
+
+void attrs_bs2() { set_attrs<__nv_bfloat16, PART_STR, 2>(); }
+
+}  // namespace pair
+}  // namespace cgfd

@@ -1,0 +1,15 @@
+// pair_bv0.cu -- instantiates the paired velocity kernels of RK stage kind
+// 0 (first stage) with BF16 storage for the 8 stencil directions.
+#include "stage_pair_impl.cuh"
+
+namespace cgfd {
+namespace pair {
+
+void launch_bv0(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
+  launch_dirs<__nv_bfloat16, PART_VEL, 0>(pl, m, a, err, s);
+}
+
+void attrs_bv0() { set_attrs<__nv_bfloat16, PART_VEL, 0>(); }
+
+}  // namespace pair
+}  // namespace cgfd

@@ -1,0 +1,16 @@
+// pair_bv1.cu -- instantiates the paired velocity kernels of RK stage kind
+// 1 (inner stages) with BF16 storage for the 8 stencil directions.
+#include "stage_pair_impl.cuh"
+
+namespace cgfd {
+namespace pair {
+
+void launch_bv1(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
+  launch_dirs<__nv_bfloat16, PART_VEL, 1>(pl, m, a, err, s);
+}
+
+void attrs_bv1() { set_attrs<__nv_bfloat16, PART_VEL, 1>(); }
+
+int resident_bv() { return resident_ctas<__nv_bfloat16, PART_VEL>(); }
+}  // namespace pair
+}  // namespace cgfd

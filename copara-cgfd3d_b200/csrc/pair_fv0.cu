@@ -1,0 +1,15 @@
+// pair_fv0.cu -- instantiates the paired velocity kernels of RK stage kind
+// 0 (first stage) with FP32 storage for the 8 stencil directions.
+#include "stage_pair_impl.cuh"
+
+namespace cgfd {
+namespace pair {
+
+void launch_fv0(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
+  launch_dirs<float, PART_VEL, 0>(pl, m, a, err, s);
+}
+
+void attrs_fv0() { set_attrs<float, PART_VEL, 0>(); }
+
+}  // namespace pair
+}  // namespace cgfd

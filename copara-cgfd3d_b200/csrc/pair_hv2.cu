@@ -1,0 +1,15 @@
+// pair_hv2.cu -- instantiates the paired velocity kernels of RK stage kind
+// 2 (final stage) with FP16 storage for the 8 stencil directions.
+#include "stage_pair_impl.cuh"
+
+namespace cgfd {
+namespace pair {
+
+void launch_hv2(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
+  launch_dirs<__half, PART_VEL, 2>(pl, m, a, err, s);
+}
+
+void attrs_hv2() { set_attrs<__half, PART_VEL, 2>(); }
+
+}  // namespace pair
+}  // namespace cgfd

@@ -47,9 +47,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
   return true;
 }
 // box at (x, y, z, c) of a 4-D tensor map into shared memory, completing on
-// the mbarrier; x * 4 bytes must be a multiple of 16 (the callers' tiles
+// the mbarrier; x times the element size must be a multiple of 16 bytes (the callers' tiles
 // start on 16-byte boundaries by construction)
-__device__ __forceinline__ void tma_load(float *dst, const CUtensorMap *map, int x, int y, int z,
+__device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, int x, int y, int z,
                                          int c, uint64_t *bar) {
   asm volatile(
       "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"

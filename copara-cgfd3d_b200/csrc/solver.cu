@@ -41,9 +41,11 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // ------------------------------ kernels -----------------------------------
 
-// reference layout (i*ny+j)*nz+k  ->  internal layout (x fastest)
-__global__ void to_internal_kernel(const float *__restrict__ src, float *__restrict__ dst,
-                                   Geom g, int nx, int ny, int nz) {
+// reference layout (i*ny+j)*nz+k  ->  internal layout (x fastest), stored
+// as T in units of 1/isc
+template <typename T>
+__global__ void to_internal_kernel(const float *__restrict__ src, T *__restrict__ dst, Geom g,
+                                   int nx, int ny, int nz, float isc) {
   const long n = (long)nx * ny * nz;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n;
        q += (long)gridDim.x * blockDim.x) {
@@ -51,11 +53,12 @@ __global__ void to_internal_kernel(const float *__restrict__ src, float *__restr
     const long r = q / nz;
     const int j = (int)(r % ny);
     const int i = (int)(r / ny);
-    dst[gidx(g, i + XSH, j, k)] = src[q];
+    Elem<T>::st(dst + gidx(g, i + XSH, j, k), src[q] * isc);
   }
 }
-__global__ void to_reference_kernel(const float *__restrict__ src, float *__restrict__ dst,
-                                    Geom g, int nx, int ny, int nz) {
+template <typename T>
+__global__ void to_reference_kernel(const T *__restrict__ src, float *__restrict__ dst, Geom g,
+                                    int nx, int ny, int nz, float sc) {
   const long n = (long)nx * ny * nz;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n;
        q += (long)gridDim.x * blockDim.x) {
@@ -63,59 +66,79 @@ __global__ void to_reference_kernel(const float *__restrict__ src, float *__rest
     const long r = q / nz;
     const int j = (int)(r % ny);
     const int i = (int)(r / ny);
-    dst[q] = src[gidx(g, i + XSH, j, k)];
+    dst[q] = Elem<T>::ld(src + gidx(g, i + XSH, j, k)) * sc;
   }
 }
 
 // Point sources (LoadMoment/LoadForce, src/calculate.cu:6130-6255), applied
 // to the stage output; one thread walks the list so that repeated cells add
 // up in a fixed order.
+template <typename T>
 __global__ void inject_sources_kernel(SourceArgs s) {
+  using E = Elem<T>;
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int t2 = (s.tindex >= 0) ? s.tindex : 2 * (*s.step) + s.tinc;
   const size_t fs = s.g.fstride;
+  T *out = static_cast<T *>(s.out), *tw = static_cast<T *>(s.tw);
+  // W_out += adt*S, tW += bdt*S in stored units of the component
+  auto add = [&](int comp, size_t o, float S) {
+    const float a = s.adt * s.isc[comp], b = s.bdt * s.isc[comp];
+    if (s.rk == 3) {
+      E::st(out + o, E::ld(out + o) + b * S);
+    } else {
+      E::st(out + o, E::ld(out + o) + a * S);
+      E::st(tw + o, E::ld(tw + o) + b * S);
+    }
+  };
   for (int q = 0; q < s.nmnt; ++q) {
     const float stf = s.mstf[(size_t)q * s.nstfm + t2];
     const int c = s.mcell[q];
-    for (int m = 0; m < 6; ++m) {
-      const float S = -s.mcoef[6 * q + m] * stf;
-      const size_t o = (size_t)(TXX + m) * fs + c;
-      if (s.rk == 3) {
-        s.out[o] += s.bdt * S;
-      } else {
-        s.out[o] += s.adt * S;
-        s.tw[o] += s.bdt * S;
-      }
-    }
+    for (int m = 0; m < 6; ++m)
+      add(TXX + m, (size_t)(TXX + m) * fs + c, -s.mcoef[6 * q + m] * stf);
   }
   for (int q = 0; q < s.nfrc; ++q) {
     const float stf = s.fstf[(size_t)q * s.nstff + t2];
     const int c = s.fcell[q];
-    for (int m = 0; m < 3; ++m) {
-      const float S = stf * s.fcoef[3 * q + m];
-      const size_t o = (size_t)(VX + m) * fs + c;
-      if (s.rk == 3) {
-        s.out[o] += s.bdt * S;
-      } else {
-        s.out[o] += s.adt * S;
-        s.tw[o] += s.bdt * S;
-      }
-    }
+    for (int m = 0; m < 3; ++m) add(VX + m, (size_t)(VX + m) * fs + c, stf * s.fcoef[3 * q + m]);
   }
+}
+void launch_sources(const SourceArgs &s, cudaStream_t st) {
+  if (s.elem == ELEM_F16) inject_sources_kernel<__half><<<1, 32, 0, st>>>(s);
+  else if (s.elem == ELEM_BF16) inject_sources_kernel<__nv_bfloat16><<<1, 32, 0, st>>>(s);
+  else inject_sources_kernel<float><<<1, 32, 0, st>>>(s);
 }
 
 // Receiver recording (PWpick, src/calculate.cu:2780-2830) from FW after a
 // step, into seis[(c*nrecv + r)*nt + t]; then advances the step counter.
-__global__ void record_kernel(const float *__restrict__ fw, size_t fstride,
+struct Scales {
+  float sc[NCOMP];
+};
+template <typename T>
+__global__ void record_kernel(const T *__restrict__ fw, size_t fstride,
                               const int *__restrict__ cells, int nrecv, int nt,
-                              float *__restrict__ seis, int *step) {
+                              float *__restrict__ seis, int *step, Scales s) {
   const int t = *step;
   for (int q = threadIdx.x; q < 9 * nrecv; q += blockDim.x) {
     const int c = q / nrecv, r = q % nrecv;
-    if (t < nt) seis[((size_t)c * nrecv + r) * nt + t] = fw[(size_t)c * fstride + cells[r]];
+    if (t < nt)
+      seis[((size_t)c * nrecv + r) * nt + t] =
+          Elem<T>::ld(fw + (size_t)c * fstride + cells[r]) * s.sc[c];
   }
   __syncthreads();
   if (threadIdx.x == 0) *step = t + 1;
+}
+
+// multiplies component comp of the four field sets by factor (a power of two:
+// exact unless it leaves the storage type's range)
+template <typename T>
+__global__ void rescale_kernel(T *sets, size_t fstride, int comp, float factor) {
+  const size_t n = fstride;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x)
+    for (int s = 0; s < 4; ++s) {
+      T *p = sets + ((size_t)s * NCOMP + comp) * fstride + q;
+      Elem<T>::st(p, Elem<T>::ld(p) * factor);
+    }
 }
 
 }  // namespace
@@ -125,8 +148,11 @@ struct cgfd_solver {
   Geom g{};
   cudaStream_t st = nullptr;
   std::string err;
-  float *state = nullptr;  // 4 sets of 9 components: FW, Wa, Wb, tW
-  float *set[4] = {nullptr, nullptr, nullptr, nullptr};
+  void *state = nullptr;   // 4 sets of 9 components: FW, Wa, Wb, tW
+  void *set[4] = {nullptr, nullptr, nullptr, nullptr};
+  int elem = ELEM_F32;     // storage element type of the sets
+  int sexp[NCOMP] = {};    // per-component scale exponents: stored = value * 2^-sexp
+  bool user_scales = false;
   int wcur = 0;            // set that holds "W" (last stage output)
   float *media = nullptr;  // lam2mu, mu, irho
   float *metric = nullptr; // zeta_x, zeta_y, zeta_z, jac
@@ -144,6 +170,7 @@ struct cgfd_solver {
   int nmnt = 0, nfrc = 0, nstfm = 0, nstff = 0;
   std::vector<int> mloc, floc;
   std::vector<float> m6, f3;
+  std::vector<float> hmstf, hfstf;  // host copies of the source time functions
   int *d_mcell = nullptr, *d_fcell = nullptr;
   float *d_mcoef = nullptr, *d_fcoef = nullptr, *d_mstf = nullptr, *d_fstf = nullptr;
   // receivers
@@ -220,15 +247,23 @@ long ref_n(const cgfd_solver *h) {
   return (long)(h->d.ni + 6) * (h->d.nj + 6) * (h->d.nk + 6);
 }
 
-// host float array (reference layout) -> internal array at dst
-int upload_ref(cgfd_solver *h, const float *host, float *dst) {
+// host float array (reference layout) -> internal array at dst, stored as
+// element type elem in units of 1/isc
+int upload_ref(cgfd_solver *h, const float *host, void *dst, int elem = ELEM_F32,
+               float isc = 1.f) {
   const long n = ref_n(h);
   float *tmp = nullptr;
   CK(h, cudaMalloc(&tmp, n * sizeof(float)));
   cudaError_t e = cudaMemcpyAsync(tmp, host, n * sizeof(float), cudaMemcpyHostToDevice, h->st);
   if (e == cudaSuccess) {
-    to_internal_kernel<<<592, 256, 0, h->st>>>(tmp, dst, h->g, h->d.ni + 6, h->d.nj + 6,
-                                                h->d.nk + 6);
+    const int nx = h->d.ni + 6, ny = h->d.nj + 6, nz = h->d.nk + 6;
+    if (elem == ELEM_F16)
+      to_internal_kernel<<<592, 256, 0, h->st>>>(tmp, (__half *)dst, h->g, nx, ny, nz, isc);
+    else if (elem == ELEM_BF16)
+      to_internal_kernel<<<592, 256, 0, h->st>>>(tmp, (__nv_bfloat16 *)dst, h->g, nx, ny, nz,
+                                                  isc);
+    else
+      to_internal_kernel<<<592, 256, 0, h->st>>>(tmp, (float *)dst, h->g, nx, ny, nz, isc);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
@@ -237,12 +272,19 @@ int upload_ref(cgfd_solver *h, const float *host, float *dst) {
   return CGFD_OK;
 }
 
-int download_ref(cgfd_solver *h, const float *src, float *host) {
+int download_ref(cgfd_solver *h, const void *src, float *host, int elem = ELEM_F32,
+                 float sc = 1.f) {
   const long n = ref_n(h);
   float *tmp = nullptr;
   CK(h, cudaMalloc(&tmp, n * sizeof(float)));
-  to_reference_kernel<<<592, 256, 0, h->st>>>(src, tmp, h->g, h->d.ni + 6, h->d.nj + 6,
-                                               h->d.nk + 6);
+  const int nx = h->d.ni + 6, ny = h->d.nj + 6, nz = h->d.nk + 6;
+  if (elem == ELEM_F16)
+    to_reference_kernel<<<592, 256, 0, h->st>>>((const __half *)src, tmp, h->g, nx, ny, nz, sc);
+  else if (elem == ELEM_BF16)
+    to_reference_kernel<<<592, 256, 0, h->st>>>((const __nv_bfloat16 *)src, tmp, h->g, nx, ny,
+                                                 nz, sc);
+  else
+    to_reference_kernel<<<592, 256, 0, h->st>>>((const float *)src, tmp, h->g, nx, ny, nz, sc);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(host, tmp, n * sizeof(float), cudaMemcpyDeviceToHost, h->st);
@@ -327,6 +369,21 @@ void surface_matrices(const cgfd_solver *h, std::vector<float> &out) {
     }
 }
 
+// the receiver record of one step (after its four stages)
+void launch_record(cgfd_solver *h) {
+  Scales s;
+  for (int c = 0; c < NCOMP; ++c) s.sc[c] = std::ldexp(1.f, h->sexp[c]);
+  if (h->elem == ELEM_F16)
+    record_kernel<<<1, 256, 0, h->st>>>((const __half *)h->set[0], h->g.fstride, h->d_rcell,
+                                        h->nrecv, h->d.nt, h->d_seis, h->d_step, s);
+  else if (h->elem == ELEM_BF16)
+    record_kernel<<<1, 256, 0, h->st>>>((const __nv_bfloat16 *)h->set[0], h->g.fstride,
+                                        h->d_rcell, h->nrecv, h->d.nt, h->d_seis, h->d_step, s);
+  else
+    record_kernel<<<1, 256, 0, h->st>>>((const float *)h->set[0], h->g.fstride, h->d_rcell,
+                                        h->nrecv, h->d.nt, h->d_seis, h->d_step, s);
+}
+
 StageArgs stage_args(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, int out_set) {
   StageArgs a{};
   a.g = h->g;
@@ -339,6 +396,11 @@ StageArgs stage_args(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, in
   a.fw = h->set[0];
   a.out = h->set[out_set];
   a.tw = h->set[3];
+  a.elem = h->elem;
+  for (int c = 0; c < NCOMP; ++c) {
+    a.sc[c] = std::ldexp(1.f, h->sexp[c]);
+    a.isc[c] = std::ldexp(1.f, -h->sexp[c]);
+  }
   const size_t fs = h->g.fstride;
   a.lam2mu = h->media; a.mu = h->media + fs; a.irho = h->media + 2 * fs;
   a.zx = h->metric; a.zy = h->metric + fs; a.zz = h->metric + 2 * fs; a.jac = h->metric + 3 * fs;
@@ -385,7 +447,9 @@ int launch_stage(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, int ou
     s.step = h->d_step;
     s.adt = a.adt; s.bdt = a.bdt;
     s.out = a.out; s.tw = a.tw; s.rk = rk;
-    inject_sources_kernel<<<1, 32, 0, h->st>>>(s);
+    s.elem = a.elem;
+    for (int c = 0; c < NCOMP; ++c) s.isc[c] = a.isc[c];
+    launch_sources(s, h->st);
     CK(h, cudaGetLastError());
   }
   return CGFD_OK;
@@ -400,8 +464,7 @@ int enqueue_step(cgfd_solver *h, int p) {
     int st = launch_stage(h, rk, dd[0], dd[1], dd[2], ins[rk], outs[rk], -1);
     if (st) return st;
   }
-  record_kernel<<<1, 256, 0, h->st>>>(h->set[0], h->g.fstride, h->d_rcell, h->nrecv,
-                                      h->d.nt, h->d_seis, h->d_step);
+  launch_record(h);
   CK(h, cudaGetLastError());
   return CGFD_OK;
 }
@@ -442,7 +505,11 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
     return arg_fail(nullptr, "PML wider than the grid");
   if (d->con_index < LFD || d->con_index > d->nk + LFD - 1)
     return arg_fail(nullptr, "con_index must lie in [3, nk+2]");
-  if (d->storage != CGFD_STORE_F32) return arg_fail(nullptr, "storage type not supported");
+  if (d->storage != CGFD_STORE_F32 && d->storage != CGFD_STORE_F16 &&
+      d->storage != CGFD_STORE_BF16)
+    return arg_fail(nullptr, "unknown storage type");
+  if (d->storage != CGFD_STORE_F32 && d->kernel != CGFD_KERNEL_FUSED)
+    return arg_fail(nullptr, "16-bit storage runs on the default kernel family only");
   if (d->kernel != CGFD_KERNEL_FUSED && d->kernel != CGFD_KERNEL_SIMPLE &&
       d->kernel != CGFD_KERNEL_SCALAR)
     return arg_fail(nullptr, "unknown kernel family");
@@ -456,6 +523,9 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
 
   cgfd_solver *h = new cgfd_solver();
   h->d = *d;
+  h->elem = d->storage == CGFD_STORE_F16    ? ELEM_F16
+            : d->storage == CGFD_STORE_BF16 ? ELEM_BF16
+                                            : ELEM_F32;
   Geom &g = h->g;
   g.ni = d->ni; g.nj = d->nj; g.nk = d->nk;
   g.px = (int)align_up((size_t)XO + d->ni + 4, 32);
@@ -493,7 +563,8 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
     return CGFD_OK;
   };
   const size_t fs = g.fstride;
-  if (!st) st = alloc(&h->state, 4 * 9 * fs);
+  // the four field sets, 9 components of fs elements of the storage type each
+  if (!st) st = alloc((float **)&h->state, (4 * 9 * fs * elem_size(h->elem) + 3) / 4);
   if (!st) st = alloc(&h->media, 3 * fs);
   if (!st) st = alloc(&h->metric, 4 * fs);
   const size_t plen = align_up(g.px, 64) * 3 + align_up(g.nyi, 64) * 3 + align_up(g.nzi, 64) * 3;
@@ -517,11 +588,14 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
     delete h;
     return st;
   }
-  for (int q = 0; q < 4; ++q) h->set[q] = h->state + (size_t)q * 9 * fs;
+  for (int q = 0; q < 4; ++q)
+    h->set[q] = (char *)h->state + (size_t)q * 9 * fs * elem_size(h->elem);
   if (d->kernel == CGFD_KERNEL_FUSED || d->kernel == CGFD_KERNEL_SCALAR) {
+    float *fsets[4] = {(float *)h->set[0], (float *)h->set[1], (float *)h->set[2],
+                       (float *)h->set[3]};
     h->plan = (d->kernel == CGFD_KERNEL_FUSED)
-                  ? pair_create_plan(g, h->set, h->media, h->metric, h->aux)
-                  : fused_create_plan(g, h->set, h->media, h->metric);
+                  ? pair_create_plan(g, h->elem, h->set, h->media, h->metric, h->aux)
+                  : fused_create_plan(g, fsets, h->media, h->metric);
     if (!h->plan) {
       free_all(h);
       delete h;
@@ -670,8 +744,8 @@ int cgfd_upload_pml(cgfd_solver *h, const double *apdx, const double *apdy, cons
 
 static int upload_points(cgfd_solver *h, int n, const int *loc, int ncoef, const float *coef,
                          int nstf, const float *stf, std::vector<int> &hloc,
-                         std::vector<float> &hcoef, int *&dcell, float *&dstf, int &cnt,
-                         int &cnstf) {
+                         std::vector<float> &hcoef, std::vector<float> &hstf, int *&dcell,
+                         float *&dstf, int &cnt, int &cnstf) {
   if (n < 0 || (n > 0 && (!loc || !coef || !stf || nstf < 1))) return arg_fail(h, "bad sources");
   for (int q = 0; q < n; ++q)
     if (!valid_loc(h, loc + 3 * q)) return arg_fail(h, "source outside the valid grid");
@@ -680,6 +754,8 @@ static int upload_points(cgfd_solver *h, int n, const int *loc, int ncoef, const
   if (dstf) { cudaFree(dstf); dstf = nullptr; }
   hloc.assign(loc, loc + 3 * n);
   hcoef.assign(coef, coef + (size_t)ncoef * n);
+  if (n > 0) hstf.assign(stf, stf + (size_t)n * nstf);
+  else hstf.clear();
   cnt = n;
   cnstf = nstf;
   if (n > 0) {
@@ -697,15 +773,15 @@ static int upload_points(cgfd_solver *h, int n, const int *loc, int ncoef, const
 int cgfd_upload_moments(cgfd_solver *h, int n, const int *loc, const float *m6, int nstf,
                         const float *stf) {
   if (!h) return arg_fail(h, "null handle");
-  return upload_points(h, n, loc, 6, m6, nstf, stf, h->mloc, h->m6, h->d_mcell, h->d_mstf,
-                       h->nmnt, h->nstfm);
+  return upload_points(h, n, loc, 6, m6, nstf, stf, h->mloc, h->m6, h->hmstf, h->d_mcell,
+                       h->d_mstf, h->nmnt, h->nstfm);
 }
 
 int cgfd_upload_forces(cgfd_solver *h, int n, const int *loc, const float *f3, int nstf,
                        const float *stf) {
   if (!h) return arg_fail(h, "null handle");
-  return upload_points(h, n, loc, 3, f3, nstf, stf, h->floc, h->f3, h->d_fcell, h->d_fstf,
-                       h->nfrc, h->nstff);
+  return upload_points(h, n, loc, 3, f3, nstf, stf, h->floc, h->f3, h->hfstf, h->d_fcell,
+                       h->d_fstf, h->nfrc, h->nstff);
 }
 
 int cgfd_set_receivers(cgfd_solver *h, int n, const int *loc) {
@@ -726,6 +802,47 @@ int cgfd_set_receivers(cgfd_solver *h, int n, const int *loc) {
     CK(h, cudaMemset(h->d_seis, 0, ns * sizeof(float)));
   }
   invalidate(h);
+  return CGFD_OK;
+}
+
+// sets the per-component scale exponents of 16-bit storage, rescaling the
+// stored fields so that the values they stand for do not change
+static int apply_scales(cgfd_solver *h, const int *e) {
+  for (int c = 0; c < NCOMP; ++c) {
+    if (e[c] == h->sexp[c]) continue;
+    const float f = std::ldexp(1.f, h->sexp[c] - e[c]);
+    if (h->elem == ELEM_F16)
+      rescale_kernel<<<592, 256, 0, h->st>>>((__half *)h->state, h->g.fstride, c, f);
+    else if (h->elem == ELEM_BF16)
+      rescale_kernel<<<592, 256, 0, h->st>>>((__nv_bfloat16 *)h->state, h->g.fstride, c, f);
+    CK(h, cudaGetLastError());
+    h->sexp[c] = e[c];
+  }
+  CK(h, cudaStreamSynchronize(h->st));
+  return CGFD_OK;
+}
+
+int cgfd_set_field_scales(cgfd_solver *h, const int *exp2) {
+  if (!h || !exp2) return arg_fail(h, "null argument");
+  for (int c = 0; c < NCOMP; ++c)
+    if (exp2[c] < -60 || exp2[c] > 60) return arg_fail(h, "scale exponent out of range");
+  if (h->elem == ELEM_F32) {
+    for (int c = 0; c < NCOMP; ++c)
+      if (exp2[c] != 0) return arg_fail(h, "scales apply to 16-bit storage only");
+    return CGFD_OK;
+  }
+  DevGuard guard(h->d.device);
+  CK(h, cudaStreamSynchronize(h->st));
+  int st = apply_scales(h, exp2);
+  if (st) return st;
+  h->user_scales = true;
+  invalidate(h);
+  return CGFD_OK;
+}
+
+int cgfd_get_field_scales(cgfd_solver *h, int *exp2) {
+  if (!h || !exp2) return arg_fail(h, "null argument");
+  for (int c = 0; c < NCOMP; ++c) exp2[c] = h->sexp[c];
   return CGFD_OK;
 }
 
@@ -772,6 +889,54 @@ int cgfd_prepare(cgfd_solver *h) {
     }
     CK(h, cudaMalloc(&h->d_fcoef, c.size() * sizeof(float)));
     CK(h, cudaMemcpy(h->d_fcoef, c.data(), c.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if (h->elem == ELEM_F16 && !h->user_scales) {
+    // FP16 scale exponents from an estimate of the peak magnitudes: the
+    // stress a moment source builds at its cell is bounded by its rate
+    // coefficient M/(h^3 J) times the integral of |STF|; velocities follow
+    // through the impedance rho*vs (sigma ~ rho vs v), and a force's velocity
+    // rate f/(h^3 J rho) the other way round (sigma ~ rho vp v).  The peak is
+    // put at 2^12 stored units, 2^4 below the FP16 maximum.
+    const double dt2 = 0.5 * h->d.stept;
+    double sT = 0, sV = 0;
+    auto stf_int = [&](const std::vector<float> &stf, int q, int n) {
+      double a = 0;
+      for (int t = 0; t < n; ++t) a += std::fabs(stf[(size_t)q * n + t]) * dt2;
+      return a;
+    };
+    for (int q = 0; q < h->nmnt; ++q) {
+      const int cell = cell_of(h, &h->mloc[3 * q]);
+      float jac = 1.f, mu = 0.f, irho = 1.f;
+      CK(h, cell_value(h->metric + 3 * fs, cell, &jac));
+      CK(h, cell_value(h->media + fs, cell, &mu));
+      CK(h, cell_value(h->media + 2 * fs, cell, &irho));
+      double m = 0;
+      for (int c = 0; c < 6; ++c) m = std::fmax(m, std::fabs(h->m6[6 * q + c]));
+      const double sig = m / (h3 * jac) * stf_int(h->hmstf, q, h->nstfm);
+      const double z = std::sqrt(std::fmax((double)mu, 1e-30) / irho);  // rho vs
+      sT = std::fmax(sT, sig);
+      sV = std::fmax(sV, sig / z);
+    }
+    for (int q = 0; q < h->nfrc; ++q) {
+      const int cell = cell_of(h, &h->floc[3 * q]);
+      float jac = 1.f, l2m = 0.f, irho = 1.f;
+      CK(h, cell_value(h->metric + 3 * fs, cell, &jac));
+      CK(h, cell_value(h->media, cell, &l2m));
+      CK(h, cell_value(h->media + 2 * fs, cell, &irho));
+      double f = 0;
+      for (int c = 0; c < 3; ++c) f = std::fmax(f, std::fabs(h->f3[3 * q + c]));
+      const double v = 2.0 * f * irho / (h3 * jac) * stf_int(h->hfstf, q, h->nstff);
+      sV = std::fmax(sV, v);
+      sT = std::fmax(sT, v * std::sqrt(std::fmax((double)l2m, 1e-30) / irho));  // rho vp
+    }
+    auto ex = [](double peak) {
+      return peak > 0 ? (int)std::ceil(std::log2(peak / 4096.0)) : 0;
+    };
+    int e[NCOMP];
+    for (int c = 0; c < NCOMP; ++c) e[c] = c < 3 ? ex(sV) : ex(sT);
+    for (int c = 0; c < NCOMP; ++c) e[c] = e[c] < -60 ? -60 : (e[c] > 60 ? 60 : e[c]);
+    int st2 = apply_scales(h, e);
+    if (st2) return st2;
   }
   h->prepared = true;
   int st = build_graphs(h);
@@ -845,12 +1010,13 @@ int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms) {
           sa.step = h->d_step;
           sa.adt = a.adt; sa.bdt = a.bdt;
           sa.out = a.out; sa.tw = a.tw; sa.rk = rk;
-          inject_sources_kernel<<<1, 32, 0, h->st>>>(sa);
+          sa.elem = a.elem;
+          for (int c = 0; c < NCOMP; ++c) sa.isc[c] = a.isc[c];
+          launch_sources(sa, h->st);
           CK(h, cudaGetLastError());
         }
       }
-      record_kernel<<<1, 256, 0, h->st>>>(h->set[0], h->g.fstride, h->d_rcell, h->nrecv,
-                                          h->d.nt, h->d_seis, h->d_step);
+      launch_record(h);
       CK(h, cudaGetLastError());
     }
     h->steps++;
@@ -941,28 +1107,28 @@ int cgfd_get_seismograms(cgfd_solver *h, float *out, int *nt_done) {
   return CGFD_OK;
 }
 
-static float *set_ptr(cgfd_solver *h, int set, int comp) {
+static void *set_ptr(cgfd_solver *h, int set, int comp) {
   if (comp < 0 || comp > 8) return nullptr;
   int s;
   if (set == CGFD_SET_FW) s = 0;
   else if (set == CGFD_SET_W) s = h->wcur;
   else if (set == CGFD_SET_TW) s = 3;
   else return nullptr;
-  return h->set[s] + (size_t)comp * h->g.fstride;
+  return (char *)h->set[s] + (size_t)comp * h->g.fstride * elem_size(h->elem);
 }
 
 int cgfd_get_field(cgfd_solver *h, int set, int comp, float *out) {
   if (!h || !out) return arg_fail(h, "null argument");
-  float *p = set_ptr(h, set, comp);
+  void *p = set_ptr(h, set, comp);
   if (!p) return arg_fail(h, "bad set or component");
   DevGuard guard(h->d.device);
   CK(h, cudaStreamSynchronize(h->st));
-  return download_ref(h, p, out);
+  return download_ref(h, p, out, h->elem, std::ldexp(1.f, h->sexp[comp]));
 }
 
 int cgfd_set_field(cgfd_solver *h, int set, int comp, const float *in) {
   if (!h || !in) return arg_fail(h, "null argument");
-  float *p = set_ptr(h, set, comp);
+  void *p = set_ptr(h, set, comp);
   if (!p) return arg_fail(h, "bad set or component");
   DevGuard guard(h->d.device);
   CK(h, cudaStreamSynchronize(h->st));
@@ -976,14 +1142,19 @@ int cgfd_set_field(cgfd_solver *h, int set, int comp, const float *in) {
         const long t = ((long)i * ny + j) * nz + k;
         v[t] = in[t];
       }
-  return upload_ref(h, v.data(), p);
+  return upload_ref(h, v.data(), p, h->elem, std::ldexp(1.f, -h->sexp[comp]));
 }
 
 int cgfd_check_finite(cgfd_solver *h, long long *n_bad) {
   if (!h) return arg_fail(h, "null handle");
   DevGuard guard(h->d.device);
-  nonfinite_partial_kernel<<<h->nf_blocks, NF_THREADS, 0, h->st>>>(h->set[0], 9 * h->g.fstride,
-                                                                   h->d_partials);
+  if (h->elem == ELEM_F32)
+    nonfinite_partial_kernel<<<h->nf_blocks, NF_THREADS, 0, h->st>>>(
+        (const float *)h->set[0], 9 * h->g.fstride, h->d_partials);
+  else
+    nonfinite16_partial_kernel<<<h->nf_blocks, NF_THREADS, 0, h->st>>>(
+        (const uint16_t *)h->set[0], 9 * h->g.fstride,
+        (uint16_t)(h->elem == ELEM_F16 ? 0x7C00u : 0x7F80u), h->d_partials);
   CK(h, cudaGetLastError());
   nonfinite_sum_kernel<<<1, NF_THREADS, 0, h->st>>>(h->d_partials, h->nf_blocks);
   CK(h, cudaGetLastError());

@@ -286,7 +286,7 @@ __device__ __forceinline__ void vel_cell(const StageArgs &a, const Cell &e, cons
   }
 #pragma unroll
   for (int q = 0; q < 3; ++q)
-    rk_store<KIND>(a.out, a.tw, (size_t)(VX + q) * fs + e.c, pw.U0(q),
+    rk_store<KIND>(static_cast<float *>(a.out), static_cast<float *>(a.tw), (size_t)(VX + q) * fs + e.c, pw.U0(q),
                    KIND == 1 ? pw.U1(q) : 0.f, hw[q], a.adt, a.bdt);
 }
 
@@ -419,7 +419,7 @@ __device__ __forceinline__ void str_cell(const StageArgs &a, const Cell &e, cons
   }
 #pragma unroll
   for (int q = 0; q < 6; ++q)
-    rk_store<KIND>(a.out, a.tw, (size_t)(TXX + q) * fs + e.c, pw.U0(q),
+    rk_store<KIND>(static_cast<float *>(a.out), static_cast<float *>(a.tw), (size_t)(TXX + q) * fs + e.c, pw.U0(q),
                    KIND == 1 ? pw.U1(q) : 0.f, hw[q], a.adt, a.bdt);
 }
 
@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(TT, 3)
     };
     // planes below the chunk come straight from global memory (centre only)
     for (int p = z0 - LAG; p < z0; ++p) {
-      if (active) push(a.in + (size_t)C0 * fs, fs, gidx(g, e.ix, e.iy, p));
+      if (active) push(static_cast<const float *>(a.in) + (size_t)C0 * fs, fs, gidx(g, e.ix, e.iy, p));
       else push(ring, 0, 0);  // keeps the window shape; values unused
     }
     // A wait that expires sets the CTA-wide abort flag; the flag is read only

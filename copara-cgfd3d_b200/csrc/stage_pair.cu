@@ -27,24 +27,29 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 // 4-D map {x: nx, y: ny, z: nz, component: nc} over float arrays with the
 // given pitches (elements), box {bx, by, 1, bc}
-bool make_map(CUtensorMap *m, const float *base, int nx, int ny, int nz, int nc, size_t pitch_y,
-              size_t pitch_z, size_t pitch_c, int bx, int by, int bc) {
+bool make_map(CUtensorMap *m, const void *base, int nx, int ny, int nz, int nc, size_t pitch_y,
+              size_t pitch_z, size_t pitch_c, int bx, int by, int bc, int elem = ELEM_F32) {
   auto fn = encode_fn();
   if (!fn || !base) return false;
+  const size_t es_b = elem_size(elem);
   cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)nc};
-  cuuint64_t strides[3] = {(cuuint64_t)pitch_y * 4, (cuuint64_t)pitch_z * 4,
-                           (cuuint64_t)pitch_c * 4};
+  cuuint64_t strides[3] = {(cuuint64_t)(pitch_y * es_b), (cuuint64_t)(pitch_z * es_b),
+                           (cuuint64_t)(pitch_c * es_b)};
   cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)bc};
   cuuint32_t es[4] = {1, 1, 1, 1};
-  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)base, dims, strides, box, es,
+  const CUtensorMapDataType dt = elem == ELEM_F16    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                 : elem == ELEM_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                     : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  CUresult r = fn(m, dt, 4, (void *)base, dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
 // a map over ncomp arrays of the internal field layout
-bool field_map(CUtensorMap *m, const Geom &g, const float *base, int ncomp, int bx, int by,
-               int bc) {
-  return make_map(m, base, g.px, g.nyi, g.nzi, ncomp, g.px, g.plane, g.fstride, bx, by, bc);
+bool field_map(CUtensorMap *m, const Geom &g, const void *base, int ncomp, int bx, int by,
+               int bc, int elem = ELEM_F32) {
+  return make_map(m, base, g.px, g.nyi, g.nzi, ncomp, g.px, g.plane, g.fstride, bx, by, bc,
+                  elem);
 }
 // a map over one auxiliary set (9 components) of direction d
 bool aux_map(CUtensorMap *m, const Geom &g, int d, const float *base, int bc) {
@@ -78,23 +83,26 @@ bool pair_supported(const Geom &g) {
   return (XO % 4) == 0 && XO >= 4 && g.px % 32 == 0 && g.nk >= 4;
 }
 
-void *pair_create_plan(const Geom &g, float *const sets[4], const float *media,
+void *pair_create_plan(const Geom &g, int elem, void *const sets[4], const float *media,
                        const float *metric, float *const aux[3]) {
   static bool attrs = false;
   if (!attrs) {
-    attrs_v0(); attrs_v1(); attrs_v2();
-    attrs_s0(); attrs_s1(); attrs_s2();
+    attrs_fv0(); attrs_fv1(); attrs_fv2(); attrs_fs0(); attrs_fs1(); attrs_fs2();
+    attrs_hv0(); attrs_hv1(); attrs_hv2(); attrs_hs0(); attrs_hs1(); attrs_hs2();
+    attrs_bv0(); attrs_bv1(); attrs_bv2(); attrs_bs0(); attrs_bs1(); attrs_bs2();
     attrs = true;
   }
   Plan *pl = new (std::nothrow) Plan();
   if (!pl) return nullptr;
+  pl->elem = elem;
   bool ok = true;
   constexpr int NCV = PartInfo<PART_VEL>::NC, NCS = PartInfo<PART_STR>::NC;
+  const int hx = (elem == ELEM_F32) ? Halo<float>::HX : Halo<__half>::HX;
   for (int q = 0; q < 4; ++q) {
-    ok = ok && field_map(&pl->haloV[q], g, sets[q], 9, HX, HY, NCV);
-    ok = ok && field_map(&pl->haloS[q], g, sets[q], 9, HX, HY, NCS);
-    ok = ok && field_map(&pl->ctrV[q], g, sets[q], 9, CX, TY, 3);
-    ok = ok && field_map(&pl->ctrT[q], g, sets[q], 9, CX, TY, 6);
+    ok = ok && field_map(&pl->haloV[q], g, sets[q], 9, hx, HY, NCV, elem);
+    ok = ok && field_map(&pl->haloS[q], g, sets[q], 9, hx, HY, NCS, elem);
+    ok = ok && field_map(&pl->ctrV[q], g, sets[q], 9, CX, TY, 3, elem);
+    ok = ok && field_map(&pl->ctrT[q], g, sets[q], 9, CX, TY, 6, elem);
   }
   ok = ok && field_map(&pl->coefV, g, media, 3, CX, TY, PartInfo<PART_VEL>::NCOEF);
   ok = ok && field_map(&pl->coefS, g, media, 3, CX, TY, PartInfo<PART_STR>::NCOEF);
@@ -121,7 +129,10 @@ void *pair_create_plan(const Geom &g, float *const sets[4], const float *media,
   const int xorg = 0;
   const int ntx = (g.ni - xorg + CX - 1) / CX, nty = (g.nj + TY - 1) / TY;
   const int ntiles = ntx * nty;
-  const int rv = resident_vel(), rs = resident_str();
+  const int rv = elem == ELEM_F16 ? resident_hv() : elem == ELEM_BF16 ? resident_bv()
+                                                                    : resident_fv();
+  const int rs = elem == ELEM_F16 ? resident_hs() : elem == ELEM_BF16 ? resident_bs()
+                                                                    : resident_fs();
   const int G = rv < rs ? rv : rs;
   // (every chunk has at least 4 planes: the kernel's initial issue of four
   // entries relies on it)
@@ -218,16 +229,14 @@ void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *er
   }
   // both parts' item counters restart at zero
   cudaMemsetAsync(pl.wk.counter, 0, 2 * sizeof(int), s);
-  if (kind == 0) {
-    launch_v0(pl, mv, a, err, s);
-    launch_s0(pl, ms, a, err, s);
-  } else if (kind == 1) {
-    launch_v1(pl, mv, a, err, s);
-    launch_s1(pl, ms, a, err, s);
-  } else {
-    launch_v2(pl, mv, a, err, s);
-    launch_s2(pl, ms, a, err, s);
-  }
+  typedef void (*LaunchFn)(const Plan &, const Maps &, const StageArgs &, int *, cudaStream_t);
+  static const LaunchFn fns[3][2][3] = {
+      {{launch_fv0, launch_fv1, launch_fv2}, {launch_fs0, launch_fs1, launch_fs2}},
+      {{launch_hv0, launch_hv1, launch_hv2}, {launch_hs0, launch_hs1, launch_hs2}},
+      {{launch_bv0, launch_bv1, launch_bv2}, {launch_bs0, launch_bs1, launch_bs2}}};
+  const int e = pl.elem == ELEM_F16 ? 1 : pl.elem == ELEM_BF16 ? 2 : 0;
+  fns[e][0][kind](pl, mv, a, err, s);
+  fns[e][1][kind](pl, ms, a, err, s);
   launch_timg(a, s);
 }
 

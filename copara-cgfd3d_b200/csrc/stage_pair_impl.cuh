@@ -56,9 +56,15 @@ using namespace ptx;
 
 constexpr int TX = 32, TY = 4, TT = TX * TY;  // threads per CTA
 constexpr int CX = 2 * TX;                    // cells per tile row
-constexpr int HX = CX + 8, HY = TY + 6;       // halo box (x from -4, y from -3)
-constexpr int HPL = HX * HY;                  // floats per component per halo plane
-constexpr int PWT = CX * TY;                  // floats per pointwise tile
+constexpr int HY = TY + 6;                    // halo box rows (y from -3)
+constexpr int PWT = CX * TY;                  // values per pointwise tile
+// halo box columns per storage type: x from -HOFF, so that the box origin is
+// 16-byte aligned (x from -4 for FP32, -8 for 16-bit storage)
+template <typename T> struct Halo {
+  static constexpr int HOFF = (sizeof(T) == 4) ? 4 : 8;
+  static constexpr int HX = CX + 2 * HOFF;
+  static constexpr int HPL = HX * HY;  // values per component per halo plane
+};
 constexpr int NSLOT = 4;
 enum { PART_VEL = 0, PART_STR = 1 };
 #ifndef CGFD_PAIR_UNROLL
@@ -77,25 +83,37 @@ template <> struct PartInfo<PART_STR> {
   static constexpr int NC = 3, C0 = VX, NS = 6, S0 = TXX, NCOEF = 2, COEF0 = 0;
 };
 
-// Slot layout (floats): halo [NC][HY][HX], then pointwise tiles of PWT
-// floats: u0 [NS] (FW, or tW in the final stage), u1 [NS] (tW in the inner
-// stages), coef [NCOEF], met [3] (zeta_x, zeta_y, zeta_z).  Every region
-// starts on 128 B (a tensor copy's shared-memory destination must) and the
-// slot stride is a multiple of 128 B.
-template <int PART> struct Slot {
+// Slot layout (byte offsets): halo [NC][HY][HX] of the storage type T, then
+// pointwise tiles of PWT values: u0 [NS] (FW, or tW in the final stage) and
+// u1 [NS] (tW in the inner stages) of type T, coef [NCOEF] and met [3]
+// (zeta_x, zeta_y, zeta_z) of FP32.  Every region starts on 128 B (a tensor
+// copy's shared-memory destination must) and the slot stride is a multiple
+// of 128 B.
+constexpr uint32_t up128(uint32_t b) { return (b + 127u) / 128u * 128u; }
+template <typename T, int PART> struct Slot {
   static constexpr int NC = PartInfo<PART>::NC, NS = PartInfo<PART>::NS;
-  static constexpr uint32_t HALO_B = (uint32_t)(HPL * NC * 4);
-  static constexpr uint32_t HALO_F = (HALO_B + 127u) / 128u * 32u;  // floats, padded
-  static constexpr uint32_t U0 = HALO_F, U1 = U0 + NS * PWT, COEF = U1 + NS * PWT;
-  static constexpr uint32_t MET = COEF + PartInfo<PART>::NCOEF * PWT;
-  static constexpr uint32_t FLOATS = MET + 3 * PWT;
-  static constexpr uint32_t BYTES = FLOATS * 4;
+  static constexpr uint32_t HALO_B = (uint32_t)(Halo<T>::HPL * NC * sizeof(T));
+  static constexpr uint32_t U0 = up128(HALO_B);
+  static constexpr uint32_t U_B = (uint32_t)(NS * PWT * sizeof(T));  // one register set
+  static constexpr uint32_t U1 = U0 + up128(U_B);
+  static constexpr uint32_t COEF = U1 + up128(U_B);
+  static constexpr uint32_t MET = COEF + (uint32_t)(PartInfo<PART>::NCOEF * PWT * 4);
+  static constexpr uint32_t BYTES = MET + 3 * PWT * 4;
   static constexpr size_t SMEM = (size_t)NSLOT * BYTES + 128 + 128;  // + barriers, align slack
 };
-static_assert(Slot<PART_VEL>::BYTES % 128 == 0 && Slot<PART_STR>::BYTES % 128 == 0, "slots");
+static_assert(Slot<float, PART_VEL>::BYTES % 128 == 0 && Slot<float, PART_STR>::BYTES % 128 == 0,
+              "slots");
+static_assert(Slot<__half, PART_VEL>::BYTES % 128 == 0 && Slot<__half, PART_STR>::BYTES % 128 == 0,
+              "slots");
 // two CTAs per SM: 228 KB of shared memory per SM, 1 KB of it reserved per CTA
-static_assert(2 * (Slot<PART_VEL>::SMEM + 1024) <= 233472, "two velocity CTAs per SM");
-static_assert(2 * (Slot<PART_STR>::SMEM + 1024) <= 233472, "two stress CTAs per SM");
+static_assert(2 * (Slot<float, PART_VEL>::SMEM + 1024) <= 233472, "two velocity CTAs per SM");
+static_assert(2 * (Slot<float, PART_STR>::SMEM + 1024) <= 233472, "two stress CTAs per SM");
+
+// resident CTAs per SM the kernels are compiled for (registers <= 255): two.
+// With FP32 storage shared memory allows no more (four 27.5 KB slots per
+// CTA); with 16-bit storage three would fit, but at <= 168 registers the
+// stress part spills and the 400x400x200 hill ran 13% slower.
+template <typename T> struct MinCtas { static constexpr int value = 2; };
 
 // Tensor maps of one launch.  halo/u0/u1/coef/met feed the ring; the aux
 // maps (per direction: stage input, FA, tA) only drive L2 prefetches.
@@ -128,6 +146,13 @@ __device__ __forceinline__ f2 mul2(f2 a, f2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ f2 add2(f2 a, f2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ f2 neg2(f2 a) { return make_float2(-a.x, -a.y); }
 __device__ __forceinline__ f2 lds2(const float *p) { return *reinterpret_cast<const f2 *>(p); }
+// a pair of stored values (any storage type) as float2
+template <typename T> __device__ __forceinline__ f2 ldp(const T *p) { return Elem<T>::ld2(p); }
+// r times a power-of-two component scale; FP32 storage is unscaled
+template <typename T> __device__ __forceinline__ float scaled(float r, float s) {
+  if constexpr (sizeof(T) == 4) return r;
+  else return r * s;
+}
 
 // DRP/opt MacCormack 5-point operator on a pair, in the forward form
 // (m1 = p - s, c0 = p, p1..p3 = p + s..3s for the marching sign s; r = s/h)
@@ -142,22 +167,23 @@ __device__ __forceinline__ f2 drp2(f2 m1, f2 c0, f2 p1, f2 p2, f2 p3, float r) {
 
 // x-derivative of the pair (halo columns cb, cb+1 of row R) with the centre
 // pair C already in registers; r = X/h
-template <int X>
-__device__ __forceinline__ f2 dx_pair(const float *R, int cb, f2 C, float r) {
+template <int X, typename T>
+__device__ __forceinline__ f2 dx_pair(const T *R, int cb, f2 C, float r) {
   if constexpr (X > 0) {
-    const f2 La = lds2(R + cb - 2), Lb = lds2(R + cb + 2), Lc = lds2(R + cb + 4);
+    const f2 La = ldp(R + cb - 2), Lb = ldp(R + cb + 2), Lc = ldp(R + cb + 4);
     return drp2(F2(La.y, C.x), C, F2(C.y, Lb.x), Lb, F2(Lb.y, Lc.x), r);
   } else {
-    const f2 Lz = lds2(R + cb - 4), La = lds2(R + cb - 2), Lb = lds2(R + cb + 2);
+    const f2 Lz = ldp(R + cb - 4), La = ldp(R + cb - 2), Lb = ldp(R + cb + 2);
     return drp2(F2(C.y, Lb.x), C, F2(La.y, C.x), La, F2(Lz.y, La.x), r);
   }
 }
 // y-derivative of the pair from the component's halo plane P (row ry of
 // this thread, column cb), centre pair C in registers; r = Y/h
-template <int Y>
-__device__ __forceinline__ f2 dy_pair(const float *P, int ry, int cb, f2 C, float r) {
-  const f2 m1 = lds2(P + (ry - Y) * HX + cb), p1 = lds2(P + (ry + Y) * HX + cb);
-  const f2 p2 = lds2(P + (ry + 2 * Y) * HX + cb), p3 = lds2(P + (ry + 3 * Y) * HX + cb);
+template <int Y, typename T>
+__device__ __forceinline__ f2 dy_pair(const T *P, int ry, int cb, f2 C, float r) {
+  constexpr int HX = Halo<T>::HX;
+  const f2 m1 = ldp(P + (ry - Y) * HX + cb), p1 = ldp(P + (ry + Y) * HX + cb);
+  const f2 p2 = ldp(P + (ry + 2 * Y) * HX + cb), p3 = ldp(P + (ry + 3 * Y) * HX + cb);
   return drp2(m1, C, p1, p2, p3, r);
 }
 
@@ -178,20 +204,40 @@ __device__ __forceinline__ void st2(float *p0, float *p1, int m, f2 v) {
     if (m & 2) *p1 = v.y;
   }
 }
+// the same for a field set of storage type T (second cell at p + 1)
+template <typename T>
+__device__ __forceinline__ f2 ldt2(const T *p, int m) {
+  if (m == 3) return Elem<T>::ld2(p);
+  f2 r = F2(0.f, 0.f);
+  if (m & 1) r.x = Elem<T>::ld(p);
+  if (m & 2) r.y = Elem<T>::ld(p + 1);
+  return r;
+}
+template <typename T>
+__device__ __forceinline__ void stt2(T *p, int m, f2 v) {
+  if (m == 3) {
+    Elem<T>::st2(p, v);
+  } else {
+    if (m & 1) Elem<T>::st(p, v.x);
+    if (m & 2) Elem<T>::st(p + 1, v.y);
+  }
+}
 
 // RK update of one pair (Iteration*): KIND 0 first stage (u0 = FW),
-// 1 inner (u0 = FW, u1 = tW), 2 final (u0 = tW)
-template <int KIND>
-__device__ __forceinline__ void rk_store2(float *out, float *tw, int m, f2 u0, f2 u1, f2 hh,
-                                          float adt, float bdt) {
+// 1 inner (u0 = FW, u1 = tW), 2 final (u0 = tW).  u0, u1 and the outputs are
+// in stored units; adt, bdt carry the component's inverse scale (every set of
+// a component shares its scale).
+template <int KIND, typename T>
+__device__ __forceinline__ void rk_store2(T *out, T *tw, int m, f2 u0, f2 u1, f2 hh, float adt,
+                                          float bdt) {
   if (KIND == 0) {
-    st2(out, out + 1, m, fma2(S2(adt), hh, u0));
-    st2(tw, tw + 1, m, fma2(S2(bdt), hh, u0));
+    stt2(out, m, fma2(S2(adt), hh, u0));
+    stt2(tw, m, fma2(S2(bdt), hh, u0));
   } else if (KIND == 1) {
-    st2(out, out + 1, m, fma2(S2(adt), hh, u0));
-    st2(tw, tw + 1, m, fma2(S2(bdt), hh, u1));
+    stt2(out, m, fma2(S2(adt), hh, u0));
+    stt2(tw, m, fma2(S2(bdt), hh, u1));
   } else {
-    st2(out, out + 1, m, fma2(S2(bdt), hh, u0));
+    stt2(out, m, fma2(S2(bdt), hh, u0));
   }
 }
 
@@ -274,10 +320,12 @@ struct Plane {
 };
 
 // Pointwise operands of this thread's pair in the current slot.
+template <typename T>
 struct Pw2 {
-  const float *u0, *u1, *coef, *met;
-  __device__ f2 U0(int q) const { return lds2(u0 + q * PWT); }
-  __device__ f2 U1(int q) const { return lds2(u1 + q * PWT); }
+  const T *u0, *u1;
+  const float *coef, *met;
+  __device__ f2 U0(int q) const { return ldp(u0 + q * PWT); }
+  __device__ f2 U1(int q) const { return ldp(u1 + q * PWT); }
   __device__ f2 C(int q) const { return lds2(coef + q * PWT); }
   __device__ f2 M(int q) const { return lds2(met + q * PWT); }
 };
@@ -308,14 +356,22 @@ struct AuxIdx {
 // layers' velocities come from the traction-image kernel (timg.cu); only
 // their z auxiliaries are updated here.
 // w[s][q]: staged component s on plane iz + (3 - q) * Z (q = 3: this plane).
-template <int X, int Y, int Z, int KIND>
+template <typename T, int X, int Y, int Z, int KIND>
 __device__ __forceinline__ void vel_pair(const StageArgs &a, const Pair &e, const Plane &pl,
-                                         const float *H, int ry, int cb, const Pw2 &pw,
+                                         const T *H, int ry, int cb, const Pw2<T> &pw,
                                          const f2 (&w)[6][5], float rx, float rys, float rz) {
+  constexpr int HX = Halo<T>::HX, HPL = Halo<T>::HPL;
   const size_t fs = a.g.fstride;
-  auto dx = [&](int s) { return dx_pair<X>(H + s * HPL + ry * HX, cb, w[s][3], rx); };
-  auto dy = [&](int s) { return dy_pair<Y>(H + s * HPL, ry, cb, w[s][3], rys); };
-  auto dz = [&](int s) { return drp2(w[s][4], w[s][3], w[s][2], w[s][1], w[s][0], rz); };
+  // 1/h factors carry the staged component's scale (stored units -> values)
+  auto sr = [&](float r, int s) { return scaled<T>(r, a.sc[TXX + s]); };
+  auto dx = [&](int s) { return dx_pair<X>(H + s * HPL + ry * HX, cb, w[s][3], sr(rx, s)); };
+  auto dy = [&](int s) { return dy_pair<Y>(H + s * HPL, ry, cb, w[s][3], sr(rys, s)); };
+  auto dz = [&](int s) {
+    return drp2(w[s][4], w[s][3], w[s][2], w[s][1], w[s][0], sr(rz, s));
+  };
+  T *out = static_cast<T *>(a.out), *tw = static_cast<T *>(a.tw);
+  auto adt = [&](int c) { return scaled<T>(a.adt, a.isc[c]); };
+  auto bdt = [&](int c) { return scaled<T>(a.bdt, a.isc[c]); };
 
   if (pl.lean) {
     const f2 irho = pw.C(0);
@@ -339,8 +395,8 @@ __device__ __forceinline__ void vel_pair(const StageArgs &a, const Pair &e, cons
     }
 #pragma unroll
     for (int q = 0; q < 3; ++q)
-      rk_store2<KIND>(a.out + (VX + q) * fs + pl.c, a.tw + (VX + q) * fs + pl.c, 3, pw.U0(q),
-                      KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], a.adt, a.bdt);
+      rk_store2<KIND>(out + (VX + q) * fs + pl.c, tw + (VX + q) * fs + pl.c, 3, pw.U0(q),
+                      KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], adt(VX + q), bdt(VX + q));
     return;
   }
 
@@ -410,8 +466,8 @@ __device__ __forceinline__ void vel_pair(const StageArgs &a, const Pair &e, cons
   if (!xy) return;
 #pragma unroll
   for (int q = 0; q < 3; ++q)
-    rk_store2<KIND>(a.out + (VX + q) * fs + pl.c, a.tw + (VX + q) * fs + pl.c, e.m, pw.U0(q),
-                    KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], a.adt, a.bdt);
+    rk_store2<KIND>(out + (VX + q) * fs + pl.c, tw + (VX + q) * fs + pl.c, e.m, pw.U0(q),
+                    KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], adt(VX + q), bdt(VX + q));
 }
 
 // --------------------------- stress part ----------------------------------
@@ -426,15 +482,21 @@ __device__ __forceinline__ f2 mat_row(const float *mv, size_t plane, int r, f2 u
               fma2(lds2(mv + (r + 1) * plane), v, mul2(lds2(mv + r * plane), u)));
 }
 
-template <int X, int Y, int Z, int KIND>
+template <typename T, int X, int Y, int Z, int KIND>
 __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, const Plane &pl,
-                                         const float *H, int ry, int cb, const Pw2 &pw,
+                                         const T *H, int ry, int cb, const Pw2<T> &pw,
                                          const f2 (&w)[3][5], float rx, float rys, float rz) {
+  constexpr int HX = Halo<T>::HX, HPL = Halo<T>::HPL;
   const Geom &g = a.g;
   const size_t fs = g.fstride;
-  auto dx = [&](int s) { return dx_pair<X>(H + s * HPL + ry * HX, cb, w[s][3], rx); };
-  auto dy = [&](int s) { return dy_pair<Y>(H + s * HPL, ry, cb, w[s][3], rys); };
-  auto dz = [&](int s) { return drp2(w[s][4], w[s][3], w[s][2], w[s][1], w[s][0], rz); };
+  // 1/h factors carry the staged component's scale (stored units -> values)
+  auto sr = [&](float r, int s) { return scaled<T>(r, a.sc[VX + s]); };
+  auto dx = [&](int s) { return dx_pair<X>(H + s * HPL + ry * HX, cb, w[s][3], sr(rx, s)); };
+  auto dy = [&](int s) { return dy_pair<Y>(H + s * HPL, ry, cb, w[s][3], sr(rys, s)); };
+  auto dz = [&](int s) {
+    return drp2(w[s][4], w[s][3], w[s][2], w[s][1], w[s][0], sr(rz, s));
+  };
+  T *out = static_cast<T *>(a.out), *tw = static_cast<T *>(a.tw);
 
   // general path: issue every stage-input auxiliary load before the stencil
   const bool gen = !pl.lean;
@@ -463,13 +525,13 @@ __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, cons
     DzVz = add2(mat_row(mv + 9 * g.plane, g.plane, 6, DyVx, DyVy, DyVz),
                 mat_row(mv, g.plane, 6, DxVx, DxVy, DxVz));
   } else if (pl.iz == g.top - 1) {  // 2-point (M22)
-    DzVx = mul2(add2(w[0][2], neg2(w[0][3])), S2(rz));
-    DzVy = mul2(add2(w[1][2], neg2(w[1][3])), S2(rz));
-    DzVz = mul2(add2(w[2][2], neg2(w[2][3])), S2(rz));
+    DzVx = mul2(add2(w[0][2], neg2(w[0][3])), S2(sr(rz, 0)));
+    DzVy = mul2(add2(w[1][2], neg2(w[1][3])), S2(sr(rz, 1)));
+    DzVz = mul2(add2(w[2][2], neg2(w[2][3])), S2(sr(rz, 2)));
   } else if (pl.iz == g.top - 2) {  // Gottlieb 2-4 (M24)
     auto m24 = [&](int s) {
       return mul2(fma2(S2(CGFD_MA2), w[s][1], fma2(S2(CGFD_MA1), w[s][2],
-                                                  mul2(S2(CGFD_MA0), w[s][3]))), S2(rz));
+                                                  mul2(S2(CGFD_MA0), w[s][3]))), S2(sr(rz, s)));
     };
     DzVx = m24(0);
     DzVy = m24(1);
@@ -568,17 +630,19 @@ __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, cons
   const int m = gen ? e.m : 3;
 #pragma unroll
   for (int q = 0; q < 6; ++q)
-    rk_store2<KIND>(a.out + (TXX + q) * fs + pl.c, a.tw + (TXX + q) * fs + pl.c, m, pw.U0(q),
-                    KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], a.adt, a.bdt);
+    rk_store2<KIND>(out + (TXX + q) * fs + pl.c, tw + (TXX + q) * fs + pl.c, m, pw.U0(q),
+                    KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], scaled<T>(a.adt, a.isc[TXX + q]),
+                    scaled<T>(a.bdt, a.isc[TXX + q]));
 }
 
 // ------------------------------ the march ---------------------------------
 // items: tile index fastest, so the CTAs resident at one time work on
 // neighbouring tiles of the same z-chunk and share halo rows in L2
-template <int PART, int X, int Y, int Z, int KIND>
-__global__ void __launch_bounds__(TT, 2)
+template <typename T, int PART, int X, int Y, int Z, int KIND>
+__global__ void __launch_bounds__(TT, MinCtas<T>::value)
     pair_kernel(const __grid_constant__ Maps maps, const StageArgs a, const Work wk, int *err) {
-  using S = Slot<PART>;
+  using S = Slot<T, PART>;
+  constexpr int HOFF = Halo<T>::HOFF, HX = Halo<T>::HX, HPL = Halo<T>::HPL;
   constexpr int NC = PartInfo<PART>::NC, C0 = PartInfo<PART>::C0;
   constexpr int NS = PartInfo<PART>::NS, S0 = PartInfo<PART>::S0;
   constexpr int NCOEF = PartInfo<PART>::NCOEF, COEF0 = PartInfo<PART>::COEF0;
@@ -586,7 +650,7 @@ __global__ void __launch_bounds__(TT, 2)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // align the ring on the shared-window address itself
   unsigned char *sbase = smem_raw + ((128u - (su32(smem_raw) & 127u)) & 127u);
-  float *ring = reinterpret_cast<float *>(sbase);
+  unsigned char *ring = sbase;  // NSLOT slots of S::BYTES
   uint64_t *bars = reinterpret_cast<uint64_t *>(sbase + (size_t)NSLOT * S::BYTES);
   __shared__ int abort_flag;
 
@@ -595,14 +659,14 @@ __global__ void __launch_bounds__(TT, 2)
   const size_t fs = g.fstride;
   const bool flat = a.flat;
   // bytes one plane delivers: halo always, pointwise only for computed planes
-  const uint32_t pw_bytes = (uint32_t)(PWT * 4) *
-      (NS * (KIND == 1 ? 2 : 1) + NCOEF + (flat ? 0 : 3));
+  const uint32_t pw_bytes = S::U_B * (KIND == 1 ? 2u : 1u) +
+                            (uint32_t)(PWT * 4) * (NCOEF + (flat ? 0 : 3));
 
   if (tid == 0) {
     abort_flag = 0;
     bool aligned = ((su32(bars) & 7u) == 0);
     for (int s = 0; s < NSLOT; ++s)
-      aligned = aligned && ((su32(ring + (size_t)s * S::FLOATS) & 127u) == 0);
+      aligned = aligned && ((su32(ring + (size_t)s * S::BYTES) & 127u) == 0);
     if (!aligned) {
       abort_flag = 1;
       if (err) atomicExch(err, 2);
@@ -617,7 +681,7 @@ __global__ void __launch_bounds__(TT, 2)
   uint32_t ph = 0;    // parity of the next wait, per slot (same in every thread)
   uint32_t pend = 0;  // thread 0: slots with a copy not yet waited for
   const float rx = (float)X / a.h, rys = (float)Y / a.h, rz = (float)Z / a.h;
-  const int ry = ty + 3, cb = 4 + 2 * tx;
+  const int ry = ty + 3, cb = HOFF + 2 * tx;
   const int sc = ry * HX + cb;       // this pair inside a halo plane
   const int tc = ty * CX + 2 * tx;   // this pair inside a pointwise tile
   const int zlo = LFD + g.nabs[4], zhi = g.nk + LFD - g.nabs[5];  // z interior [zlo, zhi)
@@ -627,13 +691,13 @@ __global__ void __launch_bounds__(TT, 2)
   // only) go to ring slot (base + q) & 3, base counting the entries of the
   // CTA's earlier items; thread 0 issues, every thread waits, in order.
   auto issue = [&](const int4 it, int q, int s) {  // thread 0 only
-    float *slot = ring + (size_t)s * S::FLOATS;
+    unsigned char *slot = ring + (size_t)s * S::BYTES;
     const int i0 = it.x, j0 = it.y, n = it.w - it.z;
     const int p = ((DIR > 0) ? it.z : it.w - 1) + DIR * q;
     const bool compute = q < n;
     fence_proxy_async();
     mbar_expect_tx(&bars[s], S::HALO_B + (compute ? pw_bytes : 0u));
-    tma_load(slot, &maps.halo, XO + i0 - 4, j0, p, C0, &bars[s]);
+    tma_load(slot, &maps.halo, XO + i0 - HOFF, j0, p, C0, &bars[s]);
     if (compute) {
       const int cx = XO + i0, cy = LFD + j0;
       tma_load(slot + S::U0, &maps.u0, cx, cy, p, S0, &bars[s]);
@@ -728,12 +792,13 @@ __global__ void __launch_bounds__(TT, 2)
     for (int c = 0; c < NC; ++c)
 #pragma unroll
       for (int q = 0; q < 5; ++q) w[c][q] = S2(0.f);
-    auto push_smem = [&](const float *plane) {
+    auto push_smem = [&](const unsigned char *slot) {
+      const T *plane = reinterpret_cast<const T *>(slot);
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) w[c][q] = w[c][q + 1];
-        w[c][4] = lds2(plane + c * HPL + sc);
+        w[c][4] = ldp(plane + c * HPL + sc);
       }
     };
     // the three planes behind the chunk come straight from global memory
@@ -743,13 +808,13 @@ __global__ void __launch_bounds__(TT, 2)
       for (int c = 0; c < NC; ++c) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) w[c][q] = w[c][q + 1];
-        const float *src = a.in + (size_t)(C0 + c) * fs + o;
-        w[c][4] = e.m ? ld2(src, src + 1, e.m) : S2(0.f);
+        const T *src = static_cast<const T *>(a.in) + (size_t)(C0 + c) * fs + o;
+        w[c][4] = e.m ? ldt2(src, e.m) : S2(0.f);
       }
     }
     // A wait that expires sets the CTA-wide abort flag; the flag is read only
     // after a __syncthreads, so every thread leaves the march together.
-    if (wait(0)) push_smem(ring + (size_t)(base & (NSLOT - 1)) * S::FLOATS);
+    if (wait(0)) push_smem(ring + (size_t)(base & (NSLOT - 1)) * S::BYTES);
     else abort_flag = 1;
     __syncthreads();
 
@@ -757,10 +822,10 @@ __global__ void __launch_bounds__(TT, 2)
 #pragma unroll MARCH_UNROLL
     for (int q = 0; q < n; ++q) {
       const bool got = wait(q + 1);
-      if (got) push_smem(ring + (size_t)((base + q + 1) & (NSLOT - 1)) * S::FLOATS);
+      if (got) push_smem(ring + (size_t)((base + q + 1) & (NSLOT - 1)) * S::BYTES);
       else abort_flag = 1;
       if (e.m && got) {
-        const float *slot = ring + (size_t)((base + q) & (NSLOT - 1)) * S::FLOATS;
+        const unsigned char *slot = ring + (size_t)((base + q) & (NSLOT - 1)) * S::BYTES;
         Plane pl;
         pl.iz = zf + DIR * q;
         pl.k = pl.iz - LFD;
@@ -770,12 +835,15 @@ __global__ void __launch_bounds__(TT, 2)
         pl.zpml = (pl.iz < zlo) || (pl.iz >= zhi);
         pl.curved = pl.iz >= g.con && !flat;
         pl.lean = tile_int && !pl.zpml && !pl.near_top;
-        const Pw2 pw{slot + S::U0 + tc, slot + S::U1 + tc, slot + S::COEF + tc,
-                     slot + S::MET + tc};
+        const Pw2<T> pw{reinterpret_cast<const T *>(slot + S::U0) + tc,
+                        reinterpret_cast<const T *>(slot + S::U1) + tc,
+                        reinterpret_cast<const float *>(slot + S::COEF) + tc,
+                        reinterpret_cast<const float *>(slot + S::MET) + tc};
+        const T *H = reinterpret_cast<const T *>(slot);
         if constexpr (PART == PART_VEL)
-          vel_pair<X, Y, Z, KIND>(a, e, pl, slot, ry, cb, pw, w, rx, rys, rz);
+          vel_pair<T, X, Y, Z, KIND>(a, e, pl, H, ry, cb, pw, w, rx, rys, rz);
         else
-          str_pair<X, Y, Z, KIND>(a, e, pl, slot, ry, cb, pw, w, rx, rys, rz);
+          str_pair<T, X, Y, Z, KIND>(a, e, pl, H, ry, cb, pw, w, rx, rys, rz);
       }
       // the slot of entry q is free: refill it with stream position
       // base + q + NSLOT (this item's entry q + 4, or the next item's)
@@ -805,72 +873,76 @@ struct Plan {
   // auxiliaries: [direction][FA, A, tA], boxes of V (3) and T (6) components
   CUtensorMap auxV[3][3], auxT[3][3];
   Work wk;
+  int elem;     // storage element type of the field sets
   int zchunk;   // planes of the interior z-chunks
   int grid[2];
 };
 
-template <int PART, int X, int Y, int Z, int KIND>
+template <typename T, int PART, int X, int Y, int Z, int KIND>
 void launch_t(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
-  pair_kernel<PART, X, Y, Z, KIND><<<pl.grid[PART], dim3(TX, TY, 1), Slot<PART>::SMEM, s>>>(
-      m, a, pl.wk, err);
+  pair_kernel<T, PART, X, Y, Z, KIND>
+      <<<pl.grid[PART], dim3(TX, TY, 1), Slot<T, PART>::SMEM, s>>>(m, a, pl.wk, err);
 }
 
-template <int PART, int KIND>
+template <typename T, int PART, int KIND>
 void launch_dirs(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
   const int code = (a.X > 0 ? 4 : 0) + (a.Y > 0 ? 2 : 0) + (a.Z > 0 ? 1 : 0);
   switch (code) {
-    case 0: launch_t<PART, -1, -1, -1, KIND>(pl, m, a, err, s); break;
-    case 1: launch_t<PART, -1, -1, 1, KIND>(pl, m, a, err, s); break;
-    case 2: launch_t<PART, -1, 1, -1, KIND>(pl, m, a, err, s); break;
-    case 3: launch_t<PART, -1, 1, 1, KIND>(pl, m, a, err, s); break;
-    case 4: launch_t<PART, 1, -1, -1, KIND>(pl, m, a, err, s); break;
-    case 5: launch_t<PART, 1, -1, 1, KIND>(pl, m, a, err, s); break;
-    case 6: launch_t<PART, 1, 1, -1, KIND>(pl, m, a, err, s); break;
-    default: launch_t<PART, 1, 1, 1, KIND>(pl, m, a, err, s); break;
+    case 0: launch_t<T, PART, -1, -1, -1, KIND>(pl, m, a, err, s); break;
+    case 1: launch_t<T, PART, -1, -1, 1, KIND>(pl, m, a, err, s); break;
+    case 2: launch_t<T, PART, -1, 1, -1, KIND>(pl, m, a, err, s); break;
+    case 3: launch_t<T, PART, -1, 1, 1, KIND>(pl, m, a, err, s); break;
+    case 4: launch_t<T, PART, 1, -1, -1, KIND>(pl, m, a, err, s); break;
+    case 5: launch_t<T, PART, 1, -1, 1, KIND>(pl, m, a, err, s); break;
+    case 6: launch_t<T, PART, 1, 1, -1, KIND>(pl, m, a, err, s); break;
+    default: launch_t<T, PART, 1, 1, 1, KIND>(pl, m, a, err, s); break;
   }
 }
 
-template <int PART, int KIND>
+template <typename T, int PART, int KIND>
 void set_attrs() {
   auto set = [](const void *f) {
-    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Slot<PART>::SMEM);
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)Slot<T, PART>::SMEM);
   };
-  set((const void *)pair_kernel<PART, -1, -1, -1, KIND>);
-  set((const void *)pair_kernel<PART, -1, -1, 1, KIND>);
-  set((const void *)pair_kernel<PART, -1, 1, -1, KIND>);
-  set((const void *)pair_kernel<PART, -1, 1, 1, KIND>);
-  set((const void *)pair_kernel<PART, 1, -1, -1, KIND>);
-  set((const void *)pair_kernel<PART, 1, -1, 1, KIND>);
-  set((const void *)pair_kernel<PART, 1, 1, -1, KIND>);
-  set((const void *)pair_kernel<PART, 1, 1, 1, KIND>);
+  set((const void *)pair_kernel<T, PART, -1, -1, -1, KIND>);
+  set((const void *)pair_kernel<T, PART, -1, -1, 1, KIND>);
+  set((const void *)pair_kernel<T, PART, -1, 1, -1, KIND>);
+  set((const void *)pair_kernel<T, PART, -1, 1, 1, KIND>);
+  set((const void *)pair_kernel<T, PART, 1, -1, -1, KIND>);
+  set((const void *)pair_kernel<T, PART, 1, -1, 1, KIND>);
+  set((const void *)pair_kernel<T, PART, 1, 1, -1, KIND>);
+  set((const void *)pair_kernel<T, PART, 1, 1, 1, KIND>);
 }
 
-template <int PART>
+template <typename T, int PART>
 int resident_ctas() {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pair_kernel<PART, 1, 1, 1, 1>, TT,
-                                                Slot<PART>::SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pair_kernel<T, PART, 1, 1, 1, 1>, TT,
+                                                Slot<T, PART>::SMEM);
   if (per < 1) per = 1;
   if (sms < 1) sms = 1;
   return per * sms;
 }
 
-// per-(part, kind) entry points, one translation unit each (pair_*.cu)
-#define CGFD_PAIR_DECL(P, K)                                                          \
-  void launch_##P##K(const Plan &pl, const Maps &m, const StageArgs &a, int *err,   \
-                     cudaStream_t s);                                                \
-  void attrs_##P##K();
-CGFD_PAIR_DECL(v, 0)
-CGFD_PAIR_DECL(v, 1)
-CGFD_PAIR_DECL(v, 2)
-CGFD_PAIR_DECL(s, 0)
-CGFD_PAIR_DECL(s, 1)
-CGFD_PAIR_DECL(s, 2)
+// per-(storage, part, kind) entry points, one translation unit each
+// (pair_{f,h,b}{v,s}{0,1,2}.cu; f: FP32, h: FP16, b: BF16 storage)
+#define CGFD_PAIR_DECL(E, P, K)                                                          \
+  void launch_##E##P##K(const Plan &pl, const Maps &m, const StageArgs &a, int *err,   \
+                        cudaStream_t s);                                                \
+  void attrs_##E##P##K();
+#define CGFD_PAIR_DECL_E(E)                                                   \
+  CGFD_PAIR_DECL(E, v, 0) CGFD_PAIR_DECL(E, v, 1) CGFD_PAIR_DECL(E, v, 2)     \
+  CGFD_PAIR_DECL(E, s, 0) CGFD_PAIR_DECL(E, s, 1) CGFD_PAIR_DECL(E, s, 2)     \
+  int resident_##E##v();                                                      \
+  int resident_##E##s();
+CGFD_PAIR_DECL_E(f)
+CGFD_PAIR_DECL_E(h)
+CGFD_PAIR_DECL_E(b)
+#undef CGFD_PAIR_DECL_E
 #undef CGFD_PAIR_DECL
-int resident_vel();
-int resident_str();
 
 }  // namespace pair
 }  // namespace cgfd

@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(128) stage_simple_kernel(StageArgs a) {
   const long c = (long)gidx(g, ix, iy, iz);
   const long sx = 1, sy = g.px, sz = (long)g.plane;
   const size_t fs = g.fstride;
-  const float *in = a.in;
+  const float *in = static_cast<const float *>(a.in);  // FP32 storage only
   const float *Vx = in + VX * fs, *Vy = in + VY * fs, *Vz = in + VZ * fs;
   const float *Txx = in + TXX * fs, *Tyy = in + TYY * fs, *Tzz = in + TZZ * fs;
   const float *Txy = in + TXY * fs, *Txz = in + TXZ * fs, *Tyz = in + TYZ * fs;
@@ -246,8 +246,8 @@ __global__ void __launch_bounds__(128) stage_simple_kernel(StageArgs a) {
   }
 
   // ---- RK update (Iteration*) ----
-  float *out = a.out, *tw = a.tw;
-  const float *fw = a.fw;
+  float *out = static_cast<float *>(a.out), *tw = static_cast<float *>(a.tw);
+  const float *fw = static_cast<const float *>(a.fw);
 #pragma unroll
   for (int q = 0; q < 9; ++q) {
     const size_t o = q * fs + c;

@@ -22,7 +22,9 @@ __device__ __forceinline__ float drp5(float m1, float c0, float p1, float p2, fl
   return (CGFD_DA_1 * m1 + CGFD_DA0 * c0 + CGFD_DA1 * p1 + CGFD_DA2 * p2 + CGFD_DA3 * p3) * r;
 }
 
+template <typename T>
 __global__ void __launch_bounds__(128) timg_kernel(StageArgs a) {
+  using E = Elem<T>;
   const Geom &g = a.g;
   const int i = blockIdx.x * 32 + threadIdx.x;
   const int j = blockIdx.y * 4 + threadIdx.y;
@@ -45,23 +47,27 @@ __global__ void __launch_bounds__(128) timg_kernel(StageArgs a) {
   const size_t py = ((size_t)iz * g.nya + ya) * g.px + ix;
   const int kind = a.rk == 0 ? 0 : (a.rk < 3 ? 1 : 2);
   constexpr int TC[3][3] = {{TXX, TXY, TXZ}, {TXY, TYY, TYZ}, {TXZ, TYZ, TZZ}};
-  const float *in = a.in;
+  const T *in = static_cast<const T *>(a.in);
+  const T *fw = static_cast<const T *>(a.fw);
+  T *out = static_cast<T *>(a.out), *tw = static_cast<T *>(a.tw);
 
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
-    const float *T1 = in + TC[q][0] * fs, *T2 = in + TC[q][1] * fs, *T3 = in + TC[q][2] * fs;
+    const T *T1 = in + TC[q][0] * fs, *T2 = in + TC[q][1] * fs, *T3 = in + TC[q][2] * fs;
+    // stored units to values (exact powers of two)
+    const float s1 = a.sc[TC[q][0]], s2 = a.sc[TC[q][1]], s3 = a.sc[TC[q][2]];
     float vx[5], vy[5], vz[7];
 #pragma unroll
     for (int d = -1; d <= 3; ++d) {
       const long gx = c + a.X * d, gy = c + a.Y * d * sy;
-      vx[d + 1] = (a.flat ? 1.f : a.jac[gx]) * T1[gx];
-      vy[d + 1] = (a.flat ? 1.f : a.jac[gy]) * T2[gy];
+      vx[d + 1] = (a.flat ? 1.f : a.jac[gx]) * (E::ld(T1 + gx) * s1);
+      vy[d + 1] = (a.flat ? 1.f : a.jac[gy]) * (E::ld(T2 + gy) * s2);
     }
 #pragma unroll
     for (int n = 0; n < 7; ++n) {
       const long gz = c + (n - 3) * sz;
-      vz[n] = a.flat ? T3[gz]
-                     : a.jac[gz] * (a.zx[gz] * T1[gz] + a.zy[gz] * T2[gz] + a.zz[gz] * T3[gz]);
+      const float t1 = E::ld(T1 + gz) * s1, t2 = E::ld(T2 + gz) * s2, t3 = E::ld(T3 + gz) * s3;
+      vz[n] = a.flat ? t3 : a.jac[gz] * (a.zx[gz] * t1 + a.zy[gz] * t2 + a.zz[gz] * t3);
     }
     if (s == 0) {
       vz[3] = 0.f; vz[4] = -vz[2]; vz[5] = -vz[1]; vz[6] = -vz[0];
@@ -103,17 +109,19 @@ __global__ void __launch_bounds__(128) timg_kernel(StageArgs a) {
     }
     if (xpml) aux(0, px, hax);
     if (ypml) aux(1, py, hay);
+    // RK update in stored units (every set of a component shares its scale)
     const size_t o = (size_t)(VX + q) * fs + c;
+    const float adt = a.adt * a.isc[VX + q], bdt = a.bdt * a.isc[VX + q];
     if (kind == 0) {
-      const float u0 = in[o];
-      a.out[o] = u0 + a.adt * hv;
-      a.tw[o] = u0 + a.bdt * hv;
+      const float u0 = E::ld(in + o);
+      E::st(out + o, u0 + adt * hv);
+      E::st(tw + o, u0 + bdt * hv);
     } else if (kind == 1) {
-      const float u0 = a.fw[o], u1 = a.tw[o];
-      a.out[o] = u0 + a.adt * hv;
-      a.tw[o] = u1 + a.bdt * hv;
+      const float u0 = E::ld(fw + o), u1 = E::ld(tw + o);
+      E::st(out + o, u0 + adt * hv);
+      E::st(tw + o, u1 + bdt * hv);
     } else {
-      a.out[o] = a.tw[o] + a.bdt * hv;
+      E::st(out + o, E::ld(tw + o) + bdt * hv);
     }
   }
 }
@@ -123,7 +131,12 @@ __global__ void __launch_bounds__(128) timg_kernel(StageArgs a) {
 void launch_timg(const StageArgs &a, void *stream) {
   dim3 block(32, 4, 1);
   dim3 grid((a.g.ni + 31) / 32, (a.g.nj + 3) / 4, 3);
-  timg_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(a);
+  if (a.elem == ELEM_F16)
+    timg_kernel<__half><<<grid, block, 0, (cudaStream_t)stream>>>(a);
+  else if (a.elem == ELEM_BF16)
+    timg_kernel<__nv_bfloat16><<<grid, block, 0, (cudaStream_t)stream>>>(a);
+  else
+    timg_kernel<float><<<grid, block, 0, (cudaStream_t)stream>>>(a);
 }
 
 }  // namespace cgfd

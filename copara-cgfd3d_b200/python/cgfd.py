@@ -66,6 +66,8 @@ _SIGS = {
     "cgfd_get_field": (C.c_int, [_P, C.c_int, C.c_int, _fp]),
     "cgfd_set_field": (C.c_int, [_P, C.c_int, C.c_int, _fp]),
     "cgfd_check_finite": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
+    "cgfd_set_field_scales": (C.c_int, [_P, _ip]),
+    "cgfd_get_field_scales": (C.c_int, [_P, _ip]),
     "cgfd_count_nonfinite_noalloc": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_longlong),
                                                C.c_void_p]),
     "cgfd_metric_from_coords": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double,
@@ -234,6 +236,17 @@ class Solver:
         if st not in (OK, ERR_NONFINITE):
             self._chk(st)
         return n.value
+
+    def set_field_scales(self, exp2) -> None:
+        """Scale exponents of 16-bit storage per component (stored value s
+        stands for s * 2**exp2[c])."""
+        e = (C.c_int * 9)(*[int(x) for x in exp2])
+        self._chk(_lib.cgfd_set_field_scales(self._h, e))
+
+    def field_scales(self) -> list:
+        e = (C.c_int * 9)()
+        self._chk(_lib.cgfd_get_field_scales(self._h, e))
+        return list(e)
 
 
 NOALLOC_MAX_VALUES = 16384 * 8192

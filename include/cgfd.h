@@ -175,6 +175,17 @@ int cgfd_set_field(cgfd_solver *h, int set, int comp, const float *in);
  * Returns CGFD_ERR_NONFINITE when the count is not zero. */
 int cgfd_check_finite(cgfd_solver *h, long long *n_bad);
 
+/* Per-component scale exponents of 16-bit storage: a stored value s of
+ * component c stands for s * 2^exp2[c] (exact: powers of two).  FP16 storage
+ * picks them at cgfd_prepare from the sources and the medium (the estimated
+ * peak lands at 2^12 stored units); BF16 keeps them at 0 (its exponent range
+ * is FP32's).  Setting them rescales the stored fields so that the values
+ * they stand for do not change, and keeps them from then on.  FP32 storage
+ * accepts only zeros.  exp2: 9 ints in [-60, 60].
+ * No reference counterpart (the reference stores FP32 only). */
+int cgfd_set_field_scales(cgfd_solver *h, const int *exp2);
+int cgfd_get_field_scales(cgfd_solver *h, int *exp2);
+
 /* NaN/Inf count of any float array on the device (d_values, n values), the
  * same count cgfd_check_finite makes for a solver's wavefield, for callers
  * that cannot call cudaMalloc when they run the check: a host application

@@ -67,3 +67,14 @@ def test_create_rejects_pml_on_top_and_oversized_pml():
     d = cgfd.make_desc(20, 20, 20, 100.0, 0.005, 10, 10, (12, 12, 4, 4, 4, 0))
     with pytest.raises(cgfd.CgfdError):
         cgfd.Solver(d)
+
+
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_16bit_storage_needs_the_default_kernel(kernel):
+    import cgfd
+    d = cgfd.make_desc(20, 20, 20, 100.0, 0.005, 10, 10, (4, 4, 4, 4, 4, 0),
+                       storage=cgfd.STORE_BF16, kernel=kernel)
+    with pytest.raises(cgfd.CgfdError) as e:
+        cgfd.Solver(d)
+    assert e.value.status == cgfd.ERR_ARG
+    assert "16-bit" in cgfd.last_error(None)

@@ -1,0 +1,81 @@
+"""16-bit field storage (FP16 with per-component power-of-two scales, BF16):
+the nine wavefields and the RK registers are stored at 16 bits, the
+arithmetic stays FP32.  There is no reference counterpart to match bit for
+bit; the checks are accuracy bounds against the solver's own FP32 storage
+(which matches the reference within 1e-5) on the same inputs, plus exact
+properties of the storage conversions and scales.
+
+Measured on a B200 (seismogram relative L2 of Vx..Vz against FP32 storage):
+small flat 60 steps FP16 1.7e-3 / BF16 1.5e-2; small hill FP16 2.8e-3 / BF16
+9.3e-3; the 160x160x80 flat half-space, 500 steps, FP16 7.0e-3 / BF16 6.3e-2.
+The bounds below leave about 3x margin.
+"""
+import numpy as np
+import pytest
+
+import cgfd
+import models
+from helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+STORES = {"f16": cgfd.STORE_F16, "bf16": cgfd.STORE_BF16}
+
+
+def _run(m, steps, storage):
+    s = cgfd.Solver(m.desc(storage=storage))
+    m.load(s)
+    s.step(steps)
+    seis, nbad, scales = s.seismograms(), s.check_finite(), s.field_scales()
+    s.close()
+    return seis, nbad, scales
+
+
+@pytest.mark.parametrize("name,bound", [("small_flat", {"f16": 6e-3, "bf16": 5e-2}),
+                                        ("small_hill", {"f16": 1e-2, "bf16": 3e-2})])
+@pytest.mark.parametrize("store", list(STORES))
+def test_16bit_storage_tracks_fp32_storage(name, bound, store):
+    m = getattr(models, name)(nt=60)
+    ref, nbad, _ = _run(m, 60, cgfd.STORE_F32)
+    seis, nbad16, scales = _run(m, 60, STORES[store])
+    assert nbad == 0 and nbad16 == 0
+    e = rel_l2(seis[:3], ref[:3])
+    assert e < bound[store], (name, store, e, scales)
+
+
+@pytest.mark.parametrize("store,bound,peak", [("f16", 2e-2, 1e-2), ("bf16", 0.2, 0.1)])
+def test_flat_halfspace_160x160x80_500_steps_16bit(store, bound, peak):
+    """The FP16/BF16 variant of the 160x160x80 flat half-space model."""
+    m = models.config_c1()
+    ref, _, _ = _run(m, m.nt, cgfd.STORE_F32)
+    seis, nbad, scales = _run(m, m.nt, STORES[store])
+    assert nbad == 0
+    assert rel_l2(seis[:3], ref[:3]) < bound
+    pk, pk_ref = np.abs(seis[:3]).max(), np.abs(ref[:3]).max()
+    assert abs(pk - pk_ref) / pk_ref < peak
+    if store == "f16":
+        assert scales[0] != 0 or scales[3] != 0  # the automatic scales were set
+    else:
+        assert scales == [0] * 9
+
+
+@pytest.mark.parametrize("store,ulp", [("f16", 2.0 ** -11), ("bf16", 2.0 ** -8)])
+def test_field_round_trip_and_rescale_are_exact(store, ulp):
+    m = models.small_flat(nt=4)
+    s = cgfd.Solver(m.desc(storage=STORES[store]))
+    m.load(s)
+    rng = np.random.default_rng(5)
+    f = np.zeros(m.shape, np.float32)
+    f[3:-3, 3:-3, 3:-3] = rng.standard_normal((m.ni, m.nj, m.nk)).astype(np.float32) * 100.0
+    s.set_field(4, f)
+    g = s.get_field(4)
+    v = f[3:-3, 3:-3, 3:-3]
+    assert np.all(np.abs(g[3:-3, 3:-3, 3:-3] - v) <= ulp * np.abs(v) + 1e-30)
+    assert not np.any(g[:3]) and not np.any(g[-3:])  # ghosts stay zero
+    # a power-of-two rescale does not change the values the fields stand for
+    e = s.field_scales()
+    e2 = [x + 3 for x in e]
+    s.set_field_scales(e2)
+    assert s.field_scales() == e2
+    assert np.array_equal(s.get_field(4), g)
+    s.close()
