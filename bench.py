@@ -40,7 +40,10 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--kernel", choices=("fused", "simple", "scalar"), default="fused")
-    p.add_argument("--config", choices=("hill400", "flat160", "hill256"), default="hill400")
+    p.add_argument("--config", choices=("hill400", "flat160", "hill256", "batch64"),
+                   default="hill400")
+    p.add_argument("--autotune", action="store_true",
+                   help="tune the work list before timing (state unchanged)")
     p.add_argument("--storage", choices=("f32", "f16", "bf16"), default="f32",
                    help="storage type of the field sets (arithmetic is FP32)")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -61,7 +64,59 @@ def build_model(cfg, nt):
 def workload_name(cfg):
     return {"hill400": "gaussian_hill_400x400x200_pml20",
             "flat160": "flat_halfspace_160x160x80_pml12",
-            "hill256": "gaussian_hill_256x256x128_pml20"}[cfg]
+            "hill256": "gaussian_hill_256x256x128_pml20",
+            "batch64": "batch_64_hill_models_96-256_pml12"}[cfg]
+
+
+def run_batch(args, dist, rank, world, local):
+    """64 uneven hill models (seed 7) stepped together as one batch."""
+    import cgfd
+    import models
+    K, W = args.steps, args.warmup
+    ms_models = models.batch_models(n=64, seed=7, nt=W + K + 2 + (4 if args.autotune else 0))
+    b = cgfd.Batch([m.desc(device=local) for m in ms_models])
+    for m, s in zip(ms_models, b.models):
+        m.load(s)
+    b.prepare()
+    tuned = None
+    if args.autotune:
+        tuned = b.autotune(steps=1)
+    b.step(W)
+    b.sync()
+    barrier(dist)
+    with ClockSampler(local) as clk:
+        ms = b.step_timed(K)
+    ms = allmax(dist, ms)
+    cells = sum(m.cells for m in ms_models)
+    nbad = sum(s.check_finite() for s in b.models)
+    b.close()
+    if rank != 0:
+        return
+    value = world * cells * K / (ms / 1e3) / 1e9
+    bps = sum(algorithmic_bytes_per_step(m) for m in ms_models)
+    achieved = bps / (ms / K / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    n_src = sum(1 for m in ms_models if len(m.mnt_loc) + len(m.frc_loc))
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded model generator)",
+        "config": {"workload": workload_name(args.config), "models": len(ms_models),
+                   "cells": cells, "kernel": "fused", "storage": "f32", "replicas": world,
+                   "autotuned_ms_per_step": tuned,
+                   "l2": "state >> L2 (126 MB), no flush needed",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                     "algorithmic_bytes_per_step": bps,
+                     "launch": "whole batched step (4 stages: velocity + stress pair_kernel, "
+                               "timg, sources; receiver record)"},
+        "clocks": clk.summary(),
+        "gpu_launches": K * (4 * (3 + (1 if n_src else 0)) + 1),
+        "nonfinite": nbad,
+    }
+    print(json.dumps(line))
 
 
 def algorithmic_bytes_per_step(m, elem=4):
@@ -254,6 +309,11 @@ def main():
         run_reference(args)
         return
     dist, rank, world, local = dist_init(args.gpus)
+    if args.config == "batch64":
+        run_batch(args, dist, rank, world, local)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     import cgfd
     kernel = {"fused": cgfd.KERNEL_FUSED, "simple": cgfd.KERNEL_SIMPLE,
               "scalar": cgfd.KERNEL_SCALAR}[args.kernel]
@@ -265,6 +325,7 @@ def main():
     s = cgfd.Solver(m.desc(kernel=kernel, device=local, storage=storage))
     m.load(s)
     s.prepare()
+    tuned = s.autotune(steps=2) if args.autotune else None
     s.step(W)
     s.sync()
     barrier(dist)
@@ -311,6 +372,7 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded model generator)",
         "config": {"workload": workload_name(args.config), "cells": m.cells,
                    "kernel": args.kernel, "storage": args.storage, "replicas": world,
+                   "autotuned_ms_per_step": tuned,
                    "l2": "state >> L2 (126 MB), no flush needed",
                    "parallelism": "replicas" if world > 1 else "single"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -145,12 +145,35 @@ void launch_stage_fused(const void *plan, const StageArgs &a, int in_set, int *e
 int fused_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str);
 // The paired kernels (two x-adjacent cells per thread, stage_pair.cu); aux
 // holds the three directions' auxiliary arrays (null: no PML there).
+// Shape of the paired kernels' work list (the autotuner's knobs): about
+// items_per_cta items per resident CTA, z-chunks of at least min_chunk
+// planes, PML columns weighted (1 + pml_weight per direction) in the cost
+// order.
+struct WorkParams {
+  int items_per_cta = 6;
+  int min_chunk = 16;
+  double pml_weight = 1.0;
+};
 bool pair_supported(const Geom &g);
+bool pair_set_work(void *plan, const WorkParams &wp);
+WorkParams pair_get_work(const void *plan);
 void *pair_create_plan(const Geom &g, int elem, void *const sets[4], const float *media,
                        const float *metric, float *const aux[3]);
 void pair_destroy_plan(void *plan);
 void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *err,
                        void *stream);
 int pair_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str);
+// A batch of models (FP32 storage) in one persistent launch per stage part:
+// per-model buffers as n x 4 sets, n media, n metrics, n x 3 auxiliaries.
+void *pair_create_batch_plan(int n, const Geom *gs, void *const *sets, const float *const *media,
+                             const float *const *metric, float *const *aux);
+// the models' stage arguments, [pattern * 4 + stage][model]
+bool pair_batch_set_args(void *plan, const StageArgs *args);
+// both parts and the traction image of stage rep.rk (step pattern `pattern`)
+// for every model; rep carries the stage's X, Y, Z and rk
+void launch_stage_pair_batch(const void *plan, int pattern, const StageArgs &rep, int *err,
+                             void *stream);
+// the traction image of n models (args: device array, one per model)
+void launch_timg_batch(const StageArgs *args, int n, int max_ni, int max_nj, void *stream);
 
 }  // namespace cgfd

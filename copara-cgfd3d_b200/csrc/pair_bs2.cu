@@ -6,7 +6,7 @@ namespace cgfd {
 namespace pair {
 
 void launch_bs2(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
-  launch_dirs<__nv_bfloat16, PART_STR, 2>(pl, m, a, err, s);
+  launch_dirs<__nv_bfloat16, PART_STR, 2>(pl, m, a, pl.wk, err, s);
 }
 
 void attrs_bs2() { set_attrs<__nv_bfloat16, PART_STR, 2>(); }

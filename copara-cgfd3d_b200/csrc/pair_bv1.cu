@@ -6,7 +6,7 @@ namespace cgfd {
 namespace pair {
 
 void launch_bv1(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
-  launch_dirs<__nv_bfloat16, PART_VEL, 1>(pl, m, a, err, s);
+  launch_dirs<__nv_bfloat16, PART_VEL, 1>(pl, m, a, pl.wk, err, s);
 }
 
 void attrs_bv1() { set_attrs<__nv_bfloat16, PART_VEL, 1>(); }

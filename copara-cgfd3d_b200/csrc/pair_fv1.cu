@@ -1,16 +1,24 @@
 // pair_fv1.cu -- instantiates the paired velocity kernels of RK stage kind
-// 1 (inner stages) with FP32 storage for the 8 stencil directions.
+// 1 (inner stages) with FP32 storage for the 8 stencil directions,
+// single-model and batched.
 #include "stage_pair_impl.cuh"
 
 namespace cgfd {
 namespace pair {
 
 void launch_fv1(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
-  launch_dirs<float, PART_VEL, 1>(pl, m, a, err, s);
+  launch_dirs<float, PART_VEL, 1>(pl, m, a, pl.wk, err, s);
 }
 
 void attrs_fv1() { set_attrs<float, PART_VEL, 1>(); }
 
 int resident_fv() { return resident_ctas<float, PART_VEL>(); }
+void launch_fv1_b(const Plan &pl, const StageArgs &a, const Work &wk, int *err,
+                 cudaStream_t s) {
+  launch_dirs<float, PART_VEL, 1, true>(pl, Maps{}, a, wk, err, s);
+}
+
+void attrs_fv1_b() { set_attrs<float, PART_VEL, 1, true>(); }
+int resident_fv_b() { return resident_ctas<float, PART_VEL, true>(); }
 }  // namespace pair
 }  // namespace cgfd

@@ -1,15 +1,22 @@
 // pair_fv2.cu -- instantiates the paired velocity kernels of RK stage kind
-// 2 (final stage) with FP32 storage for the 8 stencil directions.
+// 2 (final stage) with FP32 storage for the 8 stencil directions,
+// single-model and batched.
 #include "stage_pair_impl.cuh"
 
 namespace cgfd {
 namespace pair {
 
 void launch_fv2(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
-  launch_dirs<float, PART_VEL, 2>(pl, m, a, err, s);
+  launch_dirs<float, PART_VEL, 2>(pl, m, a, pl.wk, err, s);
 }
 
 void attrs_fv2() { set_attrs<float, PART_VEL, 2>(); }
 
+void launch_fv2_b(const Plan &pl, const StageArgs &a, const Work &wk, int *err,
+                 cudaStream_t s) {
+  launch_dirs<float, PART_VEL, 2, true>(pl, Maps{}, a, wk, err, s);
+}
+
+void attrs_fv2_b() { set_attrs<float, PART_VEL, 2, true>(); }
 }  // namespace pair
 }  // namespace cgfd

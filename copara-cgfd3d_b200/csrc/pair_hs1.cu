@@ -6,7 +6,7 @@ namespace cgfd {
 namespace pair {
 
 void launch_hs1(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
-  launch_dirs<__half, PART_STR, 1>(pl, m, a, err, s);
+  launch_dirs<__half, PART_STR, 1>(pl, m, a, pl.wk, err, s);
 }
 
 void attrs_hs1() { set_attrs<__half, PART_STR, 1>(); }

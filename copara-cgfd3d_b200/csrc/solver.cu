@@ -74,9 +74,8 @@ __global__ void to_reference_kernel(const T *__restrict__ src, float *__restrict
 // to the stage output; one thread walks the list so that repeated cells add
 // up in a fixed order.
 template <typename T>
-__global__ void inject_sources_kernel(SourceArgs s) {
+__device__ void inject_sources_body(const SourceArgs &s) {
   using E = Elem<T>;
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int t2 = (s.tindex >= 0) ? s.tindex : 2 * (*s.step) + s.tinc;
   const size_t fs = s.g.fstride;
   T *out = static_cast<T *>(s.out), *tw = static_cast<T *>(s.tw);
@@ -102,6 +101,14 @@ __global__ void inject_sources_kernel(SourceArgs s) {
     for (int m = 0; m < 3; ++m) add(VX + m, (size_t)(VX + m) * fs + c, stf * s.fcoef[3 * q + m]);
   }
 }
+template <typename T>
+__global__ void inject_sources_kernel(SourceArgs s) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) inject_sources_body<T>(s);
+}
+// a batch of models (FP32 storage): block b injects model b's sources
+__global__ void inject_sources_batch_kernel(const SourceArgs *sa) {
+  if (threadIdx.x == 0) inject_sources_body<float>(sa[blockIdx.x]);
+}
 void launch_sources(const SourceArgs &s, cudaStream_t st) {
   if (s.elem == ELEM_F16) inject_sources_kernel<__half><<<1, 32, 0, st>>>(s);
   else if (s.elem == ELEM_BF16) inject_sources_kernel<__nv_bfloat16><<<1, 32, 0, st>>>(s);
@@ -114,9 +121,9 @@ struct Scales {
   float sc[NCOMP];
 };
 template <typename T>
-__global__ void record_kernel(const T *__restrict__ fw, size_t fstride,
-                              const int *__restrict__ cells, int nrecv, int nt,
-                              float *__restrict__ seis, int *step, Scales s) {
+__device__ void record_body(const T *__restrict__ fw, size_t fstride,
+                            const int *__restrict__ cells, int nrecv, int nt,
+                            float *__restrict__ seis, int *step, const Scales &s) {
   const int t = *step;
   for (int q = threadIdx.x; q < 9 * nrecv; q += blockDim.x) {
     const int c = q / nrecv, r = q % nrecv;
@@ -126,6 +133,26 @@ __global__ void record_kernel(const T *__restrict__ fw, size_t fstride,
   }
   __syncthreads();
   if (threadIdx.x == 0) *step = t + 1;
+}
+template <typename T>
+__global__ void record_kernel(const T *__restrict__ fw, size_t fstride,
+                              const int *__restrict__ cells, int nrecv, int nt,
+                              float *__restrict__ seis, int *step, Scales s) {
+  record_body<T>(fw, fstride, cells, nrecv, nt, seis, step, s);
+}
+// receiver record of one model of a batch (FP32 storage)
+struct RecordArgs {
+  const float *fw;
+  size_t fstride;
+  const int *cells;
+  int nrecv, nt;
+  float *seis;
+  int *step;
+  Scales s;
+};
+__global__ void record_batch_kernel(const RecordArgs *ra) {
+  const RecordArgs &r = ra[blockIdx.x];
+  record_body<float>(r.fw, r.fstride, r.cells, r.nrecv, r.nt, r.seis, r.step, r.s);
 }
 
 // multiplies component comp of the four field sets by factor (a power of two:
@@ -1167,6 +1194,420 @@ int cgfd_check_finite(cgfd_solver *h, long long *n_bad) {
     h->err = "non-finite values in the wavefield";
     return CGFD_ERR_NONFINITE;
   }
+  return CGFD_OK;
+}
+
+
+}  // extern "C"
+
+// ------------------------- autotuning, batches -----------------------------
+
+// Device state of a solver that a tuning run changes: the field sets, the
+// ADE auxiliaries, the seismograms; saved before and put back after.
+struct Snapshot {
+  std::vector<std::pair<void *, size_t>> bufs;  // (device buffer, bytes)
+  std::vector<void *> copies;
+  int steps = 0;
+};
+static int snapshot_take(cgfd_solver *h, Snapshot &sn) {
+  sn.bufs.clear();
+  sn.bufs.push_back({h->state, 4 * 9 * h->g.fstride * elem_size(h->elem)});
+  for (int d = 0; d < 3; ++d)
+    if (h->aux[d]) sn.bufs.push_back({h->aux[d], 3 * 9 * h->g.astride[d] * sizeof(float)});
+  if (h->d_seis)
+    sn.bufs.push_back({h->d_seis, (size_t)9 * h->nrecv * (h->d.nt > 0 ? h->d.nt : 1) * 4});
+  sn.steps = h->steps;
+  for (auto &b : sn.bufs) {
+    void *c = nullptr;
+    CK(h, cudaMalloc(&c, b.second));
+    sn.copies.push_back(c);
+    CK(h, cudaMemcpyAsync(c, b.first, b.second, cudaMemcpyDeviceToDevice, h->st));
+  }
+  CK(h, cudaStreamSynchronize(h->st));
+  return CGFD_OK;
+}
+static int snapshot_restore(cgfd_solver *h, Snapshot &sn) {
+  for (size_t q = 0; q < sn.bufs.size(); ++q)
+    CK(h, cudaMemcpyAsync(sn.bufs[q].first, sn.copies[q], sn.bufs[q].second,
+                          cudaMemcpyDeviceToDevice, h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  for (void *c : sn.copies) cudaFree(c);
+  sn.copies.clear();
+  h->steps = sn.steps;
+  return CGFD_OK;
+}
+// the work-list shapes the autotuner tries
+static std::vector<WorkParams> tuning_candidates() {
+  std::vector<WorkParams> v;
+  for (int ipc : {3, 6, 12})
+    for (int mc : {12, 24})
+      for (double pw : {1.0, 2.0}) v.push_back(WorkParams{ipc, mc, pw});
+  return v;
+}
+
+extern "C" {
+
+int cgfd_autotune(cgfd_solver *h, int steps, float *best_ms) {
+  if (!h || steps < 1) return arg_fail(h, "bad arguments");
+  if (h->d.kernel != CGFD_KERNEL_FUSED) return arg_fail(h, "autotuning needs the default kernel");
+  int st = cgfd_prepare(h);
+  if (st) return st;
+  DevGuard guard(h->d.device);
+  Snapshot sn;
+  st = snapshot_take(h, sn);
+  if (st) return st;
+  float best = 1e30f;
+  WorkParams bestp = pair_get_work(h->plan);
+  for (const WorkParams &wp : tuning_candidates()) {
+    if (!pair_set_work(h->plan, wp)) continue;
+    h->graphs_ok = false;
+    st = build_graphs(h);
+    if (st) break;
+    h->steps = sn.steps;
+    float ms = 0;
+    st = cgfd_step(h, 1);  // warm-up
+    if (!st) st = cgfd_step_timed(h, steps, &ms, nullptr);
+    if (st) break;
+    if (ms < best) { best = ms; bestp = wp; }
+  }
+  int st2 = snapshot_restore(h, sn);
+  if (!st) st = st2;
+  if (!pair_set_work(h->plan, bestp) && !st) st = cuda_fail(h, cudaErrorUnknown, "work list");
+  h->graphs_ok = false;
+  if (!st) st = build_graphs(h);
+  if (best_ms) *best_ms = best / steps;
+  return st;
+}
+
+}  // extern "C"
+
+struct cgfd_batch {
+  std::vector<cgfd_solver *> m;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  void *plan = nullptr;
+  int *d_err = nullptr;
+  SourceArgs *d_src = nullptr;   // [stage][model]
+  RecordArgs *d_rec = nullptr;   // [model]
+  bool any_src = false;
+  cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev = nullptr;      // orders the batch's and the members' streams
+  bool ready = false;
+  int steps = 0;
+  std::string err;
+};
+
+static int batch_fail(cgfd_batch *b, int code, const std::string &msg) {
+  if (b) b->err = msg;
+  set_global_error(msg.c_str());
+  return code;
+}
+#define BCK(b, call)                                                                  \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return batch_fail((b), CGFD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+static void batch_free(cgfd_batch *b) {
+  for (auto &g : b->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  if (b->plan) { pair_destroy_plan(b->plan); b->plan = nullptr; }
+  cudaFree(b->d_err);
+  cudaFree(b->d_src);
+  cudaFree(b->d_rec);
+  b->d_err = nullptr; b->d_src = nullptr; b->d_rec = nullptr;
+  if (b->ev) { cudaEventDestroy(b->ev); b->ev = nullptr; }
+  if (b->st) { cudaStreamDestroy(b->st); b->st = nullptr; }
+}
+
+// the batched step of pattern p: per stage one launch per part over every
+// model, the traction image, the sources; then the receiver record
+static int batch_enqueue(cgfd_batch *b, int p, const std::vector<StageArgs> &args) {
+  const int n = (int)b->m.size();
+  for (int rk = 0; rk < 4; ++rk) {
+    launch_stage_pair_batch(b->plan, p, args[(size_t)(p * 4 + rk) * n], b->d_err, b->st);
+    BCK(b, cudaGetLastError());
+    if (b->any_src) {
+      inject_sources_batch_kernel<<<n, 32, 0, b->st>>>(b->d_src + (size_t)rk * n);
+      BCK(b, cudaGetLastError());
+    }
+  }
+  record_batch_kernel<<<n, 256, 0, b->st>>>(b->d_rec);
+  BCK(b, cudaGetLastError());
+  return CGFD_OK;
+}
+
+static int batch_build(cgfd_batch *b) {
+  const int n = (int)b->m.size();
+  static const int ins[4] = {0, 1, 2, 1}, outs[4] = {1, 2, 1, 0};
+  std::vector<StageArgs> args((size_t)16 * n);
+  std::vector<SourceArgs> src((size_t)4 * n);
+  std::vector<RecordArgs> rec(n);
+  b->any_src = false;
+  for (int i = 0; i < n; ++i) {
+    cgfd_solver *h = b->m[i];
+    for (int p = 0; p < 4; ++p)
+      for (int rk = 0; rk < 4; ++rk) {
+        const int *dd = DIRS[p][rk];
+        args[(size_t)(p * 4 + rk) * n + i] =
+            stage_args(h, rk, dd[0], dd[1], dd[2], ins[rk], outs[rk]);
+      }
+    for (int rk = 0; rk < 4; ++rk) {
+      const StageArgs &a = args[(size_t)rk * n + i];
+      SourceArgs &s = src[(size_t)rk * n + i];
+      s = SourceArgs{};
+      s.g = h->g;
+      s.nmnt = h->nmnt; s.nfrc = h->nfrc;
+      s.mcell = h->d_mcell; s.mcoef = h->d_mcoef; s.mstf = h->d_mstf; s.nstfm = h->nstfm;
+      s.fcell = h->d_fcell; s.fcoef = h->d_fcoef; s.fstf = h->d_fstf; s.nstff = h->nstff;
+      s.tinc = (rk == 0) ? 0 : (rk < 3 ? 1 : 2);
+      s.tindex = -1;
+      s.step = h->d_step;
+      s.adt = a.adt; s.bdt = a.bdt;
+      s.out = a.out; s.tw = a.tw; s.rk = rk;
+      s.elem = a.elem;
+      for (int c = 0; c < NCOMP; ++c) s.isc[c] = a.isc[c];
+    }
+    if (h->nmnt + h->nfrc > 0) b->any_src = true;
+    RecordArgs &r = rec[i];
+    r.fw = (const float *)h->set[0];
+    r.fstride = h->g.fstride;
+    r.cells = h->d_rcell;
+    r.nrecv = h->nrecv;
+    r.nt = h->d.nt;
+    r.seis = h->d_seis;
+    r.step = h->d_step;
+    for (int c = 0; c < NCOMP; ++c) r.s.sc[c] = 1.f;
+  }
+  if (!b->plan) {
+    std::vector<Geom> gs(n);
+    std::vector<void *> sets((size_t)4 * n);
+    std::vector<const float *> media(n), metric(n);
+    std::vector<float *> aux((size_t)3 * n);
+    for (int i = 0; i < n; ++i) {
+      cgfd_solver *h = b->m[i];
+      gs[i] = h->g;
+      for (int q = 0; q < 4; ++q) sets[(size_t)4 * i + q] = h->set[q];
+      media[i] = h->media;
+      metric[i] = h->metric;
+      for (int d = 0; d < 3; ++d) aux[(size_t)3 * i + d] = h->aux[d];
+    }
+    b->plan = pair_create_batch_plan(n, gs.data(), sets.data(), media.data(), metric.data(),
+                                     aux.data());
+    if (!b->plan) return batch_fail(b, CGFD_ERR_CUDA, "batch plan (tensor maps or work list)");
+  }
+  if (!pair_batch_set_args(b->plan, args.data()))
+    return batch_fail(b, CGFD_ERR_CUDA, "batch stage arguments");
+  if (!b->d_src) BCK(b, cudaMalloc(&b->d_src, src.size() * sizeof(SourceArgs)));
+  if (!b->d_rec) BCK(b, cudaMalloc(&b->d_rec, rec.size() * sizeof(RecordArgs)));
+  BCK(b, cudaMemcpy(b->d_src, src.data(), src.size() * sizeof(SourceArgs),
+                    cudaMemcpyHostToDevice));
+  BCK(b, cudaMemcpy(b->d_rec, rec.data(), rec.size() * sizeof(RecordArgs),
+                    cudaMemcpyHostToDevice));
+  for (int p = 0; p < 4; ++p) {
+    if (b->graph[p]) { cudaGraphExecDestroy(b->graph[p]); b->graph[p] = nullptr; }
+    cudaGraph_t gr = nullptr;
+    BCK(b, cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+    int st = batch_enqueue(b, p, args);
+    cudaError_t e = cudaStreamEndCapture(b->st, &gr);
+    if (st) { if (gr) cudaGraphDestroy(gr); return st; }
+    BCK(b, e);
+    e = cudaGraphInstantiate(&b->graph[p], gr, 0);
+    cudaGraphDestroy(gr);
+    BCK(b, e);
+  }
+  b->ready = true;
+  return CGFD_OK;
+}
+
+extern "C" {
+
+int cgfd_batch_create(const cgfd_desc *descs, int n, cgfd_batch **out) {
+  if (!descs || !out || n < 1) return batch_fail(nullptr, CGFD_ERR_ARG, "bad batch arguments");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (descs[i].storage != CGFD_STORE_F32)
+      return batch_fail(nullptr, CGFD_ERR_ARG, "batched models use FP32 storage");
+    if (descs[i].kernel != CGFD_KERNEL_FUSED)
+      return batch_fail(nullptr, CGFD_ERR_ARG, "batched models use the default kernel family");
+    if (descs[i].device != descs[0].device)
+      return batch_fail(nullptr, CGFD_ERR_ARG, "batched models share one device");
+  }
+  cgfd_batch *b = new cgfd_batch();
+  b->device = descs[0].device;
+  for (int i = 0; i < n; ++i) {
+    cgfd_solver *h = nullptr;
+    int st = cgfd_create(&descs[i], &h);
+    if (st) {
+      for (cgfd_solver *x : b->m) cgfd_destroy(x);
+      delete b;
+      return st;
+    }
+    b->m.push_back(h);
+  }
+  DevGuard guard(b->device);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(int));
+  if (e != cudaSuccess) {
+    batch_free(b);
+    for (cgfd_solver *x : b->m) cgfd_destroy(x);
+    delete b;
+    return batch_fail(nullptr, CGFD_ERR_CUDA, "batch setup");
+  }
+  *out = b;
+  return CGFD_OK;
+}
+
+int cgfd_batch_solver(cgfd_batch *b, int i, cgfd_solver **h) {
+  if (!b || !h || i < 0 || i >= (int)b->m.size())
+    return batch_fail(b, CGFD_ERR_ARG, "bad model index");
+  *h = b->m[i];
+  b->ready = false;  // the caller may upload new inputs through it
+  return CGFD_OK;
+}
+
+int cgfd_batch_prepare(cgfd_batch *b) {
+  if (!b) return batch_fail(b, CGFD_ERR_ARG, "null handle");
+  for (cgfd_solver *h : b->m) {
+    if (!h->prepared || !h->graphs_ok) b->ready = false;
+    int st = cgfd_prepare(h);
+    if (st) return batch_fail(b, st, h->err);
+    if (h->steps != b->m[0]->steps)
+      return batch_fail(b, CGFD_ERR_STATE, "batched models must be at the same step");
+  }
+  if (b->ready) return CGFD_OK;
+  DevGuard guard(b->device);
+  return batch_build(b);
+}
+
+int cgfd_batch_step(cgfd_batch *b, int n_steps) {
+  if (!b || n_steps < 0) return batch_fail(b, CGFD_ERR_ARG, "bad arguments");
+  int st = cgfd_batch_prepare(b);
+  if (st) return st;
+  DevGuard guard(b->device);
+  for (cgfd_solver *h : b->m) {
+    const int last = h->steps + n_steps - 1;
+    if (n_steps > 0 && h->nrecv && last >= h->d.nt)
+      return batch_fail(b, CGFD_ERR_ARG, "more steps than a model's seismogram buffer (nt)");
+    if (n_steps > 0 && ((h->nmnt && 2 * last + 2 >= h->nstfm) ||
+                        (h->nfrc && 2 * last + 2 >= h->nstff)))
+      return batch_fail(b, CGFD_ERR_ARG, "a model's source time function is too short");
+    BCK(b, cudaMemcpyAsync(h->d_step, &h->steps, sizeof(int), cudaMemcpyHostToDevice, b->st));
+  }
+  // the batch's stream follows the work queued on the members' streams, and
+  // the members' streams (seismograms, fields) follow the batch
+  for (cgfd_solver *h : b->m) {
+    BCK(b, cudaEventRecord(b->ev, h->st));
+    BCK(b, cudaStreamWaitEvent(b->st, b->ev, 0));
+  }
+  const int s0 = b->m[0]->steps;
+  for (int s = 0; s < n_steps; ++s) BCK(b, cudaGraphLaunch(b->graph[(s0 + s) % 4], b->st));
+  BCK(b, cudaEventRecord(b->ev, b->st));
+  for (cgfd_solver *h : b->m) {
+    BCK(b, cudaStreamWaitEvent(h->st, b->ev, 0));
+    h->steps += n_steps;
+    h->wcur = 0;
+  }
+  return CGFD_OK;
+}
+
+int cgfd_batch_sync(cgfd_batch *b, double timeout_s) {
+  if (!b) return batch_fail(b, CGFD_ERR_ARG, "null handle");
+  DevGuard guard(b->device);
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    cudaError_t e = cudaStreamQuery(b->st);
+    if (e == cudaSuccess) {
+      int flag = 0;
+      BCK(b, cudaMemcpy(&flag, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+      if (flag)
+        return batch_fail(b, flag == 2 ? CGFD_ERR_CUDA : CGFD_ERR_TIMEOUT,
+                          flag == 2 ? "stage kernel alignment self-check failed"
+                                    : "a bounded wait inside a stage kernel expired");
+      return CGFD_OK;
+    }
+    if (e != cudaErrorNotReady) BCK(b, e);
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (timeout_s >= 0 && el > timeout_s)
+      return batch_fail(b, CGFD_ERR_TIMEOUT, "timeout waiting for the device");
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+}
+
+int cgfd_batch_step_timed(cgfd_batch *b, int n_steps, float *ms) {
+  if (!b || n_steps < 1 || !ms) return batch_fail(b, CGFD_ERR_ARG, "bad arguments");
+  int st = cgfd_batch_prepare(b);
+  if (st) return st;
+  DevGuard guard(b->device);
+  cudaEvent_t e0, e1;
+  BCK(b, cudaEventCreate(&e0));
+  BCK(b, cudaEventCreate(&e1));
+  BCK(b, cudaEventRecord(e0, b->st));
+  st = cgfd_batch_step(b, n_steps);
+  if (st) return st;
+  BCK(b, cudaEventRecord(e1, b->st));
+  st = cgfd_batch_sync(b, -1);
+  if (st) return st;
+  BCK(b, cudaEventElapsedTime(ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return CGFD_OK;
+}
+
+int cgfd_batch_autotune(cgfd_batch *b, int steps, float *best_ms) {
+  if (!b || steps < 1) return batch_fail(b, CGFD_ERR_ARG, "bad arguments");
+  int st = cgfd_batch_prepare(b);
+  if (st) return st;
+  DevGuard guard(b->device);
+  std::vector<Snapshot> sn(b->m.size());
+  for (size_t i = 0; i < b->m.size(); ++i) {
+    st = snapshot_take(b->m[i], sn[i]);
+    if (st) return batch_fail(b, st, b->m[i]->err);
+  }
+  float best = 1e30f;
+  WorkParams bestp = pair_get_work(b->plan);
+  for (const WorkParams &wp : tuning_candidates()) {
+    if (!pair_set_work(b->plan, wp)) continue;
+    b->ready = false;
+    st = batch_build(b);
+    if (st) break;
+    for (size_t i = 0; i < b->m.size(); ++i) b->m[i]->steps = sn[i].steps;
+    float ms = 0;
+    st = cgfd_batch_step(b, 1);  // warm-up
+    if (!st) st = cgfd_batch_step_timed(b, steps, &ms);
+    if (st) break;
+    if (ms < best) { best = ms; bestp = wp; }
+  }
+  for (size_t i = 0; i < b->m.size(); ++i) {
+    int st2 = snapshot_restore(b->m[i], sn[i]);
+    if (!st) st = st2;
+  }
+  if (!pair_set_work(b->plan, bestp) && !st) st = batch_fail(b, CGFD_ERR_CUDA, "work list");
+  b->ready = false;
+  if (!st) st = batch_build(b);
+  if (best_ms) *best_ms = best / steps;
+  return st;
+}
+
+int cgfd_batch_last_error(cgfd_batch *b, char *buf, size_t len) {
+  if (!buf || len == 0) return CGFD_ERR_ARG;
+  const std::string &m = b ? b->err : std::string();
+  std::snprintf(buf, len, "%s", m.c_str());
+  return CGFD_OK;
+}
+
+int cgfd_batch_destroy(cgfd_batch *b) {
+  if (!b) return CGFD_OK;
+  {
+    DevGuard guard(b->device);
+    if (b->st) cudaStreamSynchronize(b->st);
+    batch_free(b);
+  }
+  for (cgfd_solver *h : b->m) cgfd_destroy(h);
+  delete b;
   return CGFD_OK;
 }
 

@@ -67,34 +67,28 @@ bool aux_map(CUtensorMap *m, const Geom &g, int d, const float *base, int bc) {
 
 using namespace pair;
 
-#ifndef CGFD_PAIR_ITEMS_PER_CTA
-#define CGFD_PAIR_ITEMS_PER_CTA 6
-#endif
-#ifndef CGFD_PAIR_MIN_CHUNK
-#define CGFD_PAIR_MIN_CHUNK 16
-#endif
-// work list shape: about this many items per resident CTA, z-chunks of at
-// least this many planes
-constexpr int ITEMS_PER_CTA = CGFD_PAIR_ITEMS_PER_CTA, MIN_CHUNK = CGFD_PAIR_MIN_CHUNK;
-
 bool pair_supported(const Geom &g) {
   // tile boxes start on 16-byte boundaries (XO and i0 multiples of 4, px of
   // 32) and every z-chunk has at least 4 planes
   return (XO % 4) == 0 && XO >= 4 && g.px % 32 == 0 && g.nk >= 4;
 }
 
-void *pair_create_plan(const Geom &g, int elem, void *const sets[4], const float *media,
-                       const float *metric, float *const aux[3]) {
-  static bool attrs = false;
-  if (!attrs) {
-    attrs_fv0(); attrs_fv1(); attrs_fv2(); attrs_fs0(); attrs_fs1(); attrs_fs2();
-    attrs_hv0(); attrs_hv1(); attrs_hv2(); attrs_hs0(); attrs_hs1(); attrs_hs2();
-    attrs_bv0(); attrs_bv1(); attrs_bv2(); attrs_bs0(); attrs_bs1(); attrs_bs2();
-    attrs = true;
-  }
-  Plan *pl = new (std::nothrow) Plan();
-  if (!pl) return nullptr;
-  pl->elem = elem;
+namespace pair {
+namespace {
+
+void set_all_attrs() {
+  static bool done = false;
+  if (done) return;
+  attrs_fv0(); attrs_fv1(); attrs_fv2(); attrs_fs0(); attrs_fs1(); attrs_fs2();
+  attrs_hv0(); attrs_hv1(); attrs_hv2(); attrs_hs0(); attrs_hs1(); attrs_hs2();
+  attrs_bv0(); attrs_bv1(); attrs_bv2(); attrs_bs0(); attrs_bs1(); attrs_bs2();
+  attrs_fv0_b(); attrs_fv1_b(); attrs_fv2_b(); attrs_fs0_b(); attrs_fs1_b(); attrs_fs2_b();
+  done = true;
+}
+
+// tensor maps of one model's buffers
+bool model_maps(ModelMaps *pl, int *has_aux, const Geom &g, int elem, void *const sets[4],
+                const float *media, const float *metric, float *const aux[3]) {
   bool ok = true;
   constexpr int NCV = PartInfo<PART_VEL>::NC, NCS = PartInfo<PART_STR>::NC;
   const int hx = (elem == ELEM_F32) ? Halo<float>::HX : Halo<__half>::HX;
@@ -108,7 +102,7 @@ void *pair_create_plan(const Geom &g, int elem, void *const sets[4], const float
   ok = ok && field_map(&pl->coefS, g, media, 3, CX, TY, PartInfo<PART_STR>::NCOEF);
   ok = ok && field_map(&pl->met, g, metric, 4, CX, TY, 3);
   for (int d = 0; d < 3; ++d) {
-    pl->wk.has_aux[d] = aux[d] != nullptr;
+    has_aux[d] = aux[d] != nullptr;
     if (!aux[d]) continue;
     const size_t ss = 9 * g.astride[d];
     for (int t = 0; t < 3; ++t) {  // FA, A, tA
@@ -116,101 +110,13 @@ void *pair_create_plan(const Geom &g, int elem, void *const sets[4], const float
       ok = ok && aux_map(&pl->auxT[d][t], g, d, aux[d] + t * ss, 6);
     }
   }
-  if (!ok) {
-    delete pl;
-    return nullptr;
-  }
-  // work items: the bottom PML layer as a z-chunk of its own, the rest in
-  // pieces long enough to amortise the four window planes read around each
-  // chunk and numerous enough to balance
-  // x tiles start at the grid's first column (a tile whose PML columns share
-  // it with interior columns costs about as much per plane as a tile of PML
-  // columns alone: the boundary path is latency-bound per plane)
-  const int xorg = 0;
-  const int ntx = (g.ni - xorg + CX - 1) / CX, nty = (g.nj + TY - 1) / TY;
-  const int ntiles = ntx * nty;
-  const int rv = elem == ELEM_F16 ? resident_hv() : elem == ELEM_BF16 ? resident_bv()
-                                                                    : resident_fv();
-  const int rs = elem == ELEM_F16 ? resident_hs() : elem == ELEM_BF16 ? resident_bs()
-                                                                    : resident_fs();
-  const int G = rv < rs ? rv : rs;
-  // (every chunk has at least 4 planes: the kernel's initial issue of four
-  // entries relies on it)
-  std::vector<int> zb{LFD};
-  const int zlo = LFD + g.nabs[4], ztop = g.nk + LFD;
-  if (g.nabs[4] >= 8 && ztop - zlo >= 8) zb.push_back(zlo);
-  const int zr = zb.back(), rest = ztop - zr;
-  int pieces = 1;
-  while ((long)ntiles * ((long)zb.size() - 1 + pieces) < (long)ITEMS_PER_CTA * G &&
-         rest / (pieces + 1) >= MIN_CHUNK)
-    ++pieces;
-  for (int q = 1; q <= pieces; ++q) zb.push_back(zr + (int)((long)rest * q / pieces));
-  for (size_t c = 0; c + 1 < zb.size(); ++c)
-    if (zb[c + 1] - zb[c] < 4) {
-      delete pl;
-      return nullptr;
-    }
-  pl->zchunk = (rest + pieces - 1) / pieces;
-  // order: the most expensive first (estimated cost: planes x sum over the
-  // tile's valid columns of (1 + number of PML directions)), so the cheap
-  // items fill the tail; equal costs keep the (z-chunk, tile) order, so
-  // neighbouring tiles of a class run together and share halo rows in L2
-  struct It { int4 v; double cost; };
-  std::vector<It> items;
-  for (size_t c = 0; c + 1 < zb.size(); ++c) {
-    const bool zp = zb[c] < zlo;
-    for (int t = 0; t < ntiles; ++t) {
-      const int i0 = xorg + (t % ntx) * CX, j0 = (t / ntx) * TY;
-      double w = 0;
-      for (int j = j0; j < j0 + TY && j < g.nj; ++j) {
-        const bool yp = j < g.nabs[2] || j >= g.nj - g.nabs[3];
-        for (int i = i0 < 0 ? 0 : i0; i < i0 + CX && i < g.ni; ++i) {
-          const bool xp = i < g.nabs[0] || i >= g.ni - g.nabs[1];
-          w += 1 + (xp ? 1 : 0) + (yp ? 1 : 0) + (zp ? 1 : 0);
-        }
-      }
-      items.push_back({make_int4(i0, j0, zb[c], zb[c + 1]), w * (zb[c + 1] - zb[c])});
-    }
-  }
-  std::stable_sort(items.begin(), items.end(),
-                   [](const It &x, const It &y) { return x.cost > y.cost; });
-  std::vector<int4> hv(items.size());
-  for (size_t q = 0; q < items.size(); ++q) hv[q] = items[q].v;
-  Work &wk = pl->wk;
-  wk.nitems = (int)hv.size();
-  int4 *d_items = nullptr;
-  int *d_counter = nullptr;
-  if (cudaMalloc(&d_items, hv.size() * sizeof(int4)) != cudaSuccess ||
-      cudaMemcpy(d_items, hv.data(), hv.size() * sizeof(int4), cudaMemcpyHostToDevice) !=
-          cudaSuccess ||
-      cudaMalloc(&d_counter, 2 * sizeof(int)) != cudaSuccess ||
-      cudaMemset(d_counter, 0, 2 * sizeof(int)) != cudaSuccess) {
-    cudaFree(d_items);
-    cudaFree(d_counter);
-    delete pl;
-    return nullptr;
-  }
-  wk.items = d_items;
-  wk.counter = d_counter;
-  pl->grid[0] = wk.nitems < rv ? wk.nitems : rv;
-  pl->grid[1] = wk.nitems < rs ? wk.nitems : rs;
-  return pl;
+  return ok;
 }
 
-void pair_destroy_plan(void *plan) {
-  Plan *pl = reinterpret_cast<Plan *>(plan);
-  if (!pl) return;
-  cudaFree((void *)pl->wk.items);
-  cudaFree(pl->wk.counter);
-  delete pl;
-}
-
-void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *err,
-                       void *stream) {
-  const Plan &pl = *reinterpret_cast<const Plan *>(plan);
-  cudaStream_t s = (cudaStream_t)stream;
-  const int kind = a.rk == 0 ? 0 : (a.rk < 3 ? 1 : 2);
-  Maps mv, ms;
+// the maps of one stage (stage input set, RK kind, stage index) for the
+// velocity (mv) and stress (ms) parts
+void stage_maps(const ModelMaps &pl, int rk, int in_set, Maps &mv, Maps &ms) {
+  const int kind = rk == 0 ? 0 : (rk < 3 ? 1 : 2);
   mv.halo = pl.haloV[in_set];
   mv.u0 = kind == 2 ? pl.ctrV[3] : pl.ctrV[0];
   mv.u1 = pl.ctrV[3];
@@ -223,10 +129,162 @@ void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *er
   ms.met = pl.met;
   for (int d = 0; d < 3; ++d) {
     // prefetched sets: stage input (FA in the first stage, else A), FA, tA
-    const int in = (a.rk == 0) ? 0 : 1;
+    const int in = (rk == 0) ? 0 : 1;
     mv.aux[d][0] = pl.auxV[d][in]; mv.aux[d][1] = pl.auxV[d][0]; mv.aux[d][2] = pl.auxV[d][2];
     ms.aux[d][0] = pl.auxT[d][in]; ms.aux[d][1] = pl.auxT[d][0]; ms.aux[d][2] = pl.auxT[d][2];
   }
+}
+
+// Work items of one or more models (tile x z-chunk): the bottom PML layer is
+// a z-chunk of its own (when it has >= 8 planes), the rest is cut into pieces
+// of about len planes (>= MIN_CHUNK; every chunk has >= 4 planes, which the
+// kernel's initial issue of four entries relies on).  Order: the most
+// expensive first (estimated cost: planes x sum over the tile's valid
+// columns of (1 + pml_weight x number of PML directions)), so the cheap
+// items fill the tail; equal costs keep the (model, z-chunk, tile) order, so
+// neighbouring tiles of a class run together and share halo rows in L2.
+std::vector<int4> build_items(const std::vector<Geom> &gs, int G, const WorkParams &wp,
+                              int *zchunk) {
+  // target chunk length: enough items (items_per_cta per resident CTA) over
+  // all models' tile columns
+  double colplanes = 0;
+  for (const Geom &g : gs)
+    colplanes += (double)((g.ni + CX - 1) / CX) * ((g.nj + TY - 1) / TY) * g.nk;
+  const double target = (double)wp.items_per_cta * G;
+  struct It { int4 v; double cost; };
+  std::vector<It> items;
+  for (size_t mdl = 0; mdl < gs.size(); ++mdl) {
+    const Geom &g = gs[mdl];
+    const int ntx = (g.ni + CX - 1) / CX, nty = (g.nj + TY - 1) / TY;
+    const int ntiles = ntx * nty;
+    std::vector<int> zb{LFD};
+    const int zlo = LFD + g.nabs[4], ztop = g.nk + LFD;
+    if (g.nabs[4] >= 8 && ztop - zlo >= 8) zb.push_back(zlo);
+    const int zr = zb.back(), rest = ztop - zr;
+    int pieces = 1;
+    if (gs.size() == 1) {
+      while ((long)ntiles * ((long)zb.size() - 1 + pieces) < (long)target &&
+             rest / (pieces + 1) >= wp.min_chunk)
+        ++pieces;
+    } else {
+      const double len = colplanes / target > wp.min_chunk ? colplanes / target : wp.min_chunk;
+      pieces = (int)(rest / len + 0.5);
+      if (pieces < 1) pieces = 1;
+      while (pieces > 1 && rest / pieces < 4) --pieces;
+    }
+    for (int q = 1; q <= pieces; ++q) zb.push_back(zr + (int)((long)rest * q / pieces));
+    if (zchunk && mdl == 0) *zchunk = (rest + pieces - 1) / pieces;
+    for (size_t c = 0; c + 1 < zb.size(); ++c) {
+      if (zb[c + 1] - zb[c] < 4) return {};
+      const bool zp = zb[c] < zlo;
+      for (int t = 0; t < ntiles; ++t) {
+        const int i0 = (t % ntx) * CX, j0 = (t / ntx) * TY;
+        double w = 0;
+        for (int j = j0; j < j0 + TY && j < g.nj; ++j) {
+          const bool yp = j < g.nabs[2] || j >= g.nj - g.nabs[3];
+          for (int i = i0; i < i0 + CX && i < g.ni; ++i) {
+            const bool xp = i < g.nabs[0] || i >= g.ni - g.nabs[1];
+            w += 1 + wp.pml_weight * ((xp ? 1 : 0) + (yp ? 1 : 0) + (zp ? 1 : 0));
+          }
+        }
+        items.push_back({make_int4(i0, j0, zb[c] | (zb[c + 1] << 16), (int)mdl),
+                         w * (zb[c + 1] - zb[c])});
+      }
+    }
+  }
+  std::stable_sort(items.begin(), items.end(),
+                   [](const It &x, const It &y) { return x.cost > y.cost; });
+  std::vector<int4> hv(items.size());
+  for (size_t q = 0; q < items.size(); ++q) hv[q] = items[q].v;
+  return hv;
+}
+
+// uploads a work list into the plan (replacing an earlier one)
+bool upload_items(Plan *pl, const std::vector<int4> &hv, int rv, int rs) {
+  Work &wk = pl->wk;
+  if (hv.empty()) return false;
+  cudaFree((void *)wk.items);
+  wk.items = nullptr;
+  int4 *d_items = nullptr;
+  if (cudaMalloc(&d_items, hv.size() * sizeof(int4)) != cudaSuccess ||
+      cudaMemcpy(d_items, hv.data(), hv.size() * sizeof(int4), cudaMemcpyHostToDevice) !=
+          cudaSuccess) {
+    cudaFree(d_items);
+    return false;
+  }
+  if (!wk.counter) {
+    if (cudaMalloc(&wk.counter, 2 * sizeof(int)) != cudaSuccess ||
+        cudaMemset(wk.counter, 0, 2 * sizeof(int)) != cudaSuccess)
+      return false;
+  }
+  wk.items = d_items;
+  wk.nitems = (int)hv.size();
+  pl->grid[0] = wk.nitems < rv ? wk.nitems : rv;
+  pl->grid[1] = wk.nitems < rs ? wk.nitems : rs;
+  return true;
+}
+
+void resident(int elem, bool batch, int *rv, int *rs) {
+  if (batch) {
+    *rv = resident_fv_b();
+    *rs = resident_fs_b();
+  } else {
+    *rv = elem == ELEM_F16 ? resident_hv() : elem == ELEM_BF16 ? resident_bv() : resident_fv();
+    *rs = elem == ELEM_F16 ? resident_hs() : elem == ELEM_BF16 ? resident_bs() : resident_fs();
+  }
+}
+
+}  // namespace
+}  // namespace pair
+
+void *pair_create_plan(const Geom &g, int elem, void *const sets[4], const float *media,
+                       const float *metric, float *const aux[3]) {
+  set_all_attrs();
+  Plan *pl = new (std::nothrow) Plan();
+  if (!pl) return nullptr;
+  pl->elem = elem;
+  pl->geoms.push_back(g);
+  pl->mm.resize(1);
+  if (!model_maps(&pl->mm[0], pl->wk.has_aux, g, elem, sets, media, metric, aux) ||
+      !pair_set_work(pl, WorkParams{})) {
+    pair_destroy_plan(pl);
+    return nullptr;
+  }
+  return pl;
+}
+
+WorkParams pair_get_work(const void *plan) {
+  return reinterpret_cast<const Plan *>(plan)->params;
+}
+
+bool pair_set_work(void *plan, const WorkParams &wp) {
+  Plan *pl = reinterpret_cast<Plan *>(plan);
+  int rv = 0, rs = 0;
+  resident(pl->elem, pl->nmodels > 0, &rv, &rs);
+  const int G = rv < rs ? rv : rs;
+  std::vector<int4> hv = build_items(pl->geoms, G, wp, &pl->zchunk);
+  if (!upload_items(pl, hv, rv, rs)) return false;
+  pl->params = wp;
+  return true;
+}
+
+void pair_destroy_plan(void *plan) {
+  Plan *pl = reinterpret_cast<Plan *>(plan);
+  if (!pl) return;
+  cudaFree((void *)pl->wk.items);
+  cudaFree(pl->wk.counter);
+  cudaFree(pl->d_bargs);
+  cudaFree(pl->d_bmaps);
+  delete pl;
+}
+
+void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *err,
+                       void *stream) {
+  const Plan &pl = *reinterpret_cast<const Plan *>(plan);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int kind = a.rk == 0 ? 0 : (a.rk < 3 ? 1 : 2);
+  Maps mv, ms;
+  stage_maps(pl.mm[0], a.rk, in_set, mv, ms);
   // both parts' item counters restart at zero
   cudaMemsetAsync(pl.wk.counter, 0, 2 * sizeof(int), s);
   typedef void (*LaunchFn)(const Plan &, const Maps &, const StageArgs &, int *, cudaStream_t);
@@ -238,6 +296,71 @@ void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *er
   fns[e][0][kind](pl, mv, a, err, s);
   fns[e][1][kind](pl, ms, a, err, s);
   launch_timg(a, s);
+}
+
+// ---------------------------- batched models ------------------------------
+
+void *pair_create_batch_plan(int n, const Geom *gs, void *const *sets, const float *const *media,
+                             const float *const *metric, float *const *aux) {
+  set_all_attrs();
+  Plan *pl = new (std::nothrow) Plan();
+  if (!pl) return nullptr;
+  pl->elem = ELEM_F32;
+  pl->nmodels = n;
+  pl->geoms.assign(gs, gs + n);
+  pl->mm.resize(n);
+  bool ok = true;
+  for (int i = 0; i < n && ok; ++i) {
+    int ha[3];
+    ok = model_maps(&pl->mm[i], ha, gs[i], ELEM_F32, sets + 4 * i, media[i], metric[i],
+                    aux + 3 * i);
+  }
+  // per stage, part and model: the maps of that stage (input set per stage
+  // as in the step schedule: FW, Wa, Wb, Wa)
+  static const int ins[4] = {0, 1, 2, 1};
+  std::vector<Maps> hm((size_t)8 * n);
+  for (int rk = 0; rk < 4 && ok; ++rk)
+    for (int i = 0; i < n; ++i)
+      stage_maps(pl->mm[i], rk, ins[rk], hm[(size_t)(rk * 2) * n + i],
+                 hm[(size_t)(rk * 2 + 1) * n + i]);
+  ok = ok && cudaMalloc(&pl->d_bmaps, hm.size() * sizeof(Maps)) == cudaSuccess &&
+       cudaMemcpy(pl->d_bmaps, hm.data(), hm.size() * sizeof(Maps), cudaMemcpyHostToDevice) ==
+           cudaSuccess &&
+       cudaMalloc(&pl->d_bargs, (size_t)16 * n * sizeof(StageArgs)) == cudaSuccess;
+  if (!ok || !pair_set_work(pl, WorkParams{})) {
+    pair_destroy_plan(pl);
+    return nullptr;
+  }
+  return pl;
+}
+
+bool pair_batch_set_args(void *plan, const StageArgs *args) {
+  Plan *pl = reinterpret_cast<Plan *>(plan);
+  return cudaMemcpy(pl->d_bargs, args, (size_t)16 * pl->nmodels * sizeof(StageArgs),
+                    cudaMemcpyHostToDevice) == cudaSuccess;
+}
+
+void launch_stage_pair_batch(const void *plan, int pattern, const StageArgs &rep, int *err,
+                             void *stream) {
+  const Plan &pl = *reinterpret_cast<const Plan *>(plan);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int rk = rep.rk, kind = rk == 0 ? 0 : (rk < 3 ? 1 : 2), n = pl.nmodels;
+  Work wv = pl.wk, ws = pl.wk;
+  wv.bargs = ws.bargs = pl.d_bargs + (size_t)(pattern * 4 + rk) * n;
+  wv.bmaps = pl.d_bmaps + (size_t)(rk * 2) * n;
+  ws.bmaps = pl.d_bmaps + (size_t)(rk * 2 + 1) * n;
+  typedef void (*LaunchFn)(const Plan &, const StageArgs &, const Work &, int *, cudaStream_t);
+  static const LaunchFn fv[3] = {launch_fv0_b, launch_fv1_b, launch_fv2_b};
+  static const LaunchFn fs[3] = {launch_fs0_b, launch_fs1_b, launch_fs2_b};
+  cudaMemsetAsync(pl.wk.counter, 0, 2 * sizeof(int), s);
+  fv[kind](pl, rep, wv, err, s);
+  fs[kind](pl, rep, ws, err, s);
+  int mi = 0, mj = 0;
+  for (const Geom &g : pl.geoms) {
+    mi = g.ni > mi ? g.ni : mi;
+    mj = g.nj > mj ? g.nj : mj;
+  }
+  launch_timg_batch(wv.bargs, n, mi, mj, s);
 }
 
 int pair_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str) {

@@ -49,6 +49,7 @@
 #include <cudaTypedefs.h>
 
 #include <cstdint>
+#include <vector>
 
 namespace cgfd {
 namespace pair {
@@ -126,15 +127,19 @@ struct Maps {
   CUtensorMap aux[3][3];  // [direction][ain, afw, ta], box {64, 4, 1, NS}
 };
 
-// Work list of a launch: items {i0, j0, z0, z1} (tile origin and z range),
-// ordered by decreasing estimated cost; CTAs take them in order from an
-// atomic counter (reset before every launch), so expensive PML items start
-// first and the cheap interior items fill the tail.
+// Work list of a launch: items {i0, j0, z0 | z1 << 16, model} (tile
+// origin, z range, model of a batch), ordered by decreasing estimated cost;
+// CTAs take them in order from an atomic counter (reset before every
+// launch), so expensive PML items start first and the cheap interior items
+// fill the tail.  A batched launch reads each model's stage arguments and
+// tensor maps from the device arrays bargs / bmaps (one entry per model).
 struct Work {
   const int4 *items;
   int *counter;       // [0]: velocity launch, [1]: stress launch
   int nitems;
-  int has_aux[3];     // direction has a PML (aux maps valid)
+  int has_aux[3];     // direction has a PML (aux maps valid; single model)
+  const StageArgs *bargs;
+  const Maps *bmaps;
 };
 
 // ---------------------------- float2 helpers ------------------------------
@@ -638,7 +643,7 @@ __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, cons
 // ------------------------------ the march ---------------------------------
 // items: tile index fastest, so the CTAs resident at one time work on
 // neighbouring tiles of the same z-chunk and share halo rows in L2
-template <typename T, int PART, int X, int Y, int Z, int KIND>
+template <typename T, int PART, int X, int Y, int Z, int KIND, bool B>
 __global__ void __launch_bounds__(TT, MinCtas<T>::value)
     pair_kernel(const __grid_constant__ Maps maps, const StageArgs a, const Work wk, int *err) {
   using S = Slot<T, PART>;
@@ -654,13 +659,7 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
   uint64_t *bars = reinterpret_cast<uint64_t *>(sbase + (size_t)NSLOT * S::BYTES);
   __shared__ int abort_flag;
 
-  const Geom &g = a.g;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const size_t fs = g.fstride;
-  const bool flat = a.flat;
-  // bytes one plane delivers: halo always, pointwise only for computed planes
-  const uint32_t pw_bytes = S::U_B * (KIND == 1 ? 2u : 1u) +
-                            (uint32_t)(PWT * 4) * (NCOEF + (flat ? 0 : 3));
 
   if (tid == 0) {
     abort_flag = 0;
@@ -680,52 +679,13 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
 
   uint32_t ph = 0;    // parity of the next wait, per slot (same in every thread)
   uint32_t pend = 0;  // thread 0: slots with a copy not yet waited for
-  const float rx = (float)X / a.h, rys = (float)Y / a.h, rz = (float)Z / a.h;
   const int ry = ty + 3, cb = HOFF + 2 * tx;
   const int sc = ry * HX + cb;       // this pair inside a halo plane
   const int tc = ty * CX + 2 * tx;   // this pair inside a pointwise tile
-  const int zlo = LFD + g.nabs[4], zhi = g.nk + LFD - g.nabs[5];  // z interior [zlo, zhi)
   const int kinda = (KIND == 1) ? 3 : (KIND == 2 ? 2 : 1);        // aux sets read
 
-  // Item entries q = 0..n (plane zf + DIR*q; entry n is read for the window
-  // only) go to ring slot (base + q) & 3, base counting the entries of the
-  // CTA's earlier items; thread 0 issues, every thread waits, in order.
-  auto issue = [&](const int4 it, int q, int s) {  // thread 0 only
-    unsigned char *slot = ring + (size_t)s * S::BYTES;
-    const int i0 = it.x, j0 = it.y, n = it.w - it.z;
-    const int p = ((DIR > 0) ? it.z : it.w - 1) + DIR * q;
-    const bool compute = q < n;
-    fence_proxy_async();
-    mbar_expect_tx(&bars[s], S::HALO_B + (compute ? pw_bytes : 0u));
-    tma_load(slot, &maps.halo, XO + i0 - HOFF, j0, p, C0, &bars[s]);
-    if (compute) {
-      const int cx = XO + i0, cy = LFD + j0;
-      tma_load(slot + S::U0, &maps.u0, cx, cy, p, S0, &bars[s]);
-      if (KIND == 1) tma_load(slot + S::U1, &maps.u1, cx, cy, p, S0, &bars[s]);
-      tma_load(slot + S::COEF, &maps.coef, cx, cy, p, COEF0, &bars[s]);
-      if (!flat) tma_load(slot + S::MET, &maps.met, cx, cy, p, 0, &bars[s]);
-      // the plane's PML auxiliaries into L2 (tile- and plane-uniform presence)
-      const bool xp = wk.has_aux[0] && (i0 < g.nabs[0] || i0 + CX > g.ni - g.nabs[1]);
-      const bool yp = wk.has_aux[1] && (j0 < g.nabs[2] || j0 + TY > g.nj - g.nabs[3]);
-      const bool zp = wk.has_aux[2] && (p < zlo || p >= zhi);
-      if (xp || yp || zp) {
-        const int xa_t = (i0 < g.nabs[0]) ? max(i0, 0) : i0 - (g.ni - g.nabs[1]) + g.xaoff;
-        const int ya_t = (j0 < g.nabs[2]) ? j0 : j0 - (g.nj - g.nabs[3]) + g.nabs[2];
-        const int za = (p - LFD < g.nabs[4]) ? p - LFD : p - LFD - (g.nk - g.nabs[5]) + g.nabs[4];
-        const int c0 = (PART == PART_VEL) ? 0 : 3;
-        const int cxp = max(cx, 0);  // prefetch boxes start inside the arrays
-        for (int t = 0; t < kinda; ++t) {
-          const int set = (KIND == 2 && t == 1) ? 2 : t;  // final stage: ain, ta
-          if (xp) tma_prefetch(&maps.aux[0][set], xa_t, cy, p, c0);
-          if (yp) tma_prefetch(&maps.aux[1][set], cxp, ya_t, p, c0);
-          if (zp) tma_prefetch(&maps.aux[2][set], cxp, cy, za, c0);
-        }
-      }
-    }
-    pend |= 1u << s;
-  };
-
   __shared__ int s_next;
+  __shared__ StageArgs s_args;  // batched launch: the current item's model
   int base = 0;  // stream position of the current item's entry 0
   for (;;) {
     // the next item, taken only when this CTA is free (a CTA never holds a
@@ -734,10 +694,69 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
     __syncthreads();
     const int cur = s_next;
     if (cur >= wk.nitems || abort_flag) break;  // CTA-uniform
-    const int4 it = wk.items[cur];
+    const int4 it4 = wk.items[cur];
+    const int model = B ? it4.w : 0;
+    if (B) {  // this item's model: its stage arguments into shared memory
+      const uint32_t *src = reinterpret_cast<const uint32_t *>(wk.bargs + model);
+      uint32_t *dst = reinterpret_cast<uint32_t *>(&s_args);
+      for (int w = tid; w < (int)(sizeof(StageArgs) / 4); w += TT) dst[w] = src[w];
+      __syncthreads();
+    }
+    const StageArgs &A = B ? s_args : a;
+    const Maps &M = B ? wk.bmaps[model] : maps;
+    const Geom &g = A.g;
+    const size_t fs = g.fstride;
+    const bool flat = A.flat;
+    // bytes one plane delivers: halo always, pointwise only for computed planes
+    const uint32_t pw_bytes = S::U_B * (KIND == 1 ? 2u : 1u) +
+                              (uint32_t)(PWT * 4) * (NCOEF + (flat ? 0 : 3));
+    const float rx = (float)X / A.h, rys = (float)Y / A.h, rz = (float)Z / A.h;
+    const int zlo = LFD + g.nabs[4], zhi = g.nk + LFD - g.nabs[5];  // z interior [zlo, zhi)
+    const bool aux_on[3] = {B ? A.ain[0] != nullptr : wk.has_aux[0] != 0,
+                         B ? A.ain[1] != nullptr : wk.has_aux[1] != 0,
+                         B ? A.ain[2] != nullptr : wk.has_aux[2] != 0};
+    const int4 it = make_int4(it4.x, it4.y, it4.z & 0xffff, it4.z >> 16);
     const int i0 = it.x, j0 = it.y, z0 = it.z, z1 = it.w;
     const int n = z1 - z0;                  // planes computed (>= 4)
     const int zf = (DIR > 0) ? z0 : z1 - 1;  // first plane in march order
+    // Item entries q = 0..n (plane zf + DIR*q; entry n is read for the window
+    // only) go to ring slot (base + q) & 3, base counting the entries of the
+    // CTA's earlier items; thread 0 issues, every thread waits, in order.
+    auto issue = [&](const int4 it, int q, int s) {  // thread 0 only
+      unsigned char *slot = ring + (size_t)s * S::BYTES;
+      const int i0 = it.x, j0 = it.y, n = it.w - it.z;
+      const int p = ((DIR > 0) ? it.z : it.w - 1) + DIR * q;
+      const bool compute = q < n;
+      fence_proxy_async();
+      mbar_expect_tx(&bars[s], S::HALO_B + (compute ? pw_bytes : 0u));
+      tma_load(slot, &M.halo, XO + i0 - HOFF, j0, p, C0, &bars[s]);
+      if (compute) {
+        const int cx = XO + i0, cy = LFD + j0;
+        tma_load(slot + S::U0, &M.u0, cx, cy, p, S0, &bars[s]);
+        if (KIND == 1) tma_load(slot + S::U1, &M.u1, cx, cy, p, S0, &bars[s]);
+        tma_load(slot + S::COEF, &M.coef, cx, cy, p, COEF0, &bars[s]);
+        if (!flat) tma_load(slot + S::MET, &M.met, cx, cy, p, 0, &bars[s]);
+        // the plane's PML auxiliaries into L2 (tile- and plane-uniform presence)
+        const bool xp = aux_on[0] && (i0 < g.nabs[0] || i0 + CX > g.ni - g.nabs[1]);
+        const bool yp = aux_on[1] && (j0 < g.nabs[2] || j0 + TY > g.nj - g.nabs[3]);
+        const bool zp = aux_on[2] && (p < zlo || p >= zhi);
+        if (xp || yp || zp) {
+          const int xa_t = (i0 < g.nabs[0]) ? max(i0, 0) : i0 - (g.ni - g.nabs[1]) + g.xaoff;
+          const int ya_t = (j0 < g.nabs[2]) ? j0 : j0 - (g.nj - g.nabs[3]) + g.nabs[2];
+          const int za = (p - LFD < g.nabs[4]) ? p - LFD : p - LFD - (g.nk - g.nabs[5]) + g.nabs[4];
+          const int c0 = (PART == PART_VEL) ? 0 : 3;
+          const int cxp = max(cx, 0);  // prefetch boxes start inside the arrays
+          for (int t = 0; t < kinda; ++t) {
+            const int set = (KIND == 2 && t == 1) ? 2 : t;  // final stage: ain, ta
+            if (xp) tma_prefetch(&M.aux[0][set], xa_t, cy, p, c0);
+            if (yp) tma_prefetch(&M.aux[1][set], cxp, ya_t, p, c0);
+            if (zp) tma_prefetch(&M.aux[2][set], cxp, cy, za, c0);
+          }
+        }
+      }
+      pend |= 1u << s;
+    };
+
     if (tid == 0)
       for (int q = 0; q < NSLOT; ++q) issue(it, q, (base + q) & (NSLOT - 1));
     auto wait = [&](int q) -> bool {  // every thread, in march order
@@ -769,20 +788,20 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
     e.iBx = S2(1.f); e.apdx = S2(0.f); e.dbx = S2(0.f); e.bbx = S2(1.f);
     e.iBy = 1.f; e.apdy = 0.f; e.dby = 0.f; e.bby = 1.f;
     if (e.m & 1) {
-      e.bbx.x = a.b[0][e.ix]; e.iBx.x = 1.f / e.bbx.x;
-      e.apdx.x = a.apd[0][e.ix]; e.dbx.x = a.db[0][e.ix];
+      e.bbx.x = A.b[0][e.ix]; e.iBx.x = 1.f / e.bbx.x;
+      e.apdx.x = A.apd[0][e.ix]; e.dbx.x = A.db[0][e.ix];
     }
     if (e.m & 2) {
-      e.bbx.y = a.b[0][e.ix + 1]; e.iBx.y = 1.f / e.bbx.y;
-      e.apdx.y = a.apd[0][e.ix + 1]; e.dbx.y = a.db[0][e.ix + 1];
+      e.bbx.y = A.b[0][e.ix + 1]; e.iBx.y = 1.f / e.bbx.y;
+      e.apdx.y = A.apd[0][e.ix + 1]; e.dbx.y = A.db[0][e.ix + 1];
     }
     if (e.m) {
-      e.bby = a.b[1][e.iy]; e.iBy = 1.f / e.bby;
-      e.apdy = a.apd[1][e.iy]; e.dby = a.db[1][e.iy];
+      e.bby = A.b[1][e.iy]; e.iBy = 1.f / e.bby;
+      e.apdy = A.apd[1][e.iy]; e.dby = A.db[1][e.iy];
     }
     // tile-uniform: no x/y PML anywhere in this tile (and B = 1, DB = APD = 0
     // outside the layers, which the solver checks at upload)
-    const bool tile_int = a.plain_interior && (i0 >= g.nabs[0]) &&
+    const bool tile_int = A.plain_interior && (i0 >= g.nabs[0]) &&
                           (i0 + CX <= g.ni - g.nabs[1]) && (j0 >= g.nabs[2]) &&
                           (j0 + TY <= g.nj - g.nabs[3]);
 
@@ -808,7 +827,7 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
       for (int c = 0; c < NC; ++c) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) w[c][q] = w[c][q + 1];
-        const T *src = static_cast<const T *>(a.in) + (size_t)(C0 + c) * fs + o;
+        const T *src = static_cast<const T *>(A.in) + (size_t)(C0 + c) * fs + o;
         w[c][4] = e.m ? ldt2(src, e.m) : S2(0.f);
       }
     }
@@ -841,9 +860,9 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
                         reinterpret_cast<const float *>(slot + S::MET) + tc};
         const T *H = reinterpret_cast<const T *>(slot);
         if constexpr (PART == PART_VEL)
-          vel_pair<T, X, Y, Z, KIND>(a, e, pl, H, ry, cb, pw, w, rx, rys, rz);
+          vel_pair<T, X, Y, Z, KIND>(A, e, pl, H, ry, cb, pw, w, rx, rys, rz);
         else
-          str_pair<T, X, Y, Z, KIND>(a, e, pl, H, ry, cb, pw, w, rx, rys, rz);
+          str_pair<T, X, Y, Z, KIND>(A, e, pl, H, ry, cb, pw, w, rx, rys, rz);
       }
       // the slot of entry q is free: refill it with stream position
       // base + q + NSLOT (this item's entry q + 4, or the next item's)
@@ -864,63 +883,78 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
   }
 }
 
-// Tensor maps and launch shape of one solver (host side, stage_pair.cu).
-struct Plan {
-  // per field set (FW, Wa, Wb, tW): halo boxes of the two parts and the
-  // pointwise boxes of V (3) and T (6) components
+// Tensor maps of one model's buffers (host side, stage_pair.cu): per field
+// set (FW, Wa, Wb, tW) the halo boxes of the two parts and the pointwise
+// boxes of V (3) and T (6) components; media, metric; auxiliaries per
+// direction and set (FA, A, tA) for V and T components.
+struct ModelMaps {
   CUtensorMap haloV[4], haloS[4], ctrV[4], ctrT[4];
   CUtensorMap coefV, coefS, met;
-  // auxiliaries: [direction][FA, A, tA], boxes of V (3) and T (6) components
   CUtensorMap auxV[3][3], auxT[3][3];
-  Work wk;
-  int elem;     // storage element type of the field sets
-  int zchunk;   // planes of the interior z-chunks
-  int grid[2];
 };
 
-template <typename T, int PART, int X, int Y, int Z, int KIND>
-void launch_t(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
-  pair_kernel<T, PART, X, Y, Z, KIND>
-      <<<pl.grid[PART], dim3(TX, TY, 1), Slot<T, PART>::SMEM, s>>>(m, a, pl.wk, err);
+// Launch plan of one solver or of a batch of models.
+struct Plan {
+  std::vector<ModelMaps> mm;   // one per model
+  std::vector<Geom> geoms;
+  Work wk;
+  int elem;                    // storage element type of the field sets
+  int zchunk;                  // planes of the (first model's) interior z-chunks
+  int grid[2];
+  WorkParams params;
+  int nmodels = 0;             // 0: single-model plan; else a batch of nmodels
+  StageArgs *d_bargs = nullptr;  // batch: [pattern * 4 + stage][model]
+  Maps *d_bmaps = nullptr;       // batch: [stage][part][model]
+};
+
+// a: the single model's stage arguments (X, Y, Z and the stage kind come
+// from it in every case); a batched launch (B) takes each model's arguments
+// and maps from pl.wk instead
+template <typename T, int PART, int X, int Y, int Z, int KIND, bool B>
+void launch_t(const Plan &pl, const Maps &m, const StageArgs &a, const Work &wk, int *err,
+              cudaStream_t s) {
+  pair_kernel<T, PART, X, Y, Z, KIND, B>
+      <<<pl.grid[PART], dim3(TX, TY, 1), Slot<T, PART>::SMEM, s>>>(m, a, wk, err);
 }
 
-template <typename T, int PART, int KIND>
-void launch_dirs(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cudaStream_t s) {
+template <typename T, int PART, int KIND, bool B = false>
+void launch_dirs(const Plan &pl, const Maps &m, const StageArgs &a, const Work &wk, int *err,
+                 cudaStream_t s) {
   const int code = (a.X > 0 ? 4 : 0) + (a.Y > 0 ? 2 : 0) + (a.Z > 0 ? 1 : 0);
   switch (code) {
-    case 0: launch_t<T, PART, -1, -1, -1, KIND>(pl, m, a, err, s); break;
-    case 1: launch_t<T, PART, -1, -1, 1, KIND>(pl, m, a, err, s); break;
-    case 2: launch_t<T, PART, -1, 1, -1, KIND>(pl, m, a, err, s); break;
-    case 3: launch_t<T, PART, -1, 1, 1, KIND>(pl, m, a, err, s); break;
-    case 4: launch_t<T, PART, 1, -1, -1, KIND>(pl, m, a, err, s); break;
-    case 5: launch_t<T, PART, 1, -1, 1, KIND>(pl, m, a, err, s); break;
-    case 6: launch_t<T, PART, 1, 1, -1, KIND>(pl, m, a, err, s); break;
-    default: launch_t<T, PART, 1, 1, 1, KIND>(pl, m, a, err, s); break;
+    case 0: launch_t<T, PART, -1, -1, -1, KIND, B>(pl, m, a, wk, err, s); break;
+    case 1: launch_t<T, PART, -1, -1, 1, KIND, B>(pl, m, a, wk, err, s); break;
+    case 2: launch_t<T, PART, -1, 1, -1, KIND, B>(pl, m, a, wk, err, s); break;
+    case 3: launch_t<T, PART, -1, 1, 1, KIND, B>(pl, m, a, wk, err, s); break;
+    case 4: launch_t<T, PART, 1, -1, -1, KIND, B>(pl, m, a, wk, err, s); break;
+    case 5: launch_t<T, PART, 1, -1, 1, KIND, B>(pl, m, a, wk, err, s); break;
+    case 6: launch_t<T, PART, 1, 1, -1, KIND, B>(pl, m, a, wk, err, s); break;
+    default: launch_t<T, PART, 1, 1, 1, KIND, B>(pl, m, a, wk, err, s); break;
   }
 }
 
-template <typename T, int PART, int KIND>
+template <typename T, int PART, int KIND, bool B = false>
 void set_attrs() {
   auto set = [](const void *f) {
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)Slot<T, PART>::SMEM);
   };
-  set((const void *)pair_kernel<T, PART, -1, -1, -1, KIND>);
-  set((const void *)pair_kernel<T, PART, -1, -1, 1, KIND>);
-  set((const void *)pair_kernel<T, PART, -1, 1, -1, KIND>);
-  set((const void *)pair_kernel<T, PART, -1, 1, 1, KIND>);
-  set((const void *)pair_kernel<T, PART, 1, -1, -1, KIND>);
-  set((const void *)pair_kernel<T, PART, 1, -1, 1, KIND>);
-  set((const void *)pair_kernel<T, PART, 1, 1, -1, KIND>);
-  set((const void *)pair_kernel<T, PART, 1, 1, 1, KIND>);
+  set((const void *)pair_kernel<T, PART, -1, -1, -1, KIND, B>);
+  set((const void *)pair_kernel<T, PART, -1, -1, 1, KIND, B>);
+  set((const void *)pair_kernel<T, PART, -1, 1, -1, KIND, B>);
+  set((const void *)pair_kernel<T, PART, -1, 1, 1, KIND, B>);
+  set((const void *)pair_kernel<T, PART, 1, -1, -1, KIND, B>);
+  set((const void *)pair_kernel<T, PART, 1, -1, 1, KIND, B>);
+  set((const void *)pair_kernel<T, PART, 1, 1, -1, KIND, B>);
+  set((const void *)pair_kernel<T, PART, 1, 1, 1, KIND, B>);
 }
 
-template <typename T, int PART>
+template <typename T, int PART, bool B = false>
 int resident_ctas() {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pair_kernel<T, PART, 1, 1, 1, 1>, TT,
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pair_kernel<T, PART, 1, 1, 1, 1, B>, TT,
                                                 Slot<T, PART>::SMEM);
   if (per < 1) per = 1;
   if (sms < 1) sms = 1;
@@ -928,11 +962,16 @@ int resident_ctas() {
 }
 
 // per-(storage, part, kind) entry points, one translation unit each
-// (pair_{f,h,b}{v,s}{0,1,2}.cu; f: FP32, h: FP16, b: BF16 storage)
+// (pair_{f,h,b}{v,s}{0,1,2}.cu; f: FP32, h: FP16, b: BF16 storage); the
+// FP32 units also hold the batched kernels (suffix _b)
 #define CGFD_PAIR_DECL(E, P, K)                                                          \
   void launch_##E##P##K(const Plan &pl, const Maps &m, const StageArgs &a, int *err,   \
                         cudaStream_t s);                                                \
   void attrs_##E##P##K();
+#define CGFD_PAIR_DECL_B(P, K)                                                           \
+  void launch_f##P##K##_b(const Plan &pl, const StageArgs &a, const Work &wk, int *err, \
+                          cudaStream_t s);                                              \
+  void attrs_f##P##K##_b();
 #define CGFD_PAIR_DECL_E(E)                                                   \
   CGFD_PAIR_DECL(E, v, 0) CGFD_PAIR_DECL(E, v, 1) CGFD_PAIR_DECL(E, v, 2)     \
   CGFD_PAIR_DECL(E, s, 0) CGFD_PAIR_DECL(E, s, 1) CGFD_PAIR_DECL(E, s, 2)     \
@@ -941,6 +980,11 @@ int resident_ctas() {
 CGFD_PAIR_DECL_E(f)
 CGFD_PAIR_DECL_E(h)
 CGFD_PAIR_DECL_E(b)
+CGFD_PAIR_DECL_B(v, 0) CGFD_PAIR_DECL_B(v, 1) CGFD_PAIR_DECL_B(v, 2)
+CGFD_PAIR_DECL_B(s, 0) CGFD_PAIR_DECL_B(s, 1) CGFD_PAIR_DECL_B(s, 2)
+int resident_fv_b();
+int resident_fs_b();
+#undef CGFD_PAIR_DECL_B
 #undef CGFD_PAIR_DECL_E
 #undef CGFD_PAIR_DECL
 

@@ -22,13 +22,11 @@ __device__ __forceinline__ float drp5(float m1, float c0, float p1, float p2, fl
   return (CGFD_DA_1 * m1 + CGFD_DA0 * c0 + CGFD_DA1 * p1 + CGFD_DA2 * p2 + CGFD_DA3 * p3) * r;
 }
 
+// one cell (i, j) of layer iz
 template <typename T>
-__global__ void __launch_bounds__(128) timg_kernel(StageArgs a) {
+__device__ __forceinline__ void timg_cell(const StageArgs &a, int i, int j, int iz) {
   using E = Elem<T>;
   const Geom &g = a.g;
-  const int i = blockIdx.x * 32 + threadIdx.x;
-  const int j = blockIdx.y * 4 + threadIdx.y;
-  const int iz = g.top - 2 + blockIdx.z;
   if (i >= g.ni || j >= g.nj) return;
   const int ix = i + XO, iy = j + LFD;
   const long c = (long)gidx(g, ix, iy, iz);
@@ -126,7 +124,26 @@ __global__ void __launch_bounds__(128) timg_kernel(StageArgs a) {
   }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(128) timg_kernel(StageArgs a) {
+  timg_cell<T>(a, blockIdx.x * 32 + threadIdx.x, blockIdx.y * 4 + threadIdx.y,
+               a.g.top - 2 + blockIdx.z);
+}
+
+// n models: blockIdx.z = model * 3 + layer; the grid covers the largest model
+__global__ void __launch_bounds__(128) timg_batch_kernel(const StageArgs *args) {
+  const StageArgs &a = args[blockIdx.z / 3];
+  timg_cell<float>(a, blockIdx.x * 32 + threadIdx.x, blockIdx.y * 4 + threadIdx.y,
+                   a.g.top - 2 + (int)(blockIdx.z % 3));
+}
+
 }  // namespace
+
+void launch_timg_batch(const StageArgs *args, int n, int max_ni, int max_nj, void *stream) {
+  dim3 block(32, 4, 1);
+  dim3 grid((max_ni + 31) / 32, (max_nj + 3) / 4, 3 * n);
+  timg_batch_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(args);
+}
 
 void launch_timg(const StageArgs &a, void *stream) {
   dim3 block(32, 4, 1);

@@ -67,6 +67,16 @@ _SIGS = {
     "cgfd_set_field": (C.c_int, [_P, C.c_int, C.c_int, _fp]),
     "cgfd_check_finite": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "cgfd_set_field_scales": (C.c_int, [_P, _ip]),
+    "cgfd_autotune": (C.c_int, [_P, C.c_int, _fp]),
+    "cgfd_batch_create": (C.c_int, [C.POINTER(Desc), C.c_int, C.POINTER(_P)]),
+    "cgfd_batch_solver": (C.c_int, [_P, C.c_int, C.POINTER(_P)]),
+    "cgfd_batch_prepare": (C.c_int, [_P]),
+    "cgfd_batch_step": (C.c_int, [_P, C.c_int]),
+    "cgfd_batch_step_timed": (C.c_int, [_P, C.c_int, _fp]),
+    "cgfd_batch_sync": (C.c_int, [_P, C.c_double]),
+    "cgfd_batch_autotune": (C.c_int, [_P, C.c_int, _fp]),
+    "cgfd_batch_last_error": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
+    "cgfd_batch_destroy": (C.c_int, [_P]),
     "cgfd_get_field_scales": (C.c_int, [_P, _ip]),
     "cgfd_count_nonfinite_noalloc": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_longlong),
                                                C.c_void_p]),
@@ -129,11 +139,16 @@ def make_desc(ni, nj, nk, steph, stept, nt, con_index, nabs, storage=STORE_F32,
 class Solver:
     """One solver on one GPU (mirrors ChildProcs)."""
 
-    def __init__(self, desc: Desc):
-        h = _P()
-        st = _lib.cgfd_create(C.byref(desc), C.byref(h))
-        if st:
-            raise CgfdError(st, last_error(None))
+    def __init__(self, desc: Desc, _handle=None):
+        if _handle is None:
+            h = _P()
+            st = _lib.cgfd_create(C.byref(desc), C.byref(h))
+            if st:
+                raise CgfdError(st, last_error(None))
+            self._owned = True
+        else:  # a member of a Batch: the batch owns it
+            h = _handle
+            self._owned = False
         self._h = h
         self.desc = desc
         self.shape = (desc.ni + 6, desc.nj + 6, desc.nk + 6)
@@ -145,8 +160,16 @@ class Solver:
 
     def close(self):
         if getattr(self, "_h", None):
-            _lib.cgfd_destroy(self._h)
+            if self._owned:
+                _lib.cgfd_destroy(self._h)
             self._h = None
+
+    def autotune(self, steps: int = 3) -> float:
+        """Picks the fastest work-list shape (state unchanged); returns its
+        milliseconds per step."""
+        ms = C.c_float()
+        self._chk(_lib.cgfd_autotune(self._h, steps, C.byref(ms)))
+        return ms.value
 
     def __del__(self):
         self.close()
@@ -247,6 +270,70 @@ class Solver:
         e = (C.c_int * 9)()
         self._chk(_lib.cgfd_get_field_scales(self._h, e))
         return list(e)
+
+
+class Batch:
+    """Several models stepped together in one persistent launch per stage
+    part (cgfd_batch_*); models[i] is the member Solver for uploads, fields
+    and seismograms."""
+
+    def __init__(self, descs):
+        arr = (Desc * len(descs))(*descs)
+        h = _P()
+        st = _lib.cgfd_batch_create(arr, len(descs), C.byref(h))
+        if st:
+            raise CgfdError(st, last_error(None))
+        self._h = h
+        self.models = []
+        for i, d in enumerate(descs):
+            m = _P()
+            self._chk(_lib.cgfd_batch_solver(self._h, i, C.byref(m)))
+            self.models.append(Solver(d, _handle=m))
+
+    def _chk(self, st):
+        if st:
+            buf = C.create_string_buffer(1024)
+            _lib.cgfd_batch_last_error(self._h, buf, 1024)
+            raise CgfdError(st, buf.value.decode(errors="replace"))
+
+    @property
+    def cells(self) -> int:
+        return sum(d.ni * d.nj * d.nk for d in (m.desc for m in self.models))
+
+    def prepare(self):
+        self._chk(_lib.cgfd_batch_prepare(self._h))
+
+    def step(self, n: int):
+        self._chk(_lib.cgfd_batch_step(self._h, n))
+
+    def sync(self, timeout_s: float = 600.0):
+        self._chk(_lib.cgfd_batch_sync(self._h, timeout_s))
+
+    def step_timed(self, n: int) -> float:
+        ms = C.c_float()
+        self._chk(_lib.cgfd_batch_step_timed(self._h, n, C.byref(ms)))
+        return ms.value
+
+    def autotune(self, steps: int = 2) -> float:
+        ms = C.c_float()
+        self._chk(_lib.cgfd_batch_autotune(self._h, steps, C.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for m in self.models:
+                m._h = None
+            _lib.cgfd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 NOALLOC_MAX_VALUES = 16384 * 8192

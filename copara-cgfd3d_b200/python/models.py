@@ -11,7 +11,9 @@ directly from seeded parameters:
   * gaussian_hill: Gaussian-hill topography on a hybrid grid (curvilinear
     above the conversion layer ConIndex, Cartesian below) with vertically
     stretched spacing, layered media with a seeded correlated perturbation,
-    double-couple source (the 400x400x200 benchmark model and small cases).
+    double-couple source (the 400x400x200 benchmark model and small cases);
+  * batch_models: many uneven hill models with random point sources, for the
+    batched solver (64 models, sides 96..256, in the default set).
 
 Grid coordinates are extended into the ghost cells by linear extrapolation
 (common::interpolated_extend, src/common.cpp:67-95); the metric, CFS-PML
@@ -300,3 +302,36 @@ def small_hill(nt=40, ni=30, nj=26, nk=22, seed=7, **kw) -> Model:
                          corr_len=200.0, seed=seed, src_depth=900.0, f0=0.08,
                          t0=0.25, n_side=3, rcv_spacing=500.0, velabs=7000.0,
                          name="small_hill", **kw)
+
+
+def batch_models(n=64, seed=7, nt=1000, side=(96, 256), nabs_cells=12, h=100.0,
+                 name="batch") -> list:
+    """n independent models of uneven size for a batch: sides U{96..256}
+    (nz = side/2), Gaussian hill height U(0, 2000) m and width U(1, 5) km,
+    two layers with vp U(3000, 7000) and vs = vp/1.73 (density 2600/2800), a
+    random point moment source (M_ij ~ N(0, 1) x 1e15) with a Ricker STF of
+    f0 U(1, 4) Hz, 5 x 5 surface receivers, 12-cell CFS-PML, dt from a CFL
+    number of 0.8 (vp_max dt / min spacing); seeded."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        s = int(rng.integers(side[0], side[1] + 1))
+        nk = s // 2
+        hill_h = float(rng.uniform(0.0, 2000.0))
+        hill_w = float(rng.uniform(1000.0, 5000.0))
+        vp1, vp2 = sorted(rng.uniform(3000.0, 7000.0, 2))
+        dz_top, dz_bot = 0.5 * h, 1.5 * h
+        dt = 0.8 * dz_top / max(vp1, vp2)
+        f0 = float(rng.uniform(1.0, 4.0))
+        depth = nk * h
+        m = gaussian_hill(ni=s, nj=s, nk=nk, h=h, dt=dt, nt=nt, dz_top=dz_top, dz_bot=dz_bot,
+                          hill_h=hill_h, hill_w=hill_w, con_depth=min(3000.0, 0.3 * depth),
+                          layers=((-0.3 * depth, vp1, 2600.0), (-1e30, vp2, 2800.0)),
+                          perturb=0.0, nabs=(nabs_cells,) * 5 + (0,),
+                          src_depth=float(rng.uniform(0.2, 0.5)) * depth, stf_kind="Ricker",
+                          f0=f0, t0=1.2 / f0, n_side=5, rcv_spacing=0.1 * s * h,
+                          velabs=1.2 * max(vp1, vp2), name=f"{name}_{q}")
+        m6 = (rng.standard_normal(6) * 1e15).astype(np.float32)[None, :]
+        m = dataclasses.replace(m, mnt_m6=m6, info=dict(m.info, f0=f0, vp=(vp1, vp2)))
+        out.append(m)
+    return out

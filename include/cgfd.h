@@ -202,6 +202,43 @@ int cgfd_get_field_scales(cgfd_solver *h, int *exp2);
 int cgfd_count_nonfinite_noalloc(const float *d_values, size_t n, long long *n_bad,
                                  void *stream);
 
+/* ------------------------------ autotuning ------------------------------- */
+
+/* Tries the work-list shapes of the default kernel family (items per
+ * resident CTA, z-chunk length, PML cost weight), times `steps` steps of
+ * each (after one warm-up step), keeps the fastest and reports its time per
+ * step in *ms_per_step.  The wavefields, auxiliaries, seismograms and step
+ * count are saved before and restored after, so the simulation is
+ * unchanged; the run needs steps + 1 steps of room in nt and the source time
+ * functions, and a second copy of that state in device memory.
+ * No reference counterpart (the reference reads BlockPerGrid/ThreadPerBlock
+ * from its configuration file). */
+int cgfd_autotune(cgfd_solver *h, int steps, float *ms_per_step);
+
+/* ---------------------- batches of models (one GPU) ----------------------- */
+
+/* A batch steps n independent models (each its own grid, medium, PML,
+ * sources, receivers and dt; FP32 storage, default kernel family) together
+ * through one persistent launch per stage part, so that uneven models share
+ * the GPU without per-model launch tails.  Each model is a member solver:
+ * fill it through the usual upload calls on the handle cgfd_batch_solver
+ * returns, read its seismograms and fields there.  All members must be at the
+ * same step when the batch steps.
+ * No reference counterpart (the reference runs one model per MPI job). */
+typedef struct cgfd_batch cgfd_batch;
+
+int cgfd_batch_create(const cgfd_desc *descs, int n, cgfd_batch **out);
+int cgfd_batch_solver(cgfd_batch *b, int i, cgfd_solver **h);
+int cgfd_batch_prepare(cgfd_batch *b);
+int cgfd_batch_step(cgfd_batch *b, int n_steps);
+/* n_steps steps timed with CUDA events on the batch's stream (whole batch) */
+int cgfd_batch_step_timed(cgfd_batch *b, int n_steps, float *ms);
+int cgfd_batch_sync(cgfd_batch *b, double timeout_s);
+/* cgfd_autotune for the batch's shared work list */
+int cgfd_batch_autotune(cgfd_batch *b, int steps, float *ms_per_step);
+int cgfd_batch_last_error(cgfd_batch *b, char *buf, size_t len);
+int cgfd_batch_destroy(cgfd_batch *b);
+
 /* ---------------- host pre-processing helpers (FP64) ---------------------- */
 
 /* Grid metric from node coordinates (full arrays, reference layout), by
