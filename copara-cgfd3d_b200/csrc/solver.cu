@@ -8,6 +8,7 @@
 // 2678-2830), driven by the step loop of src/simulation.cc:252-711.
 #include "../../include/cgfd.h"
 #include "cgfd_internal.cuh"
+#include "ncwrite.h"
 #include "nonfinite.cuh"
 
 #include <cuda_runtime.h>
@@ -168,6 +169,44 @@ __global__ void rescale_kernel(T *sets, size_t fstride, int comp, float factor) 
     }
 }
 
+// Peak ground velocity (IterationFinalPV, src/calculate.cu:6736-6851): after
+// a step, max |V| per component over time at each surface cell of FW.
+template <typename T>
+__global__ void pgv_kernel(const T *__restrict__ fw, Geom g, float *__restrict__ pgv, float s0,
+                           float s1, float s2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= g.ni || j >= g.nj) return;
+  const size_t m = (size_t)(j + LFD) * g.px + i + XO;
+  const size_t c = (size_t)g.top * g.plane + m;
+  const float sc[3] = {s0, s1, s2};
+  for (int q = 0; q < 3; ++q) {
+    const float v = fabsf(Elem<T>::ld(fw + (size_t)q * g.fstride + c) * sc[q]);
+    float *p = pgv + (size_t)q * g.plane + m;
+    *p = fmaxf(*p, v);
+  }
+}
+
+// Sub-volume of a field set (SWpick, src/calculate.cu:2230-2493): components
+// in mask order, then i, j, k with k fastest, from reference indices
+// start + n*stride.
+template <typename T>
+__global__ void snapshot_kernel(const T *__restrict__ set, Geom g, int mask, int3 st, int3 cnt,
+                                int3 sd, Scales s, float *__restrict__ out) {
+  const long per = (long)cnt.x * cnt.y * cnt.z;
+  int slot = 0;
+  for (int c = 0; c < NCOMP; ++c) {
+    if (!(mask & (1 << c))) continue;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < per;
+         q += (long)gridDim.x * blockDim.x) {
+      const int k = (int)(q % cnt.z), j = (int)((q / cnt.z) % cnt.y), i = (int)(q / cnt.z / cnt.y);
+      const size_t o = (size_t)c * g.fstride +
+                       gidx(g, st.x + i * sd.x + XSH, st.y + j * sd.y, st.z + k * sd.z);
+      out[slot * per + q] = Elem<T>::ld(set + o) * s.sc[c];
+    }
+    ++slot;
+  }
+}
+
 }  // namespace
 
 struct cgfd_solver {
@@ -211,6 +250,7 @@ struct cgfd_solver {
   // graphs (one per step%4 pattern)
   cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
   bool graphs_ok = false;
+  float *d_pgv = nullptr;  // peak ground velocity, [3][plane] at the surface (optional)
   // fused kernels: tensor maps and launch shape; device error flag (bounded
   // waits that expired, alignment self-check)
   void *plan = nullptr;
@@ -264,7 +304,8 @@ void free_all(cgfd_solver *h) {
     if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; }
   void *ptrs[] = {h->state, h->media, h->metric, h->pml, h->aux[0], h->aux[1], h->aux[2],
                   h->matv, h->d_mcell, h->d_fcell, h->d_mcoef, h->d_fcoef, h->d_mstf,
-                  h->d_fstf, h->d_rcell, h->d_seis, h->d_step, h->d_partials, h->d_err};
+                  h->d_fstf, h->d_rcell, h->d_seis, h->d_step, h->d_partials, h->d_err,
+                  h->d_pgv};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->st) cudaStreamDestroy(h->st);
@@ -411,6 +452,20 @@ void launch_record(cgfd_solver *h) {
                                         h->nrecv, h->d.nt, h->d_seis, h->d_step, s);
 }
 
+// the peak-velocity update of one step
+void launch_pgv(cgfd_solver *h) {
+  const float s0 = std::ldexp(1.f, h->sexp[0]), s1 = std::ldexp(1.f, h->sexp[1]),
+              s2 = std::ldexp(1.f, h->sexp[2]);
+  dim3 grid((h->d.ni + 127) / 128, h->d.nj);
+  if (h->elem == ELEM_F16)
+    pgv_kernel<<<grid, 128, 0, h->st>>>((const __half *)h->set[0], h->g, h->d_pgv, s0, s1, s2);
+  else if (h->elem == ELEM_BF16)
+    pgv_kernel<<<grid, 128, 0, h->st>>>((const __nv_bfloat16 *)h->set[0], h->g, h->d_pgv, s0,
+                                        s1, s2);
+  else
+    pgv_kernel<<<grid, 128, 0, h->st>>>((const float *)h->set[0], h->g, h->d_pgv, s0, s1, s2);
+}
+
 StageArgs stage_args(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, int out_set) {
   StageArgs a{};
   a.g = h->g;
@@ -493,6 +548,10 @@ int enqueue_step(cgfd_solver *h, int p) {
   }
   launch_record(h);
   CK(h, cudaGetLastError());
+  if (h->d_pgv) {
+    launch_pgv(h);
+    CK(h, cudaGetLastError());
+  }
   return CGFD_OK;
 }
 
@@ -1045,6 +1104,10 @@ int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms) {
       }
       launch_record(h);
       CK(h, cudaGetLastError());
+      if (h->d_pgv) {
+        launch_pgv(h);
+        CK(h, cudaGetLastError());
+      }
     }
     h->steps++;
   }
@@ -1608,6 +1671,152 @@ int cgfd_batch_destroy(cgfd_batch *b) {
   }
   for (cgfd_solver *h : b->m) cgfd_destroy(h);
   delete b;
+  return CGFD_OK;
+}
+
+
+// ------------------------------- outputs -----------------------------------
+
+int cgfd_enable_peak_velocity(cgfd_solver *h, int on) {
+  if (!h) return arg_fail(h, "null handle");
+  DevGuard guard(h->d.device);
+  CK(h, cudaStreamSynchronize(h->st));
+  if (on) {
+    if (!h->d_pgv) CK(h, cudaMalloc(&h->d_pgv, 3 * h->g.plane * sizeof(float)));
+    CK(h, cudaMemset(h->d_pgv, 0, 3 * h->g.plane * sizeof(float)));
+  } else if (h->d_pgv) {
+    cudaFree(h->d_pgv);
+    h->d_pgv = nullptr;
+  }
+  invalidate(h);  // the step graphs gain or lose the update
+  return CGFD_OK;
+}
+
+int cgfd_get_peak_velocity(cgfd_solver *h, float *out) {
+  if (!h || !out) return arg_fail(h, "null argument");
+  if (!h->d_pgv) {
+    h->err = "peak velocity is not enabled";
+    return CGFD_ERR_STATE;
+  }
+  DevGuard guard(h->d.device);
+  CK(h, cudaStreamSynchronize(h->st));
+  std::vector<float> v(3 * h->g.plane);
+  CK(h, cudaMemcpy(v.data(), h->d_pgv, v.size() * sizeof(float), cudaMemcpyDeviceToHost));
+  const int ni = h->d.ni, nj = h->d.nj;
+  for (int q = 0; q < 3; ++q)
+    for (int i = 0; i < ni; ++i)
+      for (int j = 0; j < nj; ++j)
+        out[((size_t)q * ni + i) * nj + j] =
+            v[(size_t)q * h->g.plane + (size_t)(j + LFD) * h->g.px + i + XO];
+  return CGFD_OK;
+}
+
+int cgfd_get_snapshot(cgfd_solver *h, int set, const int *start, const int *count,
+                      const int *stride, int comp_mask, float *out) {
+  if (!h || !start || !count || !stride || !out) return arg_fail(h, "null argument");
+  if (comp_mask <= 0 || comp_mask >= (1 << NCOMP)) return arg_fail(h, "bad component mask");
+  const int n3[3] = {h->d.ni + 6, h->d.nj + 6, h->d.nk + 6};
+  for (int a = 0; a < 3; ++a) {
+    if (count[a] < 1 || stride[a] < 1 || start[a] < 0 ||
+        start[a] + (long)(count[a] - 1) * stride[a] >= n3[a])
+      return arg_fail(h, "snapshot outside the grid");
+  }
+  void *base = set_ptr(h, set, 0);
+  if (!base) return arg_fail(h, "bad set");
+  int nc = 0;
+  for (int c = 0; c < NCOMP; ++c) nc += (comp_mask >> c) & 1;
+  const size_t n = (size_t)nc * count[0] * count[1] * count[2];
+  DevGuard guard(h->d.device);
+  CK(h, cudaStreamSynchronize(h->st));
+  float *tmp = nullptr;
+  CK(h, cudaMalloc(&tmp, n * sizeof(float)));
+  Scales sc;
+  for (int c = 0; c < NCOMP; ++c) sc.sc[c] = std::ldexp(1.f, h->sexp[c]);
+  const int3 st3 = make_int3(start[0], start[1], start[2]);
+  const int3 cn3 = make_int3(count[0], count[1], count[2]);
+  const int3 sd3 = make_int3(stride[0], stride[1], stride[2]);
+  if (h->elem == ELEM_F16)
+    snapshot_kernel<<<592, 256, 0, h->st>>>((const __half *)base, h->g, comp_mask, st3, cn3, sd3,
+                                            sc, tmp);
+  else if (h->elem == ELEM_BF16)
+    snapshot_kernel<<<592, 256, 0, h->st>>>((const __nv_bfloat16 *)base, h->g, comp_mask, st3,
+                                            cn3, sd3, sc, tmp);
+  else
+    snapshot_kernel<<<592, 256, 0, h->st>>>((const float *)base, h->g, comp_mask, st3, cn3, sd3,
+                                            sc, tmp);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, tmp, n * sizeof(float), cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return cuda_fail(h, e, "snapshot");
+  return CGFD_OK;
+}
+
+// seismo.nc of the reference (src/seisnc.cpp:1229-1364) in NetCDF classic:
+// TimeNum (record) x PointNum; Vx..Tyz, currTime = (it+1)*stept, Pnum, Lnum,
+// posx/posy/posz
+int cgfd_write_seismograms_nc(cgfd_solver *h, const char *path, const float *pos) {
+  if (!h || !path) return arg_fail(h, "null argument");
+  const int n = h->nrecv, nt = h->d.nt;
+  int done = 0;
+  std::vector<float> seis((size_t)9 * n * (nt > 0 ? nt : 1));
+  int st = cgfd_get_seismograms(h, n ? seis.data() : nullptr, &done);
+  if (st) return st;
+  // [c][recv][t] -> per component [t][recv]
+  std::vector<std::vector<float>> comp(9, std::vector<float>((size_t)done * n));
+  for (int c = 0; c < 9; ++c)
+    for (int r = 0; r < n; ++r)
+      for (int t = 0; t < done; ++t)
+        comp[c][(size_t)t * n + r] = seis[((size_t)c * n + r) * nt + t];
+  std::vector<float> tcur(done);
+  for (int t = 0; t < done; ++t) tcur[t] = (float)((t + 1) * h->d.stept);
+  std::vector<int> pnum(n), lnum(n, 1);
+  std::vector<float> px(n), py(n), pz(n);
+  std::vector<int> rloc;
+  for (int r = 0; r < n; ++r) {
+    pnum[r] = r + 1;
+    px[r] = pos ? pos[3 * r] : 0.f;
+    py[r] = pos ? pos[3 * r + 1] : 0.f;
+    pz[r] = pos ? pos[3 * r + 2] : 0.f;
+  }
+  using namespace nc;
+  std::vector<Dim> dims = {{"TimeNum", 0}, {"PointNum", (size_t)n}};
+  static const char *names[9] = {"Vx", "Vy", "Vz", "Txx", "Tyy", "Tzz", "Txy", "Txz", "Tyz"};
+  std::vector<Var> vars;
+  for (int c = 0; c < 9; ++c) vars.push_back({names[c], NC_FLOAT, {0, 1}, comp[c].data()});
+  vars.push_back({"currTime", NC_FLOAT, {0}, tcur.data()});
+  vars.push_back({"Pnum", NC_INT, {1}, pnum.data()});
+  vars.push_back({"Lnum", NC_INT, {1}, lnum.data()});
+  vars.push_back({"posx", NC_FLOAT, {1}, px.data()});
+  vars.push_back({"posy", NC_FLOAT, {1}, py.data()});
+  vars.push_back({"posz", NC_FLOAT, {1}, pz.data()});
+  const std::string content("Velocity and Stress seismogram", 31);  // with its NUL, as written
+  if (!write_classic(path, dims, {{"Content", content}}, vars, (size_t)done)) {
+    h->err = std::string("cannot write ") + path;
+    return CGFD_ERR_ARG;
+  }
+  return CGFD_OK;
+}
+
+// peakvel.nc of the reference (src/seisnc.cpp:1671-1757) in NetCDF classic:
+// i x j; Vx, Vy, Vz (the reference's file holds Vy in its Vz variable; this
+// one holds Vz)
+int cgfd_write_peak_velocity_nc(cgfd_solver *h, const char *path) {
+  if (!h || !path) return arg_fail(h, "null argument");
+  std::vector<float> pv((size_t)3 * h->d.ni * h->d.nj);
+  int st = cgfd_get_peak_velocity(h, pv.data());
+  if (st) return st;
+  using namespace nc;
+  const size_t m = (size_t)h->d.ni * h->d.nj;
+  std::vector<Dim> dims = {{"i", (size_t)h->d.ni}, {"j", (size_t)h->d.nj}};
+  std::vector<Var> vars = {{"Vx", NC_FLOAT, {0, 1}, pv.data()},
+                           {"Vy", NC_FLOAT, {0, 1}, pv.data() + m},
+                           {"Vz", NC_FLOAT, {0, 1}, pv.data() + 2 * m}};
+  if (!write_classic(path, dims, {}, vars, 0)) {
+    h->err = std::string("cannot write ") + path;
+    return CGFD_ERR_ARG;
+  }
   return CGFD_OK;
 }
 

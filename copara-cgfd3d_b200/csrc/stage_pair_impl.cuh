@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
   using S = Slot<T, PART>;
   constexpr int HOFF = Halo<T>::HOFF, HX = Halo<T>::HX, HPL = Halo<T>::HPL;
   constexpr int NC = PartInfo<PART>::NC, C0 = PartInfo<PART>::C0;
-  constexpr int NS = PartInfo<PART>::NS, S0 = PartInfo<PART>::S0;
+  constexpr int S0 = PartInfo<PART>::S0;
   constexpr int NCOEF = PartInfo<PART>::NCOEF, COEF0 = PartInfo<PART>::COEF0;
   constexpr int DIR = (Z > 0) ? -1 : 1;  // march direction in z
   extern __shared__ __align__(128) unsigned char smem_raw[];

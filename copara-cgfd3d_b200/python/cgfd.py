@@ -68,6 +68,11 @@ _SIGS = {
     "cgfd_check_finite": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "cgfd_set_field_scales": (C.c_int, [_P, _ip]),
     "cgfd_autotune": (C.c_int, [_P, C.c_int, _fp]),
+    "cgfd_enable_peak_velocity": (C.c_int, [_P, C.c_int]),
+    "cgfd_get_peak_velocity": (C.c_int, [_P, _fp]),
+    "cgfd_get_snapshot": (C.c_int, [_P, C.c_int, _ip, _ip, _ip, C.c_int, _fp]),
+    "cgfd_write_seismograms_nc": (C.c_int, [_P, C.c_char_p, _fp]),
+    "cgfd_write_peak_velocity_nc": (C.c_int, [_P, C.c_char_p]),
     "cgfd_batch_create": (C.c_int, [C.POINTER(Desc), C.c_int, C.POINTER(_P)]),
     "cgfd_batch_solver": (C.c_int, [_P, C.c_int, C.POINTER(_P)]),
     "cgfd_batch_prepare": (C.c_int, [_P]),
@@ -163,6 +168,36 @@ class Solver:
             if self._owned:
                 _lib.cgfd_destroy(self._h)
             self._h = None
+
+    def enable_peak_velocity(self, on: bool = True):
+        self._chk(_lib.cgfd_enable_peak_velocity(self._h, int(on)))
+
+    def peak_velocity(self) -> np.ndarray:
+        """max |V| per component over the steps since enabling, [3][ni][nj]."""
+        out = np.empty((3, self.desc.ni, self.desc.nj), np.float32)
+        self._chk(_lib.cgfd_get_peak_velocity(self._h, _f(out)))
+        return out
+
+    def snapshot(self, start, count, stride=(1, 1, 1), comps=range(9), set_=SET_FW):
+        """Sub-volume of a field set (reference full-array indices), returned
+        as [component][i][j][k]."""
+        mask = 0
+        for c in comps:
+            mask |= 1 << c
+        n = bin(mask).count("1")
+        out = np.empty((n,) + tuple(int(c) for c in count), np.float32)
+        a = [np.ascontiguousarray(x, np.int32) for x in (start, count, stride)]
+        self._chk(_lib.cgfd_get_snapshot(self._h, set_, _i(a[0]), _i(a[1]), _i(a[2]), mask,
+                                         _f(out)))
+        return out
+
+    def write_seismograms_nc(self, path: str, pos=None):
+        p = None if pos is None else _as(pos, np.float32).reshape(-1)
+        self._chk(_lib.cgfd_write_seismograms_nc(self._h, path.encode(),
+                                                 None if p is None else _f(p)))
+
+    def write_peak_velocity_nc(self, path: str):
+        self._chk(_lib.cgfd_write_peak_velocity_nc(self._h, path.encode()))
 
     def autotune(self, steps: int = 3) -> float:
         """Picks the fastest work-list shape (state unchanged); returns its

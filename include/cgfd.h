@@ -202,6 +202,30 @@ int cgfd_get_field_scales(cgfd_solver *h, int *exp2);
 int cgfd_count_nonfinite_noalloc(const float *d_values, size_t n, long long *n_bad,
                                  void *stream);
 
+/* -------------------------------- outputs --------------------------------- */
+
+/* Peak ground velocity (the reference's IterationFinalPV / PV_export): when
+ * enabled, every step updates max |V| per component at each surface cell
+ * (maxima reset to zero on enabling).  out: [3][ni][nj] (valid cells, j
+ * fastest). */
+int cgfd_enable_peak_velocity(cgfd_solver *h, int on);
+int cgfd_get_peak_velocity(cgfd_solver *h, float *out);
+
+/* Sub-volume of a field set (the reference's SWpick/snap_export): reference
+ * full-array indices start + n*stride (n < count) per axis; components of
+ * comp_mask (bit c = component c) in order; out: [component][i][j][k], k
+ * fastest. */
+int cgfd_get_snapshot(cgfd_solver *h, int set, const int *start, const int *count,
+                      const int *stride, int comp_mask, float *out);
+
+/* The reference's seismo.nc / peakvel.nc variables and dimensions, written
+ * as NetCDF classic (64-bit offset) files: seismograms of the steps done
+ * (Vx..Tyz [TimeNum][PointNum], currTime, Pnum, Lnum, posx/y/z from pos =
+ * 3 floats per receiver or NULL for zeros); peak velocities Vx, Vy, Vz [i][j].
+ * The reference writes NetCDF-4 (HDF5); no HDF5 library is used here. */
+int cgfd_write_seismograms_nc(cgfd_solver *h, const char *path, const float *pos);
+int cgfd_write_peak_velocity_nc(cgfd_solver *h, const char *path);
+
 /* ------------------------------ autotuning ------------------------------- */
 
 /* Tries the work-list shapes of the default kernel family (items per
