@@ -34,6 +34,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include <vector_types.h>
+
 #include "elem.cuh"
 
 namespace cgfd {
@@ -173,6 +175,16 @@ bool pair_batch_set_args(void *plan, const StageArgs *args);
 // for every model; rep carries the stage's X, Y, Z and rk
 void launch_stage_pair_batch(const void *plan, int pattern, const StageArgs &rep, int *err,
                              void *stream);
+// learned absorbing layer (mlp.cu): the correction of every layer cell
+// (gain: [depth][9]; delta: 9 x n scratch), and the training features of
+// the layer's cells
+size_t mlp_delta_smem();
+void launch_mlp_step(const float *fw, size_t fs, const float *lam2mu, const float *irho,
+                     const int4 *cells, int n, const void *w, const float *gain, float *delta,
+                     void *stream);
+void launch_mlp_features(const float *fw, size_t fs, const float *lam2mu, const float *irho,
+                         const int4 *cells, int n, float *xs, float *scales, float *zs,
+                         void *stream);
 // the traction image of n models (args: device array, one per model)
 void launch_timg_batch(const StageArgs *args, int n, int max_ni, int max_nj, void *stream);
 

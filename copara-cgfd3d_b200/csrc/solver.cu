@@ -251,6 +251,15 @@ struct cgfd_solver {
   cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
   bool graphs_ok = false;
   float *d_pgv = nullptr;  // peak ground velocity, [3][plane] at the surface (optional)
+  // learned absorbing layer (optional): cells {internal index, normal
+  // offset, 0, 0}, their reference indices, FP16 weights, 9 x n scratch
+  int mlp_n = 0;
+  int4 *d_mlp_cells = nullptr;
+  std::vector<int> mlp_ijk;
+  void *d_mlp_w = nullptr;
+  float *d_mlp_delta = nullptr;
+  float *d_mlp_gain = nullptr;  // [width][9]
+  int mlp_width = 0;
   // fused kernels: tensor maps and launch shape; device error flag (bounded
   // waits that expired, alignment self-check)
   void *plan = nullptr;
@@ -305,7 +314,7 @@ void free_all(cgfd_solver *h) {
   void *ptrs[] = {h->state, h->media, h->metric, h->pml, h->aux[0], h->aux[1], h->aux[2],
                   h->matv, h->d_mcell, h->d_fcell, h->d_mcoef, h->d_fcoef, h->d_mstf,
                   h->d_fstf, h->d_rcell, h->d_seis, h->d_step, h->d_partials, h->d_err,
-                  h->d_pgv};
+                  h->d_pgv, h->d_mlp_cells, h->d_mlp_w, h->d_mlp_delta};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->st) cudaStreamDestroy(h->st);
@@ -452,6 +461,13 @@ void launch_record(cgfd_solver *h) {
                                         h->nrecv, h->d.nt, h->d_seis, h->d_step, s);
 }
 
+// the learned layer's correction of FW after a step
+void launch_mlp(cgfd_solver *h) {
+  const size_t fs = h->g.fstride;
+  launch_mlp_step((const float *)h->set[0], fs, h->media, h->media + 2 * fs, h->d_mlp_cells,
+                  h->mlp_n, h->d_mlp_w, h->d_mlp_gain, h->d_mlp_delta, h->st);
+}
+
 // the peak-velocity update of one step
 void launch_pgv(cgfd_solver *h) {
   const float s0 = std::ldexp(1.f, h->sexp[0]), s1 = std::ldexp(1.f, h->sexp[1]),
@@ -545,6 +561,10 @@ int enqueue_step(cgfd_solver *h, int p) {
     const int *dd = DIRS[p][rk];
     int st = launch_stage(h, rk, dd[0], dd[1], dd[2], ins[rk], outs[rk], -1);
     if (st) return st;
+  }
+  if (h->mlp_n) {
+    launch_mlp(h);
+    CK(h, cudaGetLastError());
   }
   launch_record(h);
   CK(h, cudaGetLastError());
@@ -1101,6 +1121,10 @@ int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms) {
           launch_sources(sa, h->st);
           CK(h, cudaGetLastError());
         }
+      }
+      if (h->mlp_n) {
+        launch_mlp(h);
+        CK(h, cudaGetLastError());
       }
       launch_record(h);
       CK(h, cudaGetLastError());
@@ -1817,6 +1841,108 @@ int cgfd_write_peak_velocity_nc(cgfd_solver *h, const char *path) {
     h->err = std::string("cannot write ") + path;
     return CGFD_ERR_ARG;
   }
+  return CGFD_OK;
+}
+
+
+// ------------------------- learned absorbing layer -------------------------
+
+int cgfd_set_boundary_mlp(cgfd_solver *h, int width, const void *weights_fp16) {
+  if (!h) return arg_fail(h, "null handle");
+  DevGuard guard(h->d.device);
+  CK(h, cudaStreamSynchronize(h->st));
+  for (void **p : {(void **)&h->d_mlp_cells, &h->d_mlp_w, (void **)&h->d_mlp_delta,
+                   (void **)&h->d_mlp_gain})
+    if (*p) { cudaFree(*p); *p = nullptr; }
+  h->mlp_n = 0;
+  h->mlp_width = 0;
+  h->mlp_ijk.clear();
+  invalidate(h);
+  if (!weights_fp16) return CGFD_OK;
+  if (h->elem != ELEM_F32) return arg_fail(h, "the learned layer needs FP32 storage");
+  const int ni = h->d.ni, nj = h->d.nj, nk = h->d.nk;
+  if (width < 1 || width > 16 || ni < width + 5 || nj < width + 5 || nk < width + 5)
+    return arg_fail(h, "bad layer width for this grid");
+  const int *nb = h->d.nabs;
+  // nearest absorbing face of a valid cell within the layer: 0 x-, 1 x+,
+  // 2 y-, 3 y+, 4 z- (bottom); -1 outside the layer
+  int depth = 0;  // of the last cell face() placed in the layer
+  auto face = [&](int i, int j, int k) {
+    const int dist[5] = {nb[0] > 0 ? i : 1 << 30, nb[1] > 0 ? ni - 1 - i : 1 << 30,
+                         nb[2] > 0 ? j : 1 << 30, nb[3] > 0 ? nj - 1 - j : 1 << 30,
+                         nb[4] > 0 ? k : 1 << 30};
+    int best = -1, bd = width;
+    for (int f = 0; f < 5; ++f)
+      if (dist[f] < bd) { bd = dist[f]; best = f; }
+    depth = bd;
+    return best;
+  };
+  const long step[5] = {1, -1, (long)h->g.px, -(long)h->g.px, (long)h->g.plane};
+  std::vector<int4> cells;
+  for (int i = 0; i < ni; ++i)
+    for (int j = 0; j < nj; ++j)
+      for (int k = 0; k < nk; ++k) {
+        const int f = face(i, j, k);
+        if (f < 0) continue;
+        cells.push_back(
+            make_int4((int)gidx(h->g, i + XO, j + LFD, k + LFD), (int)step[f], depth, 0));
+        h->mlp_ijk.insert(h->mlp_ijk.end(), {i + LFD, j + LFD, k + LFD});
+      }
+  h->mlp_n = (int)cells.size();
+  if (!h->mlp_n) return CGFD_OK;
+  CK(h, cudaMalloc(&h->d_mlp_cells, cells.size() * sizeof(int4)));
+  CK(h, cudaMemcpy(h->d_mlp_cells, cells.data(), cells.size() * sizeof(int4),
+                   cudaMemcpyHostToDevice));
+  CK(h, cudaMalloc(&h->d_mlp_w, CGFD_MLP_PARAMS * 2));
+  CK(h, cudaMemcpy(h->d_mlp_w, weights_fp16, CGFD_MLP_PARAMS * 2, cudaMemcpyHostToDevice));
+  CK(h, cudaMalloc(&h->d_mlp_delta, (size_t)9 * h->mlp_n * sizeof(float)));
+  CK(h, cudaMalloc(&h->d_mlp_gain, (size_t)9 * width * sizeof(float)));
+  h->mlp_width = width;
+  return cgfd_set_boundary_mlp_gains(h, nullptr);
+}
+
+int cgfd_set_boundary_mlp_gains(cgfd_solver *h, const float *gains) {
+  if (!h) return arg_fail(h, "null handle");
+  if (!h->mlp_n) return arg_fail(h, "no learned layer set");
+  DevGuard guard(h->d.device);
+  CK(h, cudaStreamSynchronize(h->st));
+  std::vector<float> g((size_t)9 * h->mlp_width, 1.f);
+  if (gains) std::memcpy(g.data(), gains, g.size() * sizeof(float));
+  for (float v : g)
+    if (!std::isfinite(v)) return arg_fail(h, "non-finite gain");
+  CK(h, cudaMemcpy(h->d_mlp_gain, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice));
+  invalidate(h);
+  return CGFD_OK;
+}
+
+int cgfd_boundary_mlp_cells(cgfd_solver *h, int *ijk, int *n) {
+  if (!h || !n) return arg_fail(h, "null argument");
+  const int cap = *n;
+  *n = h->mlp_n;
+  if (ijk && cap >= h->mlp_n)
+    std::memcpy(ijk, h->mlp_ijk.data(), h->mlp_ijk.size() * sizeof(int));
+  return CGFD_OK;
+}
+
+int cgfd_boundary_mlp_features(cgfd_solver *h, float *x, float *scale, float *rho_vp) {
+  if (!h || !x || !scale || !rho_vp) return arg_fail(h, "null argument");
+  if (!h->mlp_n) return arg_fail(h, "no learned layer set");
+  DevGuard guard(h->d.device);
+  CK(h, cudaStreamSynchronize(h->st));
+  const size_t n = h->mlp_n, fs = h->g.fstride;
+  float *d = nullptr;
+  CK(h, cudaMalloc(&d, n * (45 + 2) * sizeof(float)));
+  launch_mlp_features((const float *)h->set[0], fs, h->media, h->media + 2 * fs, h->d_mlp_cells,
+                      h->mlp_n, d, d + n * 45, d + n * 46, h->st);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(x, d, n * 45 * sizeof(float), cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(scale, d + n * 45, n * sizeof(float), cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(rho_vp, d + n * 46, n * sizeof(float), cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(h, e, "layer features");
   return CGFD_OK;
 }
 

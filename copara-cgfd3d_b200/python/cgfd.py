@@ -68,6 +68,11 @@ _SIGS = {
     "cgfd_check_finite": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "cgfd_set_field_scales": (C.c_int, [_P, _ip]),
     "cgfd_autotune": (C.c_int, [_P, C.c_int, _fp]),
+    "cgfd_set_boundary_mlp": (C.c_int, [_P, C.c_int, C.c_void_p]),
+    "cgfd_set_boundary_mlp_gains": (C.c_int, [_P, _fp]),
+    "cgfd_boundary_mlp_cells": (C.c_int, [_P, _ip, _ip]),
+    "cgfd_boundary_mlp_features": (C.c_int, [_P, _fp, _fp, _fp]),
+    "cgfd_mlp_gradient": (C.c_int, [C.c_void_p, _fp, _fp, C.c_int, _fp, _fp]),
     "cgfd_enable_peak_velocity": (C.c_int, [_P, C.c_int]),
     "cgfd_get_peak_velocity": (C.c_int, [_P, _fp]),
     "cgfd_get_snapshot": (C.c_int, [_P, C.c_int, _ip, _ip, _ip, C.c_int, _fp]),
@@ -168,6 +173,40 @@ class Solver:
             if self._owned:
                 _lib.cgfd_destroy(self._h)
             self._h = None
+
+    def set_boundary_mlp(self, width: int, weights):
+        """Learned layer correction (weights: CGFD_MLP_PARAMS values, stored
+        as FP16; None disables)."""
+        if weights is None:
+            self._chk(_lib.cgfd_set_boundary_mlp(self._h, width, None))
+            return
+        w = np.ascontiguousarray(weights, np.float16)
+        assert w.size == MLP_PARAMS
+        self._chk(_lib.cgfd_set_boundary_mlp(self._h, width, w.ctypes.data_as(C.c_void_p)))
+
+    def set_boundary_mlp_gains(self, gains=None):
+        """Per (depth, component) gains of the correction, [width][9]; None: 1."""
+        if gains is None:
+            self._chk(_lib.cgfd_set_boundary_mlp_gains(self._h, None))
+            return
+        g = np.ascontiguousarray(gains, np.float32)
+        self._chk(_lib.cgfd_set_boundary_mlp_gains(self._h, _f(g)))
+
+    def boundary_mlp_cells(self) -> np.ndarray:
+        n = C.c_int(0)
+        self._chk(_lib.cgfd_boundary_mlp_cells(self._h, None, C.byref(n)))
+        out = np.empty((n.value, 3), np.int32)
+        self._chk(_lib.cgfd_boundary_mlp_cells(self._h, _i(out), C.byref(n)))
+        return out
+
+    def boundary_mlp_features(self):
+        """(x [n][45], scale [n], rho*vp [n]) of the layer's cells now."""
+        n = len(self.boundary_mlp_cells())
+        x = np.empty((n, 45), np.float32)
+        sc = np.empty(n, np.float32)
+        z = np.empty(n, np.float32)
+        self._chk(_lib.cgfd_boundary_mlp_features(self._h, _f(x), _f(sc), _f(z)))
+        return x, sc, z
 
     def enable_peak_velocity(self, on: bool = True):
         self._chk(_lib.cgfd_enable_peak_velocity(self._h, int(on)))
@@ -305,6 +344,24 @@ class Solver:
         e = (C.c_int * 9)()
         self._chk(_lib.cgfd_get_field_scales(self._h, e))
         return list(e)
+
+
+MLP_PARAMS = 7689
+
+
+def mlp_gradient(weights, x, t):
+    """Mean squared error of the layer MLP on samples (x [n][45] -> t [n][9])
+    and its gradient (device kernel); returns (loss, grad)."""
+    w = np.ascontiguousarray(weights, np.float16)
+    x = _as(x, np.float32)
+    t = _as(t, np.float32)
+    g = np.empty(MLP_PARAMS, np.float32)
+    loss = C.c_float()
+    st = _lib.cgfd_mlp_gradient(w.ctypes.data_as(C.c_void_p), _f(x), _f(t), len(x), _f(g),
+                                C.byref(loss))
+    if st:
+        raise CgfdError(st, last_error(None))
+    return loss.value, g
 
 
 class Batch:

@@ -226,6 +226,38 @@ int cgfd_get_snapshot(cgfd_solver *h, int set, const int *start, const int *coun
 int cgfd_write_seismograms_nc(cgfd_solver *h, const char *path, const float *pos);
 int cgfd_write_peak_velocity_nc(cgfd_solver *h, const char *path);
 
+/* ------------------------ learned absorbing layer ------------------------ */
+
+/* Parameters of the layer's MLP (45 -> 64 -> 64 -> 9, SiLU), FP16, in the
+ * order W1 [64][45], b1 [64], W2 [64][64], b2 [64], W3 [9][64], b3 [9]. */
+#define CGFD_MLP_PARAMS 7689
+
+/* Enables (weights != NULL) or disables the learned correction of the thin
+ * absorbing layer: after every step, each valid cell within `width` cells of
+ * an absorbing face gets FW += MLP(features), the features being the 9
+ * components at the cell and the next 4 cells along its inward normal,
+ * stresses over rho*vp, normalised by their largest magnitude (the output
+ * is scaled back the same way).  FP32 storage only.
+ * No reference counterpart (the reference has sponge and CFS-PML layers). */
+int cgfd_set_boundary_mlp(cgfd_solver *h, int width, const void *weights_fp16);
+/* Gains of the correction per depth in the layer (0: the cells next to the
+ * domain's edge) and component: gains [width][9], the correction of a cell
+ * at depth d, component c is multiplied by gains[d*9+c]; NULL sets all to 1
+ * (the default after cgfd_set_boundary_mlp). */
+int cgfd_set_boundary_mlp_gains(cgfd_solver *h, const float *gains);
+/* The layer's cells (reference indices, 3 ints each), in the order of the
+ * features below; *n: capacity in, count out. */
+int cgfd_boundary_mlp_cells(cgfd_solver *h, int *ijk, int *n);
+/* The current normalised features of the layer's cells (training samples):
+ * x [n][45], the per-cell scale and rho*vp. */
+int cgfd_boundary_mlp_features(cgfd_solver *h, float *x, float *scale, float *rho_vp);
+/* Training: for n samples of features x [n][45] and target outputs t [n][9],
+ * the mean over samples of the squared output error and its gradient with
+ * respect to the parameters (FP32, CGFD_MLP_PARAMS values), on the current
+ * device. */
+int cgfd_mlp_gradient(const void *weights_fp16, const float *x, const float *t, int n,
+                      float *grad, float *loss);
+
 /* ------------------------------ autotuning ------------------------------- */
 
 /* Tries the work-list shapes of the default kernel family (items per

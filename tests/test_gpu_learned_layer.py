@@ -1,0 +1,103 @@
+"""The learned thin absorbing layer's device kernels against the CPU
+restatement (oracle/mlp_oracle.py): the training gradient, and the
+correction the solver applies to the layer cells after a step."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import cgfd
+import models
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                "oracle"))
+import mlp_oracle as M  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def test_device_gradient_matches_oracle():
+    rng = np.random.default_rng(4)
+    w = M.init_weights(2)
+    x = rng.uniform(-1, 1, (700, M.NIN)).astype(np.float32)
+    t = (rng.standard_normal((700, M.NOUT)) * 0.2).astype(np.float32)
+    loss, g = cgfd.mlp_gradient(w, x, t)
+    loss_ref, g_ref = M.loss_grad(w.astype(np.float64), x, t)
+    assert abs(loss - loss_ref) <= 1e-5 * loss_ref
+    assert np.linalg.norm(g - g_ref) <= 1e-5 * np.linalg.norm(g_ref)
+
+
+def test_layer_correction_matches_oracle():
+    m = models.small_flat(nt=20, nabs=(5, 5, 5, 5, 5, 0))
+    w = M.init_weights(5, scale=0.5)
+    w[M.OW3:] = (np.random.default_rng(6).standard_normal(M.NPAR - M.OW3) * 0.05)
+    w = w.astype(np.float16)
+    a, b = cgfd.Solver(m.desc()), cgfd.Solver(m.desc())
+    for s in (a, b):
+        m.load(s)
+        s.step(12)
+    a.set_boundary_mlp(4, np.zeros(M.NPAR, np.float16))  # features only
+    b.set_boundary_mlp(4, w)
+    gains = np.random.default_rng(8).uniform(0.0, 1.5, (4, 9)).astype(np.float32)
+    b.set_boundary_mlp_gains(gains)
+    a.step(1)
+    b.step(1)
+    x, scale, z = a.boundary_mlp_features()
+    cells = a.boundary_mlp_cells()
+    assert len(cells) > 0 and np.array_equal(cells, b.boundary_mlp_cells())
+    y, _, _ = M.forward(w, x)
+    on = scale > 1e-30
+    d = np.minimum.reduce([cells[:, 0] - 3, m.ni + 2 - cells[:, 0], cells[:, 1] - 3,
+                           m.nj + 2 - cells[:, 1], cells[:, 2] - 3])
+    assert d.min() == 0 and d.max() == 3
+    delta = (M.correction(y, x[:, :9], gains[d]) * scale[:, None]
+             * np.where(np.arange(9) < 3, 1.0, z[:, None]))
+    delta[~on] = 0.0
+    fa = np.stack([a.get_field(c) for c in range(9)])
+    fb = np.stack([b.get_field(c) for c in range(9)])
+    i, j, k = cells[:, 0], cells[:, 1], cells[:, 2]
+    got = (fb[:, i, j, k] - fa[:, i, j, k]).T
+    ref_scale = np.abs(delta).max()
+    assert ref_scale > 0
+    assert np.abs(got - delta).max() <= 1e-4 * ref_scale + 1e-6 * np.abs(fa[:, i, j, k]).max()
+    # cells outside the layer are untouched
+    mask = np.ones(fa.shape[1:], bool)
+    mask[i, j, k] = False
+    assert np.array_equal(fa[:, mask], fb[:, mask])
+    a.close()
+    b.close()
+
+
+def test_training_plumbing_reduces_the_one_step_residual():
+    import learned_layer as L
+    s = L.Setup(interior=(24, 24, 12), pad=20, steps=30)
+    rng = np.random.default_rng(1)
+    x, t, sc, dep = L.teacher_samples(s, (12, 12, 6), rng.standard_normal(6) * 1e16, 5.0,
+                                      rng=rng, per_step=500)
+    assert len(x) > 1000 and np.isfinite(t).all()
+    w0 = L.init_weights(0)
+    w, hist = L.train(x, t, w0, iters=60, batch=4000, lr=3e-3)
+    assert hist[-1] < hist[0]
+    g = L.fit_gains(w, x, t, sc, dep)
+    assert g.shape == (4, 9) and ((g >= 0) & (g <= 1)).all()
+
+
+def test_committed_weights_lower_the_reflected_energy():
+    """The trained layer (data/layer_mlp_w4.npz) on a source it was not
+    trained on: less reflected energy than the plain 4-cell PML over 200
+    steps, and a small, decaying late field over 1500 steps."""
+    import learned_layer as L
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                        "copara-cgfd3d_b200", "data", "layer_mlp_w4.npz")
+    d = np.load(path)
+    s = L.Setup()
+    src, m6, f0 = (20, 27, 9), np.array([0.7, -1.1, 0.4, 0.9, -0.3, 0.5]) * 1e16, 4.5
+    r = L.evaluate(s, src, m6, f0, mlp=d["weights"], gains=d["gains"])
+    assert r["pml4_mlp"] < 0.95 * r["pml4"] < 0.01
+    m, off = L.domain(s, 4, src, m6, f0, nt=1502)
+    rcv = L.interior_receivers(s)
+    u = np.abs(L.run_layer(m, off, rcv, 1500, d["weights"], d["gains"]))
+    assert np.isfinite(u).all()
+    # the late field is small and not growing
+    assert u[:, :, 1000:].max() <= min(1e-4 * u.max(), u[:, :, 500:1000].max())
