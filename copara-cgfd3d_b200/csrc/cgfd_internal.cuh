@@ -95,6 +95,11 @@ struct StageArgs {
   float isc[NCOMP];    // its inverse (stored units per value)
   const float *lam2mu, *mu, *irho;
   const float *zx, *zy, *zz, *jac;
+  // planes iz < zu_end (<= ConIndex) have one zeta_z on every valid cell,
+  // zzp[iz]: the tiled kernels skip their metric tiles (zeta_x, zeta_y are
+  // not used below ConIndex)
+  const float *zzp;
+  int zu_end;
   bool flat;           // metric is zeta=(0,0,1), jac=1 everywhere
   bool plain_interior; // B = 1 and DB = APD = 0 outside the PML layers
   const float *matv;   // 18 planes: matVx2Vz[0..8], matVy2Vz[0..8]

@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <string>
 #include <thread>
 #include <vector>
@@ -222,6 +223,8 @@ struct cgfd_solver {
   int wcur = 0;            // set that holds "W" (last stage output)
   float *media = nullptr;  // lam2mu, mu, irho
   float *metric = nullptr; // zeta_x, zeta_y, zeta_z, jac
+  float *zzp = nullptr;    // per plane: uniform zeta_z below ConIndex
+  int zu_end = 0;          // planes iz < zu_end have one (zzp)
   float *pml = nullptr;    // apd x y z, b x y z, db x y z
   float *pmlp[9] = {};
   float *aux[3] = {nullptr, nullptr, nullptr};  // per direction: FA, A, tA sets
@@ -314,7 +317,7 @@ void free_all(cgfd_solver *h) {
   void *ptrs[] = {h->state, h->media, h->metric, h->pml, h->aux[0], h->aux[1], h->aux[2],
                   h->matv, h->d_mcell, h->d_fcell, h->d_mcoef, h->d_fcoef, h->d_mstf,
                   h->d_fstf, h->d_rcell, h->d_seis, h->d_step, h->d_partials, h->d_err,
-                  h->d_pgv, h->d_mlp_cells, h->d_mlp_w, h->d_mlp_delta};
+                  h->d_pgv, h->d_mlp_cells, h->d_mlp_w, h->d_mlp_delta, h->zzp};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->st) cudaStreamDestroy(h->st);
@@ -502,6 +505,8 @@ StageArgs stage_args(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, in
   const size_t fs = h->g.fstride;
   a.lam2mu = h->media; a.mu = h->media + fs; a.irho = h->media + 2 * fs;
   a.zx = h->metric; a.zy = h->metric + fs; a.zz = h->metric + 2 * fs; a.jac = h->metric + 3 * fs;
+  a.zzp = h->zzp;
+  a.zu_end = h->zu_end;
   a.flat = h->flat;
   a.plain_interior = h->plain_interior;
   a.matv = h->matv;
@@ -673,6 +678,7 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
   if (!st) st = alloc((float **)&h->state, (4 * 9 * fs * elem_size(h->elem) + 3) / 4);
   if (!st) st = alloc(&h->media, 3 * fs);
   if (!st) st = alloc(&h->metric, 4 * fs);
+  if (!st) st = alloc(&h->zzp, g.nzi);
   const size_t plen = align_up(g.px, 64) * 3 + align_up(g.nyi, 64) * 3 + align_up(g.nzi, 64) * 3;
   if (!st) st = alloc(&h->pml, plen);
   for (int q = 0; q < 3 && !st; ++q)
@@ -764,6 +770,23 @@ int cgfd_upload_metric(cgfd_solver *h, const double *zx, const double *zy, const
         if (zx[t] != 0.0 || zy[t] != 0.0 || zz[t] != 1.0 || jac[t] != 1.0) flat = false;
       }
   h->flat = flat;
+  // The run of planes from the bottom, below ConIndex, whose zeta_z (as
+  // stored, FP32) is one value on every valid cell: the tiled kernels take
+  // it from a per-plane table instead of loading the plane's metric tile
+  // (zeta_x and zeta_y are not used below ConIndex).
+  std::vector<float> zzp(h->g.nzi, 0.f);
+  int zu_end = LFD;
+  for (int k = LFD; k < h->d.nk + LFD && k < h->g.con; ++k, ++zu_end) {
+    const float v = (float)zz[((long)LFD * ny + LFD) * nz + k];
+    bool same = true;
+    for (int i = LFD; i < h->d.ni + LFD && same; ++i)
+      for (int j = LFD; j < h->d.nj + LFD && same; ++j)
+        same = (float)zz[((long)i * ny + j) * nz + k] == v;
+    if (!same) break;
+    zzp[k] = v;
+  }
+  CK(h, cudaMemcpy(h->zzp, zzp.data(), zzp.size() * sizeof(float), cudaMemcpyHostToDevice));
+  h->zu_end = zu_end;
   h->top_zeta.assign(3 * (size_t)nx * ny, 0.0);
   for (int i = 0; i < nx; ++i)
     for (int j = 0; j < ny; ++j) {

@@ -322,6 +322,12 @@ struct Plane {
   int iz, k;
   size_t c;           // linear index of the first cell
   bool zpml, top, near_top, curved, lean;
+  bool met;           // the plane's metric tile was loaded
+  float zz;           // zeta_z of the plane when no tile was loaded
+  // zeta_z of this thread's pair
+  template <typename P> __device__ __forceinline__ f2 zeta_z(const P &pw) const {
+    return met ? pw.M(2) : S2(zz);
+  }
 };
 
 // Pointwise operands of this thread's pair in the current slot.
@@ -380,8 +386,7 @@ __device__ __forceinline__ void vel_pair(const StageArgs &a, const Pair &e, cons
 
   if (pl.lean) {
     const f2 irho = pw.C(0);
-    f2 ztz = S2(1.f);
-    if (!a.flat) ztz = pw.M(2);
+    const f2 ztz = pl.zeta_z(pw);
     f2 hw[3];
     if (pl.curved) {
       const f2 ztx = pw.M(0), zty = pw.M(1);
@@ -413,11 +418,9 @@ __device__ __forceinline__ void vel_pair(const StageArgs &a, const Pair &e, cons
   if (my) ay.load(a, 1, ix.y, ix.y + 1, my, 0);
   if (mz) az.load(a, 2, ix.z, ix.z + 1, mz, 0);
   const f2 irho = pw.C(0);
-  f2 ztx = S2(0.f), zty = S2(0.f), ztz = S2(1.f);
-  if (!a.flat) {
-    ztz = pw.M(2);
-    if (pl.curved) { ztx = pw.M(0); zty = pw.M(1); }
-  }
+  f2 ztx = S2(0.f), zty = S2(0.f);
+  const f2 ztz = pl.zeta_z(pw);
+  if (pl.curved) { ztx = pw.M(0); zty = pw.M(1); }
   f2 dxi[3], det[3], dzt[3];
   dxi[0] = mul2(dx(0), irho);  // DxTxx
   dxi[1] = mul2(dx(3), irho);  // DxTxy
@@ -549,11 +552,9 @@ __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, cons
 
   const f2 lam2mu = pw.C(0), miu = pw.C(1);
   const f2 lambda = fma2(S2(-2.f), miu, lam2mu);
-  f2 ztx = S2(0.f), zty = S2(0.f), ztz = S2(1.f);
-  if (!a.flat) {
-    ztz = pw.M(2);
-    if (pl.curved) { ztx = pw.M(0); zty = pw.M(1); }
-  }
+  f2 ztx = S2(0.f), zty = S2(0.f);
+  const f2 ztz = pl.zeta_z(pw);
+  if (pl.curved) { ztx = pw.M(0); zty = pw.M(1); }
   // components in the set order Txx Tyy Tzz Txy Txz Tyz (index q = comp - 3)
   f2 dxi[6], det[6], dzt[6];
   {
@@ -707,9 +708,12 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
     const Geom &g = A.g;
     const size_t fs = g.fstride;
     const bool flat = A.flat;
-    // bytes one plane delivers: halo always, pointwise only for computed planes
-    const uint32_t pw_bytes = S::U_B * (KIND == 1 ? 2u : 1u) +
-                              (uint32_t)(PWT * 4) * (NCOEF + (flat ? 0 : 3));
+    // bytes one plane delivers: halo always, pointwise only for computed
+    // planes, the metric tile only where the plane's metric is not uniform
+    const uint32_t pw_bytes = S::U_B * (KIND == 1 ? 2u : 1u) + (uint32_t)(PWT * 4) * NCOEF;
+    auto met_tile = [&](int p) { return !flat && p >= A.zu_end; };
+    // zeta_z of a plane without a metric tile (loaded one plane ahead)
+    auto zz_of = [&](int p) { return flat ? 1.f : (p < A.zu_end ? A.zzp[p] : 0.f); };
     const float rx = (float)X / A.h, rys = (float)Y / A.h, rz = (float)Z / A.h;
     const int zlo = LFD + g.nabs[4], zhi = g.nk + LFD - g.nabs[5];  // z interior [zlo, zhi)
     const bool aux_on[3] = {B ? A.ain[0] != nullptr : wk.has_aux[0] != 0,
@@ -728,14 +732,16 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
       const int p = ((DIR > 0) ? it.z : it.w - 1) + DIR * q;
       const bool compute = q < n;
       fence_proxy_async();
-      mbar_expect_tx(&bars[s], S::HALO_B + (compute ? pw_bytes : 0u));
+      const bool met = compute && met_tile(p);
+      mbar_expect_tx(&bars[s], S::HALO_B + (compute ? pw_bytes : 0u) +
+                                   (met ? (uint32_t)(PWT * 4) * 3u : 0u));
       tma_load(slot, &M.halo, XO + i0 - HOFF, j0, p, C0, &bars[s]);
       if (compute) {
         const int cx = XO + i0, cy = LFD + j0;
         tma_load(slot + S::U0, &M.u0, cx, cy, p, S0, &bars[s]);
         if (KIND == 1) tma_load(slot + S::U1, &M.u1, cx, cy, p, S0, &bars[s]);
         tma_load(slot + S::COEF, &M.coef, cx, cy, p, COEF0, &bars[s]);
-        if (!flat) tma_load(slot + S::MET, &M.met, cx, cy, p, 0, &bars[s]);
+        if (met) tma_load(slot + S::MET, &M.met, cx, cy, p, 0, &bars[s]);
         // the plane's PML auxiliaries into L2 (tile- and plane-uniform presence)
         const bool xp = aux_on[0] && (i0 < g.nabs[0] || i0 + CX > g.ni - g.nabs[1]);
         const bool yp = aux_on[1] && (j0 < g.nabs[2] || j0 + TY > g.nj - g.nabs[3]);
@@ -838,8 +844,11 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
     __syncthreads();
 
     size_t c = gidx(g, e.ix, e.iy, zf);
+    float zzn = zz_of(zf);
 #pragma unroll MARCH_UNROLL
     for (int q = 0; q < n; ++q) {
+      const float zzc = zzn;
+      if (q + 1 < n) zzn = zz_of(zf + DIR * (q + 1));
       const bool got = wait(q + 1);
       if (got) push_smem(ring + (size_t)((base + q + 1) & (NSLOT - 1)) * S::BYTES);
       else abort_flag = 1;
@@ -854,6 +863,8 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
         pl.zpml = (pl.iz < zlo) || (pl.iz >= zhi);
         pl.curved = pl.iz >= g.con && !flat;
         pl.lean = tile_int && !pl.zpml && !pl.near_top;
+        pl.met = met_tile(pl.iz);
+        pl.zz = zzc;
         const Pw2<T> pw{reinterpret_cast<const T *>(slot + S::U0) + tc,
                         reinterpret_cast<const T *>(slot + S::U1) + tc,
                         reinterpret_cast<const float *>(slot + S::COEF) + tc,
