@@ -156,10 +156,16 @@ int fused_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str)
 // items_per_cta items per resident CTA, z-chunks of at least min_chunk
 // planes, PML columns weighted (1 + pml_weight per direction) in the cost
 // order.
+#ifndef CGFD_TAIL_CHUNK
+#define CGFD_TAIL_CHUNK 8
+#endif
 struct WorkParams {
   int items_per_cta = 6;
   int min_chunk = 16;
   double pml_weight = 1.0;
+  // the last G items (one per resident CTA) are cut into chunks of about
+  // this many planes, so that the launch ends on short items (0: no cut)
+  int tail_chunk = CGFD_TAIL_CHUNK;
 };
 bool pair_supported(const Geom &g);
 bool pair_set_work(void *plan, const WorkParams &wp);

@@ -194,8 +194,36 @@ std::vector<int4> build_items(const std::vector<Geom> &gs, int G, const WorkPara
   }
   std::stable_sort(items.begin(), items.end(),
                    [](const It &x, const It &y) { return x.cost > y.cost; });
-  std::vector<int4> hv(items.size());
-  for (size_t q = 0; q < items.size(); ++q) hv[q] = items[q].v;
+  std::vector<int4> hv;
+  hv.reserve(items.size());
+  // guided end: the last G items (the cheapest) become short chunks, ordered
+  // piece by piece (the first piece of every cut item, then the second...)
+  // so that CTAs running together stay on neighbouring columns
+  size_t ncut = 0;
+  if (wp.tail_chunk >= 4) {
+    while (ncut < (size_t)G && ncut < items.size()) {
+      const int4 v = items[items.size() - 1 - ncut].v;
+      if ((v.z >> 16) - (v.z & 0xffff) < 2 * wp.tail_chunk) break;
+      ++ncut;
+    }
+  }
+  const size_t keep = items.size() - ncut;
+  for (size_t q = 0; q < keep; ++q) hv.push_back(items[q].v);
+  std::vector<std::vector<int4>> pieces(ncut);
+  size_t maxp = 0;
+  for (size_t q = 0; q < ncut; ++q) {
+    const int4 v = items[keep + q].v;
+    const int z0 = v.z & 0xffff, z1 = v.z >> 16, np = (z1 - z0) / wp.tail_chunk;
+    for (int t = 0; t < np; ++t) {
+      const int a0 = z0 + (int)((long)(z1 - z0) * t / np);
+      const int a1 = z0 + (int)((long)(z1 - z0) * (t + 1) / np);
+      pieces[q].push_back(make_int4(v.x, v.y, a0 | (a1 << 16), v.w));
+    }
+    maxp = std::max(maxp, pieces[q].size());
+  }
+  for (size_t t = 0; t < maxp; ++t)
+    for (size_t q = 0; q < ncut; ++q)
+      if (t < pieces[q].size()) hv.push_back(pieces[q][t]);
   return hv;
 }
 
