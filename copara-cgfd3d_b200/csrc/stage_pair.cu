@@ -143,6 +143,27 @@ void stage_maps(const ModelMaps &pl, int rk, int in_set, Maps &mv, Maps &ms) {
 // columns of (1 + pml_weight x number of PML directions)), so the cheap
 // items fill the tail; equal costs keep the (model, z-chunk, tile) order, so
 // neighbouring tiles of a class run together and share halo rows in L2.
+// x origin of the tile grid (tiles start at i = t * CX - offset).  The
+// stage kernels' time follows the number of tile-planes, and a tile that
+// touches an x layer runs the slower boundary path for all its columns.
+// Candidates 0 and 32 keep every tile row of the field, media and metric
+// boxes on a 128-byte boundary (the internal x origin XO is 32); 32 is taken
+// when it needs no more tile columns and puts fewer valid columns into tiles
+// that touch an x layer (on the 400-wide hill with 20-cell layers: 80
+// instead of 144 columns).
+int tile_x_offset(const Geom &g) {
+  auto ntx = [&](int o) { return (g.ni + o + CX - 1) / CX; };
+  auto boundary_cols = [&](int o) {
+    int n = 0;
+    for (int t = 0; t < ntx(o); ++t) {
+      const int i0 = t * CX - o, a = std::max(i0, 0), b = std::min(i0 + CX, g.ni);
+      if (a < g.nabs[0] || b > g.ni - g.nabs[1]) n += b - a;
+    }
+    return n;
+  };
+  return (ntx(32) == ntx(0) && boundary_cols(32) < boundary_cols(0)) ? 32 : 0;
+}
+
 std::vector<int4> build_items(const std::vector<Geom> &gs, int G, const WorkParams &wp,
                               int *zchunk) {
   // target chunk length: enough items (items_per_cta per resident CTA) over
@@ -155,7 +176,8 @@ std::vector<int4> build_items(const std::vector<Geom> &gs, int G, const WorkPara
   std::vector<It> items;
   for (size_t mdl = 0; mdl < gs.size(); ++mdl) {
     const Geom &g = gs[mdl];
-    const int ntx = (g.ni + CX - 1) / CX, nty = (g.nj + TY - 1) / TY;
+    const int xoff = tile_x_offset(g);
+    const int ntx = (g.ni + xoff + CX - 1) / CX, nty = (g.nj + TY - 1) / TY;
     const int ntiles = ntx * nty;
     std::vector<int> zb{LFD};
     const int zlo = LFD + g.nabs[4], ztop = g.nk + LFD;
@@ -178,11 +200,11 @@ std::vector<int4> build_items(const std::vector<Geom> &gs, int G, const WorkPara
       if (zb[c + 1] - zb[c] < 4) return {};
       const bool zp = zb[c] < zlo;
       for (int t = 0; t < ntiles; ++t) {
-        const int i0 = (t % ntx) * CX, j0 = (t / ntx) * TY;
+        const int i0 = (t % ntx) * CX - xoff, j0 = (t / ntx) * TY;
         double w = 0;
         for (int j = j0; j < j0 + TY && j < g.nj; ++j) {
           const bool yp = j < g.nabs[2] || j >= g.nj - g.nabs[3];
-          for (int i = i0; i < i0 + CX && i < g.ni; ++i) {
+          for (int i = std::max(i0, 0); i < i0 + CX && i < g.ni; ++i) {
             const bool xp = i < g.nabs[0] || i >= g.ni - g.nabs[1];
             w += 1 + wp.pml_weight * ((xp ? 1 : 0) + (yp ? 1 : 0) + (zp ? 1 : 0));
           }
