@@ -85,6 +85,15 @@ struct StageArgs {
   int X, Y, Z;         // +1 forward / -1 backward per axis
   float h;             // steph
   float adt, bdt;      // RK4A[rk]*dt (0 for rk 3), RK4B[rk]*dt
+  // tW elision (the paired kernels, their traction image and sources): the
+  // first stage writes no tW; the second rebuilds it from FW and the first
+  // stage's output as FW + rtw * (W - FW), rtw = RK4B[0]/RK4A[0], which
+  // equals FW + RK4B[0]*dt*RHS because W = FW + RK4A[0]*dt*RHS.  (The ADE
+  // auxiliaries keep their tA: rebuilding it would hold the stage input's
+  // auxiliaries in registers up to the update, which cost more in the
+  // latency-bound PML tiles than the bytes saved.)
+  bool tw_skip;
+  float rtw;
   // field sets, of the storage element type elem (ELEM_F32 / F16 / BF16)
   const void *in;      // stencil input set (FW for rk 0, else previous W)
   const void *fw;      // FW (rk 1,2 read it)
@@ -129,6 +138,7 @@ struct SourceArgs {
   int tindex;          // >= 0: use it; < 0: 2*(*step)+tinc
   const int *step;     // device step counter
   float adt, bdt;
+  bool tw_skip;        // first stage: tW is not written (see StageArgs)
   void *out, *tw;      // field sets of element type elem
   int elem;
   float isc[NCOMP];
@@ -173,6 +183,7 @@ WorkParams pair_get_work(const void *plan);
 void *pair_create_plan(const Geom &g, int elem, void *const sets[4], const float *media,
                        const float *metric, float *const aux[3]);
 void pair_destroy_plan(void *plan);
+// the paired kernels run with a.tw_skip set (tW elision)
 void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *err,
                        void *stream);
 int pair_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str);

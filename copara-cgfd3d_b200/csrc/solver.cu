@@ -88,7 +88,9 @@ __device__ void inject_sources_body(const SourceArgs &s) {
       E::st(out + o, E::ld(out + o) + b * S);
     } else {
       E::st(out + o, E::ld(out + o) + a * S);
-      E::st(tw + o, E::ld(tw + o) + b * S);
+      // under tW elision the first stage's tW is rebuilt from W later, and
+      // W already carries this source term
+      if (!(s.tw_skip && s.rk == 0)) E::st(tw + o, E::ld(tw + o) + b * S);
     }
   };
   for (int q = 0; q < s.nmnt; ++q) {
@@ -101,6 +103,25 @@ __device__ void inject_sources_body(const SourceArgs &s) {
     const float stf = s.fstf[(size_t)q * s.nstff + t2];
     const int c = s.fcell[q];
     for (int m = 0; m < 3; ++m) add(VX + m, (size_t)(VX + m) * fs + c, stf * s.fcoef[3 * q + m]);
+  }
+}
+// tW elision, single-stage driving: after a first stage run alone, tW (valid
+// cells) is written as the reference's first stage leaves it,
+// tW = FW + r * (W - FW), so the state between stages matches the
+// reference's; the next stage rebuilds it the same way anyway.
+template <typename T>
+__global__ void rebuild_tw_kernel(Geom g, const T *fw, const T *w, T *tw, float r) {
+  using E = Elem<T>;
+  const long n = (long)g.ni * g.nj * g.nk;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+       t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.ni), j = (int)(t / g.ni % g.nj), k = (int)(t / ((long)g.ni * g.nj));
+    const size_t o = gidx(g, i + XO, j + LFD, k + LFD);
+    for (int c = 0; c < NCOMP; ++c) {
+      const size_t q = (size_t)c * g.fstride + o;
+      const float f = E::ld(fw + q);
+      E::st(tw + q, f + r * (E::ld(w + q) - f));
+    }
   }
 }
 template <typename T>
@@ -493,6 +514,8 @@ StageArgs stage_args(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, in
   a.h = (float)h->d.steph;
   a.adt = (rk < 3) ? (float)(RKA[rk] * h->d.stept) : 0.f;
   a.bdt = (float)(RKB[rk] * h->d.stept);
+  a.tw_skip = h->d.kernel == CGFD_KERNEL_FUSED;
+  a.rtw = (float)(RKB[0] / RKA[0]);
   a.in = h->set[in_set];
   a.fw = h->set[0];
   a.out = h->set[out_set];
@@ -548,7 +571,7 @@ int launch_stage(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, int ou
     s.tinc = (rk == 0) ? 0 : (rk < 3 ? 1 : 2);
     s.tindex = tindex;
     s.step = h->d_step;
-    s.adt = a.adt; s.bdt = a.bdt;
+    s.adt = a.adt; s.bdt = a.bdt; s.tw_skip = a.tw_skip;
     s.out = a.out; s.tw = a.tw; s.rk = rk;
     s.elem = a.elem;
     for (int c = 0; c < NCOMP; ++c) s.isc[c] = a.isc[c];
@@ -1137,7 +1160,7 @@ int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms) {
           sa.tinc = (rk == 0) ? 0 : (rk < 3 ? 1 : 2);
           sa.tindex = -1;
           sa.step = h->d_step;
-          sa.adt = a.adt; sa.bdt = a.bdt;
+          sa.adt = a.adt; sa.bdt = a.bdt; sa.tw_skip = a.tw_skip;
           sa.out = a.out; sa.tw = a.tw; sa.rk = rk;
           sa.elem = a.elem;
           for (int c = 0; c < NCOMP; ++c) sa.isc[c] = a.isc[c];
@@ -1197,6 +1220,20 @@ int cgfd_rk_stage(cgfd_solver *h, int rk, int curr_t, int X, int Y, int Z) {
   if (rk == 3 && in == 0) return arg_fail(h, "stage 3 needs a previous stage output");
   st = launch_stage(h, rk, X, Y, Z, in, out, tindex);
   if (st) return st;
+  if (rk == 0 && h->d.kernel == CGFD_KERNEL_FUSED) {  // tW elision: materialise tW
+    const float r = (float)(RKB[0] / RKA[0]);
+    if (h->elem == ELEM_F16)
+      rebuild_tw_kernel<<<592, 256, 0, h->st>>>(h->g, (const __half *)h->set[0],
+                                                (const __half *)h->set[out], (__half *)h->set[3], r);
+    else if (h->elem == ELEM_BF16)
+      rebuild_tw_kernel<<<592, 256, 0, h->st>>>(h->g, (const __nv_bfloat16 *)h->set[0],
+                                                (const __nv_bfloat16 *)h->set[out],
+                                                (__nv_bfloat16 *)h->set[3], r);
+    else
+      rebuild_tw_kernel<<<592, 256, 0, h->st>>>(h->g, (const float *)h->set[0],
+                                                (const float *)h->set[out], (float *)h->set[3], r);
+    CK(h, cudaGetLastError());
+  }
   h->wcur = out;
   return CGFD_OK;
 }
@@ -1460,8 +1497,9 @@ static int batch_build(cgfd_batch *b) {
     for (int p = 0; p < 4; ++p)
       for (int rk = 0; rk < 4; ++rk) {
         const int *dd = DIRS[p][rk];
-        args[(size_t)(p * 4 + rk) * n + i] =
-            stage_args(h, rk, dd[0], dd[1], dd[2], ins[rk], outs[rk]);
+        StageArgs &a = args[(size_t)(p * 4 + rk) * n + i];
+        a = stage_args(h, rk, dd[0], dd[1], dd[2], ins[rk], outs[rk]);
+        a.tw_skip = true;  // the batched paired kernels run with tW elision
       }
     for (int rk = 0; rk < 4; ++rk) {
       const StageArgs &a = args[(size_t)rk * n + i];
@@ -1474,7 +1512,7 @@ static int batch_build(cgfd_batch *b) {
       s.tinc = (rk == 0) ? 0 : (rk < 3 ? 1 : 2);
       s.tindex = -1;
       s.step = h->d_step;
-      s.adt = a.adt; s.bdt = a.bdt;
+      s.adt = a.adt; s.bdt = a.bdt; s.tw_skip = a.tw_skip;
       s.out = a.out; s.tw = a.tw; s.rk = rk;
       s.elem = a.elem;
       for (int c = 0; c < NCOMP; ++c) s.isc[c] = a.isc[c];

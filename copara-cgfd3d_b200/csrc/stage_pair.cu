@@ -115,16 +115,17 @@ bool model_maps(ModelMaps *pl, int *has_aux, const Geom &g, int elem, void *cons
 
 // the maps of one stage (stage input set, RK kind, stage index) for the
 // velocity (mv) and stress (ms) parts
-void stage_maps(const ModelMaps &pl, int rk, int in_set, Maps &mv, Maps &ms) {
+// (rebuild: the second stage under tW elision, whose u1 is the stage input)
+void stage_maps(const ModelMaps &pl, int rk, int in_set, bool rebuild, Maps &mv, Maps &ms) {
   const int kind = rk == 0 ? 0 : (rk < 3 ? 1 : 2);
   mv.halo = pl.haloV[in_set];
   mv.u0 = kind == 2 ? pl.ctrV[3] : pl.ctrV[0];
-  mv.u1 = pl.ctrV[3];
+  mv.u1 = rebuild ? pl.ctrV[in_set] : pl.ctrV[3];
   mv.coef = pl.coefV;
   mv.met = pl.met;
   ms.halo = pl.haloS[in_set];
   ms.u0 = kind == 2 ? pl.ctrT[3] : pl.ctrT[0];
-  ms.u1 = pl.ctrT[3];
+  ms.u1 = rebuild ? pl.ctrT[in_set] : pl.ctrT[3];
   ms.coef = pl.coefS;
   ms.met = pl.met;
   for (int d = 0; d < 3; ++d) {
@@ -135,14 +136,6 @@ void stage_maps(const ModelMaps &pl, int rk, int in_set, Maps &mv, Maps &ms) {
   }
 }
 
-// Work items of one or more models (tile x z-chunk): the bottom PML layer is
-// a z-chunk of its own (when it has >= 8 planes), the rest is cut into pieces
-// of about len planes (>= MIN_CHUNK; every chunk has >= 4 planes, which the
-// kernel's initial issue of four entries relies on).  Order: the most
-// expensive first (estimated cost: planes x sum over the tile's valid
-// columns of (1 + pml_weight x number of PML directions)), so the cheap
-// items fill the tail; equal costs keep the (model, z-chunk, tile) order, so
-// neighbouring tiles of a class run together and share halo rows in L2.
 // x origin of the tile grid (tiles start at i = t * CX - offset).  The
 // stage kernels' time follows the number of tile-planes, and a tile that
 // touches an x layer runs the slower boundary path for all its columns.
@@ -164,6 +157,14 @@ int tile_x_offset(const Geom &g) {
   return (ntx(32) == ntx(0) && boundary_cols(32) < boundary_cols(0)) ? 32 : 0;
 }
 
+// Work items of one or more models (tile x z-chunk): the bottom PML layer is
+// a z-chunk of its own (when it has >= 8 planes), the rest is cut into pieces
+// of about len planes (>= MIN_CHUNK; every chunk has >= 4 planes, which the
+// kernel's initial issue of four entries relies on).  Order: the most
+// expensive first (estimated cost: planes x sum over the tile's valid
+// columns of (1 + pml_weight x number of PML directions)), so the cheap
+// items fill the tail; equal costs keep the (model, z-chunk, tile) order, so
+// neighbouring tiles of a class run together and share halo rows in L2.
 std::vector<int4> build_items(const std::vector<Geom> &gs, int G, const WorkParams &wp,
                               int *zchunk) {
   // target chunk length: enough items (items_per_cta per resident CTA) over
@@ -334,7 +335,7 @@ void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *er
   cudaStream_t s = (cudaStream_t)stream;
   const int kind = a.rk == 0 ? 0 : (a.rk < 3 ? 1 : 2);
   Maps mv, ms;
-  stage_maps(pl.mm[0], a.rk, in_set, mv, ms);
+  stage_maps(pl.mm[0], a.rk, in_set, a.tw_skip && a.rk == 1, mv, ms);
   // both parts' item counters restart at zero
   cudaMemsetAsync(pl.wk.counter, 0, 2 * sizeof(int), s);
   typedef void (*LaunchFn)(const Plan &, const Maps &, const StageArgs &, int *, cudaStream_t);
@@ -366,12 +367,13 @@ void *pair_create_batch_plan(int n, const Geom *gs, void *const *sets, const flo
                     aux + 3 * i);
   }
   // per stage, part and model: the maps of that stage (input set per stage
-  // as in the step schedule: FW, Wa, Wb, Wa)
+  // as in the step schedule: FW, Wa, Wb, Wa; batched stages run with tW
+  // elision)
   static const int ins[4] = {0, 1, 2, 1};
   std::vector<Maps> hm((size_t)8 * n);
   for (int rk = 0; rk < 4 && ok; ++rk)
     for (int i = 0; i < n; ++i)
-      stage_maps(pl->mm[i], rk, ins[rk], hm[(size_t)(rk * 2) * n + i],
+      stage_maps(pl->mm[i], rk, ins[rk], rk == 1, hm[(size_t)(rk * 2) * n + i],
                  hm[(size_t)(rk * 2 + 1) * n + i]);
   ok = ok && cudaMalloc(&pl->d_bmaps, hm.size() * sizeof(Maps)) == cudaSuccess &&
        cudaMemcpy(pl->d_bmaps, hm.data(), hm.size() * sizeof(Maps), cudaMemcpyHostToDevice) ==

@@ -228,19 +228,22 @@ __device__ __forceinline__ void stt2(T *p, int m, f2 v) {
   }
 }
 
-// RK update of one pair (Iteration*): KIND 0 first stage (u0 = FW),
-// 1 inner (u0 = FW, u1 = tW), 2 final (u0 = tW).  u0, u1 and the outputs are
-// in stored units; adt, bdt carry the component's inverse scale (every set of
-// a component shares its scale).
+// RK update of one pair (Iteration*): KIND 0 first stage (u0 = FW; no tW
+// under tW elision), 1 inner (u0 = FW, u1 = tW; in the second stage under
+// elision u1 = the stage input W and tW = FW + rtw*(W - FW) + bdt*h),
+// 2 final (u0 = tW).  u0, u1 and the outputs are in stored units; adt, bdt
+// carry the component's inverse scale (every set of a component shares its
+// scale, so the rebuild is the same in stored units).
 template <int KIND, typename T>
-__device__ __forceinline__ void rk_store2(T *out, T *tw, int m, f2 u0, f2 u1, f2 hh, float adt,
-                                          float bdt) {
+__device__ __forceinline__ void rk_store2(const StageArgs &a, T *out, T *tw, int m, f2 u0, f2 u1,
+                                          f2 hh, float adt, float bdt) {
   if (KIND == 0) {
     stt2(out, m, fma2(S2(adt), hh, u0));
-    stt2(tw, m, fma2(S2(bdt), hh, u0));
+    if (!a.tw_skip) stt2(tw, m, fma2(S2(bdt), hh, u0));
   } else if (KIND == 1) {
     stt2(out, m, fma2(S2(adt), hh, u0));
-    stt2(tw, m, fma2(S2(bdt), hh, u1));
+    const f2 base = (a.tw_skip && a.rk == 1) ? fma2(S2(a.rtw), add2(u1, neg2(u0)), u0) : u1;
+    stt2(tw, m, fma2(S2(bdt), hh, base));
   } else {
     stt2(out, m, fma2(S2(bdt), hh, u0));
   }
@@ -405,7 +408,7 @@ __device__ __forceinline__ void vel_pair(const StageArgs &a, const Pair &e, cons
     }
 #pragma unroll
     for (int q = 0; q < 3; ++q)
-      rk_store2<KIND>(out + (VX + q) * fs + pl.c, tw + (VX + q) * fs + pl.c, 3, pw.U0(q),
+      rk_store2<KIND>(a, out + (VX + q) * fs + pl.c, tw + (VX + q) * fs + pl.c, 3, pw.U0(q),
                       KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], adt(VX + q), bdt(VX + q));
     return;
   }
@@ -474,7 +477,7 @@ __device__ __forceinline__ void vel_pair(const StageArgs &a, const Pair &e, cons
   if (!xy) return;
 #pragma unroll
   for (int q = 0; q < 3; ++q)
-    rk_store2<KIND>(out + (VX + q) * fs + pl.c, tw + (VX + q) * fs + pl.c, e.m, pw.U0(q),
+    rk_store2<KIND>(a, out + (VX + q) * fs + pl.c, tw + (VX + q) * fs + pl.c, e.m, pw.U0(q),
                     KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], adt(VX + q), bdt(VX + q));
 }
 
@@ -636,7 +639,7 @@ __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, cons
   const int m = gen ? e.m : 3;
 #pragma unroll
   for (int q = 0; q < 6; ++q)
-    rk_store2<KIND>(out + (TXX + q) * fs + pl.c, tw + (TXX + q) * fs + pl.c, m, pw.U0(q),
+    rk_store2<KIND>(a, out + (TXX + q) * fs + pl.c, tw + (TXX + q) * fs + pl.c, m, pw.U0(q),
                     KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], scaled<T>(a.adt, a.isc[TXX + q]),
                     scaled<T>(a.bdt, a.isc[TXX + q]));
 }

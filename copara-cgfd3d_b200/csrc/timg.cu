@@ -80,6 +80,9 @@ __device__ __forceinline__ void timg_cell(const StageArgs &a, int i, int j, int 
                               : rhojac * drp5(vz[4], vz[3], vz[2], vz[1], vz[0], rz);
     float hv = DxT * iBx + DyT * iBy + DzT;
     // auxiliaries: X then Y, each read before it is written (own cell only)
+    // under tW elision the first stage writes no tW and the second rebuilds
+    // it (StageArgs::tw_skip)
+    const bool rebuild = a.tw_skip && a.rk == 1;
     auto aux = [&](int d, size_t p, float h) {
       const size_t o = q * g.astride[d] + p;
       const float ai = a.ain[d][o];
@@ -113,9 +116,10 @@ __device__ __forceinline__ void timg_cell(const StageArgs &a, int i, int j, int 
     if (kind == 0) {
       const float u0 = E::ld(in + o);
       E::st(out + o, u0 + adt * hv);
-      E::st(tw + o, u0 + bdt * hv);
+      if (!a.tw_skip) E::st(tw + o, u0 + bdt * hv);
     } else if (kind == 1) {
-      const float u0 = E::ld(fw + o), u1 = E::ld(tw + o);
+      const float u0 = E::ld(fw + o);
+      const float u1 = rebuild ? u0 + a.rtw * (E::ld(in + o) - u0) : E::ld(tw + o);
       E::st(out + o, u0 + adt * hv);
       E::st(tw + o, u1 + bdt * hv);
     } else {

@@ -117,3 +117,29 @@ def test_tiled_kernels_match_simple_kernel_on_hill_400x400x200():
             assert e < 1e-5, (kern, cgfd.COMPONENTS[c], e)
         for c, e in enumerate(comp_errors(out[kern][0], ref[0])):
             assert e < 1e-5, (kern, cgfd.COMPONENTS[c], e)
+
+
+@pytest.mark.parametrize("nstages", [1, 2, 3])
+def test_rk_accumulator_between_stages_matches_fp64_oracle(nstages):
+    """The default kernels skip tW in the first stage and
+    rebuild them in the second from FW and the first stage's output; driven
+    stage by stage, tW is materialised after the first stage.  tW after 1, 2
+    and 3 stages, and W after them, against the oracle (PML on five faces,
+    a moment and a force source)."""
+    import pyoracle
+    m, _, _, init = cases.build("hill_stage4")
+    dirs = [(1, 1, 1), (-1, -1, -1), (1, 1, 1)]
+    p = cgfd.Solver(m.desc(kernel=cgfd.KERNEL_FUSED))
+    o = pyoracle.OracleSolver(m.desc(), 0)
+    for s in (p, o):
+        m.load(s)
+        for c in range(9):
+            s.set_field(c, init[c])
+        for st in range(nstages):
+            s.rk_stage(st, 0, *dirs[st])
+    for fset, what in ((cgfd.SET_TW, "tW"), (cgfd.SET_W, "W")):
+        got = np.stack([p.get_field(c, fset) for c in range(9)])
+        ref = np.stack([o.get_field(c, fset) for c in range(9)])
+        _cmp(valid(got), valid(ref), TOL, f"{what} after {nstages} stage(s)")
+    p.close()
+    o.close()
