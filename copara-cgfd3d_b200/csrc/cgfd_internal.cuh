@@ -143,6 +143,12 @@ struct SourceArgs {
   int elem;
   float isc[NCOMP];
   int rk;
+  // focal points (cgfd_upload_focal): cells, series [6][nfoc][fnt]
+  int nfoc, fnt;
+  const int *foccell;
+  const float *focmom;
+  float fdt, dt, h;
+  const float *jac;
 };
 
 void launch_stage_simple(const StageArgs &a, void *stream);

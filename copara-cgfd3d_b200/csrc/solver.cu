@@ -132,6 +132,70 @@ __global__ void inject_sources_kernel(SourceArgs s) {
 __global__ void inject_sources_batch_kernel(const SourceArgs *sa) {
   if (threadIdx.x == 0) inject_sources_body<float>(sa[blockIdx.x]);
 }
+// Focal points (LoadRmom without SrcSmooth, src/calculate.cu:6257-6319):
+// each adds -M(t) / (h^3 J) to its cell's stress RHS; M(t) as the
+// reference's ExtractValue (src/calculate.cu:2586-2613) computes it, in
+// single precision as there: linear between the samples PL and PR =
+// PL + 1, PR = PL when t lies within 1e-5 s of a sample, zero outside
+// [0, dt*(n-1)] (indices are also clamped to the series).  Points may share
+// a cell, hence atomic additions.
+__device__ __forceinline__ float focal_value(const float *stf, int n, float DT, float time) {
+  const float Tend = DT * (float)(n - 1);
+  if (time > Tend || time < 0.f) return 0.f;
+  int PL = (int)(time / DT);
+  const bool on = (double)fabsf(time - DT * floorf(time / DT)) < 1e-5;
+  int PR = on ? PL : PL + 1;
+  PL = PL < n - 1 ? PL : n - 1;
+  PR = PR < n - 1 ? PR : n - 1;
+  return stf[PL] + (stf[PR] - stf[PL]) * ((time - DT * (float)PL) / DT);
+}
+__device__ __forceinline__ void atomic_add_elem(float *p, float v) { atomicAdd(p, v); }
+__device__ __forceinline__ void atomic_add_elem(__half *p, float v) {
+  atomicAdd(p, __float2half_rn(v));
+}
+__device__ __forceinline__ void atomic_add_elem(__nv_bfloat16 *p, float v) {
+  atomicAdd(p, __float2bfloat16_rn(v));
+}
+template <typename T>
+__device__ void inject_focal_body(const SourceArgs &s, int t0, int tstride) {
+  // the stage's time (src/calculate.cu:1422): (currT + tinc/2) * stept
+  const int currT = (s.tindex >= 0) ? (s.tindex - s.tinc) / 2 : *s.step;
+  const float time = (float)(((double)currT + s.tinc * 0.5) * (double)s.dt);
+  const float h3 = s.h * s.h * s.h;
+  const size_t fs = s.g.fstride;
+  T *out = static_cast<T *>(s.out), *tw = static_cast<T *>(s.tw);
+  const bool to_tw = s.rk != 3 && !(s.tw_skip && s.rk == 0);
+  for (int q = t0; q < s.nfoc; q += tstride) {
+    const int c = s.foccell[q];
+    const float A = 1.f / (h3 * s.jac[c]);
+    for (int m = 0; m < 6; ++m) {
+      const float M = focal_value(s.focmom + ((size_t)m * s.nfoc + q) * s.fnt, s.fnt, s.fdt, time);
+      const float S = -M * A;
+      const int comp = TXX + m;
+      const size_t o = (size_t)comp * fs + c;
+      const float a = s.adt * s.isc[comp], b = s.bdt * s.isc[comp];
+      atomic_add_elem(out + o, (s.rk == 3 ? b : a) * S);
+      if (to_tw) atomic_add_elem(tw + o, b * S);
+    }
+  }
+}
+template <typename T>
+__global__ void inject_focal_kernel(SourceArgs s) {
+  inject_focal_body<T>(s, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+// a batch of models (FP32 storage): blockIdx.y = model
+__global__ void inject_focal_batch_kernel(const SourceArgs *sa) {
+  inject_focal_body<float>(sa[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x,
+                           gridDim.x * blockDim.x);
+}
+int focal_blocks(int nfoc) { return nfoc <= 0 ? 1 : ((nfoc + 127) / 128 < 296 ? (nfoc + 127) / 128 : 296); }
+void launch_focal(const SourceArgs &s, cudaStream_t st) {
+  const int nb = focal_blocks(s.nfoc);
+  if (s.elem == ELEM_F16) inject_focal_kernel<__half><<<nb, 128, 0, st>>>(s);
+  else if (s.elem == ELEM_BF16) inject_focal_kernel<__nv_bfloat16><<<nb, 128, 0, st>>>(s);
+  else inject_focal_kernel<float><<<nb, 128, 0, st>>>(s);
+}
+
 void launch_sources(const SourceArgs &s, cudaStream_t st) {
   if (s.elem == ELEM_F16) inject_sources_kernel<__half><<<1, 32, 0, st>>>(s);
   else if (s.elem == ELEM_BF16) inject_sources_kernel<__nv_bfloat16><<<1, 32, 0, st>>>(s);
@@ -263,6 +327,13 @@ struct cgfd_solver {
   std::vector<float> hmstf, hfstf;  // host copies of the source time functions
   int *d_mcell = nullptr, *d_fcell = nullptr;
   float *d_mcoef = nullptr, *d_fcoef = nullptr, *d_mstf = nullptr, *d_fstf = nullptr;
+  // focal (finite-fault) points: cells and moment series [6][nfoc][fnt]
+  int nfoc = 0, fnt = 0;
+  double fdt = 0;
+  std::vector<int> focloc;
+  std::vector<float> hfocmom;
+  int *d_foccell = nullptr;
+  float *d_focmom = nullptr;
   // receivers
   int nrecv = 0;
   int *d_rcell = nullptr;
@@ -338,7 +409,8 @@ void free_all(cgfd_solver *h) {
   void *ptrs[] = {h->state, h->media, h->metric, h->pml, h->aux[0], h->aux[1], h->aux[2],
                   h->matv, h->d_mcell, h->d_fcell, h->d_mcoef, h->d_fcoef, h->d_mstf,
                   h->d_fstf, h->d_rcell, h->d_seis, h->d_step, h->d_partials, h->d_err,
-                  h->d_pgv, h->d_mlp_cells, h->d_mlp_w, h->d_mlp_delta, h->zzp};
+                  h->d_pgv, h->d_mlp_cells, h->d_mlp_w, h->d_mlp_delta, h->zzp,
+                  h->d_foccell, h->d_focmom};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->st) cudaStreamDestroy(h->st);
@@ -557,28 +629,49 @@ void dispatch_stage(cgfd_solver *h, const StageArgs &a, int in_set) {
     launch_stage_fused(h->plan, a, in_set, h->d_err, h->st);
 }
 
+// the sources of one stage (tindex < 0: from the device step counter)
+SourceArgs source_args(const cgfd_solver *h, const StageArgs &a, int tindex) {
+  SourceArgs s{};
+  const int rk = a.rk;
+  s.g = h->g;
+  s.nmnt = h->nmnt; s.nfrc = h->nfrc;
+  s.mcell = h->d_mcell; s.mcoef = h->d_mcoef; s.mstf = h->d_mstf; s.nstfm = h->nstfm;
+  s.fcell = h->d_fcell; s.fcoef = h->d_fcoef; s.fstf = h->d_fstf; s.nstff = h->nstff;
+  s.tinc = (rk == 0) ? 0 : (rk < 3 ? 1 : 2);
+  s.tindex = tindex;
+  s.step = h->d_step;
+  s.adt = a.adt; s.bdt = a.bdt; s.tw_skip = a.tw_skip;
+  s.out = a.out; s.tw = a.tw; s.rk = rk;
+  s.elem = a.elem;
+  for (int c = 0; c < NCOMP; ++c) s.isc[c] = a.isc[c];
+  s.nfoc = h->nfoc; s.fnt = h->fnt;
+  s.foccell = h->d_foccell; s.focmom = h->d_focmom;
+  s.fdt = (float)h->fdt; s.dt = (float)h->d.stept; s.h = (float)h->d.steph;
+  s.jac = h->metric + 3 * h->g.fstride;
+  return s;
+}
+
+// point sources, then focal points (separate launches: both may touch a cell)
+int launch_stage_sources(cgfd_solver *h, const StageArgs &a, int tindex) {
+  if (h->nmnt + h->nfrc + h->nfoc == 0) return CGFD_OK;
+  const SourceArgs s = source_args(h, a, tindex);
+  if (h->nmnt + h->nfrc > 0) {
+    launch_sources(s, h->st);
+    CK(h, cudaGetLastError());
+  }
+  if (h->nfoc > 0) {
+    launch_focal(s, h->st);
+    CK(h, cudaGetLastError());
+  }
+  return CGFD_OK;
+}
+
 int launch_stage(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, int out_set,
                  int tindex) {
   StageArgs a = stage_args(h, rk, X, Y, Z, in_set, out_set);
   dispatch_stage(h, a, in_set);
   CK(h, cudaGetLastError());
-  if (h->nmnt + h->nfrc > 0) {
-    SourceArgs s{};
-    s.g = h->g;
-    s.nmnt = h->nmnt; s.nfrc = h->nfrc;
-    s.mcell = h->d_mcell; s.mcoef = h->d_mcoef; s.mstf = h->d_mstf; s.nstfm = h->nstfm;
-    s.fcell = h->d_fcell; s.fcoef = h->d_fcoef; s.fstf = h->d_fstf; s.nstff = h->nstff;
-    s.tinc = (rk == 0) ? 0 : (rk < 3 ? 1 : 2);
-    s.tindex = tindex;
-    s.step = h->d_step;
-    s.adt = a.adt; s.bdt = a.bdt; s.tw_skip = a.tw_skip;
-    s.out = a.out; s.tw = a.tw; s.rk = rk;
-    s.elem = a.elem;
-    for (int c = 0; c < NCOMP; ++c) s.isc[c] = a.isc[c];
-    launch_sources(s, h->st);
-    CK(h, cudaGetLastError());
-  }
-  return CGFD_OK;
+  return launch_stage_sources(h, a, tindex);
 }
 
 // the four stages of one step of pattern p, reading tindex from the device
@@ -936,6 +1029,38 @@ int cgfd_upload_forces(cgfd_solver *h, int n, const int *loc, const float *f3, i
                        h->d_fstf, h->nfrc, h->nstff);
 }
 
+int cgfd_upload_focal(cgfd_solver *h, int n, const int *loc, int fnt, double fdt,
+                      const float *mom) {
+  if (!h) return arg_fail(h, "null handle");
+  if (n < 0 || (n > 0 && (!loc || !mom || fnt < 1 || !(fdt > 0.0))))
+    return arg_fail(h, "bad focal sources");
+  for (int q = 0; q < n; ++q)
+    if (!valid_loc(h, loc + 3 * q)) return arg_fail(h, "focal source outside the valid grid");
+  DevGuard guard(h->d.device);
+  CK(h, cudaStreamSynchronize(h->st));
+  if (h->d_foccell) { cudaFree(h->d_foccell); h->d_foccell = nullptr; }
+  if (h->d_focmom) { cudaFree(h->d_focmom); h->d_focmom = nullptr; }
+  h->nfoc = 0;
+  h->focloc.clear();
+  h->hfocmom.clear();
+  if (n > 0) {
+    const size_t nm = (size_t)6 * n * fnt;
+    std::vector<int> cells(n);
+    for (int q = 0; q < n; ++q) cells[q] = cell_of(h, loc + 3 * q);
+    CK(h, cudaMalloc(&h->d_foccell, n * sizeof(int)));
+    CK(h, cudaMemcpy(h->d_foccell, cells.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(h, cudaMalloc(&h->d_focmom, nm * sizeof(float)));
+    CK(h, cudaMemcpy(h->d_focmom, mom, nm * sizeof(float), cudaMemcpyHostToDevice));
+    h->focloc.assign(loc, loc + 3 * n);
+    h->hfocmom.assign(mom, mom + nm);
+    h->nfoc = n;
+    h->fnt = fnt;
+    h->fdt = fdt;
+  }
+  invalidate(h);
+  return CGFD_OK;
+}
+
 int cgfd_set_receivers(cgfd_solver *h, int n, const int *loc) {
   if (!h || n < 0 || (n > 0 && !loc)) return arg_fail(h, "bad receivers");
   for (int q = 0; q < n; ++q)
@@ -1081,6 +1206,31 @@ int cgfd_prepare(cgfd_solver *h) {
       sV = std::fmax(sV, v);
       sT = std::fmax(sT, v * std::sqrt(std::fmax((double)l2m, 1e-30) / irho));  // rho vp
     }
+    if (h->nfoc > 0) {
+      // focal points: the series are moment rates added to the stress RHS;
+      // the point with the largest integral of its largest component bounds
+      // the stress it builds (points are assumed not to pile up in a cell)
+      int qmax = 0;
+      double imax = 0;
+      for (int q = 0; q < h->nfoc; ++q) {
+        double im = 0;
+        for (int m = 0; m < 6; ++m) {
+          double a = 0;
+          const float *ser = &h->hfocmom[((size_t)m * h->nfoc + q) * h->fnt];
+          for (int t = 0; t < h->fnt; ++t) a += std::fabs(ser[t]) * h->fdt;
+          im = std::fmax(im, a);
+        }
+        if (im > imax) { imax = im; qmax = q; }
+      }
+      const int cell = cell_of(h, &h->focloc[3 * qmax]);
+      float jac = 1.f, mu = 0.f, irho = 1.f;
+      CK(h, cell_value(h->metric + 3 * fs, cell, &jac));
+      CK(h, cell_value(h->media + fs, cell, &mu));
+      CK(h, cell_value(h->media + 2 * fs, cell, &irho));
+      const double sig = imax / (h3 * jac);
+      sT = std::fmax(sT, sig);
+      sV = std::fmax(sV, sig / std::sqrt(std::fmax((double)mu, 1e-30) / irho));
+    }
     auto ex = [](double peak) {
       return peak > 0 ? (int)std::ceil(std::log2(peak / 4096.0)) : 0;
     };
@@ -1151,22 +1301,8 @@ int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms) {
         CK(h, cudaGetLastError());
         CK(h, cudaEventRecord(ev[8 * (size_t)s + 2 * rk + 1], h->st));
         // sources exactly as in the graph
-        if (h->nmnt + h->nfrc > 0) {
-          SourceArgs sa{};
-          sa.g = h->g;
-          sa.nmnt = h->nmnt; sa.nfrc = h->nfrc;
-          sa.mcell = h->d_mcell; sa.mcoef = h->d_mcoef; sa.mstf = h->d_mstf; sa.nstfm = h->nstfm;
-          sa.fcell = h->d_fcell; sa.fcoef = h->d_fcoef; sa.fstf = h->d_fstf; sa.nstff = h->nstff;
-          sa.tinc = (rk == 0) ? 0 : (rk < 3 ? 1 : 2);
-          sa.tindex = -1;
-          sa.step = h->d_step;
-          sa.adt = a.adt; sa.bdt = a.bdt; sa.tw_skip = a.tw_skip;
-          sa.out = a.out; sa.tw = a.tw; sa.rk = rk;
-          sa.elem = a.elem;
-          for (int c = 0; c < NCOMP; ++c) sa.isc[c] = a.isc[c];
-          launch_sources(sa, h->st);
-          CK(h, cudaGetLastError());
-        }
+        int sst = launch_stage_sources(h, a, -1);
+        if (sst) return sst;
       }
       if (h->mlp_n) {
         launch_mlp(h);
@@ -1437,6 +1573,7 @@ struct cgfd_batch {
   SourceArgs *d_src = nullptr;   // [stage][model]
   RecordArgs *d_rec = nullptr;   // [model]
   bool any_src = false;
+  int max_foc = 0;  // most focal points of any member
   cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t ev = nullptr;      // orders the batch's and the members' streams
   bool ready = false;
@@ -1479,6 +1616,11 @@ static int batch_enqueue(cgfd_batch *b, int p, const std::vector<StageArgs> &arg
       inject_sources_batch_kernel<<<n, 32, 0, b->st>>>(b->d_src + (size_t)rk * n);
       BCK(b, cudaGetLastError());
     }
+    if (b->max_foc > 0) {  // after the point sources (both may touch a cell)
+      inject_focal_batch_kernel<<<dim3(focal_blocks(b->max_foc), n), 128, 0, b->st>>>(
+          b->d_src + (size_t)rk * n);
+      BCK(b, cudaGetLastError());
+    }
   }
   record_batch_kernel<<<n, 256, 0, b->st>>>(b->d_rec);
   BCK(b, cudaGetLastError());
@@ -1492,6 +1634,7 @@ static int batch_build(cgfd_batch *b) {
   std::vector<SourceArgs> src((size_t)4 * n);
   std::vector<RecordArgs> rec(n);
   b->any_src = false;
+  b->max_foc = 0;
   for (int i = 0; i < n; ++i) {
     cgfd_solver *h = b->m[i];
     for (int p = 0; p < 4; ++p)
@@ -1501,23 +1644,10 @@ static int batch_build(cgfd_batch *b) {
         a = stage_args(h, rk, dd[0], dd[1], dd[2], ins[rk], outs[rk]);
         a.tw_skip = true;  // the batched paired kernels run with tW elision
       }
-    for (int rk = 0; rk < 4; ++rk) {
-      const StageArgs &a = args[(size_t)rk * n + i];
-      SourceArgs &s = src[(size_t)rk * n + i];
-      s = SourceArgs{};
-      s.g = h->g;
-      s.nmnt = h->nmnt; s.nfrc = h->nfrc;
-      s.mcell = h->d_mcell; s.mcoef = h->d_mcoef; s.mstf = h->d_mstf; s.nstfm = h->nstfm;
-      s.fcell = h->d_fcell; s.fcoef = h->d_fcoef; s.fstf = h->d_fstf; s.nstff = h->nstff;
-      s.tinc = (rk == 0) ? 0 : (rk < 3 ? 1 : 2);
-      s.tindex = -1;
-      s.step = h->d_step;
-      s.adt = a.adt; s.bdt = a.bdt; s.tw_skip = a.tw_skip;
-      s.out = a.out; s.tw = a.tw; s.rk = rk;
-      s.elem = a.elem;
-      for (int c = 0; c < NCOMP; ++c) s.isc[c] = a.isc[c];
-    }
+    for (int rk = 0; rk < 4; ++rk)
+      src[(size_t)rk * n + i] = source_args(h, args[(size_t)rk * n + i], -1);
     if (h->nmnt + h->nfrc > 0) b->any_src = true;
+    if (h->nfoc > b->max_foc) b->max_foc = h->nfoc;
     RecordArgs &r = rec[i];
     r.fw = (const float *)h->set[0];
     r.fstride = h->g.fstride;

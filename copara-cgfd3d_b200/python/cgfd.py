@@ -70,6 +70,7 @@ _SIGS = {
     "cgfd_autotune": (C.c_int, [_P, C.c_int, _fp]),
     "cgfd_set_boundary_mlp": (C.c_int, [_P, C.c_int, C.c_void_p]),
     "cgfd_set_boundary_mlp_gains": (C.c_int, [_P, _fp]),
+    "cgfd_upload_focal": (C.c_int, [_P, C.c_int, _ip, C.c_int, C.c_double, _fp]),
     "cgfd_boundary_mlp_cells": (C.c_int, [_P, _ip, _ip]),
     "cgfd_boundary_mlp_features": (C.c_int, [_P, _fp, _fp, _fp]),
     "cgfd_mlp_gradient": (C.c_int, [C.c_void_p, _fp, _fp, C.c_int, _fp, _fp]),
@@ -279,6 +280,14 @@ class Solver:
         stf = _as(stf, np.float32).reshape(len(loc), -1)
         self._chk(_lib.cgfd_upload_forces(self._h, len(loc), _i(loc), _f(f3),
                                           stf.shape[1], _f(stf)))
+
+    def upload_focal(self, loc, fdt, mom):
+        """Finite-fault points: loc (n, 3), mom [6][n][fnt] moment series
+        sampled every fdt seconds (cgfd_upload_focal); n = 0 removes them."""
+        loc = _as(loc, np.int32).reshape(-1, 3)
+        mom = _as(mom, np.float32).reshape(6, len(loc), -1) if len(loc) else np.zeros(1, np.float32)
+        fnt = mom.shape[-1] if len(loc) else 1
+        self._chk(_lib.cgfd_upload_focal(self._h, len(loc), _i(loc), fnt, float(fdt), _f(mom)))
 
     def set_receivers(self, loc):
         loc = _as(loc, np.int32).reshape(-1, 3)

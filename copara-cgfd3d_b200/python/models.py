@@ -56,6 +56,11 @@ class Model:
     frc_stf: np.ndarray
     rcv_loc: np.ndarray     # (n, 3) int32
     info: dict = dataclasses.field(default_factory=dict)
+    # focal (finite-fault) points: (n, 3) int32, moment series [6][n][fnt]
+    # float32 sampled every foc_dt seconds from t = 0
+    foc_loc: np.ndarray = None
+    foc_mom: np.ndarray = None
+    foc_dt: float = 0.0
 
     @property
     def cells(self) -> int:
@@ -79,6 +84,8 @@ class Model:
             solver.upload_moments(self.mnt_loc, self.mnt_m6, self.mnt_stf)
         if len(self.frc_loc):
             solver.upload_forces(self.frc_loc, self.frc_f3, self.frc_stf)
+        if self.foc_loc is not None and len(self.foc_loc):
+            solver.upload_focal(self.foc_loc, self.foc_dt, self.foc_mom)
         if len(self.rcv_loc):
             solver.set_receivers(self.rcv_loc)
 
@@ -335,3 +342,42 @@ def batch_models(n=64, seed=7, nt=1000, side=(96, 256), nabs_cells=12, h=100.0,
         m = dataclasses.replace(m, mnt_m6=m6, info=dict(m.info, f0=f0, vp=(vp1, vp2)))
         out.append(m)
     return out
+
+
+def with_finite_fault(m: Model, center, length=8, width=5, strike=30.0, dip=60.0, rake=90.0,
+                      m0=1e15, vr=2500.0, rise=0.4, fdt=None, seed=3) -> Model:
+    """Adds a planar finite fault of length x width points (one per cell on a
+    grid of h spacing along strike and down dip) centred at the reference
+    index `center`: a rupture spreading from the centre at speed vr, each
+    point's moment rate a triangle of duration `rise` scaled by a random
+    slip weight (seed), the mechanism (strike, dip, rake) from angle2moment,
+    the series sampled every fdt (default 1.7 * stept, which is not a
+    multiple of the half step, so stage times fall between samples)."""
+    rng = np.random.default_rng(seed)
+    h = m.steph
+    fdt = fdt or 1.7 * m.stept
+    m6 = np.asarray(cgfd.angle2moment(strike, dip, rake), np.float64)
+    st, dp = math.radians(strike), math.radians(dip)
+    sv = np.array([math.sin(st), math.cos(st), 0.0])              # along strike (x east, y north)
+    dv = np.array([math.cos(dp) * math.cos(st), -math.cos(dp) * math.sin(st), -math.sin(dp)])
+    pts, dist = [], []
+    for a in range(length):
+        for b in range(width):
+            sa, db = (a - (length - 1) / 2) * h, (b - (width - 1) / 2) * h
+            p = np.array(center, np.float64) + (sa * sv + db * dv) / h
+            pts.append(np.rint(p).astype(np.int32))
+            dist.append(math.hypot(sa, db))
+    loc = np.array(pts, np.int32)
+    n = len(loc)
+    t_end = max(dist) / vr + rise
+    fnt = int(math.ceil(t_end / fdt)) + 3
+    t = np.arange(fnt) * fdt
+    w = rng.uniform(0.5, 1.5, n)
+    w *= 1.0 / w.sum()
+    mom = np.zeros((6, n, fnt), np.float32)
+    for q in range(n):
+        t0 = dist[q] / vr
+        tri = np.clip(1.0 - np.abs(t - t0 - rise / 2) / (rise / 2), 0.0, None) * (2.0 / rise)
+        for c in range(6):
+            mom[c, q] = m0 * w[q] * m6[c] * tri
+    return dataclasses.replace(m, foc_loc=loc, foc_mom=mom, foc_dt=float(fdt))

@@ -127,6 +127,20 @@ int cgfd_upload_moments(cgfd_solver *h, int n, const int *loc, const float *m6,
 int cgfd_upload_forces(cgfd_solver *h, int n, const int *loc, const float *f3,
                        int nstf, const float *stf);
 
+/* Finite-fault (focal) sources: n points at loc (3n ints), each with its own
+ * moment time series mom [6][n][fnt] (Mxx, Myy, Mzz, Mxy, Mxz, Myz in N m,
+ * the subfault's moment included) sampled every fdt seconds from t = 0.  In
+ * every stage each point adds -M(t) / (h^3 J) to the stress RHS at
+ * t = (step + tinc/2) * stept, M(t) interpolated linearly between samples
+ * and zero outside [0, fdt*(fnt-1)].  Replaces H_Rmnt + InterpFocus /
+ * ExtractValue + LoadRmom (src/calculate.cu:2586-2643, 1421-1428,
+ * 6257-6319; without the SrcSmooth spreading); the series stay on the
+ * device and are interpolated there every stage, where the reference
+ * interpolates on the host and copies the values every stage.  n = 0
+ * removes them. */
+int cgfd_upload_focal(cgfd_solver *h, int n, const int *loc, int fnt, double fdt,
+                      const float *mom);
+
 /* Receivers (3n ints).  Replaces Hpt + C2DPointPick (src/calculate.cu:2678-2746). */
 int cgfd_set_receivers(cgfd_solver *h, int n, const int *loc);
 

@@ -12,6 +12,8 @@
 //   - CalWavemix (RHS, CFS-PML ADE)                src/calculate.cu:4277-4621
 //   - CalTIMGmix (traction image, top 3 layers)    src/calculate.cu:5668-5897
 //   - LoadForce / LoadMoment                       src/calculate.cu:6130-6255
+//   - InterpFocus / ExtractValue + LoadRmom        src/calculate.cu:2586-2643,
+//     (focal points, without SrcSmooth)            1421-1428, 6257-6319
 //   - IterationBegin/Inner/Final (RK4 + ADE aux)   src/calculate.cu:6330-6734
 //   - RKite stage constants, Tindex                src/calculate.cu:12-13,1355-1422
 //   - per-step F/B direction schedule              src/simulation.cc:252-700
@@ -35,6 +37,7 @@
 
 #include "../include/cgfd.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -108,6 +111,10 @@ struct Solver {
   int nmnt = 0, nfrc = 0, nstfm = 0, nstff = 0;
   std::vector<int> mloc, floc;
   std::vector<double> m6, f3, mstf, fstf;
+  int nfoc = 0, fnt = 0;
+  double fdt = 0;
+  std::vector<int> focloc;
+  std::vector<double> focmom;  // [6][nfoc][fnt]
   int nrecv = 0;
   std::vector<int> rloc;
   std::vector<double> seis;
@@ -442,9 +449,30 @@ void timg(Solver<R> &S, int rk, int X, int Y, int Z) {
       }
 }
 
-// LoadForce / LoadMoment (src/calculate.cu:6130-6255), Tindex = 2*currT+tinc.
+// ExtractValue (src/calculate.cu:2586-2613): the series at time t, linear
+// between samples PL = floor(t/DT) and PL + 1 (PR = PL when t is within 1e-5
+// of a sample), zero outside [0, DT*(n-1)].
+inline double extract_value(const double *stf, int n, double DT, double time) {
+  const double Tend = DT * (n - 1);
+  if (time > Tend || time < 0) return 0;
+  int PL = (int)(time / DT);
+  int PR = (std::fabs(time - DT * std::floor(time / DT)) < 1e-5) ? PL : PL + 1;
+  PL = std::min(PL, n - 1);
+  PR = std::min(PR, n - 1);
+  return stf[PL] + (stf[PR] - stf[PL]) * ((time - DT * PL) / DT);
+}
+
+// LoadForce / LoadMoment (src/calculate.cu:6130-6255), Tindex = 2*currT+tinc;
+// focal points as LoadRmom (6257-6319) at time (currT + tinc/2)*stept.
 template <class R>
-void sources(Solver<R> &S, int tindex) {
+void sources(Solver<R> &S, int tindex, double time) {
+  for (int q = 0; q < S.nfoc; ++q) {
+    const long g = S.gi(S.focloc[3 * q], S.focloc[3 * q + 1], S.focloc[3 * q + 2]);
+    const double A = 1.0 / (S.d.steph * S.d.steph * S.d.steph * (double)S.jac[g]);
+    for (int c = 0; c < 6; ++c)
+      S.hW[TXX + c][g] -=
+          (R)(extract_value(&S.focmom[((size_t)c * S.nfoc + q) * S.fnt], S.fnt, S.fdt, time) * A);
+  }
   const double h3 = S.d.steph * S.d.steph * S.d.steph;
   for (int q = 0; q < S.nfrc; ++q) {
     const int i = S.floc[3 * q], j = S.floc[3 * q + 1], k = S.floc[3 * q + 2];
@@ -528,7 +556,7 @@ int rk_stage(Solver<R> &S, int rk, int curr_t, int X, int Y, int Z, std::string 
   }
   rhs(S, rk, X, Y, Z);
   timg(S, rk, X, Y, Z);
-  sources(S, tindex);
+  sources(S, tindex, (curr_t + tinc * 0.5) * S.d.stept);
   update(S, rk);
   if (rk == 3) {  // wavesyn(FW, W); abssyn(3)
     for (int c = 0; c < 9; ++c) S.FW[c] = S.W[c];
@@ -691,6 +719,20 @@ int orc_upload_forces(void *h, int n, const int *loc, const float *f3, int nstf,
     S.floc.assign(loc, loc + 3 * n);
     S.f3.assign(f3, f3 + 3 * n);
     S.fstf.assign(stf, stf + (size_t)n * nstf);
+    return (int)CGFD_OK;
+  };
+  return DISPATCH(H, f);
+}
+
+int orc_upload_focal(void *h, int n, const int *loc, int fnt, double fdt, const float *mom) {
+  Handle *H = (Handle *)h;
+  auto f = [&](auto &S) {
+    if (n < 0 || (n > 0 && (!loc || !mom || fnt < 1 || !(fdt > 0)))) { H->err = "bad focal sources"; return (int)CGFD_ERR_ARG; }
+    for (int q = 0; q < n; ++q)
+      if (!valid_loc(S, loc + 3 * q)) { H->err = "focal source outside the valid grid"; return (int)CGFD_ERR_ARG; }
+    S.nfoc = n; S.fnt = fnt; S.fdt = fdt;
+    S.focloc.assign(loc, loc + 3 * n);
+    S.focmom.assign(mom, mom + (size_t)6 * n * fnt);
     return (int)CGFD_OK;
   };
   return DISPATCH(H, f);

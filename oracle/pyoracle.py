@@ -38,6 +38,7 @@ _SIGS = {
     "orc_upload_moments": (C.c_int, [_P, C.c_int, _ip, _fp, C.c_int, _fp]),
     "orc_upload_forces": (C.c_int, [_P, C.c_int, _ip, _fp, C.c_int, _fp]),
     "orc_set_receivers": (C.c_int, [_P, C.c_int, _ip]),
+    "orc_upload_focal": (C.c_int, [_P, C.c_int, _ip, C.c_int, C.c_double, _fp]),
     "orc_rk_stage": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     "orc_step": (C.c_int, [_P, C.c_int]),
     "orc_steps_done": (C.c_int, [_P, _ip]),
@@ -130,6 +131,12 @@ class OracleSolver:
         f3 = np.ascontiguousarray(f3, np.float32).reshape(-1, 3)
         stf = np.ascontiguousarray(stf, np.float32).reshape(len(loc), -1)
         self._chk(_lib.orc_upload_forces(self._h, len(loc), _i(loc), _f(f3), stf.shape[1], _f(stf)))
+
+    def upload_focal(self, loc, fdt, mom):
+        loc = np.ascontiguousarray(loc, np.int32).reshape(-1, 3)
+        mom = np.ascontiguousarray(mom, np.float32).reshape(6, len(loc), -1)
+        self._chk(_lib.orc_upload_focal(self._h, len(loc), _i(loc), mom.shape[-1], float(fdt),
+                                        _f(mom)))
 
     def set_receivers(self, loc):
         loc = np.ascontiguousarray(loc, np.int32).reshape(-1, 3)
