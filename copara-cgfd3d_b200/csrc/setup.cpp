@@ -9,11 +9,21 @@
 //   mathfunc wavelets        src/mathfunc.cpp:481-608, sampled like
 //                            source::cal_stf_moment (src/source.cpp:102-131)
 //   source::angle2moment     src/source.cpp:134-155
+//   gridmesh::read_vmapnew   src/gridmesh.cpp:72-533 (+ smooth_zdepth and
+//                            set_twoside_space 1092-1210, and the ghost
+//                            extension common::interpolated_extend,
+//                            src/common.cpp:67-130)
 #include "../../include/cgfd.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <vector>
+
+namespace cgfd {
+void set_global_error(const char *msg);
+}
 
 namespace {
 
@@ -46,6 +56,121 @@ void mirror_ghosts(double *v, const Dims &D, int ni, int nj, int nk) {
         v[D.at(i, j, 3 - s)] = v[D.at(i, j, 3 + s)];
         v[D.at(i, j, nk + 2 + s)] = v[D.at(i, j, nk + 2 - s)];
       }
+}
+
+// ---------------------------- vmap grid -----------------------------------
+
+// The spacing pair (ha0, hb0) of the two constant-spacing ends of a graded
+// layer: na intervals next to the layer above within [ha1, ha2], nb next to
+// the layer below within [hb1, hb2], together of length l; the free length
+// is shared in proportion to the two ranges (set_twoside_space).
+void two_sided_spacing(double l, int na, int nb, double ha1, double ha2, double hb1, double hb2,
+                       double *ha0, double *hb0) {
+  const double free_len = l - na * ha1 - nb * hb1;
+  const double ra = na * (ha2 - ha1), rb = nb * (hb2 - hb1);
+  const double eps = 1.e-5;
+  if (std::fabs(free_len) < eps) {
+    *ha0 = ha1;
+    *hb0 = hb1;
+  } else if (std::fabs(ra) < eps) {
+    *ha0 = ha1;
+    *hb0 = hb1 + free_len / nb;
+  } else if (std::fabs(rb) < eps) {
+    *ha0 = ha1 + free_len / na;
+    *hb0 = hb1;
+  } else {
+    *ha0 = ha1 + free_len * ra / (ra + rb) / na;
+    *hb0 = hb1 + free_len * rb / (ra + rb) / nb;
+  }
+}
+
+// Node depths z[0..n] (bottom zb to top za) of a layer of n intervals whose
+// spacing grades from hb (the layer below) to ha (the layer above)
+// (smooth_zdepth).  When the mean spacing lies between ha and hb, a
+// geometric run of intervals between constant ends, the run shortened one
+// interval at a time until the ends can take up the remaining length;
+// otherwise linear ramps over a quarter of the intervals at each end around
+// a constant middle.  False where the reference's search would not end.
+bool graded_layer(double za, double zb, double ha, double hb, int n, double *z) {
+  if (n < 1) return false;
+  std::vector<double> h(n + 2);
+  const double l = za - zb, h0 = l / n;
+  h[0] = hb;
+  h[n + 1] = ha;
+  if ((h0 >= ha && h0 <= hb) || (h0 <= ha && h0 >= hb)) {
+    int nb = 1, na = n, n0 = n;
+    for (;;) {
+      if (n0 < 0) return false;
+      double run = 0.0;
+      const double f = std::pow(ha / hb, 1.0 / (n0 + 1)) - 1.0;
+      for (int k = 1; k <= nb - 1; ++k) h[k] = hb;
+      for (int k = na + 1; k <= n + 1; ++k) h[k] = ha;
+      for (int k = nb; k <= na; ++k) {
+        h[k] = h[k - 1] * (1 + f);
+        run += h[k];
+      }
+      const double ha1 = ha * std::min(1.0, 1.0 - f), ha2 = ha * std::max(1.0, 1.0 - f);
+      const double hb1 = hb * std::min(1.0, 1.0 + f), hb2 = hb * std::max(1.0, 1.0 + f);
+      const double la1 = (n - na) * ha1, la2 = (n - na) * ha2;
+      const double lb1 = (nb - 1) * hb1, lb2 = (nb - 1) * hb2;
+      if ((la1 + lb1 <= l - run) && (l - run <= la2 + lb2)) {
+        double ha0, hb0;
+        two_sided_spacing(l - run, n - na, nb - 1, ha1, ha2, hb1, hb2, &ha0, &hb0);
+        for (int k = na + 1; k <= n; ++k) h[k] = ha0;
+        for (int k = 1; k <= nb - 1; ++k) h[k] = hb0;
+        break;
+      }
+      // the ends are too long (or too short) for the rest: hand one interval
+      // of the run to the end with the smaller (or larger) spacing
+      const bool too_long = l - run < la1 + lb1;
+      if (too_long == (ha < hb)) --na;
+      else ++nb;
+      --n0;
+    }
+  } else {
+    const int na = n / 4, nb = n / 4, n0 = n - na - nb;
+    if (nb < 1) return false;
+    const double la1 = (na + 1) * na / 2.0, lb1 = (nb + 1) * nb / 2.0;
+    const double la2 = la1 + na * lb1 / nb + na * n0;
+    const double l0 = l - na * ha - nb * hb - n0 * ha - la1 * (ha - hb) / nb;
+    const double ha0 = l0 / la2, hb0 = (na * ha0 + ha - hb) / nb;
+    for (int k = 1; k <= nb; ++k) h[k] = hb + k * hb0;
+    for (int k = nb + 1; k <= nb + n0; ++k) h[k] = h[k - 1];
+    for (int k = nb + n0 + 1; k <= n; ++k) h[k] = ha + (n - k + 1) * ha0;
+  }
+  z[0] = 0.0;
+  for (int k = 0; k < n; ++k) z[k + 1] = z[k] + h[k + 1];
+  for (int k = 0; k < n + 1; ++k) z[k] = z[k] + zb;
+  return true;
+}
+
+// Ghost nodes by linear extrapolation 2 v[edge] - v[edge -+ s], along z for
+// every (x, y) column, then y, then x over the whole array (edges and
+// corners included), as common::interpolated_extend.
+void extend_linear(double *v, const Dims &D, int ni, int nj, int nk) {
+  for (int i = 0; i < D.nx; ++i)
+    for (int j = 0; j < D.ny; ++j)
+      for (int s = 1; s <= 3; ++s) {
+        v[D.at(i, j, 3 - s)] = 2.0 * v[D.at(i, j, 3)] - v[D.at(i, j, 3 + s)];
+        v[D.at(i, j, nk + 2 + s)] = 2.0 * v[D.at(i, j, nk + 2)] - v[D.at(i, j, nk + 2 - s)];
+      }
+  for (int i = 0; i < D.nx; ++i)
+    for (int k = 0; k < D.nz; ++k)
+      for (int s = 1; s <= 3; ++s) {
+        v[D.at(i, 3 - s, k)] = 2.0 * v[D.at(i, 3, k)] - v[D.at(i, 3 + s, k)];
+        v[D.at(i, nj + 2 + s, k)] = 2.0 * v[D.at(i, nj + 2, k)] - v[D.at(i, nj + 2 - s, k)];
+      }
+  for (int j = 0; j < D.ny; ++j)
+    for (int k = 0; k < D.nz; ++k)
+      for (int s = 1; s <= 3; ++s) {
+        v[D.at(3 - s, j, k)] = 2.0 * v[D.at(3, j, k)] - v[D.at(3 + s, j, k)];
+        v[D.at(ni + 2 + s, j, k)] = 2.0 * v[D.at(ni + 2, j, k)] - v[D.at(ni + 2 - s, j, k)];
+      }
+}
+
+int grid_fail(const std::string &msg) {
+  cgfd::set_global_error(("cgfd_grid_vmap: " + msg).c_str());
+  return CGFD_ERR_ARG;
 }
 
 }  // namespace
@@ -195,6 +320,127 @@ int cgfd_angle2moment(double strike, double dip, double rake, double m6[6]) {
   m6[3] = sd * cr * c2s + 0.5 * s2d * sr * s2s;
   m6[4] = -(cd * cr * cs + c2d * sr * ss);
   m6[5] = -(cd * cr * ss - c2d * sr * cs);
+  return CGFD_OK;
+}
+
+int cgfd_grid_vmap(int ni, int nj, int nk, int nsurf, const int *gridpoints,
+                   const int *equalspacing, const double *anchor, int hybrid,
+                   double convers_depth, double *x, double *y, double *z, int *con_index) {
+  if (ni < 1 || nj < 1 || nk < 2 || nsurf < 2 || !gridpoints || !equalspacing || !anchor || !x ||
+      !y || !z || !con_index)
+    return grid_fail("bad arguments");
+  const int nl = nsurf - 1;  // layers
+  const Dims D{ni + 6, nj + 6, nk + 6};
+  const int stride = 2 + nsurf;  // per column: x, y, z_0 .. z_{nsurf-1}
+  auto col = [&](int i, int j) { return anchor + ((size_t)i * nj + j) * stride; };
+  // the reference's checks (src/gridmesh.cpp:134-158)
+  long total = 0;
+  for (int l = 0; l < nl; ++l) {
+    if (gridpoints[l] < 1) return grid_fail("every layer needs at least one interval");
+    total += gridpoints[l];
+  }
+  if (!equalspacing[0] || !equalspacing[nl - 1])
+    return grid_fail("the first and the last layer must be equally spaced");
+  for (int l = 1; l < nl; ++l)
+    if (!equalspacing[l - 1] && !equalspacing[l])
+      return grid_fail("two adjacent layers cannot both be graded");
+  if (total + 1 != nk) return grid_fail("the layers' intervals + 1 must equal nk");
+  for (int i = 0; i < ni; ++i)
+    for (int j = 0; j < nj; ++j)
+      for (int q = 1; q < nsurf; ++q)
+        if (col(i, j)[2 + q] > col(i, j)[1 + q])
+          return grid_fail("interface depths must decrease from the top down");
+
+  // the layer stack actually meshed: the given one, or (hybrid) its layers
+  // above the conversion depth, the layer holding it cut there, and one flat
+  // layer from there to the deepest point of the last interface, the nk - 1
+  // intervals shared in proportion to the layers' thickness ranges
+  std::vector<int> gp(gridpoints, gridpoints + nl);
+  std::vector<int> eq(equalspacing, equalspacing + nl);
+  int ns = nsurf;           // interfaces meshed
+  double z_conv = 0, z_bottom = 0;
+  int conv_iface = -1;      // hybrid: index of the conversion interface
+  if (hybrid) {
+    std::vector<double> iface_min(nsurf), iface_max(nsurf), layer_min(nl), layer_max(nl);
+    for (int q = 0; q < nsurf; ++q) {
+      iface_min[q] = iface_max[q] = col(0, 0)[2 + q];
+      for (int i = 0; i < ni; ++i)
+        for (int j = 0; j < nj; ++j) {
+          iface_min[q] = std::min(iface_min[q], col(i, j)[2 + q]);
+          iface_max[q] = std::max(iface_max[q], col(i, j)[2 + q]);
+        }
+    }
+    for (int l = 0; l < nl; ++l) {  // [lowest bottom, highest top]
+      layer_max[l] = iface_max[l];
+      layer_min[l] = iface_min[l + 1];
+    }
+    for (int l = 0; l < nl; ++l)
+      if (convers_depth >= layer_min[l] && convers_depth <= layer_max[l]) {
+        conv_iface = l + 1;
+        break;
+      }
+    if (conv_iface < 0) return grid_fail("the conversion depth lies in no layer");
+    z_conv = convers_depth;
+    z_bottom = iface_min[nsurf - 1];
+    ns = conv_iface + 2;
+    // thickness ranges of the new layers
+    std::vector<double> lo(conv_iface + 1), hi(conv_iface + 1);
+    for (int l = 0; l < conv_iface; ++l) {
+      lo[l] = layer_min[l];
+      hi[l] = layer_max[l];
+    }
+    lo[conv_iface - 1] = z_conv;
+    lo[conv_iface] = z_bottom;
+    hi[conv_iface] = z_conv;
+    double total_len = 0;
+    for (int l = 0; l <= conv_iface; ++l) total_len += hi[l] - lo[l];
+    gp.assign(conv_iface + 1, 0);
+    eq.assign(conv_iface + 1, 1);
+    for (int l = 0; l < conv_iface; ++l) eq[l] = equalspacing[l];
+    gp[conv_iface] = nk - 1;
+    for (int l = 0; l < conv_iface; ++l) {
+      gp[l] = (int)(nk * (hi[l] - lo[l]) / total_len);
+      gp[conv_iface] -= gp[l];
+    }
+    for (int l = 0; l <= conv_iface; ++l)
+      if (gp[l] < 1) return grid_fail("a layer of the hybrid grid receives no interval");
+  }
+  // node index of each interface: the last at the bottom (3), upwards from there
+  std::vector<int> kidx(ns);
+  kidx[ns - 1] = 3;
+  for (int q = ns - 2; q >= 0; --q) kidx[q] = kidx[q + 1] + gp[q];
+  *con_index = hybrid ? kidx[ns - 1] + gp[ns - 2] : 3;
+
+  std::vector<double> zi(ns), zv(D.nz);
+  for (int i = 0; i < ni; ++i)
+    for (int j = 0; j < nj; ++j) {
+      const double *c = col(i, j);
+      for (int q = 0; q < ns; ++q)
+        zi[q] = !hybrid || q < conv_iface ? c[2 + q] : (q == conv_iface ? z_conv : z_bottom);
+      for (int l = 0; l < ns - 1; ++l) {
+        const int top = kidx[l], bot = kidx[l + 1];
+        if (eq[l]) {
+          const double step = (zi[l] - zi[l + 1]) / (1.0 * gp[l]);
+          for (int m = bot; m <= top; ++m) zv[m] = zi[l] + (m - top) * step;
+        } else {
+          const double ha = (zi[l - 1] - zi[l]) / (1.0 * gp[l - 1]);
+          const double hb = (zi[l + 1] - zi[l + 2]) / (1.0 * gp[l + 1]);
+          if (!graded_layer(zi[l], zi[l + 1], ha, hb, gp[l], &zv[bot]))
+            return grid_fail("a graded layer cannot join its neighbours' spacings");
+        }
+        zv[top] = zi[l];
+        zv[bot] = zi[l + 1];
+      }
+      for (int k = 3; k < nk + 3; ++k) {
+        const long g = D.at(i + 3, j + 3, k);
+        x[g] = c[0];
+        y[g] = c[1];
+        z[g] = zv[k];
+      }
+    }
+  extend_linear(x, D, ni, nj, nk);
+  extend_linear(y, D, ni, nj, nk);
+  extend_linear(z, D, ni, nj, nk);
   return CGFD_OK;
 }
 

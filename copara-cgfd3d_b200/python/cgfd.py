@@ -71,6 +71,8 @@ _SIGS = {
     "cgfd_set_boundary_mlp": (C.c_int, [_P, C.c_int, C.c_void_p]),
     "cgfd_set_boundary_mlp_gains": (C.c_int, [_P, _fp]),
     "cgfd_upload_focal": (C.c_int, [_P, C.c_int, _ip, C.c_int, C.c_double, _fp]),
+    "cgfd_grid_vmap": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _ip, _ip, _dp, C.c_int,
+                                 C.c_double, _dp, _dp, _dp, _ip]),
     "cgfd_boundary_mlp_cells": (C.c_int, [_P, _ip, _ip]),
     "cgfd_boundary_mlp_features": (C.c_int, [_P, _fp, _fp, _fp]),
     "cgfd_mlp_gradient": (C.c_int, [C.c_void_p, _fp, _fp, C.c_int, _fp, _fp]),
@@ -489,6 +491,24 @@ def stf(kind, start, t0, f0, n, dt) -> np.ndarray:
     if st:
         raise CgfdError(st, "stf")
     return out
+
+
+def grid_vmap(ni, nj, nk, gridpoints, equalspacing, anchor, hybrid=False, convers_depth=0.0):
+    """Node coordinates of a vmap grid (cgfd_grid_vmap): anchor [ni][nj][2 +
+    nsurf] = x, y, z of each interface from the top down; returns (x, y, z)
+    full arrays (ni+6, nj+6, nk+6) and ConIndex."""
+    anchor = np.ascontiguousarray(anchor, np.float64)
+    nsurf = anchor.shape[-1] - 2
+    gp = np.ascontiguousarray(gridpoints, np.int32)
+    eq = np.ascontiguousarray(equalspacing, np.int32)
+    shape = (ni + 6, nj + 6, nk + 6)
+    x, y, z = (np.zeros(shape, np.float64) for _ in range(3))
+    con = C.c_int()
+    st = _lib.cgfd_grid_vmap(ni, nj, nk, nsurf, _i(gp), _i(eq), _d(anchor), int(bool(hybrid)),
+                             float(convers_depth), _d(x), _d(y), _d(z), C.byref(con))
+    if st:
+        raise CgfdError(st, last_error(None))
+    return x, y, z, con.value
 
 
 def angle2moment(strike, dip, rake) -> np.ndarray:

@@ -311,6 +311,25 @@ int cgfd_batch_destroy(cgfd_batch *b);
 
 /* ---------------- host pre-processing helpers (FP64) ---------------------- */
 
+/* Grid node coordinates of the reference's vmap grid type (grid_type =
+ * vmap: gridmesh::read_vmapnew, src/gridmesh.cpp:72-533, with smooth_zdepth
+ * and set_twoside_space, 1092-1210, and the ghost extension
+ * common::interpolated_extend, src/common.cpp:67-130), in FP64.  nsurf
+ * interfaces from the top (the surface) down are given per (i, j) column:
+ * anchor[((size_t)i*nj + j)*(2 + nsurf) + q] = x, y, z_0 .. z_{nsurf-1}
+ * (z decreasing downwards), the content of the reference's <vmap_anchor>
+ * block; per layer l = 0..nsurf-2, gridpoints[l] intervals and
+ * equalspacing[l] (0: the layer grades its spacing between its
+ * neighbours').  hybrid != 0: curvilinear above convers_depth and horizontal
+ * planes below, the layers above re-cut in proportion to their thickness as
+ * the reference does.  Outputs x, y, z as full arrays (ni+6)(nj+6)(nk+6),
+ * z fastest, and *con_index (ConIndex: the first node index of the
+ * curvilinear part; 3 when not hybrid).  The reference's input checks apply
+ * (the message is available from cgfd_last_error(NULL, ...)). */
+int cgfd_grid_vmap(int ni, int nj, int nk, int nsurf, const int *gridpoints,
+                   const int *equalspacing, const double *anchor, int hybrid,
+                   double convers_depth, double *x, double *y, double *z, int *con_index);
+
 /* Grid metric from node coordinates (full arrays, reference layout), by
  * 2-point central differences and cross products, then mirrored into the
  * ghost cells: gridmesh::calmetric (src/gridmesh.cpp:1476-1627).
