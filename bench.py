@@ -240,7 +240,9 @@ def cpu_baseline(cfg, seconds):
                       f"FP64 oracle, {el:.1f} s"}
 
 
-def dist_init(n):
+def dist_init(n, backend=None):
+    """One process per GPU (replicas): the process group of a torchrun launch.
+    backend: "nccl" (default with a GPU) or "gloo" (CPU; the tests' ranks)."""
     import torch
     import torch.distributed as dist
     if n <= 1:
@@ -248,18 +250,24 @@ def dist_init(n):
     rank = int(os.environ["RANK"])
     world = int(os.environ["WORLD_SIZE"])
     local = int(os.environ.get("LOCAL_RANK", rank))
-    torch.cuda.set_device(local)
+    backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
     import datetime
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                            device_id=torch.device("cuda", local))
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    else:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
     return dist, rank, world, local
 
 
 def allmax(dist, x):
+    """The maximum of x over ranks (device-timed values: the slowest rank)."""
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -268,7 +276,14 @@ def barrier(dist):
     if dist is not None:
         import torch
         dist.barrier()
-        torch.cuda.synchronize()
+        if dist.get_backend() == "nccl":
+            torch.cuda.synchronize()
+
+
+def replica_value(world, cells, steps, ms):
+    """Whole-job Gcell/s of `world` independent replicas of a model of
+    `cells` cells, each stepped `steps` times, the slowest taking ms."""
+    return world * cells * steps / (ms / 1e3) / 1e9
 
 
 def run_reference(args):
@@ -337,7 +352,7 @@ def main():
     stage_ms = allmax(dist, stage_ms)
     nbad = s.check_finite()
     s.close()
-    value = world * m.cells * K / (ms / 1e3) / 1e9
+    value = replica_value(world, m.cells, K, ms)
 
     e2e = None
     if not args.no_e2e:
