@@ -189,9 +189,15 @@ WorkParams pair_get_work(const void *plan);
 void *pair_create_plan(const Geom &g, int elem, void *const sets[4], const float *media,
                        const float *metric, float *const aux[3]);
 void pair_destroy_plan(void *plan);
-// the paired kernels run with a.tw_skip set (tW elision)
-void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *err,
-                       void *stream);
+// a second stream and two events (cudaStream_t / cudaEvent_t) for work
+// that may run beside the stage kernels
+struct SideStream {
+  void *stream, *fork, *join;
+};
+// the paired kernels run with a.tw_skip set (tW elision); with side, the
+// traction image runs on side->stream beside the two parts
+void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *err, void *stream,
+                       const SideStream *side = nullptr);
 int pair_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str);
 // A batch of models (FP32 storage) in one persistent launch per stage part:
 // per-model buffers as n x 4 sets, n media, n metrics, n x 3 auxiliaries.

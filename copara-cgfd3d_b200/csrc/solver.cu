@@ -299,6 +299,7 @@ struct cgfd_solver {
   cgfd_desc d{};
   Geom g{};
   cudaStream_t st = nullptr;
+  SideStream side{nullptr, nullptr, nullptr};  // traction image beside the stage kernels
   std::string err;
   void *state = nullptr;   // 4 sets of 9 components: FW, Wa, Wb, tW
   void *set[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -414,6 +415,9 @@ void free_all(cgfd_solver *h) {
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->st) cudaStreamDestroy(h->st);
+  if (h->side.stream) cudaStreamDestroy((cudaStream_t)h->side.stream);
+  if (h->side.fork) cudaEventDestroy((cudaEvent_t)h->side.fork);
+  if (h->side.join) cudaEventDestroy((cudaEvent_t)h->side.join);
 }
 
 long ref_n(const cgfd_solver *h) {
@@ -624,7 +628,7 @@ void dispatch_stage(cgfd_solver *h, const StageArgs &a, int in_set) {
   if (h->d.kernel == CGFD_KERNEL_SIMPLE)
     launch_stage_simple(a, h->st);
   else if (h->d.kernel == CGFD_KERNEL_FUSED)
-    launch_stage_pair(h->plan, a, in_set, h->d_err, h->st);
+    launch_stage_pair(h->plan, a, in_set, h->d_err, h->st, &h->side);
   else
     launch_stage_fused(h->plan, a, in_set, h->d_err, h->st);
 }
@@ -809,6 +813,14 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
     if (e == cudaSuccess) e = cudaMalloc(&h->d_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->d_err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t e1 = nullptr, e2 = nullptr;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
+    h->side.stream = s2;
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&e1, cudaEventDisableTiming);
+    h->side.fork = e1;
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&e2, cudaEventDisableTiming);
+    h->side.join = e2;
     if (e != cudaSuccess) st = cuda_fail(nullptr, e, "setup");
   }
   if (st) {

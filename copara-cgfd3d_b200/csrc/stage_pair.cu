@@ -329,13 +329,22 @@ void pair_destroy_plan(void *plan) {
   delete pl;
 }
 
-void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *err,
-                       void *stream) {
+void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *err, void *stream,
+                       const SideStream *side) {
   const Plan &pl = *reinterpret_cast<const Plan *>(plan);
   cudaStream_t s = (cudaStream_t)stream;
   const int kind = a.rk == 0 ? 0 : (a.rk < 3 ? 1 : 2);
   Maps mv, ms;
   stage_maps(pl.mm[0], a.rk, in_set, a.tw_skip && a.rk == 1, mv, ms);
+  // the traction image needs only the stage input and writes what the two
+  // parts neither write nor use (the top three layers' V, their tW and x/y
+  // auxiliaries): with a side stream it runs beside them, joined at the end
+  if (side) {
+    cudaEventRecord((cudaEvent_t)side->fork, s);
+    cudaStreamWaitEvent((cudaStream_t)side->stream, (cudaEvent_t)side->fork, 0);
+    launch_timg(a, side->stream);
+    cudaEventRecord((cudaEvent_t)side->join, (cudaStream_t)side->stream);
+  }
   // both parts' item counters restart at zero
   cudaMemsetAsync(pl.wk.counter, 0, 2 * sizeof(int), s);
   typedef void (*LaunchFn)(const Plan &, const Maps &, const StageArgs &, int *, cudaStream_t);
@@ -346,7 +355,8 @@ void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *er
   const int e = pl.elem == ELEM_F16 ? 1 : pl.elem == ELEM_BF16 ? 2 : 0;
   fns[e][0][kind](pl, mv, a, err, s);
   fns[e][1][kind](pl, ms, a, err, s);
-  launch_timg(a, s);
+  if (side) cudaStreamWaitEvent(s, (cudaEvent_t)side->join, 0);
+  else launch_timg(a, s);
 }
 
 // ---------------------------- batched models ------------------------------
