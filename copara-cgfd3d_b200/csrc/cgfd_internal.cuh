@@ -193,9 +193,12 @@ void pair_destroy_plan(void *plan);
 // that may run beside the stage kernels
 struct SideStream {
   void *stream, *fork, *join;
+  void *stream2, *fork2, *join2;  // the stress part beside the velocity part
 };
 // the paired kernels run with a.tw_skip set (tW elision); with side, the
-// traction image runs on side->stream beside the two parts
+// traction image runs on side->stream and the stress part on side->stream2,
+// beside the velocity part (the three read only the stage input and write
+// disjoint components)
 void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *err, void *stream,
                        const SideStream *side = nullptr);
 int pair_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str);

@@ -299,7 +299,8 @@ struct cgfd_solver {
   cgfd_desc d{};
   Geom g{};
   cudaStream_t st = nullptr;
-  SideStream side{nullptr, nullptr, nullptr};  // traction image beside the stage kernels
+  // traction image and stress part beside the velocity part
+  SideStream side{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   std::string err;
   void *state = nullptr;   // 4 sets of 9 components: FW, Wa, Wb, tW
   void *set[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -418,6 +419,9 @@ void free_all(cgfd_solver *h) {
   if (h->side.stream) cudaStreamDestroy((cudaStream_t)h->side.stream);
   if (h->side.fork) cudaEventDestroy((cudaEvent_t)h->side.fork);
   if (h->side.join) cudaEventDestroy((cudaEvent_t)h->side.join);
+  if (h->side.stream2) cudaStreamDestroy((cudaStream_t)h->side.stream2);
+  if (h->side.fork2) cudaEventDestroy((cudaEvent_t)h->side.fork2);
+  if (h->side.join2) cudaEventDestroy((cudaEvent_t)h->side.join2);
 }
 
 long ref_n(const cgfd_solver *h) {
@@ -821,6 +825,14 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
     h->side.fork = e1;
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&e2, cudaEventDisableTiming);
     h->side.join = e2;
+    cudaStream_t s3 = nullptr;
+    cudaEvent_t e3 = nullptr, e4 = nullptr;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s3, cudaStreamNonBlocking);
+    h->side.stream2 = s3;
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&e3, cudaEventDisableTiming);
+    h->side.fork2 = e3;
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&e4, cudaEventDisableTiming);
+    h->side.join2 = e4;
     if (e != cudaSuccess) st = cuda_fail(nullptr, e, "setup");
   }
   if (st) {

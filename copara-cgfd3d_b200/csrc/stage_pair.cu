@@ -347,6 +347,15 @@ void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *er
   }
   // both parts' item counters restart at zero
   cudaMemsetAsync(pl.wk.counter, 0, 2 * sizeof(int), s);
+  // the stress part needs the stage input's velocities, not the velocity
+  // part's output, and writes other components: with a second side stream
+  // its CTAs take the SMs as the velocity part's drain
+  cudaStream_t s2 = s;
+  if (side && side->stream2) {
+    s2 = (cudaStream_t)side->stream2;
+    cudaEventRecord((cudaEvent_t)side->fork2, s);
+    cudaStreamWaitEvent(s2, (cudaEvent_t)side->fork2, 0);
+  }
   typedef void (*LaunchFn)(const Plan &, const Maps &, const StageArgs &, int *, cudaStream_t);
   static const LaunchFn fns[3][2][3] = {
       {{launch_fv0, launch_fv1, launch_fv2}, {launch_fs0, launch_fs1, launch_fs2}},
@@ -354,7 +363,11 @@ void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *er
       {{launch_bv0, launch_bv1, launch_bv2}, {launch_bs0, launch_bs1, launch_bs2}}};
   const int e = pl.elem == ELEM_F16 ? 1 : pl.elem == ELEM_BF16 ? 2 : 0;
   fns[e][0][kind](pl, mv, a, err, s);
-  fns[e][1][kind](pl, ms, a, err, s);
+  fns[e][1][kind](pl, ms, a, err, s2);
+  if (s2 != s) {
+    cudaEventRecord((cudaEvent_t)side->join2, s2);
+    cudaStreamWaitEvent(s, (cudaEvent_t)side->join2, 0);
+  }
   if (side) cudaStreamWaitEvent(s, (cudaEvent_t)side->join, 0);
   else launch_timg(a, s);
 }
