@@ -72,6 +72,10 @@ struct Geom {
   size_t plane;        // px * nyi
   size_t fstride;      // elements between components of a set
   size_t astride[3];   // elements between components of an aux set
+  // components per aux set: 9 (one per field), or 6 for the paired kernels:
+  // V's three, then one per velocity derivative in that direction, from
+  // which the six stresses' auxiliaries follow linearly
+  int ncaux;
 };
 
 __host__ __device__ inline size_t gidx(const Geom &g, int ix, int iy, int iz) {

@@ -616,7 +616,7 @@ StageArgs stage_args(cgfd_solver *h, int rk, int X, int Y, int Z, int in_set, in
   for (int q = 0; q < 3; ++q) {
     a.apd[q] = h->pmlp[q]; a.b[q] = h->pmlp[3 + q]; a.db[q] = h->pmlp[6 + q];
     if (h->aux[q]) {
-      const size_t ss = 9 * h->g.astride[q];
+      const size_t ss = (size_t)h->g.ncaux * h->g.astride[q];
       float *FA = h->aux[q], *A = h->aux[q] + ss, *TA = h->aux[q] + 2 * ss;
       a.ain[q] = (rk == 0) ? FA : A;
       a.afw[q] = FA;
@@ -782,6 +782,7 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
   g.astride[0] = align_up((size_t)g.nzi * g.nyi * g.nxa, 64);
   g.astride[1] = align_up((size_t)g.nzi * g.nya * g.px, 64);
   g.astride[2] = align_up((size_t)g.nza * g.nyi * g.px, 64);
+  g.ncaux = (d->kernel == CGFD_KERNEL_FUSED) ? 6 : 9;
   if ((d->kernel == CGFD_KERNEL_SCALAR && !fused_supported(g)) ||
       (d->kernel == CGFD_KERNEL_FUSED && !pair_supported(g))) {
     delete h;
@@ -806,7 +807,8 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
   const size_t plen = align_up(g.px, 64) * 3 + align_up(g.nyi, 64) * 3 + align_up(g.nzi, 64) * 3;
   if (!st) st = alloc(&h->pml, plen);
   for (int q = 0; q < 3 && !st; ++q)
-    if ((q == 0 ? g.nxa : q == 1 ? g.nya : g.nza) > 0) st = alloc(&h->aux[q], 3 * 9 * g.astride[q]);
+    if ((q == 0 ? g.nxa : q == 1 ? g.nya : g.nza) > 0)
+      st = alloc(&h->aux[q], 3 * (size_t)g.ncaux * g.astride[q]);
   if (!st) st = alloc(&h->matv, 18 * g.plane);
   if (!st) {
     e = cudaMalloc(&h->d_step, sizeof(int));
@@ -1520,7 +1522,8 @@ static int snapshot_take(cgfd_solver *h, Snapshot &sn) {
   sn.bufs.clear();
   sn.bufs.push_back({h->state, 4 * 9 * h->g.fstride * elem_size(h->elem)});
   for (int d = 0; d < 3; ++d)
-    if (h->aux[d]) sn.bufs.push_back({h->aux[d], 3 * 9 * h->g.astride[d] * sizeof(float)});
+    if (h->aux[d])
+      sn.bufs.push_back({h->aux[d], 3 * (size_t)h->g.ncaux * h->g.astride[d] * sizeof(float)});
   if (h->d_seis)
     sn.bufs.push_back({h->d_seis, (size_t)9 * h->nrecv * (h->d.nt > 0 ? h->d.nt : 1) * 4});
   sn.steps = h->steps;

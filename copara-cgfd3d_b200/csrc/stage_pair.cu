@@ -54,12 +54,12 @@ bool field_map(CUtensorMap *m, const Geom &g, const void *base, int ncomp, int b
 // a map over one auxiliary set (9 components) of direction d
 bool aux_map(CUtensorMap *m, const Geom &g, int d, const float *base, int bc) {
   if (d == 0)
-    return make_map(m, base, g.nxa, g.nyi, g.nzi, 9, g.nxa, (size_t)g.nxa * g.nyi, g.astride[0],
+    return make_map(m, base, g.nxa, g.nyi, g.nzi, g.ncaux, g.nxa, (size_t)g.nxa * g.nyi, g.astride[0],
                     CX, TY, bc);
   if (d == 1)
-    return make_map(m, base, g.px, g.nya, g.nzi, 9, g.px, (size_t)g.px * g.nya, g.astride[1],
+    return make_map(m, base, g.px, g.nya, g.nzi, g.ncaux, g.px, (size_t)g.px * g.nya, g.astride[1],
                     CX, TY, bc);
-  return make_map(m, base, g.px, g.nyi, g.nza, 9, g.px, g.plane, g.astride[2], CX, TY, bc);
+  return make_map(m, base, g.px, g.nyi, g.nza, g.ncaux, g.px, g.plane, g.astride[2], CX, TY, bc);
 }
 
 }  // namespace
@@ -104,10 +104,10 @@ bool model_maps(ModelMaps *pl, int *has_aux, const Geom &g, int elem, void *cons
   for (int d = 0; d < 3; ++d) {
     has_aux[d] = aux[d] != nullptr;
     if (!aux[d]) continue;
-    const size_t ss = 9 * g.astride[d];
+    const size_t ss = (size_t)g.ncaux * g.astride[d];
     for (int t = 0; t < 3; ++t) {  // FA, A, tA
       ok = ok && aux_map(&pl->auxV[d][t], g, d, aux[d] + t * ss, 3);
-      ok = ok && aux_map(&pl->auxT[d][t], g, d, aux[d] + t * ss, 6);
+      ok = ok && aux_map(&pl->auxT[d][t], g, d, aux[d] + t * ss, 3);
     }
   }
   return ok;

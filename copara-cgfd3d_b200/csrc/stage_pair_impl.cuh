@@ -509,11 +509,16 @@ __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, cons
   };
   T *out = static_cast<T *>(a.out), *tw = static_cast<T *>(a.tw);
 
-  // general path: issue every stage-input auxiliary load before the stencil
+  // general path: issue every stage-input auxiliary load before the stencil.
+  // The stress auxiliaries are kept as one per velocity derivative of the
+  // direction (x: d/dx of Vx, Vy, Vz; y: d/dy; z: d/dzeta): each stress's
+  // ADE auxiliary is the same linear combination of them, with cell-constant
+  // coefficients, as its RHS term is of the derivatives (the ADE is linear),
+  // so three values per direction stand for six.
   const bool gen = !pl.lean;
   int mx = 0, my = 0, mz = 0;
   AuxIdx ix;
-  Aux2<KIND, 6> ax, ay, az;
+  Aux2<KIND, 3> ax, ay, az;
   if (gen) {
     ix = AuxIdx(a, e, pl);
     mx = e.mx;
@@ -585,18 +590,6 @@ __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, cons
 #pragma unroll
     for (int q = 0; q < 6; ++q)
       hw[q] = fma2(dzt[q], iBz, fma2(det[q], iBy, mul2(dxi[q], e.iBx)));
-    if (mx) {
-#pragma unroll
-      for (int q = 0; q < 6; ++q) hw[q] = fma2(neg2(ax.ai[q]), e.iBx, hw[q]);
-    }
-    if (my) {
-#pragma unroll
-      for (int q = 0; q < 6; ++q) hw[q] = fma2(neg2(ay.ai[q]), iBy, hw[q]);
-    }
-    if (mz) {
-#pragma unroll
-      for (int q = 0; q < 6; ++q) hw[q] = fma2(neg2(az.ai[q]), iBz, hw[q]);
-    }
     // surface layer: the ADE auxiliaries also take the xi (eta) part of the
     // surface-matrix d/dzeta of V (src/calculate.cu:4479-4491, 4527-4538)
     auto surf = [&](f2 z1v, f2 z2v, f2 z3v, f2 f, f2 *out) {
@@ -608,31 +601,69 @@ __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, cons
       out[4] = fma2(f, mul2(fma2(ztx, z3v, mul2(ztz, z1v)), miu), out[4]);
       out[5] = fma2(f, mul2(fma2(zty, z3v, mul2(ztz, z2v)), miu), out[5]);
     };
-    // one direction at a time: auxiliary RHS, then its RK update
-    f2 ha[6];
-    if (mx) {
-#pragma unroll
-      for (int q = 0; q < 6; ++q) ha[q] = fma2(neg2(e.apdx), ax.ai[q], mul2(dxi[q], e.dbx));
+    // the six stresses' terms of a vector v of x / y / zeta derivatives of
+    // (Vx, Vy, Vz), as dxi / det / dzt are of the derivatives themselves
+    // (on the surface layer with the surface-matrix part, scaled by B, which
+    // the auxiliary RHS of the reference carries there)
+    const float *my2 = mv + 9 * g.plane;
+    auto terms_x = [&](const f2 *v, f2 *o) {
+      o[0] = mul2(lam2mu, v[0]); o[1] = mul2(lambda, v[0]); o[2] = mul2(lambda, v[0]);
+      o[3] = mul2(v[1], miu); o[4] = mul2(v[2], miu); o[5] = S2(0.f);
       if (pl.top)
-        surf(mat_row(mv, g.plane, 0, DxVx, DxVy, DxVz), mat_row(mv, g.plane, 3, DxVx, DxVy, DxVz),
-             mat_row(mv, g.plane, 6, DxVx, DxVy, DxVz), mul2(e.dbx, e.bbx), ha);
+        surf(mat_row(mv, g.plane, 0, v[0], v[1], v[2]), mat_row(mv, g.plane, 3, v[0], v[1], v[2]),
+             mat_row(mv, g.plane, 6, v[0], v[1], v[2]), e.bbx, o);
+    };
+    auto terms_y = [&](const f2 *v, f2 *o) {
+      o[0] = mul2(lambda, v[1]); o[1] = mul2(lam2mu, v[1]); o[2] = mul2(lambda, v[1]);
+      o[3] = mul2(v[0], miu); o[4] = S2(0.f); o[5] = mul2(v[2], miu);
+      if (pl.top)
+        surf(mat_row(my2, g.plane, 0, v[0], v[1], v[2]), mat_row(my2, g.plane, 3, v[0], v[1], v[2]),
+             mat_row(my2, g.plane, 6, v[0], v[1], v[2]), S2(e.bby), o);
+    };
+    auto terms_z = [&](const f2 *v, f2 *o) {
+      const f2 tx2 = mul2(ztx, v[0]), ty2 = mul2(zty, v[1]), tz2 = mul2(ztz, v[2]);
+      o[0] = fma2(lambda, tz2, fma2(lambda, ty2, mul2(lam2mu, tx2)));
+      o[1] = fma2(lambda, tz2, fma2(lam2mu, ty2, mul2(lambda, tx2)));
+      o[2] = fma2(lam2mu, tz2, fma2(lambda, ty2, mul2(lambda, tx2)));
+      o[3] = mul2(fma2(ztx, v[1], mul2(zty, v[0])), miu);
+      o[4] = mul2(fma2(ztx, v[2], mul2(ztz, v[0])), miu);
+      o[5] = mul2(fma2(zty, v[2], mul2(ztz, v[1])), miu);
+    };
+    f2 t[6];
+    if (mx) {
+      terms_x(ax.ai, t);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) hw[q] = fma2(neg2(t[q]), e.iBx, hw[q]);
+    }
+    if (my) {
+      terms_y(ay.ai, t);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) hw[q] = fma2(neg2(t[q]), iBy, hw[q]);
+    }
+    if (mz) {
+      terms_z(az.ai, t);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) hw[q] = fma2(neg2(t[q]), iBz, hw[q]);
+    }
+    // one direction at a time: the derivative auxiliaries' RHS
+    // (-APD a + DB dV), then their RK update
+    f2 ha[3];
+    if (mx) {
+      ha[0] = fma2(neg2(e.apdx), ax.ai[0], mul2(DxVx, e.dbx));
+      ha[1] = fma2(neg2(e.apdx), ax.ai[1], mul2(DxVy, e.dbx));
+      ha[2] = fma2(neg2(e.apdx), ax.ai[2], mul2(DxVz, e.dbx));
       ax.update(a, 0, ix.x0, ix.x1, mx, 3, ha);
     }
     if (my) {
-#pragma unroll
-      for (int q = 0; q < 6; ++q)
-        ha[q] = fma2(neg2(S2(e.apdy)), ay.ai[q], mul2(det[q], S2(e.dby)));
-      if (pl.top) {
-        const float *my2 = mv + 9 * g.plane;
-        surf(mat_row(my2, g.plane, 0, DyVx, DyVy, DyVz), mat_row(my2, g.plane, 3, DyVx, DyVy, DyVz),
-             mat_row(my2, g.plane, 6, DyVx, DyVy, DyVz), S2(e.dby * e.bby), ha);
-      }
+      ha[0] = fma2(neg2(S2(e.apdy)), ay.ai[0], mul2(DyVx, S2(e.dby)));
+      ha[1] = fma2(neg2(S2(e.apdy)), ay.ai[1], mul2(DyVy, S2(e.dby)));
+      ha[2] = fma2(neg2(S2(e.apdy)), ay.ai[2], mul2(DyVz, S2(e.dby)));
       ay.update(a, 1, ix.y, ix.y + 1, my, 3, ha);
     }
     if (mz) {
-#pragma unroll
-      for (int q = 0; q < 6; ++q)
-        ha[q] = fma2(neg2(S2(ix.apdz)), az.ai[q], mul2(dzt[q], S2(ix.dbz)));
+      ha[0] = fma2(neg2(S2(ix.apdz)), az.ai[0], mul2(DzVx, S2(ix.dbz)));
+      ha[1] = fma2(neg2(S2(ix.apdz)), az.ai[1], mul2(DzVy, S2(ix.dbz)));
+      ha[2] = fma2(neg2(S2(ix.apdz)), az.ai[2], mul2(DzVz, S2(ix.dbz)));
       az.update(a, 2, ix.z, ix.z + 1, mz, 3, ha);
     }
   }
