@@ -13,6 +13,8 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <mutex>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -301,6 +303,8 @@ struct cgfd_solver {
   cudaStream_t st = nullptr;
   // traction image and stress part beside the velocity part
   SideStream side{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  // host-to-device upload staging: the copy events of the two pinned chunks
+  cudaEvent_t pin_ev[2] = {nullptr, nullptr};
   std::string err;
   void *state = nullptr;   // 4 sets of 9 components: FW, Wa, Wb, tW
   void *set[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -416,6 +420,8 @@ void free_all(cgfd_solver *h) {
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->st) cudaStreamDestroy(h->st);
+  for (int q = 0; q < 2; ++q)
+    if (h->pin_ev[q]) cudaEventDestroy(h->pin_ev[q]);
   if (h->side.stream) cudaStreamDestroy((cudaStream_t)h->side.stream);
   if (h->side.fork) cudaEventDestroy((cudaEvent_t)h->side.fork);
   if (h->side.join) cudaEventDestroy((cudaEvent_t)h->side.join);
@@ -446,6 +452,71 @@ int upload_ref(cgfd_solver *h, const float *host, void *dst, int elem = ELEM_F32
     else
       to_internal_kernel<<<592, 256, 0, h->st>>>(tmp, (float *)dst, h->g, nx, ny, nz, isc);
     e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return cuda_fail(h, e, "upload");
+  return CGFD_OK;
+}
+
+// a loop over [0, n) split over up to 16 host threads (serial when small)
+template <class F>
+void par_for(long n, F &&f) {
+  unsigned nt = std::thread::hardware_concurrency();
+  nt = nt ? (nt < 16u ? nt : 16u) : 4u;
+  if (n < (1L << 18) || nt < 2) {
+    f(0L, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  th.reserve(nt);
+  for (unsigned t = 0; t < nt; ++t) {
+    const long b = n * (long)t / nt, e = n * (long)(t + 1) / nt;
+    th.emplace_back([&f, b, e] { f(b, e); });
+  }
+  for (auto &x : th) x.join();
+}
+
+// Uploads `count` reference-layout arrays of ref_n floats into the internal
+// layout of dst[a] (FP32): fill(a, b, e, out) writes elements [b, e) of array
+// a (converted as the caller wants) to out[0 .. e-b).  Chunks pass through two
+// pinned host buffers, each filled on host threads while the other's copy
+// runs, into one device staging array, converted on the device per array.
+// The two pinned buffers are one pool for the process (portable to every
+// device, allocated at the first upload and kept until exit: page-locking
+// 128 MB costs about a tenth of a second, which every new solver would pay
+// again), used by one upload at a time.
+constexpr long PIN_CHUNK = 16L << 20;  // floats per pinned buffer (64 MB)
+std::mutex g_pin_mutex;
+float *g_pin[2] = {nullptr, nullptr};
+template <class Fill>
+int upload_fields(cgfd_solver *h, int count, Fill &&fill, float *const *dst) {
+  const long n = ref_n(h);
+  std::lock_guard<std::mutex> lock(g_pin_mutex);
+  for (int q = 0; q < 2; ++q) {
+    if (!g_pin[q])
+      CK(h, cudaHostAlloc((void **)&g_pin[q], PIN_CHUNK * sizeof(float), cudaHostAllocPortable));
+    if (!h->pin_ev[q]) CK(h, cudaEventCreateWithFlags(&h->pin_ev[q], cudaEventDisableTiming));
+  }
+  float *tmp = nullptr;
+  CK(h, cudaMalloc(&tmp, n * sizeof(float)));
+  const int nx = h->d.ni + 6, ny = h->d.nj + 6, nz = h->d.nk + 6;
+  cudaError_t e = cudaSuccess;
+  int c = 0;
+  for (int a = 0; a < count && e == cudaSuccess; ++a) {
+    for (long b = 0; b < n && e == cudaSuccess; b += PIN_CHUNK, ++c) {
+      const long end = b + PIN_CHUNK < n ? b + PIN_CHUNK : n;
+      float *buf = g_pin[c & 1];
+      e = cudaEventSynchronize(h->pin_ev[c & 1]);  // its previous copy is done
+      if (e != cudaSuccess) break;
+      par_for(end - b, [&](long x0, long x1) { fill(a, b + x0, b + x1, buf + x0); });
+      e = cudaMemcpyAsync(tmp + b, buf, (end - b) * sizeof(float), cudaMemcpyHostToDevice, h->st);
+      if (e == cudaSuccess) e = cudaEventRecord(h->pin_ev[c & 1], h->st);
+    }
+    if (e == cudaSuccess) {
+      to_internal_kernel<<<592, 256, 0, h->st>>>(tmp, dst[a], h->g, nx, ny, nz, 1.f);
+      e = cudaGetLastError();
+    }
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
   cudaFree(tmp);
@@ -894,39 +965,54 @@ int cgfd_upload_metric(cgfd_solver *h, const double *zx, const double *zy, const
   DevGuard guard(h->d.device);
   const long n = ref_n(h);
   const int nx = h->d.ni + 6, ny = h->d.nj + 6, nz = h->d.nk + 6;
-  std::vector<float> tmp(n);
+  (void)n;
   const double *src[4] = {zx, zy, zz, jac};
-  bool flat = true;
-  for (int q = 0; q < 4; ++q) {
-    for (long t = 0; t < n; ++t) tmp[t] = (float)src[q][t];
-    int st = upload_ref(h, tmp.data(), h->metric + (size_t)q * h->g.fstride);
-    if (st) return st;
-  }
+  float *dst[4];
+  for (int q = 0; q < 4; ++q) dst[q] = h->metric + (size_t)q * h->g.fstride;
+  int st = upload_fields(
+      h, 4,
+      [&](int a, long b, long e, float *o) {
+        const double *s = src[a];
+        for (long t = b; t < e; ++t) o[t - b] = (float)s[t];
+      },
+      dst);
+  if (st) return st;
   // Trivial metric (zeta = (0,0,1), J = 1) on every valid cell.  Metric values
   // in ghost cells only ever multiply zero wavefield values or are replaced by
   // the traction image, so they do not matter.
-  for (int i = LFD; i < h->d.ni + LFD && flat; ++i)
-    for (int j = LFD; j < h->d.nj + LFD && flat; ++j)
-      for (int k = LFD; k < h->d.nk + LFD && flat; ++k) {
-        const long t = ((long)i * ny + j) * nz + k;
-        if (zx[t] != 0.0 || zy[t] != 0.0 || zz[t] != 1.0 || jac[t] != 1.0) flat = false;
-      }
+  std::atomic<bool> flat{true};
+  par_for(h->d.ni, [&](long i0, long i1) {
+    for (long i = i0 + LFD; i < i1 + LFD && flat.load(std::memory_order_relaxed); ++i)
+      for (int j = LFD; j < h->d.nj + LFD; ++j)
+        for (int k = LFD; k < h->d.nk + LFD; ++k) {
+          const long t = (i * ny + j) * nz + k;
+          if (zx[t] != 0.0 || zy[t] != 0.0 || zz[t] != 1.0 || jac[t] != 1.0) {
+            flat = false;
+            return;
+          }
+        }
+  });
   h->flat = flat;
   // The run of planes from the bottom, below ConIndex, whose zeta_z (as
   // stored, FP32) is one value on every valid cell: the tiled kernels take
   // it from a per-plane table instead of loading the plane's metric tile
   // (zeta_x and zeta_y are not used below ConIndex).
   std::vector<float> zzp(h->g.nzi, 0.f);
+  const int kmax = std::min(h->d.nk + LFD, h->g.con);
+  std::vector<char> same(h->g.nzi, 0);
+  par_for(kmax > LFD ? kmax - LFD : 0, [&](long k0, long k1) {
+    for (long k = k0 + LFD; k < k1 + LFD; ++k) {
+      const float v = (float)zz[((long)LFD * ny + LFD) * nz + k];
+      bool s = true;
+      for (int i = LFD; i < h->d.ni + LFD && s; ++i)
+        for (int j = LFD; j < h->d.nj + LFD && s; ++j)
+          s = (float)zz[((long)i * ny + j) * nz + k] == v;
+      same[k] = s;
+      if (s) zzp[k] = v;
+    }
+  });
   int zu_end = LFD;
-  for (int k = LFD; k < h->d.nk + LFD && k < h->g.con; ++k, ++zu_end) {
-    const float v = (float)zz[((long)LFD * ny + LFD) * nz + k];
-    bool same = true;
-    for (int i = LFD; i < h->d.ni + LFD && same; ++i)
-      for (int j = LFD; j < h->d.nj + LFD && same; ++j)
-        same = (float)zz[((long)i * ny + j) * nz + k] == v;
-    if (!same) break;
-    zzp[k] = v;
-  }
+  while (zu_end < kmax && same[zu_end]) ++zu_end;
   CK(h, cudaMemcpy(h->zzp, zzp.data(), zzp.size() * sizeof(float), cudaMemcpyHostToDevice));
   h->zu_end = zu_end;
   h->top_zeta.assign(3 * (size_t)nx * ny, 0.0);
@@ -948,21 +1034,32 @@ int cgfd_upload_media(cgfd_solver *h, const float *alpha, const float *beta, con
   DevGuard guard(h->d.device);
   const long n = ref_n(h);
   const int nx = h->d.ni + 6, ny = h->d.nj + 6, nz = h->d.nk + 6;
-  std::vector<float> l2m(n), mu(n), ir(n);
-  for (long t = 0; t < n; ++t) {
-    const double r = rho[t];
-    l2m[t] = (float)(r * (double)alpha[t] * alpha[t]);
-    mu[t] = (float)(r * (double)beta[t] * beta[t]);
-    ir[t] = r != 0.0 ? (float)(1.0 / r) : 0.f;
-  }
+  (void)n;
   // the valid cells must have a positive density
-  for (int i = LFD; i < h->d.ni + LFD; ++i)
-    for (int j = LFD; j < h->d.nj + LFD; ++j)
-      for (int k = LFD; k < h->d.nk + LFD; ++k)
-        if (!(rho[((long)i * ny + j) * nz + k] > 0.f)) return arg_fail(h, "non-positive density");
-  int st = upload_ref(h, l2m.data(), h->media);
-  if (!st) st = upload_ref(h, mu.data(), h->media + h->g.fstride);
-  if (!st) st = upload_ref(h, ir.data(), h->media + 2 * h->g.fstride);
+  std::atomic<bool> bad{false};
+  par_for(h->d.ni, [&](long i0, long i1) {
+    for (long i = i0 + LFD; i < i1 + LFD; ++i)
+      for (int j = LFD; j < h->d.nj + LFD; ++j)
+        for (int k = LFD; k < h->d.nk + LFD; ++k)
+          if (!(rho[(i * ny + j) * nz + k] > 0.f)) {
+            bad = true;
+            return;
+          }
+  });
+  if (bad) return arg_fail(h, "non-positive density");
+  // (lambda + 2 mu, mu, 1/rho) as FP32 from double products
+  float *dst[3] = {h->media, h->media + h->g.fstride, h->media + 2 * h->g.fstride};
+  int st = upload_fields(
+      h, 3,
+      [&](int a, long b, long e, float *o) {
+        for (long t = b; t < e; ++t) {
+          const double r = rho[t];
+          o[t - b] = a == 0   ? (float)(r * (double)alpha[t] * alpha[t])
+                     : a == 1 ? (float)(r * (double)beta[t] * beta[t])
+                              : (r != 0.0 ? (float)(1.0 / r) : 0.f);
+        }
+      },
+      dst);
   if (st) return st;
   h->top_alpha.assign((size_t)nx * ny, 0.0);
   h->top_beta.assign((size_t)nx * ny, 0.0);
