@@ -168,6 +168,76 @@ void extend_linear(double *v, const Dims &D, int ni, int nj, int nk) {
       }
 }
 
+// ---------------------------- volume media ---------------------------------
+
+// Bracketing samples of v on an increasing axis a[0..n-1]: (L, R) and the
+// value to interpolate at, clamped to the axis ends (mathfunc::LocValue1d).
+void bracket(double v, const double *a, int n, int *L, int *R, double *at) {
+  *L = 0;
+  *R = n - 1;
+  *at = v;
+  if (v <= a[0]) {
+    *at = a[0];
+    *R = 1;
+  } else if (v >= a[n - 1]) {
+    *at = a[n - 1];
+    *L = n - 2;
+  } else {
+    while (*R - *L > 1) {
+      const int m = (*R - *L) / 2 + *L;
+      if (a[m] == v) {
+        *L = m;
+        *R = m + 1;
+        break;
+      }
+      if (a[m] > v) *R = m;
+      else *L = m;
+    }
+  }
+}
+
+// Lagrange weights of the n nodes X at x0, products taken as
+// mathfunc::interp3d takes them
+void lagrange(const double *X, int n, double x0, double *w) {
+  for (int i = 0; i < n; ++i) {
+    w[i] = 1.0;
+    for (int j = 0; j < n; ++j)
+      if (j != i) w[i] *= (X[j] - x0) / (X[j] - X[i]);
+  }
+}
+
+struct Volume {
+  const double *x, *y, *z;  // the axes of the selected sub-volume
+  int nx, ny, nz;
+  const float *vp, *vs, *rho;  // full volume [nvx][nvy][nvz]
+  int x0, y0, z0, nvy, nvz;     // sub-volume origin, full strides
+  // Vp, Vs, density at a point (mediapar::volume_discrete): trilinear
+  // between the bracketing samples, the point clamped to the sub-volume
+  void at(double px, double py, double pz, double *vpo, double *vso, double *dco) const {
+    int i1, i2, j1, j2, k1, k2;
+    double qx, qy, qz;
+    bracket(px, x, nx, &i1, &i2, &qx);
+    bracket(py, y, ny, &j1, &j2, &qy);
+    bracket(pz, z, nz, &k1, &k2, &qz);
+    const double X[2] = {x[i1], x[i1 + 1]}, Y[2] = {y[j1], y[j1 + 1]}, Z[2] = {z[k1], z[k1 + 1]};
+    double wx[2], wy[2], wz[2];
+    lagrange(X, 2, qx, wx);
+    lagrange(Y, 2, qy, wy);
+    lagrange(Z, 2, qz, wz);
+    const float *src[3] = {vp, vs, rho};
+    double *dst[3] = {vpo, vso, dco};
+    for (int q = 0; q < 3; ++q) {
+      double f = 0.0;
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+          for (int c = 0; c < 2; ++c)
+            f += wx[a] * wy[b] * wz[c] *
+                 (double)src[q][((size_t)(x0 + i1 + a) * nvy + (y0 + j1 + b)) * nvz + (z0 + k1 + c)];
+      *dst[q] = f;
+    }
+  }
+};
+
 int grid_fail(const std::string &msg) {
   cgfd::set_global_error(("cgfd_grid_vmap: " + msg).c_str());
   return CGFD_ERR_ARG;
@@ -441,6 +511,162 @@ int cgfd_grid_vmap(int ni, int nj, int nk, int nsurf, const int *gridpoints,
   extend_linear(x, D, ni, nj, nk);
   extend_linear(y, D, ni, nj, nk);
   extend_linear(z, D, ni, nj, nk);
+  return CGFD_OK;
+}
+
+int cgfd_media_volume(int ni, int nj, int nk, const double *x, const double *y, const double *z,
+                      int nvx, int nvy, int nvz, const double *vx, const double *vy,
+                      const double *vz, const float *vp, const float *vs, const float *rho,
+                      double crit_value, double crit_perc, int sampx, int sampy, int sampz,
+                      float *alpha, float *beta, float *dens) {
+  auto fail = [](const char *m) {
+    cgfd::set_global_error((std::string("cgfd_media_volume: ") + m).c_str());
+    return CGFD_ERR_ARG;
+  };
+  if (ni < 1 || nj < 1 || nk < 1 || !x || !y || !z || nvx < 2 || nvy < 2 || nvz < 2 || !vx ||
+      !vy || !vz || !vp || !vs || !rho || sampx < 1 || sampy < 1 || sampz < 1 || !alpha ||
+      !beta || !dens)
+    return fail("bad arguments");
+  const double *ax[3] = {vx, vy, vz};
+  const int na[3] = {nvx, nvy, nvz};
+  for (int d = 0; d < 3; ++d)
+    for (int q = 1; q < na[d]; ++q)
+      if (!(ax[d][q] > ax[d][q - 1])) return fail("volume axes must increase");
+  const Dims D{ni + 6, nj + 6, nk + 6};
+  // the sub-volume that brackets the valid nodes (mediapar::read_volume_new)
+  const double *cc[3] = {x, y, z};
+  int lo[3], hi[3];
+  for (int d = 0; d < 3; ++d) {
+    double mn = cc[d][D.at(3, 3, 3)], mx = mn;
+    for (int i = 3; i < ni + 3; ++i)
+      for (int j = 3; j < nj + 3; ++j)
+        for (int k = 3; k < nk + 3; ++k) {
+          mn = std::min(mn, cc[d][D.at(i, j, k)]);
+          mx = std::max(mx, cc[d][D.at(i, j, k)]);
+        }
+    int L, R;
+    double v;
+    bracket(mn, ax[d], na[d], &L, &R, &v);
+    lo[d] = L;
+    bracket(mx, ax[d], na[d], &L, &R, &v);
+    hi[d] = R;
+  }
+  const Volume V{vx + lo[0], vy + lo[1], vz + lo[2], hi[0] - lo[0] + 1, hi[1] - lo[1] + 1,
+                 hi[2] - lo[2] + 1, vp, vs, rho, lo[0], lo[1], lo[2], nvy, nvz};
+  // every node: Vp, Vs, density -> lambda, mu, density, and the velocity the
+  // smoothing test uses (mediapar::readdata, get2in1, set_vel3d)
+  const size_t n = (size_t)D.nx * D.ny * D.nz;
+  std::vector<double> lam(n), mu(n), den(n), vel(n);
+  for (int i = 0; i < D.nx; ++i)
+    for (int j = 0; j < D.ny; ++j)
+      for (int k = 0; k < D.nz; ++k) {
+        const long g = D.at(i, j, k);
+        double p, sv, dc;
+        V.at(x[g], y[g], z[g], &p, &sv, &dc);
+        const double m = dc * sv * sv;
+        mu[g] = (m + m) / 2.0;
+        lam[g] = ((p * p * dc - 2.0 * m) + (p * p * dc - 2.0 * m)) / 2.0;
+        den[g] = (dc + dc) / 2.0;
+        vel[g] = (std::fabs(p - p) < crit_value && std::fabs(p - p) / p < crit_perc)
+                     ? (p + p) / 2.0
+                     : (p + p) / 2.0 + 9000e3;
+      }
+  // cells whose velocity jumps against a neighbour: averages over sub-cell
+  // samples, arithmetic for density, harmonic for lambda and mu
+  // (mediapar::ApplySmooth, TwoinOne, average)
+  if (sampx > 1 || sampy > 1 || sampz > 1) {
+    auto over = [&](double a, double b) {
+      return std::fabs(a - b) >= crit_value || std::fabs(a - b) / std::min(a, b) >= crit_perc;
+    };
+    const double vec3[3] = {0.0, 2.0, 4.0};
+    std::vector<double> nlam(lam), nmu(mu), nden(den);
+    for (int i = 3; i < ni + 3; ++i)
+      for (int j = 3; j < nj + 3; ++j)
+        for (int k = 3; k < nk + 3; ++k) {
+          const long g = D.at(i, j, k);
+          const int sx = (over(vel[g], vel[D.at(i - 1, j, k)]) || over(vel[g], vel[D.at(i + 1, j, k)])) ? sampx : 1;
+          const int sy = (over(vel[g], vel[D.at(i, j - 1, k)]) || over(vel[g], vel[D.at(i, j + 1, k)])) ? sampy : 1;
+          const int sz = (over(vel[g], vel[D.at(i, j, k - 1)]) || over(vel[g], vel[D.at(i, j, k + 1)])) ? sampz : 1;
+          if (sx == 1 && sy == 1 && sz == 1) continue;
+          double rs = 0, ms = 0, ls = 0;
+          int ns = 0;
+          for (int mi = 1; mi <= sx; ++mi)
+            for (int mj = 1; mj <= sy; ++mj)
+              for (int mk = 1; mk <= sz; ++mk) {
+                const double xs = 1.0 + 2.0 / sx * (mi - 1 + 0.5);
+                const double ys = 1.0 + 2.0 / sy * (mj - 1 + 0.5);
+                const double zs = 1.0 + 2.0 / sz * (mk - 1 + 0.5);
+                double wx[3], wy[3], wz[3], p[3] = {0, 0, 0};
+                lagrange(vec3, 3, xs, wx);
+                lagrange(vec3, 3, ys, wy);
+                lagrange(vec3, 3, zs, wz);
+                for (int a = 0; a < 3; ++a)
+                  for (int b = 0; b < 3; ++b)
+                    for (int c = 0; c < 3; ++c) {
+                      const long q = D.at(i - 1 + a, j - 1 + b, k - 1 + c);
+                      const double w = wx[a] * wy[b] * wz[c];
+                      p[0] += w * x[q];
+                      p[1] += w * y[q];
+                      p[2] += w * z[q];
+                    }
+                double pv, sv, dc;
+                V.at(p[0], p[1], p[2], &pv, &sv, &dc);
+                const double m = dc * sv * sv, l = pv * pv * dc - 2.0 * m;
+                rs += 0.5 * (dc + dc);
+                // a fluid sample (mu ~ 0) resets the harmonic mu sum, as the
+                // reference's TwoinOne does
+                if (m < 1.e-20) ms = 0;
+                else ms += 0.5 / m + 0.5 / m;
+                ls += 0.5 / l + 0.5 / l;
+                ++ns;
+              }
+          nden[g] = rs / ns;
+          nmu[g] = ms > 0 ? ns * 1.0 / ms : 0.0;
+          nlam[g] = ns * 1.0 / ls;
+        }
+    lam.swap(nlam);
+    mu.swap(nmu);
+    den.swap(nden);
+  }
+  // valid nodes to (Vp, Vs, density) (mediapar::MediaStatistics)
+  std::vector<double> out[3] = {std::vector<double>(n), std::vector<double>(n),
+                                std::vector<double>(n)};
+  for (int i = 3; i < ni + 3; ++i)
+    for (int j = 3; j < nj + 3; ++j)
+      for (int k = 3; k < nk + 3; ++k) {
+        const long g = D.at(i, j, k);
+        out[0][g] = std::sqrt((lam[g] + 2.0 * mu[g]) / den[g]);
+        out[1][g] = std::sqrt(mu[g] / den[g]);
+        out[2][g] = den[g];
+      }
+  // ghost nodes (common::equivalence_extend): x from the nearest valid
+  // node, low y and low z mirrored across the first valid node, high y and
+  // high z from the last one
+  for (auto &v : out) {
+    for (int s = 1; s <= 3; ++s)
+      for (int j = 0; j < D.ny; ++j)
+        for (int k = 0; k < D.nz; ++k) {
+          v[D.at(3 - s, j, k)] = v[D.at(3, j, k)];
+          v[D.at(ni + 2 + s, j, k)] = v[D.at(ni + 2, j, k)];
+        }
+    for (int i = 0; i < D.nx; ++i)
+      for (int k = 0; k < D.nz; ++k)
+        for (int s = 1; s <= 3; ++s) {
+          v[D.at(i, 3 - s, k)] = v[D.at(i, 3 + s, k)];
+          v[D.at(i, nj + 2 + s, k)] = v[D.at(i, nj + 2, k)];
+        }
+    for (int i = 0; i < D.nx; ++i)
+      for (int j = 0; j < D.ny; ++j)
+        for (int s = 1; s <= 3; ++s) {
+          v[D.at(i, j, 3 - s)] = v[D.at(i, j, 3 + s)];
+          v[D.at(i, j, nk + 2 + s)] = v[D.at(i, j, nk + 2)];
+        }
+  }
+  for (size_t g = 0; g < n; ++g) {
+    alpha[g] = (float)out[0][g];
+    beta[g] = (float)out[1][g];
+    dens[g] = (float)out[2][g];
+  }
   return CGFD_OK;
 }
 

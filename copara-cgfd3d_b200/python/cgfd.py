@@ -71,6 +71,9 @@ _SIGS = {
     "cgfd_set_boundary_mlp": (C.c_int, [_P, C.c_int, C.c_void_p]),
     "cgfd_set_boundary_mlp_gains": (C.c_int, [_P, _fp]),
     "cgfd_upload_focal": (C.c_int, [_P, C.c_int, _ip, C.c_int, C.c_double, _fp]),
+    "cgfd_media_volume": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_int, C.c_int,
+                                    C.c_int, _dp, _dp, _dp, _fp, _fp, _fp, C.c_double,
+                                    C.c_double, C.c_int, C.c_int, C.c_int, _fp, _fp, _fp]),
     "cgfd_grid_vmap": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _ip, _ip, _dp, C.c_int,
                                  C.c_double, _dp, _dp, _dp, _ip]),
     "cgfd_boundary_mlp_cells": (C.c_int, [_P, _ip, _ip]),
@@ -509,6 +512,25 @@ def grid_vmap(ni, nj, nk, gridpoints, equalspacing, anchor, hybrid=False, conver
     if st:
         raise CgfdError(st, last_error(None))
     return x, y, z, con.value
+
+
+def media_volume(x, y, z, vx, vy, vz, vp, vs, rho, crit_value=50.0, crit_perc=0.05,
+                 samp=(1, 1, 1)):
+    """(alpha, beta, rho) full arrays from a volume model (cgfd_media_volume):
+    x, y, z grid coordinates (ni+6, nj+6, nk+6); vp, vs, rho [nvx][nvy][nvz]
+    on increasing axes vx, vy, vz."""
+    x, y, z = (np.ascontiguousarray(a, np.float64) for a in (x, y, z))
+    ni, nj, nk = (d - 6 for d in x.shape)
+    vx, vy, vz = (np.ascontiguousarray(a, np.float64) for a in (vx, vy, vz))
+    vp, vs, rho = (np.ascontiguousarray(a, np.float32) for a in (vp, vs, rho))
+    out = [np.zeros(x.shape, np.float32) for _ in range(3)]
+    st = _lib.cgfd_media_volume(ni, nj, nk, _d(x), _d(y), _d(z), len(vx), len(vy), len(vz),
+                                _d(vx), _d(vy), _d(vz), _f(vp), _f(vs), _f(rho),
+                                float(crit_value), float(crit_perc), int(samp[0]), int(samp[1]),
+                                int(samp[2]), _f(out[0]), _f(out[1]), _f(out[2]))
+    if st:
+        raise CgfdError(st, last_error(None))
+    return tuple(out)
 
 
 def angle2moment(strike, dip, rake) -> np.ndarray:

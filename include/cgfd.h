@@ -330,6 +330,26 @@ int cgfd_grid_vmap(int ni, int nj, int nk, int nsurf, const int *gridpoints,
                    const int *equalspacing, const double *anchor, int hybrid,
                    double convers_depth, double *x, double *y, double *z, int *con_index);
 
+/* Media of a volume model (the reference's media_type = volume:
+ * mediapar::read_volume_new, readdata, volume_discrete, ApplySmooth and
+ * MediaStatistics, src/mediaparas.cpp:1273-1424, 2140-2220, 376-440,
+ * 1712-1900, and common::equivalence_extend), in FP64: the volume
+ * vp / vs / rho [nvx][nvy][nvz] (the model file's Vp, Vs, rho) on increasing
+ * axes vx, vy, vz (its x, y and depth variables, compared with the grid's z
+ * as they are) is sampled at every grid node (x, y, z: full arrays, as
+ * cgfd_grid_vmap makes them) by trilinear interpolation inside the
+ * sub-volume that brackets the valid nodes (clamped at its ends); where Vp
+ * jumps against a neighbour by >= crit_value or by a fraction >= crit_perc,
+ * a valid node takes the average of samp_x * samp_y * samp_z sub-cell
+ * samples (density arithmetic, lambda and mu harmonic), when any samp > 1.
+ * Outputs alpha (Vp), beta (Vs), rho as full arrays, ghost nodes filled as
+ * the reference does, ready for cgfd_upload_media. */
+int cgfd_media_volume(int ni, int nj, int nk, const double *x, const double *y, const double *z,
+                      int nvx, int nvy, int nvz, const double *vx, const double *vy,
+                      const double *vz, const float *vp, const float *vs, const float *rho,
+                      double crit_value, double crit_perc, int samp_x, int samp_y, int samp_z,
+                      float *alpha, float *beta, float *dens);
+
 /* Grid metric from node coordinates (full arrays, reference layout), by
  * 2-point central differences and cross products, then mirrored into the
  * ghost cells: gridmesh::calmetric (src/gridmesh.cpp:1476-1627).
