@@ -143,3 +143,19 @@ def test_rk_accumulator_between_stages_matches_fp64_oracle(nstages):
         _cmp(valid(got), valid(ref), TOL, f"{what} after {nstages} stage(s)")
     p.close()
     o.close()
+
+
+def test_shifted_tile_grid_matches_fp64_oracle():
+    """A 200-cell-wide model with 10-cell x layers: the paired kernels'
+    tile grid then starts at i = -32 (fewer columns in x-layer tiles at the
+    same tile-column count), so tiles reach left of the grid and their boxes
+    start at negative x.  Seismograms and fields against the oracle."""
+    import models
+    m = models.small_hill(nt=40, ni=200, nj=20, nk=16, nabs=(10, 10, 5, 5, 5, 0))
+    init = cases.random_fields(m, 21)  # every tile active from the first step
+    steps = 30
+    ps, pfw, _ = cases.run_product(m, steps, 0, init, kernel=cgfd.KERNEL_FUSED)
+    os_, ofw, _ = cases.run_oracle(m, steps, 0, init)
+    assert np.abs(os_[:3]).max() > 0
+    _cmp(ps, os_, TOL, "seismogram")
+    _cmp(valid(pfw), valid(ofw), TOL, "FW")
