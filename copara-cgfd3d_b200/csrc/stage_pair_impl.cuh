@@ -110,11 +110,17 @@ static_assert(Slot<__half, PART_VEL>::BYTES % 128 == 0 && Slot<__half, PART_STR>
 static_assert(2 * (Slot<float, PART_VEL>::SMEM + 1024) <= 233472, "two velocity CTAs per SM");
 static_assert(2 * (Slot<float, PART_STR>::SMEM + 1024) <= 233472, "two stress CTAs per SM");
 
-// resident CTAs per SM the kernels are compiled for (registers <= 255): two.
-// With FP32 storage shared memory allows no more (four 27.5 KB slots per
-// CTA); with 16-bit storage three would fit, but at <= 168 registers the
-// stress part spills and the 400x400x200 hill ran 13% slower.
+// resident CTAs per SM the kernels are compiled for.  FP32 storage: two
+// (four 27.5 KB slots per CTA; registers <= 255).  16-bit storage: three
+// (the slots are about half as large; registers <= 168, a few bytes of
+// spills in some instantiations): 6.90 -> 5.79 ms per step on the
+// 400x400x200 hill with FP16 storage (with six stress auxiliaries per PML
+// direction the stress part needed 248 registers and three CTAs ran slower).
 template <typename T> struct MinCtas { static constexpr int value = 2; };
+template <> struct MinCtas<__half> { static constexpr int value = 3; };
+template <> struct MinCtas<__nv_bfloat16> { static constexpr int value = 3; };
+static_assert(3 * (Slot<__half, PART_VEL>::SMEM + 1024) <= 233472, "three 16-bit velocity CTAs");
+static_assert(3 * (Slot<__half, PART_STR>::SMEM + 1024) <= 233472, "three 16-bit stress CTAs");
 
 // Tensor maps of one launch.  halo/u0/u1/coef/met feed the ring; the aux
 // maps (per direction: stage input, FA, tA) only drive L2 prefetches.
