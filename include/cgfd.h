@@ -163,8 +163,8 @@ int cgfd_step(cgfd_solver *h, int n_steps);
 int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms);
 
 /* One RK stage exactly as ChildProcs::RKite(RKindex, currT, Xvec, Yvec, Zvec)
- * (src/calculate.cu:1355-1600) followed by the synchronisation the driver does
- * around it (wavesyn/abssyn, src/calculate.cu:2956-3119).  After rk_index 3 the
+ * (src/calculate.cu:1355-1600) followed by the copies the reference's time
+ * loop makes around it (wavesyn/abssyn, src/calculate.cu:2956-3119).  After rk_index 3 the
  * step state FW holds the new wavefield.  Receivers are not recorded. */
 int cgfd_rk_stage(cgfd_solver *h, int rk_index, int curr_t, int xvec, int yvec,
                   int zvec);

@@ -3,9 +3,9 @@ own device runtime (oracle/_ref/ref_wavesim, built from the reference's
 src/calculate.cu by oracle/ref/Makefile) on the parity cases of
 tests/cases.py.  Needs a GPU; run as
 
-    python tests/golden/make_golden.py <output dir>
+    python tests/golden/make_golden.py [output dir]
 
-and copy the .npz files into tests/golden/.  Each file holds the reference's
+(default: tests/golden/ itself).  Each file holds the reference's
 seismograms (full steps) and the stage output W on the valid cells (partial
 steps), plus the digest of the inputs it was made from.
 """
@@ -40,4 +40,4 @@ def main(out_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden"))
