@@ -153,6 +153,15 @@ struct SourceArgs {
   const float *focmom;
   float fdt, dt, h;
   const float *jac;
+  // source smoothing (cgfd_set_source_smoothing): kinds spread over 7^3
+  // nodes (bit 0 moments, 1 forces, 2 focal points) are left out of the
+  // point kernels and added by the spread list: nsp cells, the entries of
+  // cell u at [spoff[u], spoff[u+1]), each a source row (kind << 28 | q)
+  // and 6 coefficients
+  unsigned smooth;
+  int nsp;
+  const int *spcell, *spoff, *sprow;
+  const float *spcoef;
 };
 
 void launch_stage_simple(const StageArgs &a, void *stream);

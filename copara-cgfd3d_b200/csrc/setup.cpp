@@ -13,12 +13,18 @@
 //                            set_twoside_space 1092-1210, and the ghost
 //                            extension common::interpolated_extend,
 //                            src/common.cpp:67-130)
+//   common::reposition       src/common.cpp:225-270 (source and receiver
+//                            location, src/source.cpp:985-1300 and
+//                            src/seisplot.cpp:412-426)
+//   source smoothing         src/source.cpp:157-378 (MomentShiftPosition,
+//                            eighth_locate, cal_norm; the SrcSmooth build)
 #include "../../include/cgfd.h"
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace cgfd {
@@ -666,6 +672,271 @@ int cgfd_media_volume(int ni, int nj, int nk, const double *x, const double *y, 
     alpha[g] = (float)out[0][g];
     beta[g] = (float)out[1][g];
     dens[g] = (float)out[2][g];
+  }
+  return CGFD_OK;
+}
+
+}  // extern "C"
+
+// ------------------------- point location ---------------------------------
+
+namespace {
+
+int locate_fail(const std::string &msg) {
+  cgfd::set_global_error(("cgfd_locate_points: " + msg).c_str());
+  return CGFD_ERR_ARG;
+}
+
+// Nearest node search of common::reposition over the valid nodes: squared
+// distance, the first minimum in (i, j, k) order wins.  The i range is cut
+// into slabs searched by threads; slab results merge in i order, so ties
+// resolve as in one sequential scan.
+struct Best {
+  double d;
+  long at;  // node index, -1: none
+};
+
+void nearest_nodes(const Dims &D, int ni, int nj, int k0, int k1, const double *x,
+                   const double *y, const double *z, bool planar, int n,
+                   const std::vector<int> &pts, const double *pos, std::vector<Best> &best) {
+  unsigned nth = std::thread::hardware_concurrency();
+  nth = std::max(1u, std::min(nth, 16u));
+  if ((long)ni * nj * (k1 - k0) * (long)pts.size() < 4000000L) nth = 1;
+  nth = std::min<unsigned>(nth, (unsigned)ni);
+  std::vector<std::vector<Best>> part(nth, std::vector<Best>(pts.size(), Best{1e300, -1}));
+  auto work = [&](unsigned t) {
+    const int i0 = 3 + (int)((long)ni * t / nth), i1 = 3 + (int)((long)ni * (t + 1) / nth);
+    std::vector<Best> &b = part[t];
+    for (int i = i0; i < i1; ++i)
+      for (int j = 3; j < nj + 3; ++j)
+        for (size_t q = 0; q < pts.size(); ++q) {
+          const double *p = pos + 3 * (size_t)pts[q];
+          for (int k = k0; k < k1; ++k) {
+            const long c = D.at(i, j, k);
+            const double dx = x[c] - p[0], dy = y[c] - p[1];
+            double d = dx * dx + dy * dy;
+            if (!planar) {
+              const double dz = z[c] - p[2];
+              d += dz * dz;
+            }
+            if (d < b[q].d) b[q] = Best{d, c};
+          }
+        }
+  };
+  std::vector<std::thread> th;
+  for (unsigned t = 1; t < nth; ++t) th.emplace_back(work, t);
+  work(0);
+  for (auto &t : th) t.join();
+  for (size_t q = 0; q < pts.size(); ++q) {
+    Best b{1e300, -1};
+    for (unsigned t = 0; t < nth; ++t)
+      if (part[t][q].d < b.d) b = part[t][q];
+    best[q] = b;
+  }
+}
+
+// The Gaussian weights of cal_norm (src/source.cpp:345-378): a 7^3 block of
+// exp(-(s/1.5)^2)/(sqrt(pi) 1.5) products, s the node offset minus the
+// sub-cell shift, normalised to sum 1; when the block reaches above the
+// surface (iz + 3 > top) it is normalised again over its nodes at or below
+// the surface (iz is the node the search found, before any shift).
+bool norm_block(double shx, double shy, double shz, int iz, int top, double *w) {
+  const double a = 1.5;
+  auto g = [&](double s) { return std::exp(-s * s / (a * a)) / (std::sqrt(kPi) * a); };
+  double sum = 0.0;
+  for (int i = -3; i <= 3; ++i)
+    for (int j = -3; j <= 3; ++j)
+      for (int k = -3; k <= 3; ++k) {
+        const double v = g(i - shx) * g(j - shy) * g(k - shz);
+        w[((i + 3) * 7 + (j + 3)) * 7 + (k + 3)] = v;
+        sum += v;
+      }
+  if (sum < 1e-20) return false;
+  for (int q = 0; q < 343; ++q) w[q] /= sum;
+  if (iz + 3 > top) {
+    sum = 0.0;
+    const int kn = top + 1 - iz + 3;  // block layers at or below the surface
+    for (int i = 0; i < 7; ++i)
+      for (int j = 0; j < 7; ++j)
+        for (int k = 0; k < kn; ++k) sum += w[(i * 7 + j) * 7 + k];
+    for (int q = 0; q < 343; ++q) w[q] /= sum;
+  }
+  return true;
+}
+
+// Force points (eighth_locate, src/source.cpp:277-343, applied four times):
+// the 3^3 nodes around the point are refined to 5^3 by Lagrange
+// interpolation in index space (nodes at 0, 2, 4); the nearest of the 125
+// gives the step s in {-2..2} of this level and the centre of the next
+// level's 3^3 block.  The shift is sum s_l / 2^(l+1).
+bool force_shift(const Dims &D, const double *x, const double *y, const double *z,
+                 const int *loc, const double *p, double sh[3]) {
+  double m[3][27];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      for (int c = 0; c < 3; ++c) {
+        const long g = D.at(loc[0] - 1 + a, loc[1] - 1 + b, loc[2] - 1 + c);
+        m[0][(a * 3 + b) * 3 + c] = x[g];
+        m[1][(a * 3 + b) * 3 + c] = y[g];
+        m[2][(a * 3 + b) * 3 + c] = z[g];
+      }
+  const double nodes[3] = {0.0, 2.0, 4.0};
+  double W[5][3];  // Lagrange weights at 0..4 of the nodes 0, 2, 4
+  for (int t = 0; t < 5; ++t) lagrange(nodes, 3, (double)t, W[t]);
+  sh[0] = sh[1] = sh[2] = 0.0;
+  for (int lev = 0; lev < 4; ++lev) {
+    double f[3][125];
+    for (int i = 0; i < 5; ++i)
+      for (int j = 0; j < 5; ++j)
+        for (int k = 0; k < 5; ++k) {
+          const int o = (i * 5 + j) * 5 + k;
+          if (i % 2 == 0 && j % 2 == 0 && k % 2 == 0) {
+            for (int q = 0; q < 3; ++q) f[q][o] = m[q][((i / 2) * 3 + j / 2) * 3 + k / 2];
+            continue;
+          }
+          for (int q = 0; q < 3; ++q) {
+            double v = 0.0;
+            for (int a = 0; a < 3; ++a)
+              for (int b = 0; b < 3; ++b)
+                for (int c = 0; c < 3; ++c) v += W[i][a] * W[j][b] * W[k][c] * m[q][(a * 3 + b) * 3 + c];
+            f[q][o] = v;
+          }
+        }
+    double best = 1e20;
+    int bi = -1, bj = -1, bk = -1;
+    for (int i = 0; i < 5; ++i)
+      for (int j = 0; j < 5; ++j)
+        for (int k = 0; k < 5; ++k) {
+          const int o = (i * 5 + j) * 5 + k;
+          const double dx = f[0][o] - p[0], dy = f[1][o] - p[1], dz = f[2][o] - p[2];
+          const double d = dx * dx + dy * dy + dz * dz;
+          if (d < best) { best = d; bi = i; bj = j; bk = k; }
+        }
+    // the next level's block must lie inside the 5^3 one
+    if (bi < 1 || bi > 3 || bj < 1 || bj > 3 || bk < 1 || bk > 3) return false;
+    const double s = 1.0 / (double)(2 << lev);
+    sh[0] += (bi - 2) * s;
+    sh[1] += (bj - 2) * s;
+    sh[2] += (bk - 2) * s;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        for (int c = 0; c < 3; ++c)
+          for (int q = 0; q < 3; ++q)
+            m[q][(a * 3 + b) * 3 + c] = f[q][((bi + a - 1) * 5 + bj + b - 1) * 5 + bk + c - 1];
+  }
+  return true;
+}
+
+// Moment and focal points (MomentShiftPosition, src/source.cpp:157-275): the
+// cells within one node in x and y and three in z of the point's node are
+// sampled trilinearly at 1/8 of the index spacing; the nearest sample moves
+// the point's node to the nearest whole index and leaves a shift in
+// [-1/2, 3/8] per axis.
+bool moment_shift(const Dims &D, const double *x, const double *y, const double *z, int *loc,
+                  const double *p, double sh[3]) {
+  const int ns = 8;
+  double best = 1e20;
+  int b[3] = {-1, -1, -1};
+  const double *v[3] = {x, y, z};
+  for (int si = -1; si <= 0; ++si)
+    for (int sj = -1; sj <= 0; ++sj)
+      for (int sk = -3; sk <= 2; ++sk) {
+        double c[3][8];
+        for (int a = 0; a < 2; ++a)
+          for (int bb = 0; bb < 2; ++bb)
+            for (int cc = 0; cc < 2; ++cc) {
+              const long g = D.at(loc[0] + si + a, loc[1] + sj + bb, loc[2] + sk + cc);
+              for (int q = 0; q < 3; ++q) c[q][(a * 2 + bb) * 2 + cc] = v[q][g];
+            }
+        for (int mi = 0; mi < ns; ++mi)
+          for (int mj = 0; mj < ns; ++mj)
+            for (int mk = 0; mk < ns; ++mk) {
+              const double nodes[2] = {0.0, 1.0};
+              double wx[2], wy[2], wz[2];
+              lagrange(nodes, 2, (double)mi / ns, wx);
+              lagrange(nodes, 2, (double)mj / ns, wy);
+              lagrange(nodes, 2, (double)mk / ns, wz);
+              double d = 0.0;
+              for (int q = 0; q < 3; ++q) {
+                double f = 0.0;
+                for (int a = 0; a < 2; ++a)
+                  for (int bb = 0; bb < 2; ++bb)
+                    for (int cc = 0; cc < 2; ++cc) f += wx[a] * wy[bb] * wz[cc] * c[q][(a * 2 + bb) * 2 + cc];
+                d += (f - p[q]) * (f - p[q]);
+              }
+              // the samples are ordered by their position in the 16 x 16 x 48
+              // sub-grid (i, then j, then k), as the reference scans them
+              const int gi = (si + 1) * ns + mi, gj = (sj + 1) * ns + mj, gk = (sk + 3) * ns + mk;
+              if (d < best ||
+                  (d == best && (gi < b[0] || (gi == b[0] && (gj < b[1] || (gj == b[1] && gk < b[2])))))) {
+                best = d;
+                b[0] = gi; b[1] = gj; b[2] = gk;
+              }
+            }
+      }
+  if (b[0] < 0) return false;
+  const int half[3] = {1, 1, 3};
+  for (int q = 0; q < 3; ++q) {
+    const int s = (b[q] + ns / 2) / ns;
+    loc[q] += s - half[q];
+    sh[q] = (double)(b[q] - s * ns) / ns;
+  }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cgfd_locate_points(int ni, int nj, int nk, const double *x, const double *y, const double *z,
+                       double hyper_height, int n, const double *pos, int *loc, double *posz) {
+  if (ni < 1 || nj < 1 || nk < 1 || n < 0 || (n > 0 && (!x || !y || !z || !pos || !loc)))
+    return locate_fail("bad arguments");
+  const Dims D{ni + 6, nj + 6, nk + 6};
+  const int top = nk + 2;
+  std::vector<int> above, below;
+  for (int q = 0; q < n; ++q) (pos[3 * q + 2] > hyper_height ? above : below).push_back(q);
+  std::vector<Best> ba(above.size()), bb(below.size());
+  if (!above.empty()) nearest_nodes(D, ni, nj, top, top + 1, x, y, z, true, n, above, pos, ba);
+  if (!below.empty()) nearest_nodes(D, ni, nj, 3, nk + 3, x, y, z, false, n, below, pos, bb);
+  auto put = [&](const std::vector<int> &pts, const std::vector<Best> &best, bool surf) {
+    for (size_t t = 0; t < pts.size(); ++t) {
+      const int q = pts[t];
+      if (best[t].at < 0) return false;
+      const long c = best[t].at;
+      loc[3 * q] = (int)(c / ((long)D.ny * D.nz));
+      loc[3 * q + 1] = (int)(c / D.nz % D.ny);
+      loc[3 * q + 2] = (int)(c % D.nz);
+      if (posz) posz[q] = surf ? z[c] : pos[3 * q + 2];
+    }
+    return true;
+  };
+  if (!put(above, ba, true) || !put(below, bb, false))
+    return locate_fail("no finite distance to any valid node");
+  return CGFD_OK;
+}
+
+int cgfd_source_smoothing(int ni, int nj, int nk, const double *x, const double *y,
+                          const double *z, int kind, int n, const double *pos, int *loc,
+                          double *weights) {
+  if (ni < 1 || nj < 1 || nk < 1 || n < 0 || (kind != 0 && kind != 1) ||
+      (n > 0 && (!x || !y || !z || !pos || !loc || !weights)))
+    return locate_fail("bad smoothing arguments");
+  const Dims D{ni + 6, nj + 6, nk + 6};
+  const int top = nk + 2;
+  for (int q = 0; q < n; ++q) {
+    int *l = loc + 3 * q;
+    if (l[0] < 3 || l[0] >= ni + 3 || l[1] < 3 || l[1] >= nj + 3 || l[2] < 3 || l[2] > top)
+      return locate_fail("source outside the valid grid");
+    const int iz = l[2];
+    double sh[3];
+    const bool ok = kind == 0 ? force_shift(D, x, y, z, l, pos + 3 * q, sh)
+                              : moment_shift(D, x, y, z, l, pos + 3 * q, sh);
+    if (!ok) return locate_fail("sub-cell search left its block");
+    if (l[0] < 3 || l[0] >= ni + 3 || l[1] < 3 || l[1] >= nj + 3 || l[2] < 3 || l[2] > top)
+      return locate_fail("shifted source outside the valid grid");
+    if (!norm_block(sh[0], sh[1], sh[2], iz, top, weights + (size_t)343 * q))
+      return locate_fail("smoothing weights sum to zero");
   }
   return CGFD_OK;
 }

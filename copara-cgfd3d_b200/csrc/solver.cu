@@ -13,6 +13,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <chrono>
@@ -77,31 +78,34 @@ __global__ void to_reference_kernel(const T *__restrict__ src, float *__restrict
 // Point sources (LoadMoment/LoadForce, src/calculate.cu:6130-6255), applied
 // to the stage output; one thread walks the list so that repeated cells add
 // up in a fixed order.
+// W_out += adt*S, tW += bdt*S in stored units of the component (the last
+// stage: W_out += bdt*S)
+template <typename T>
+__device__ __forceinline__ void add_stage_term(const SourceArgs &s, int comp, size_t o, float S) {
+  using E = Elem<T>;
+  T *out = static_cast<T *>(s.out), *tw = static_cast<T *>(s.tw);
+  const float a = s.adt * s.isc[comp], b = s.bdt * s.isc[comp];
+  if (s.rk == 3) {
+    E::st(out + o, E::ld(out + o) + b * S);
+  } else {
+    E::st(out + o, E::ld(out + o) + a * S);
+    // under tW elision the first stage's tW is rebuilt from W later, and
+    // W already carries this source term
+    if (!(s.tw_skip && s.rk == 0)) E::st(tw + o, E::ld(tw + o) + b * S);
+  }
+}
 template <typename T>
 __device__ void inject_sources_body(const SourceArgs &s) {
-  using E = Elem<T>;
   const int t2 = (s.tindex >= 0) ? s.tindex : 2 * (*s.step) + s.tinc;
   const size_t fs = s.g.fstride;
-  T *out = static_cast<T *>(s.out), *tw = static_cast<T *>(s.tw);
-  // W_out += adt*S, tW += bdt*S in stored units of the component
-  auto add = [&](int comp, size_t o, float S) {
-    const float a = s.adt * s.isc[comp], b = s.bdt * s.isc[comp];
-    if (s.rk == 3) {
-      E::st(out + o, E::ld(out + o) + b * S);
-    } else {
-      E::st(out + o, E::ld(out + o) + a * S);
-      // under tW elision the first stage's tW is rebuilt from W later, and
-      // W already carries this source term
-      if (!(s.tw_skip && s.rk == 0)) E::st(tw + o, E::ld(tw + o) + b * S);
-    }
-  };
-  for (int q = 0; q < s.nmnt; ++q) {
+  auto add = [&](int comp, size_t o, float S) { add_stage_term<T>(s, comp, o, S); };
+  for (int q = 0; q < ((s.smooth & 1u) ? 0 : s.nmnt); ++q) {
     const float stf = s.mstf[(size_t)q * s.nstfm + t2];
     const int c = s.mcell[q];
     for (int m = 0; m < 6; ++m)
       add(TXX + m, (size_t)(TXX + m) * fs + c, -s.mcoef[6 * q + m] * stf);
   }
-  for (int q = 0; q < s.nfrc; ++q) {
+  for (int q = 0; q < ((s.smooth & 2u) ? 0 : s.nfrc); ++q) {
     const float stf = s.fstf[(size_t)q * s.nstff + t2];
     const int c = s.fcell[q];
     for (int m = 0; m < 3; ++m) add(VX + m, (size_t)(VX + m) * fs + c, stf * s.fcoef[3 * q + m]);
@@ -167,6 +171,7 @@ __device__ void inject_focal_body(const SourceArgs &s, int t0, int tstride) {
   const size_t fs = s.g.fstride;
   T *out = static_cast<T *>(s.out), *tw = static_cast<T *>(s.tw);
   const bool to_tw = s.rk != 3 && !(s.tw_skip && s.rk == 0);
+  if (s.smooth & 4u) return;
   for (int q = t0; q < s.nfoc; q += tstride) {
     const int c = s.foccell[q];
     const float A = 1.f / (h3 * s.jac[c]);
@@ -189,6 +194,53 @@ __global__ void inject_focal_kernel(SourceArgs s) {
 __global__ void inject_focal_batch_kernel(const SourceArgs *sa) {
   inject_focal_body<float>(sa[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x,
                            gridDim.x * blockDim.x);
+}
+// Smoothed sources (the SrcSmooth forms of LoadMoment, LoadForce and
+// LoadRmom, src/calculate.cu:6147-6175, 6210-6232, 6275-6296): one thread
+// per node of the spread list sums its entries in list order, then adds
+// the sum once per component, so the result does not depend on thread
+// timing.  Entry coefficients: moments 6 x w / (h^3 J), forces 3 x
+// w / (h^3 J rho) (x2 on the surface), focal points w / (h^3 J) in [0].
+template <typename T>
+__global__ void inject_spread_kernel(SourceArgs s) {
+  const int t2 = (s.tindex >= 0) ? s.tindex : 2 * (*s.step) + s.tinc;
+  const int currT = (s.tindex >= 0) ? (s.tindex - s.tinc) / 2 : *s.step;
+  const float time = (float)(((double)currT + s.tinc * 0.5) * (double)s.dt);
+  const size_t fs = s.g.fstride;
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < s.nsp; u += gridDim.x * blockDim.x) {
+    float S[NCOMP] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    bool vel = false, str = false;
+    for (int e = s.spoff[u]; e < s.spoff[u + 1]; ++e) {
+      const int r = s.sprow[e], kind = r >> 28, q = r & 0x0fffffff;
+      const float *c = s.spcoef + (size_t)6 * e;
+      if (kind == 0) {
+        const float stf = s.mstf[(size_t)q * s.nstfm + t2];
+        for (int m = 0; m < 6; ++m) S[TXX + m] -= c[m] * stf;
+        str = true;
+      } else if (kind == 1) {
+        const float stf = s.fstf[(size_t)q * s.nstff + t2];
+        for (int m = 0; m < 3; ++m) S[VX + m] += c[m] * stf;
+        vel = true;
+      } else {
+        for (int m = 0; m < 6; ++m)
+          S[TXX + m] -= c[0] * focal_value(s.focmom + ((size_t)m * s.nfoc + q) * s.fnt, s.fnt,
+                                           s.fdt, time);
+        str = true;
+      }
+    }
+    const size_t cell = (size_t)s.spcell[u];
+    if (vel)
+      for (int m = 0; m < 3; ++m) add_stage_term<T>(s, VX + m, (size_t)(VX + m) * fs + cell, S[VX + m]);
+    if (str)
+      for (int m = 0; m < 6; ++m)
+        add_stage_term<T>(s, TXX + m, (size_t)(TXX + m) * fs + cell, S[TXX + m]);
+  }
+}
+void launch_spread(const SourceArgs &s, cudaStream_t st) {
+  const int nb = s.nsp <= 0 ? 1 : ((s.nsp + 127) / 128 < 296 ? (s.nsp + 127) / 128 : 296);
+  if (s.elem == ELEM_F16) inject_spread_kernel<__half><<<nb, 128, 0, st>>>(s);
+  else if (s.elem == ELEM_BF16) inject_spread_kernel<__nv_bfloat16><<<nb, 128, 0, st>>>(s);
+  else inject_spread_kernel<float><<<nb, 128, 0, st>>>(s);
 }
 int focal_blocks(int nfoc) { return nfoc <= 0 ? 1 : ((nfoc + 127) / 128 < 296 ? (nfoc + 127) / 128 : 296); }
 void launch_focal(const SourceArgs &s, cudaStream_t st) {
@@ -340,6 +392,12 @@ struct cgfd_solver {
   std::vector<float> hfocmom;
   int *d_foccell = nullptr;
   float *d_focmom = nullptr;
+  // source smoothing weights per kind (moments, forces, focal points),
+  // [n][7][7][7]; the spread list by node that prepare builds from them
+  std::vector<double> smw[3];
+  int sp_n = 0;
+  int *d_sp_cell = nullptr, *d_sp_off = nullptr, *d_sp_row = nullptr;
+  float *d_sp_coef = nullptr;
   // receivers
   int nrecv = 0;
   int *d_rcell = nullptr;
@@ -416,7 +474,8 @@ void free_all(cgfd_solver *h) {
                   h->matv, h->d_mcell, h->d_fcell, h->d_mcoef, h->d_fcoef, h->d_mstf,
                   h->d_fstf, h->d_rcell, h->d_seis, h->d_step, h->d_partials, h->d_err,
                   h->d_pgv, h->d_mlp_cells, h->d_mlp_w, h->d_mlp_delta, h->zzp,
-                  h->d_foccell, h->d_focmom};
+                  h->d_foccell, h->d_focmom, h->d_sp_cell, h->d_sp_off, h->d_sp_row,
+                  h->d_sp_coef};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->st) cudaStreamDestroy(h->st);
@@ -727,19 +786,31 @@ SourceArgs source_args(const cgfd_solver *h, const StageArgs &a, int tindex) {
   s.foccell = h->d_foccell; s.focmom = h->d_focmom;
   s.fdt = (float)h->fdt; s.dt = (float)h->d.stept; s.h = (float)h->d.steph;
   s.jac = h->metric + 3 * h->g.fstride;
+  s.smooth = 0;
+  for (int k = 0; k < 3; ++k)
+    if (!h->smw[k].empty()) s.smooth |= 1u << k;
+  s.nsp = h->sp_n;
+  s.spcell = h->d_sp_cell; s.spoff = h->d_sp_off; s.sprow = h->d_sp_row;
+  s.spcoef = h->d_sp_coef;
   return s;
 }
 
-// point sources, then focal points (separate launches: both may touch a cell)
+// point sources, focal points, then the smoothed ones (separate launches:
+// they may touch the same node)
 int launch_stage_sources(cgfd_solver *h, const StageArgs &a, int tindex) {
   if (h->nmnt + h->nfrc + h->nfoc == 0) return CGFD_OK;
   const SourceArgs s = source_args(h, a, tindex);
-  if (h->nmnt + h->nfrc > 0) {
+  const int np = (h->smw[0].empty() ? h->nmnt : 0) + (h->smw[1].empty() ? h->nfrc : 0);
+  if (np > 0) {
     launch_sources(s, h->st);
     CK(h, cudaGetLastError());
   }
-  if (h->nfoc > 0) {
+  if (h->nfoc > 0 && h->smw[2].empty()) {
     launch_focal(s, h->st);
+    CK(h, cudaGetLastError());
+  }
+  if (h->sp_n > 0) {
+    launch_spread(s, h->st);
     CK(h, cudaGetLastError());
   }
   return CGFD_OK;
@@ -1141,6 +1212,7 @@ static int upload_points(cgfd_solver *h, int n, const int *loc, int ncoef, const
 int cgfd_upload_moments(cgfd_solver *h, int n, const int *loc, const float *m6, int nstf,
                         const float *stf) {
   if (!h) return arg_fail(h, "null handle");
+  h->smw[0].clear();
   return upload_points(h, n, loc, 6, m6, nstf, stf, h->mloc, h->m6, h->hmstf, h->d_mcell,
                        h->d_mstf, h->nmnt, h->nstfm);
 }
@@ -1148,6 +1220,7 @@ int cgfd_upload_moments(cgfd_solver *h, int n, const int *loc, const float *m6, 
 int cgfd_upload_forces(cgfd_solver *h, int n, const int *loc, const float *f3, int nstf,
                        const float *stf) {
   if (!h) return arg_fail(h, "null handle");
+  h->smw[1].clear();
   return upload_points(h, n, loc, 3, f3, nstf, stf, h->floc, h->f3, h->hfstf, h->d_fcell,
                        h->d_fstf, h->nfrc, h->nstff);
 }
@@ -1161,6 +1234,7 @@ int cgfd_upload_focal(cgfd_solver *h, int n, const int *loc, int fnt, double fdt
     if (!valid_loc(h, loc + 3 * q)) return arg_fail(h, "focal source outside the valid grid");
   DevGuard guard(h->d.device);
   CK(h, cudaStreamSynchronize(h->st));
+  h->smw[2].clear();
   if (h->d_foccell) { cudaFree(h->d_foccell); h->d_foccell = nullptr; }
   if (h->d_focmom) { cudaFree(h->d_focmom); h->d_focmom = nullptr; }
   h->nfoc = 0;
@@ -1179,6 +1253,23 @@ int cgfd_upload_focal(cgfd_solver *h, int n, const int *loc, int fnt, double fdt
     h->nfoc = n;
     h->fnt = fnt;
     h->fdt = fdt;
+  }
+  invalidate(h);
+  return CGFD_OK;
+}
+
+int cgfd_set_source_smoothing(cgfd_solver *h, int kind, int n, const double *weights) {
+  if (!h) return arg_fail(h, "null handle");
+  if (kind < 0 || kind > 2) return arg_fail(h, "source smoothing: kind must be 0, 1 or 2");
+  const int have = kind == 0 ? h->nmnt : (kind == 1 ? h->nfrc : h->nfoc);
+  if (!weights || n == 0) {
+    if (n != 0) return arg_fail(h, "source smoothing: weights missing");
+    h->smw[kind].clear();
+  } else {
+    if (n != have) return arg_fail(h, "source smoothing: n differs from the uploaded sources");
+    for (size_t t = 0; t < (size_t)343 * n; ++t)
+      if (!std::isfinite(weights[t])) return arg_fail(h, "source smoothing: weights not finite");
+    h->smw[kind].assign(weights, weights + (size_t)343 * n);
   }
   invalidate(h);
   return CGFD_OK;
@@ -1246,6 +1337,89 @@ int cgfd_get_field_scales(cgfd_solver *h, int *exp2) {
   return CGFD_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The spread list of the smoothed sources: every (source, valid node of its
+// 7^3 block) pair with its coefficients, ordered by node (stable, so the
+// entries of a node stay in kind, source, block order), and the offsets of
+// each node's entries.  J and 1/rho come from one download of each.
+int build_spread(cgfd_solver *h) {
+  for (auto p : {(void **)&h->d_sp_cell, (void **)&h->d_sp_off, (void **)&h->d_sp_row,
+                 (void **)&h->d_sp_coef})
+    if (*p) { cudaFree(*p); *p = nullptr; }
+  h->sp_n = 0;
+  if (h->smw[0].empty() && h->smw[1].empty() && h->smw[2].empty()) return CGFD_OK;
+  const size_t fs = h->g.fstride;
+  std::vector<float> jac(fs), irho(fs);
+  CK(h, cudaMemcpy(jac.data(), h->metric + 3 * fs, fs * sizeof(float), cudaMemcpyDeviceToHost));
+  CK(h, cudaMemcpy(irho.data(), h->media + 2 * fs, fs * sizeof(float), cudaMemcpyDeviceToHost));
+  const double h3 = h->d.steph * h->d.steph * h->d.steph;
+  struct Ent {
+    int cell, row;
+    float c[6];
+  };
+  std::vector<Ent> ents;
+  const int nk[3] = {h->nmnt, h->nfrc, h->nfoc};
+  const std::vector<int> *locs[3] = {&h->mloc, &h->floc, &h->focloc};
+  for (int kind = 0; kind < 3; ++kind) {
+    if (h->smw[kind].empty()) continue;
+    for (int q = 0; q < nk[kind]; ++q) {
+      const int *l = &(*locs[kind])[3 * q];
+      for (int a = 0; a < 7; ++a)
+        for (int b = 0; b < 7; ++b)
+          for (int c = 0; c < 7; ++c) {
+            const int ijk[3] = {l[0] + a - 3, l[1] + b - 3, l[2] + c - 3};
+            if (!valid_loc(h, ijk)) continue;
+            const double w = h->smw[kind][(size_t)343 * q + (a * 7 + b) * 7 + c];
+            Ent e{};
+            e.cell = cell_of(h, ijk);
+            e.row = (kind << 28) | q;
+            const double A = w / (h3 * (double)jac[e.cell]);
+            if (kind == 0) {
+              for (int m = 0; m < 6; ++m) e.c[m] = (float)(h->m6[6 * q + m] * A);
+            } else if (kind == 1) {
+              double F = A * (double)irho[e.cell];
+              if (ijk[2] == h->g.top) F *= 2.0;
+              for (int m = 0; m < 3; ++m) e.c[m] = (float)(h->f3[3 * q + m] * F);
+            } else {
+              e.c[0] = (float)A;
+            }
+            ents.push_back(e);
+          }
+    }
+  }
+  std::stable_sort(ents.begin(), ents.end(),
+                   [](const Ent &x, const Ent &y) { return x.cell < y.cell; });
+  std::vector<int> cells, off, rows(ents.size());
+  std::vector<float> coef((size_t)6 * ents.size());
+  for (size_t e = 0; e < ents.size(); ++e) {
+    if (e == 0 || ents[e].cell != ents[e - 1].cell) {
+      cells.push_back(ents[e].cell);
+      off.push_back((int)e);
+    }
+    rows[e] = ents[e].row;
+    for (int m = 0; m < 6; ++m) coef[6 * e + m] = ents[e].c[m];
+  }
+  off.push_back((int)ents.size());
+  if (cells.empty()) return CGFD_OK;
+  CK(h, cudaMalloc(&h->d_sp_cell, cells.size() * sizeof(int)));
+  CK(h, cudaMalloc(&h->d_sp_off, off.size() * sizeof(int)));
+  CK(h, cudaMalloc(&h->d_sp_row, rows.size() * sizeof(int)));
+  CK(h, cudaMalloc(&h->d_sp_coef, coef.size() * sizeof(float)));
+  CK(h, cudaMemcpy(h->d_sp_cell, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(h->d_sp_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(h->d_sp_row, rows.data(), rows.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(h->d_sp_coef, coef.data(), coef.size() * sizeof(float), cudaMemcpyHostToDevice));
+  h->sp_n = (int)cells.size();
+  return CGFD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int cgfd_prepare(cgfd_solver *h) {
   if (!h) return arg_fail(h, "null handle");
   if (!(h->have_metric && h->have_media && h->have_pml)) {
@@ -1290,6 +1464,8 @@ int cgfd_prepare(cgfd_solver *h) {
     CK(h, cudaMalloc(&h->d_fcoef, c.size() * sizeof(float)));
     CK(h, cudaMemcpy(h->d_fcoef, c.data(), c.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
+  int sst = build_spread(h);
+  if (sst) return sst;
   if (h->elem == ELEM_F16 && !h->user_scales) {
     // FP16 scale exponents from an estimate of the peak magnitudes: the
     // stress a moment source builds at its cell is bounded by its rate
@@ -1761,6 +1937,8 @@ static int batch_build(cgfd_batch *b) {
   b->max_foc = 0;
   for (int i = 0; i < n; ++i) {
     cgfd_solver *h = b->m[i];
+    if (!h->smw[0].empty() || !h->smw[1].empty() || !h->smw[2].empty())
+      return batch_fail(b, CGFD_ERR_ARG, "source smoothing is not available in batches");
     for (int p = 0; p < 4; ++p)
       for (int rk = 0; rk < 4; ++rk) {
         const int *dd = DIRS[p][rk];

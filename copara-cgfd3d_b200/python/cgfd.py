@@ -71,6 +71,11 @@ _SIGS = {
     "cgfd_set_boundary_mlp": (C.c_int, [_P, C.c_int, C.c_void_p]),
     "cgfd_set_boundary_mlp_gains": (C.c_int, [_P, _fp]),
     "cgfd_upload_focal": (C.c_int, [_P, C.c_int, _ip, C.c_int, C.c_double, _fp]),
+    "cgfd_set_source_smoothing": (C.c_int, [_P, C.c_int, C.c_int, _dp]),
+    "cgfd_locate_points": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_double,
+                                     C.c_int, _dp, _ip, _dp]),
+    "cgfd_source_smoothing": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_int,
+                                        C.c_int, _dp, _ip, _dp]),
     "cgfd_media_volume": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_int, C.c_int,
                                     C.c_int, _dp, _dp, _dp, _fp, _fp, _fp, C.c_double,
                                     C.c_double, C.c_int, C.c_int, C.c_int, _fp, _fp, _fp]),
@@ -293,6 +298,16 @@ class Solver:
         mom = _as(mom, np.float32).reshape(6, len(loc), -1) if len(loc) else np.zeros(1, np.float32)
         fnt = mom.shape[-1] if len(loc) else 1
         self._chk(_lib.cgfd_upload_focal(self._h, len(loc), _i(loc), fnt, float(fdt), _f(mom)))
+
+    def set_source_smoothing(self, kind, weights):
+        """Spread the uploaded sources of one kind (0 moments, 1 forces, 2
+        focal points) over 7^3 nodes with weights [n][7][7][7] from
+        source_smoothing(); None turns it off (cgfd_set_source_smoothing)."""
+        if weights is None:
+            self._chk(_lib.cgfd_set_source_smoothing(self._h, int(kind), 0, None))
+            return
+        w = _as(weights, np.float64).reshape(-1, 343)
+        self._chk(_lib.cgfd_set_source_smoothing(self._h, int(kind), len(w), _d(w)))
 
     def set_receivers(self, loc):
         loc = _as(loc, np.int32).reshape(-1, 3)
@@ -531,6 +546,40 @@ def media_volume(x, y, z, vx, vy, vz, vp, vs, rho, crit_value=50.0, crit_perc=0.
     if st:
         raise CgfdError(st, last_error(None))
     return tuple(out)
+
+
+def locate_points(x, y, z, pos, hyper_height):
+    """Nearest valid node of each point (cgfd_locate_points): x, y, z full
+    node arrays (ni+6, nj+6, nk+6), pos (n, 3).  Returns (loc (n, 3) int32,
+    posz (n,)): points above hyper_height go to the nearest surface node in
+    x-y and take its z."""
+    x, y, z = (np.ascontiguousarray(a, np.float64) for a in (x, y, z))
+    ni, nj, nk = (d - 6 for d in x.shape)
+    pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+    loc = np.zeros((len(pos), 3), np.int32)
+    posz = np.zeros(len(pos), np.float64)
+    st = _lib.cgfd_locate_points(ni, nj, nk, _d(x), _d(y), _d(z), float(hyper_height), len(pos),
+                                 _d(pos), _i(loc), _d(posz))
+    if st:
+        raise CgfdError(st, last_error(None))
+    return loc, posz
+
+
+def source_smoothing(x, y, z, kind, pos, loc):
+    """Smoothing weights (cgfd_source_smoothing): kind 0 forces, 1 moment or
+    focal points; pos (n, 3) with z as locate_points returns it, loc (n, 3)
+    from locate_points.  Returns (loc, weights (n, 7, 7, 7)); loc moves to
+    the nearest node of the sub-cell position for kind 1."""
+    x, y, z = (np.ascontiguousarray(a, np.float64) for a in (x, y, z))
+    ni, nj, nk = (d - 6 for d in x.shape)
+    pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+    loc = np.array(loc, np.int32).reshape(-1, 3)
+    w = np.zeros((len(pos), 7, 7, 7), np.float64)
+    st = _lib.cgfd_source_smoothing(ni, nj, nk, _d(x), _d(y), _d(z), int(kind), len(pos),
+                                    _d(pos), _i(loc), _d(w))
+    if st:
+        raise CgfdError(st, last_error(None))
+    return loc, w
 
 
 def angle2moment(strike, dip, rake) -> np.ndarray:

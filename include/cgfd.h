@@ -141,6 +141,18 @@ int cgfd_upload_forces(cgfd_solver *h, int n, const int *loc, const float *f3,
 int cgfd_upload_focal(cgfd_solver *h, int n, const int *loc, int fnt, double fdt,
                       const float *mom);
 
+/* Spreads the uploaded sources of one kind (0 moments, 1 forces, 2 focal
+ * points) over the 7x7x7 nodes around their nodes, as the reference's
+ * SrcSmooth build does in LoadMoment / LoadForce / LoadRmom
+ * (src/calculate.cu:6147-6175, 6210-6232, 6275-6296): node (i+a-3, j+b-3,
+ * k+c-3) of the source at (i, j, k) takes the fraction weights[q][a][b][c]
+ * (n*343 doubles, from cgfd_source_smoothing; the sources' own locations
+ * are the block centres), valid nodes only, with that node's J (and rho
+ * and the surface factor 2 for forces).  n must equal the uploaded count of
+ * that kind; weights = NULL (n = 0) turns the spreading off.  Uploading the
+ * sources of the kind again also turns it off. */
+int cgfd_set_source_smoothing(cgfd_solver *h, int kind, int n, const double *weights);
+
 /* Receivers (3n ints).  Replaces Hpt + C2DPointPick (src/calculate.cu:2678-2746). */
 int cgfd_set_receivers(cgfd_solver *h, int n, const int *loc);
 
@@ -381,6 +393,33 @@ typedef enum cgfd_stf_type {
  * dt = stept/2 and n = 2*(nt+1) (src/source.cpp:408,775). */
 int cgfd_stf(int type, double start, double t0, double f0, int n, double dt,
              float *out);
+
+/* Nearest valid node of each point (common::reposition,
+ * src/common.cpp:225-270, as source::cal_index and seisplot::locpoint use
+ * it, src/source.cpp:1040, 1105, 1170, src/seisplot.cpp:412-426): pos = 3n doubles
+ * (x, y, z) in the coordinates of x, y, z (full node arrays as for
+ * cgfd_metric_from_coords).  A point with z > hyper_height goes to the
+ * surface node nearest in x-y and takes that node's z (posz); otherwise the
+ * node nearest in 3-D, posz = its own z.  Ties go to the first node in
+ * (i, j, k) order.  loc = 3n ints out (full-array indices); posz (n
+ * doubles, may be NULL) out. */
+int cgfd_locate_points(int ni, int nj, int nk, const double *x, const double *y,
+                       const double *z, double hyper_height, int n, const double *pos,
+                       int *loc, double *posz);
+
+/* Smoothing weights of the reference's SrcSmooth build (src/source.cpp:
+ * 157-378, 1051-1073, 1114-1125, 1203-1214): kind 0 = forces (sub-cell shift
+ * from four levels of 3->5 node Lagrange refinement, eighth_locate), kind 1
+ * = moment and focal points (shift on a 1/8-index trilinear sub-grid, which
+ * also moves loc to the nearest node, MomentShiftPosition).  Then the 7^3
+ * Gaussian block (half-width 1.5 nodes) around the shift, normalised to 1,
+ * and again over its nodes at or below the surface when it reaches above.
+ * pos = 3n (z as cgfd_locate_points returns it), loc = 3n in (from
+ * cgfd_locate_points) and out (moved for kind 1), weights = n*343 out,
+ * [q][a][b][c] for node (i+a-3, j+b-3, k+c-3). */
+int cgfd_source_smoothing(int ni, int nj, int nk, const double *x, const double *y,
+                          const double *z, int kind, int n, const double *pos, int *loc,
+                          double *weights);
 
 /* Strike/dip/rake (degrees) to a unit moment tensor (mxx myy mzz mxy mxz myz):
  * source::angle2moment (src/source.cpp:134-155). */

@@ -13,7 +13,9 @@
 //   - CalTIMGmix (traction image, top 3 layers)    src/calculate.cu:5668-5897
 //   - LoadForce / LoadMoment                       src/calculate.cu:6130-6255
 //   - InterpFocus / ExtractValue + LoadRmom        src/calculate.cu:2586-2643,
-//     (focal points, without SrcSmooth)            1421-1428, 6257-6319
+//     (focal points)                               1421-1428, 6257-6319
+//   - the SrcSmooth spreading of the three kinds    src/calculate.cu:6147-6175,
+//     (weights given, 7^3 nodes per source)         6210-6232, 6275-6296
 //   - IterationBegin/Inner/Final (RK4 + ADE aux)   src/calculate.cu:6330-6734
 //   - RKite stage constants, Tindex                src/calculate.cu:12-13,1355-1422
 //   - per-step F/B direction schedule              src/simulation.cc:252-700
@@ -114,6 +116,7 @@ struct Solver {
   int nfoc = 0, fnt = 0;
   double fdt = 0;
   std::vector<int> focloc;
+  std::vector<double> smw[3];  // smoothing weights [n][7][7][7]: moments, forces, focal
   std::vector<double> focmom;  // [6][nfoc][fnt]
   int nrecv = 0;
   std::vector<int> rloc;
@@ -462,35 +465,60 @@ inline double extract_value(const double *stf, int n, double DT, double time) {
   return stf[PL] + (stf[PR] - stf[PL]) * ((time - DT * PL) / DT);
 }
 
+// The node (i+a-3, j+b-3, k+c-3) of a smoothed source at (i, j, k) takes
+// the fraction w[a][b][c]; valid nodes only (SrcSmooth branches of the
+// three Load kernels).  Unsmoothed: the source's own node, w = 1.
+template <class R, class F>
+void spread(const Solver<R> &S, const std::vector<double> &w, int q, const int *l, F &&f) {
+  if (w.empty()) {
+    f(l[0], l[1], l[2], 1.0);
+    return;
+  }
+  for (int a = 0; a < 7; ++a)
+    for (int b = 0; b < 7; ++b)
+      for (int c = 0; c < 7; ++c) {
+        const int i = l[0] + a - 3, j = l[1] + b - 3, k = l[2] + c - 3;
+        if (i < LFD || i >= S.d.ni + LFD || j < LFD || j >= S.d.nj + LFD || k < LFD ||
+            k >= S.d.nk + LFD)
+          continue;
+        f(i, j, k, w[(size_t)343 * q + (a * 7 + b) * 7 + c]);
+      }
+}
+
 // LoadForce / LoadMoment (src/calculate.cu:6130-6255), Tindex = 2*currT+tinc;
 // focal points as LoadRmom (6257-6319) at time (currT + tinc/2)*stept.
 template <class R>
 void sources(Solver<R> &S, int tindex, double time) {
-  for (int q = 0; q < S.nfoc; ++q) {
-    const long g = S.gi(S.focloc[3 * q], S.focloc[3 * q + 1], S.focloc[3 * q + 2]);
-    const double A = 1.0 / (S.d.steph * S.d.steph * S.d.steph * (double)S.jac[g]);
-    for (int c = 0; c < 6; ++c)
-      S.hW[TXX + c][g] -=
-          (R)(extract_value(&S.focmom[((size_t)c * S.nfoc + q) * S.fnt], S.fnt, S.fdt, time) * A);
-  }
   const double h3 = S.d.steph * S.d.steph * S.d.steph;
+  for (int q = 0; q < S.nfoc; ++q) {
+    double M[6];
+    for (int c = 0; c < 6; ++c)
+      M[c] = extract_value(&S.focmom[((size_t)c * S.nfoc + q) * S.fnt], S.fnt, S.fdt, time);
+    spread(S, S.smw[2], q, &S.focloc[3 * q], [&](int i, int j, int k, double w) {
+      const long g = S.gi(i, j, k);
+      const double A = w / (h3 * (double)S.jac[g]);
+      for (int c = 0; c < 6; ++c) S.hW[TXX + c][g] -= (R)(M[c] * A);
+    });
+  }
   for (int q = 0; q < S.nfrc; ++q) {
-    const int i = S.floc[3 * q], j = S.floc[3 * q + 1], k = S.floc[3 * q + 2];
-    const long g = S.gi(i, j, k);
     const R stf = S.fstf[(size_t)q * S.nstff + tindex];
-    R Aa = h3 * S.jac[g];
-    Aa = 1 / (Aa * S.rho[g]);
-    if (k == S.top) Aa = Aa * 2.0;
-    S.hW[VX][g] += stf * (R)S.f3[3 * q] * Aa;
-    S.hW[VY][g] += stf * (R)S.f3[3 * q + 1] * Aa;
-    S.hW[VZ][g] += stf * (R)S.f3[3 * q + 2] * Aa;
+    spread(S, S.smw[1], q, &S.floc[3 * q], [&](int i, int j, int k, double w) {
+      const long g = S.gi(i, j, k);
+      R Aa = h3 * S.jac[g];
+      Aa = (R)w / (Aa * S.rho[g]);
+      if (k == S.top) Aa = Aa * 2.0;
+      S.hW[VX][g] += stf * (R)S.f3[3 * q] * Aa;
+      S.hW[VY][g] += stf * (R)S.f3[3 * q + 1] * Aa;
+      S.hW[VZ][g] += stf * (R)S.f3[3 * q + 2] * Aa;
+    });
   }
   for (int q = 0; q < S.nmnt; ++q) {
-    const int i = S.mloc[3 * q], j = S.mloc[3 * q + 1], k = S.mloc[3 * q + 2];
-    const long g = S.gi(i, j, k);
     const R stf = S.mstf[(size_t)q * S.nstfm + tindex];
-    const R Aa = stf * 1.0 / (h3 * S.jac[g]);
-    for (int c = 0; c < 6; ++c) S.hW[TXX + c][g] -= (R)S.m6[6 * q + c] * Aa;
+    spread(S, S.smw[0], q, &S.mloc[3 * q], [&](int i, int j, int k, double w) {
+      const long g = S.gi(i, j, k);
+      const R Aa = stf * (R)w / (h3 * S.jac[g]);
+      for (int c = 0; c < 6; ++c) S.hW[TXX + c][g] -= (R)S.m6[6 * q + c] * Aa;
+    });
   }
 }
 
@@ -700,6 +728,7 @@ int orc_upload_moments(void *h, int n, const int *loc, const float *m6, int nstf
     for (int q = 0; q < n; ++q)
       if (!valid_loc(S, loc + 3 * q)) { H->err = "moment source outside the valid grid"; return (int)CGFD_ERR_ARG; }
     S.nmnt = n; S.nstfm = nstf;
+    S.smw[0].clear();
     S.mloc.assign(loc, loc + 3 * n);
     S.m6.assign(m6, m6 + 6 * n);
     S.mstf.assign(stf, stf + (size_t)n * nstf);
@@ -716,6 +745,7 @@ int orc_upload_forces(void *h, int n, const int *loc, const float *f3, int nstf,
     for (int q = 0; q < n; ++q)
       if (!valid_loc(S, loc + 3 * q)) { H->err = "force source outside the valid grid"; return (int)CGFD_ERR_ARG; }
     S.nfrc = n; S.nstff = nstf;
+    S.smw[1].clear();
     S.floc.assign(loc, loc + 3 * n);
     S.f3.assign(f3, f3 + 3 * n);
     S.fstf.assign(stf, stf + (size_t)n * nstf);
@@ -731,8 +761,25 @@ int orc_upload_focal(void *h, int n, const int *loc, int fnt, double fdt, const 
     for (int q = 0; q < n; ++q)
       if (!valid_loc(S, loc + 3 * q)) { H->err = "focal source outside the valid grid"; return (int)CGFD_ERR_ARG; }
     S.nfoc = n; S.fnt = fnt; S.fdt = fdt;
+    S.smw[2].clear();
     S.focloc.assign(loc, loc + 3 * n);
     S.focmom.assign(mom, mom + (size_t)6 * n * fnt);
+    return (int)CGFD_OK;
+  };
+  return DISPATCH(H, f);
+}
+
+int orc_set_source_smoothing(void *h, int kind, int n, const double *w) {
+  Handle *H = (Handle *)h;
+  auto f = [&](auto &S) {
+    if (kind < 0 || kind > 2) { H->err = "bad smoothing kind"; return (int)CGFD_ERR_ARG; }
+    const int have = kind == 0 ? S.nmnt : (kind == 1 ? S.nfrc : S.nfoc);
+    if (!w || n == 0) {
+      S.smw[kind].clear();
+      return (int)CGFD_OK;
+    }
+    if (n != have) { H->err = "smoothing count differs from the sources"; return (int)CGFD_ERR_ARG; }
+    S.smw[kind].assign(w, w + (size_t)343 * n);
     return (int)CGFD_OK;
   };
   return DISPATCH(H, f);

@@ -39,6 +39,7 @@ _SIGS = {
     "orc_upload_forces": (C.c_int, [_P, C.c_int, _ip, _fp, C.c_int, _fp]),
     "orc_set_receivers": (C.c_int, [_P, C.c_int, _ip]),
     "orc_upload_focal": (C.c_int, [_P, C.c_int, _ip, C.c_int, C.c_double, _fp]),
+    "orc_set_source_smoothing": (C.c_int, [_P, C.c_int, C.c_int, _dp]),
     "orc_rk_stage": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     "orc_step": (C.c_int, [_P, C.c_int]),
     "orc_steps_done": (C.c_int, [_P, _ip]),
@@ -137,6 +138,15 @@ class OracleSolver:
         mom = np.ascontiguousarray(mom, np.float32).reshape(6, len(loc), -1)
         self._chk(_lib.orc_upload_focal(self._h, len(loc), _i(loc), mom.shape[-1], float(fdt),
                                         _f(mom)))
+
+    def set_source_smoothing(self, kind, weights):
+        """kind 0 moments, 1 forces, 2 focal points; weights [n][7][7][7]
+        or None (off)."""
+        if weights is None:
+            self._chk(_lib.orc_set_source_smoothing(self._h, kind, 0, None))
+            return
+        w = np.ascontiguousarray(weights, np.float64).reshape(-1, 343)
+        self._chk(_lib.orc_set_source_smoothing(self._h, kind, len(w), _d(w)))
 
     def set_receivers(self, loc):
         loc = np.ascontiguousarray(loc, np.int32).reshape(-1, 3)
