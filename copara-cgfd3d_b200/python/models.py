@@ -61,6 +61,11 @@ class Model:
     foc_loc: np.ndarray = None
     foc_mom: np.ndarray = None
     foc_dt: float = 0.0
+    # source smoothing weights [n][7][7][7] (float64) of the moments, forces
+    # and focal points, or None (cgfd_set_source_smoothing)
+    mnt_smooth: np.ndarray = None
+    frc_smooth: np.ndarray = None
+    foc_smooth: np.ndarray = None
 
     @property
     def cells(self) -> int:
@@ -86,6 +91,9 @@ class Model:
             solver.upload_forces(self.frc_loc, self.frc_f3, self.frc_stf)
         if self.foc_loc is not None and len(self.foc_loc):
             solver.upload_focal(self.foc_loc, self.foc_dt, self.foc_mom)
+        for kind, w in enumerate((self.mnt_smooth, self.frc_smooth, self.foc_smooth)):
+            if w is not None:
+                solver.set_source_smoothing(kind, w)
         if len(self.rcv_loc):
             solver.set_receivers(self.rcv_loc)
 
@@ -342,6 +350,40 @@ def batch_models(n=64, seed=7, nt=1000, side=(96, 256), nabs_cells=12, h=100.0,
         m = dataclasses.replace(m, mnt_m6=m6, info=dict(m.info, f0=f0, vp=(vp1, vp2)))
         out.append(m)
     return out
+
+
+def gaussian_blocks(n, seed, top_rows=None):
+    """n smoothing blocks [n][7][7][7] shaped like the reference's SrcSmooth
+    weights: exp(-(offset - shift)^2 / 1.5^2) per axis around a seeded
+    sub-cell shift in [-1/2, 1/2), normalised to 1 (top_rows[q] < 7: over
+    the first top_rows[q] z-rows only, the rows at or below the surface)."""
+    rng = np.random.default_rng(seed)
+    o = np.arange(-3, 4, dtype=np.float64)
+    out = np.zeros((n, 7, 7, 7))
+    for q in range(n):
+        sh = rng.uniform(-0.5, 0.5, 3)
+        g = [np.exp(-(o - s) ** 2 / 2.25) for s in sh]
+        w = g[0][:, None, None] * g[1][None, :, None] * g[2][None, None, :]
+        w /= w.sum()
+        if top_rows is not None and top_rows[q] < 7:
+            w /= w[:, :, :top_rows[q]].sum()
+        out[q] = w
+    return out
+
+
+def small_hill_smoothed(nt=60, seed=21) -> Model:
+    """small_hill with its surface force and a second moment two cells from
+    the x- side (its block crosses the side), all sources spread over 7^3
+    nodes with gaussian_blocks (the force's block crosses the surface)."""
+    m = small_hill(nt=nt, force=True)
+    loc = np.concatenate([m.mnt_loc, [[5, 3 + m.nj // 3, 3 + m.nk - 8]]]).astype(np.int32)
+    m6 = np.concatenate([m.mnt_m6, 0.5 * m.mnt_m6[:, ::-1]]).astype(np.float32)
+    stf = np.concatenate([m.mnt_stf, m.mnt_stf]).astype(np.float32)
+    top = m.nk + LFD - 1
+    wm = gaussian_blocks(len(loc), seed)
+    wf = gaussian_blocks(len(m.frc_loc), seed + 1, [top + 1 - k + 3 for k in m.frc_loc[:, 2]])
+    return dataclasses.replace(m, name="small_hill_smoothed", mnt_loc=loc, mnt_m6=m6,
+                               mnt_stf=stf, mnt_smooth=wm, frc_smooth=wf)
 
 
 def with_finite_fault(m: Model, center, length=8, width=5, strike=30.0, dip=60.0, rake=90.0,

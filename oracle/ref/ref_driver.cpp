@@ -12,7 +12,9 @@
 //     wavesyn/abssyn/RKite/PWpick sequence and direction table.  ShareData,
 //     IntraBoundGS and BoundGS are not called: with one child rank and one
 //     device they only move never-written zeros into the x ghost planes.
-// Input and output are flat binary files (see oracle/refio.py).
+// Input and output are flat binary files (see oracle/refio.py).  Built with
+// the reference's SrcSmooth option (ref_wavesim_smooth) it also reads the
+// sources' smoothing blocks (H_mnt.dnorm, H_frc.dnorm) after the input.
 #include "typedata.h"
 
 #include <cuda_runtime.h>
@@ -149,6 +151,11 @@ int main(int argc, char **argv) {
     init.resize(9 * N);
     rd(fi, init.data(), init.size());
   }
+#ifdef SrcSmooth
+  // the smoothing blocks of the moments, then of the forces (7^3 each)
+  if (nmnt) rd(fi, cp.H_mnt.dnorm, (size_t)nmnt * LenNorm * LenNorm * LenNorm);
+  if (nfrc) rd(fi, cp.H_frc.dnorm, (size_t)nfrc * LenNorm * LenNorm * LenNorm);
+#endif
   fclose(fi);
 
   cp.C2DPointPick();

@@ -17,6 +17,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_BIN = os.path.join(HERE, "_ref", "ref_wavesim")
+# the same runtime built with the reference's SrcSmooth option
+REF_BIN_SMOOTH = os.path.join(HERE, "_ref", "ref_wavesim_smooth")
 MAGIC = 0x52464743
 
 
@@ -53,6 +55,17 @@ def write_input(m, path, nsteps, init_fields=None, nstages=0):
         if init_fields is not None:
             for c in range(9):
                 f.write(f32(init_fields[c]))
+        if _smoothed(m):
+            # read by the SrcSmooth build only: moment blocks, then force blocks
+            for w, loc in ((m.mnt_smooth, m.mnt_loc), (m.frc_smooth, m.frc_loc)):
+                if len(loc):
+                    f.write(f32(w))
+
+
+def _smoothed(m):
+    if getattr(m, "foc_smooth", None) is not None:
+        raise ValueError("the reference driver takes no focal points")
+    return getattr(m, "mnt_smooth", None) is not None or getattr(m, "frc_smooth", None) is not None
 
 
 def read_output(path, shape):
@@ -71,12 +84,17 @@ def read_output(path, shape):
 
 def run(m, nsteps, init_fields=None, nstages=0, timeout=1800):
     """Runs the reference on the GPU; returns read_output()'s dict."""
-    if not available():
-        raise FileNotFoundError(f"{REF_BIN} not built (make -C {HERE}/ref)")
+    smooth = _smoothed(m)
+    if smooth and ((m.mnt_smooth is None and len(m.mnt_loc)) or
+                   (m.frc_smooth is None and len(m.frc_loc))):
+        raise ValueError("the SrcSmooth build spreads every moment and force")
+    binary = REF_BIN_SMOOTH if smooth else REF_BIN
+    if not os.path.exists(binary):
+        raise FileNotFoundError(f"{binary} not built (make -C {HERE}/ref)")
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         write_input(m, fin, nsteps, init_fields, nstages)
-        p = subprocess.run([REF_BIN, fin, fout, os.path.join(td, "par")],
+        p = subprocess.run([binary, fin, fout, os.path.join(td, "par")],
                            capture_output=True, text=True, timeout=timeout)
         if p.returncode != 0:
             raise RuntimeError(f"reference driver failed ({p.returncode}):\n"

@@ -15,6 +15,8 @@ CASES = {
     "hill_stage1": (models.small_hill, dict(nt=8, ni=18, nj=16, nk=14, nabs=(3, 4, 3, 3, 4, 0)), 0, 1, 11),
     "hill_stage4": (models.small_hill, dict(nt=8, ni=18, nj=16, nk=14, nabs=(3, 4, 3, 3, 4, 0)), 0, 4, 12),
     "hill_step5": (models.small_hill, dict(nt=8, ni=18, nj=16, nk=14, nabs=(3, 4, 3, 3, 4, 0)), 5, 2, 13),
+    # moments and a surface force spread over 7^3 nodes (the SrcSmooth build)
+    "hill_smooth_60": (models.small_hill_smoothed, dict(nt=60), 60, 0, None),
 }
 
 
@@ -48,6 +50,9 @@ def model_digest(m, init=None):
     for g in m.pml:
         for a in g:
             h.update(np.ascontiguousarray(a, np.float32).tobytes())
+    for w in (m.mnt_smooth, m.frc_smooth):
+        if w is not None:
+            h.update(np.ascontiguousarray(w, np.float32).tobytes())
     if init is not None:
         h.update(np.ascontiguousarray(init).tobytes())
     return h.hexdigest()

@@ -3,9 +3,10 @@ own device runtime (oracle/_ref/ref_wavesim, built from the reference's
 src/calculate.cu by oracle/ref/Makefile) on the parity cases of
 tests/cases.py.  Needs a GPU; run as
 
-    python tests/golden/make_golden.py [output dir]
+    python tests/golden/make_golden.py [output dir [case ...]]
 
-(default: tests/golden/ itself).  Each file holds the reference's
+(default: tests/golden/ itself, every case).  Cases whose model spreads its
+sources (SrcSmooth) run on oracle/_ref/ref_wavesim_smooth.  Each file holds the reference's
 seismograms (full steps) and the stage output W on the valid cells (partial
 steps), plus the digest of the inputs it was made from.
 """
@@ -24,9 +25,9 @@ import cases  # noqa: E402
 import refio  # noqa: E402
 
 
-def main(out_dir):
+def main(out_dir, names=None):
     os.makedirs(out_dir, exist_ok=True)
-    for name in cases.CASES:
+    for name in names or cases.CASES:
         m, nsteps, nstages, init = cases.build(name)
         r = refio.run(m, nsteps, init, nstages)
         payload = dict(digest=np.array(cases.model_digest(m, init)), nsteps=nsteps,
@@ -40,4 +41,5 @@ def main(out_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden"))
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden"),
+         sys.argv[2:])
