@@ -202,12 +202,12 @@ __global__ void inject_focal_batch_kernel(const SourceArgs *sa) {
 // timing.  Entry coefficients: moments 6 x w / (h^3 J), forces 3 x
 // w / (h^3 J rho) (x2 on the surface), focal points w / (h^3 J) in [0].
 template <typename T>
-__global__ void inject_spread_kernel(SourceArgs s) {
+__device__ void inject_spread_body(const SourceArgs &s, int u0, int ustride) {
   const int t2 = (s.tindex >= 0) ? s.tindex : 2 * (*s.step) + s.tinc;
   const int currT = (s.tindex >= 0) ? (s.tindex - s.tinc) / 2 : *s.step;
   const float time = (float)(((double)currT + s.tinc * 0.5) * (double)s.dt);
   const size_t fs = s.g.fstride;
-  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < s.nsp; u += gridDim.x * blockDim.x) {
+  for (int u = u0; u < s.nsp; u += ustride) {
     float S[NCOMP] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     bool vel = false, str = false;
     for (int e = s.spoff[u]; e < s.spoff[u + 1]; ++e) {
@@ -236,8 +236,18 @@ __global__ void inject_spread_kernel(SourceArgs s) {
         add_stage_term<T>(s, TXX + m, (size_t)(TXX + m) * fs + cell, S[TXX + m]);
   }
 }
+template <typename T>
+__global__ void inject_spread_kernel(SourceArgs s) {
+  inject_spread_body<T>(s, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+// a batch of models (FP32 storage): blockIdx.y = model
+__global__ void inject_spread_batch_kernel(const SourceArgs *sa) {
+  inject_spread_body<float>(sa[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x,
+                            gridDim.x * blockDim.x);
+}
+int spread_blocks(int nsp) { return nsp <= 0 ? 1 : ((nsp + 127) / 128 < 296 ? (nsp + 127) / 128 : 296); }
 void launch_spread(const SourceArgs &s, cudaStream_t st) {
-  const int nb = s.nsp <= 0 ? 1 : ((s.nsp + 127) / 128 < 296 ? (s.nsp + 127) / 128 : 296);
+  const int nb = spread_blocks(s.nsp);
   if (s.elem == ELEM_F16) inject_spread_kernel<__half><<<nb, 128, 0, st>>>(s);
   else if (s.elem == ELEM_BF16) inject_spread_kernel<__nv_bfloat16><<<nb, 128, 0, st>>>(s);
   else inject_spread_kernel<float><<<nb, 128, 0, st>>>(s);
@@ -1874,6 +1884,7 @@ struct cgfd_batch {
   RecordArgs *d_rec = nullptr;   // [model]
   bool any_src = false;
   int max_foc = 0;  // most focal points of any member
+  int max_sp = 0;   // longest spread list (smoothed sources) of any member
   cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t ev = nullptr;      // orders the batch's and the members' streams
   bool ready = false;
@@ -1921,6 +1932,11 @@ static int batch_enqueue(cgfd_batch *b, int p, const std::vector<StageArgs> &arg
           b->d_src + (size_t)rk * n);
       BCK(b, cudaGetLastError());
     }
+    if (b->max_sp > 0) {  // the smoothed sources last
+      inject_spread_batch_kernel<<<dim3(spread_blocks(b->max_sp), n), 128, 0, b->st>>>(
+          b->d_src + (size_t)rk * n);
+      BCK(b, cudaGetLastError());
+    }
   }
   record_batch_kernel<<<n, 256, 0, b->st>>>(b->d_rec);
   BCK(b, cudaGetLastError());
@@ -1935,10 +1951,9 @@ static int batch_build(cgfd_batch *b) {
   std::vector<RecordArgs> rec(n);
   b->any_src = false;
   b->max_foc = 0;
+  b->max_sp = 0;
   for (int i = 0; i < n; ++i) {
     cgfd_solver *h = b->m[i];
-    if (!h->smw[0].empty() || !h->smw[1].empty() || !h->smw[2].empty())
-      return batch_fail(b, CGFD_ERR_ARG, "source smoothing is not available in batches");
     for (int p = 0; p < 4; ++p)
       for (int rk = 0; rk < 4; ++rk) {
         const int *dd = DIRS[p][rk];
@@ -1950,6 +1965,7 @@ static int batch_build(cgfd_batch *b) {
       src[(size_t)rk * n + i] = source_args(h, args[(size_t)rk * n + i], -1);
     if (h->nmnt + h->nfrc > 0) b->any_src = true;
     if (h->nfoc > b->max_foc) b->max_foc = h->nfoc;
+    if (h->sp_n > b->max_sp) b->max_sp = h->sp_n;
     RecordArgs &r = rec[i];
     r.fw = (const float *)h->set[0];
     r.fstride = h->g.fstride;

@@ -3,7 +3,8 @@ and focal points spread over their 7^3 blocks as the reference's SrcSmooth
 build of LoadMoment / LoadForce / LoadRmom does.  Against the FP64 oracle
 within the 1e-5 parity bar (kernel families, whole steps and single stages,
 blocks cut by the grid's sides and its surface); with one-node weights equal
-to the point sources; off again after a new upload; refused in batches."""
+to the point sources; off again after a new upload; in a batch as alone;
+with FP16 storage close to FP32."""
 import dataclasses
 import os
 
@@ -150,11 +151,46 @@ def test_smoothing_checks():
     with pytest.raises(cgfd.CgfdError, match="kind"):
         s.set_source_smoothing(3, _weights(1, 1))
     s.close()
-    ms = models.batch_models(n=2, seed=3, nt=10, side=(28, 32), nabs_cells=4)
-    b = cgfd.Batch([q.desc() for q in ms])
-    for q, sv in zip(ms, b.models):
-        q.load(sv)
-    b.models[0].set_source_smoothing(0, _weights(len(ms[0].mnt_loc), 1))
-    with pytest.raises(cgfd.CgfdError, match="batches"):
-        b.prepare()
+
+
+def test_smoothed_sources_in_a_batch_equal_single_runs():
+    ms = models.batch_models(n=3, seed=3, nt=30, side=(28, 44), nabs_cells=5)
+    ms[1] = dataclasses.replace(ms[1], mnt_smooth=_weights(len(ms[1].mnt_loc), 7))
+    ms[2] = models.with_finite_fault(ms[2], center=(3 + ms[2].ni // 2, 3 + ms[2].nj // 2,
+                                                    3 + ms[2].nk - 8),
+                                     length=5, width=3, m0=1e15, rise=0.08)
+    ms[2] = dataclasses.replace(ms[2], foc_smooth=_weights(len(ms[2].foc_loc), 8))
+    steps = 24
+    ref = []
+    for m in ms:
+        s = cgfd.Solver(m.desc())
+        m.load(s)
+        s.step(steps)
+        ref.append((s.seismograms(), _fields(s)))
+        s.close()
+    b = cgfd.Batch([m.desc() for m in ms])
+    for m, s in zip(ms, b.models):
+        m.load(s)
+    b.prepare()
+    b.step(steps)
+    b.sync()
+    for q, s in enumerate(b.models):
+        for e in comp_errors(s.seismograms(), ref[q][0]):
+            assert e < TOL, q
+        for e in comp_errors(valid(_fields(s)), valid(ref[q][1])):
+            assert e < TOL, q
     b.close()
+
+
+def test_smoothed_sources_with_fp16_storage_follow_fp32():
+    m = _model()
+    smooth = {0: _weights(len(m.mnt_loc), 9), 1: _weights(len(m.frc_loc), 10)}
+    steps = 36
+    out = {}
+    for st in (cgfd.STORE_F32, cgfd.STORE_F16):
+        s = cgfd.Solver(m.desc(storage=st))
+        out[st] = _run(s, m, steps, smooth)[0]
+        s.close()
+    assert np.isfinite(out[cgfd.STORE_F16]).all()
+    for e in comp_errors(out[cgfd.STORE_F16], out[cgfd.STORE_F32])[:3]:  # velocities
+        assert e < 2e-2
