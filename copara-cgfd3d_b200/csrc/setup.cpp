@@ -697,7 +697,7 @@ struct Best {
 };
 
 void nearest_nodes(const Dims &D, int ni, int nj, int k0, int k1, const double *x,
-                   const double *y, const double *z, bool planar, int n,
+                   const double *y, const double *z, bool planar,
                    const std::vector<int> &pts, const double *pos, std::vector<Best> &best) {
   unsigned nth = std::thread::hardware_concurrency();
   nth = std::max(1u, std::min(nth, 16u));
@@ -897,8 +897,8 @@ int cgfd_locate_points(int ni, int nj, int nk, const double *x, const double *y,
   std::vector<int> above, below;
   for (int q = 0; q < n; ++q) (pos[3 * q + 2] > hyper_height ? above : below).push_back(q);
   std::vector<Best> ba(above.size()), bb(below.size());
-  if (!above.empty()) nearest_nodes(D, ni, nj, top, top + 1, x, y, z, true, n, above, pos, ba);
-  if (!below.empty()) nearest_nodes(D, ni, nj, 3, nk + 3, x, y, z, false, n, below, pos, bb);
+  if (!above.empty()) nearest_nodes(D, ni, nj, top, top + 1, x, y, z, true, above, pos, ba);
+  if (!below.empty()) nearest_nodes(D, ni, nj, 3, nk + 3, x, y, z, false, below, pos, bb);
   auto put = [&](const std::vector<int> &pts, const std::vector<Best> &best, bool surf) {
     for (size_t t = 0; t < pts.size(); ++t) {
       const int q = pts[t];

@@ -1277,6 +1277,8 @@ int cgfd_set_source_smoothing(cgfd_solver *h, int kind, int n, const double *wei
     h->smw[kind].clear();
   } else {
     if (n != have) return arg_fail(h, "source smoothing: n differs from the uploaded sources");
+    // the spread list packs (kind, source) into one int: kind << 28 | q
+    if (n >= (1 << 28)) return arg_fail(h, "source smoothing: too many sources");
     for (size_t t = 0; t < (size_t)343 * n; ++t)
       if (!std::isfinite(weights[t])) return arg_fail(h, "source smoothing: weights not finite");
     h->smw[kind].assign(weights, weights + (size_t)343 * n);
