@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -1050,48 +1051,57 @@ int cgfd_upload_metric(cgfd_solver *h, const double *zx, const double *zy, const
   const double *src[4] = {zx, zy, zz, jac};
   float *dst[4];
   for (int q = 0; q < 4; ++q) dst[q] = h->metric + (size_t)q * h->g.fstride;
+  // Checked on the converted (stored) values of the valid cells, inside the
+  // conversion pass that streams every value anyway:
+  //  * trivial metric (zeta = (0,0,1), J = 1) everywhere: the flat path.
+  //    Metric values in ghost cells only ever multiply zero wavefield values
+  //    or are replaced by the traction image, so they do not matter;
+  //  * per plane below ConIndex, whether zeta_z is one value on every valid
+  //    cell (that of column (3, 3)): the tiled kernels take it from a
+  //    per-plane table instead of loading the plane's metric tile (zeta_x
+  //    and zeta_y are not used below ConIndex).
+  const int kmax = std::min(h->d.nk + LFD, h->g.con);
+  std::vector<float> zref(nz, 0.f);
+  for (int k = LFD; k < kmax; ++k) zref[k] = (float)zz[((long)LFD * ny + LFD) * nz + k];
+  std::atomic<bool> flat{true};
+  std::unique_ptr<std::atomic<unsigned char>[]> differs(new std::atomic<unsigned char>[nz]);
+  for (int k = 0; k < nz; ++k) differs[k].store(0, std::memory_order_relaxed);
+  const float triv[4] = {0.f, 0.f, 1.f, 1.f};
   int st = upload_fields(
       h, 4,
       [&](int a, long b, long e, float *o) {
         const double *s = src[a];
         for (long t = b; t < e; ++t) o[t - b] = (float)s[t];
+        bool nonflat = false;
+        std::vector<unsigned char> dk(a == 2 ? nz : 0, 0);
+        // runs of one z-column within [b, e)
+        for (long t = b; t < e;) {
+          const long col = t / nz;
+          const int k0 = (int)(t - col * nz);
+          const long t1 = std::min(e, (col + 1) * nz);
+          const int i = (int)(col / ny), j = (int)(col % ny);
+          if (i >= LFD && i < h->d.ni + LFD && j >= LFD && j < h->d.nj + LFD) {
+            const float *c = o + (t - b) - k0;  // c[k]: the column's value at k
+            const int kb = std::max(k0, LFD), ke = std::min(k0 + (int)(t1 - t), h->d.nk + LFD);
+            for (int k = kb; k < ke; ++k) nonflat |= c[k] != triv[a];
+            if (a == 2)
+              for (int k = kb; k < std::min(ke, kmax); ++k) dk[k] |= c[k] != zref[k];
+          }
+          t = t1;
+        }
+        if (nonflat) flat.store(false, std::memory_order_relaxed);
+        for (int k = 0; k < (int)dk.size(); ++k)
+          if (dk[k]) differs[k].store(1, std::memory_order_relaxed);
       },
       dst);
   if (st) return st;
-  // Trivial metric (zeta = (0,0,1), J = 1) on every valid cell.  Metric values
-  // in ghost cells only ever multiply zero wavefield values or are replaced by
-  // the traction image, so they do not matter.
-  std::atomic<bool> flat{true};
-  par_for(h->d.ni, [&](long i0, long i1) {
-    for (long i = i0 + LFD; i < i1 + LFD && flat.load(std::memory_order_relaxed); ++i)
-      for (int j = LFD; j < h->d.nj + LFD; ++j)
-        for (int k = LFD; k < h->d.nk + LFD; ++k) {
-          const long t = (i * ny + j) * nz + k;
-          if (zx[t] != 0.0 || zy[t] != 0.0 || zz[t] != 1.0 || jac[t] != 1.0) {
-            flat = false;
-            return;
-          }
-        }
-  });
   h->flat = flat;
-  // The run of planes from the bottom, below ConIndex, whose zeta_z (as
-  // stored, FP32) is one value on every valid cell: the tiled kernels take
-  // it from a per-plane table instead of loading the plane's metric tile
-  // (zeta_x and zeta_y are not used below ConIndex).
   std::vector<float> zzp(h->g.nzi, 0.f);
-  const int kmax = std::min(h->d.nk + LFD, h->g.con);
   std::vector<char> same(h->g.nzi, 0);
-  par_for(kmax > LFD ? kmax - LFD : 0, [&](long k0, long k1) {
-    for (long k = k0 + LFD; k < k1 + LFD; ++k) {
-      const float v = (float)zz[((long)LFD * ny + LFD) * nz + k];
-      bool s = true;
-      for (int i = LFD; i < h->d.ni + LFD && s; ++i)
-        for (int j = LFD; j < h->d.nj + LFD && s; ++j)
-          s = (float)zz[((long)i * ny + j) * nz + k] == v;
-      same[k] = s;
-      if (s) zzp[k] = v;
-    }
-  });
+  for (int k = LFD; k < kmax; ++k) {
+    same[k] = !differs[k].load(std::memory_order_relaxed);
+    if (same[k]) zzp[k] = zref[k];
+  }
   int zu_end = LFD;
   while (zu_end < kmax && same[zu_end]) ++zu_end;
   CK(h, cudaMemcpy(h->zzp, zzp.data(), zzp.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -1116,20 +1126,11 @@ int cgfd_upload_media(cgfd_solver *h, const float *alpha, const float *beta, con
   const long n = ref_n(h);
   const int nx = h->d.ni + 6, ny = h->d.nj + 6, nz = h->d.nk + 6;
   (void)n;
-  // the valid cells must have a positive density
-  std::atomic<bool> bad{false};
-  par_for(h->d.ni, [&](long i0, long i1) {
-    for (long i = i0 + LFD; i < i1 + LFD; ++i)
-      for (int j = LFD; j < h->d.nj + LFD; ++j)
-        for (int k = LFD; k < h->d.nk + LFD; ++k)
-          if (!(rho[(i * ny + j) * nz + k] > 0.f)) {
-            bad = true;
-            return;
-          }
-  });
-  if (bad) return arg_fail(h, "non-positive density");
-  // (lambda + 2 mu, mu, 1/rho) as FP32 from double products
+  // (lambda + 2 mu, mu, 1/rho) as FP32 from double products; the valid
+  // cells must have a positive density, checked in the 1/rho pass (a failed
+  // check leaves the solver without media)
   float *dst[3] = {h->media, h->media + h->g.fstride, h->media + 2 * h->g.fstride};
+  std::atomic<bool> bad{false};
   int st = upload_fields(
       h, 3,
       [&](int a, long b, long e, float *o) {
@@ -1139,9 +1140,29 @@ int cgfd_upload_media(cgfd_solver *h, const float *alpha, const float *beta, con
                      : a == 1 ? (float)(r * (double)beta[t] * beta[t])
                               : (r != 0.0 ? (float)(1.0 / r) : 0.f);
         }
+        if (a != 2) return;
+        bool nonpos = false;
+        for (long t = b; t < e;) {  // runs of one z-column within [b, e)
+          const long col = t / nz;
+          const int k0 = (int)(t - col * nz);
+          const long t1 = std::min(e, (col + 1) * nz);
+          const int i = (int)(col / ny), j = (int)(col % ny);
+          if (i >= LFD && i < h->d.ni + LFD && j >= LFD && j < h->d.nj + LFD) {
+            const float *r = rho + t - k0;
+            const int ke = std::min(k0 + (int)(t1 - t), h->d.nk + LFD);
+            for (int k = std::max(k0, LFD); k < ke; ++k) nonpos |= !(r[k] > 0.f);
+          }
+          t = t1;
+        }
+        if (nonpos) bad.store(true, std::memory_order_relaxed);
       },
       dst);
   if (st) return st;
+  if (bad) {
+    h->have_media = false;
+    invalidate(h);
+    return arg_fail(h, "non-positive density");
+  }
   h->top_alpha.assign((size_t)nx * ny, 0.0);
   h->top_beta.assign((size_t)nx * ny, 0.0);
   h->top_rho.assign((size_t)nx * ny, 0.0);

@@ -159,3 +159,27 @@ def test_shifted_tile_grid_matches_fp64_oracle():
     assert np.abs(os_[:3]).max() > 0
     _cmp(ps, os_, TOL, "seismogram")
     _cmp(valid(pfw), valid(ofw), TOL, "FW")
+
+
+def test_upload_checks_on_converted_values():
+    """The metric and media checks run inside the conversion pass: a flat
+    model takes the flat path, a hill the per-plane zeta_z table, and a
+    non-positive density on one valid cell is refused and leaves the solver
+    without media (stepping is refused until valid media arrive)."""
+    for name in ("flat_60", "hill_60"):
+        m, nsteps, nstages, init = cases.build(name)
+        ps, _, _ = cases.run_product(m, 6, 0, init)
+        os_, _, _ = cases.run_oracle(m, 6, 0, init)
+        _cmp(ps[:, :, :6], os_[:, :, :6], TOL, "seismogram")
+    m, _, _, _ = cases.build("hill_60")
+    s = cgfd.Solver(m.desc())
+    m.load(s)
+    rho = m.rho.copy()
+    rho[3 + m.ni // 2, 3 + m.nj // 3, 3 + m.nk // 2] = 0.0
+    with pytest.raises(cgfd.CgfdError, match="non-positive density"):
+        s.upload_media(m.alpha, m.beta, rho)
+    with pytest.raises(cgfd.CgfdError):
+        s.step(1)
+    s.upload_media(m.alpha, m.beta, m.rho)
+    s.step(2)
+    s.close()
