@@ -136,3 +136,24 @@ def test_oracle_spreading_conserves_the_moment():
     assert np.abs(out[0]).max() > 0
     assert np.allclose(tot[0], tot[1], rtol=1e-9, atol=0)
     assert np.count_nonzero(out[1][0]) > 300
+
+
+def test_threaded_search_breaks_ties_in_scan_order():
+    """Points exactly between nodes of a uniform grid (ties) and a search
+    large enough to run on several threads: the node found is the first
+    minimum in (i, j, k) order, as one sequential scan finds it."""
+    ni, nj, nk, h = 40, 36, 30, 10.0
+    i, j, k = np.meshgrid(np.arange(ni + 6), np.arange(nj + 6), np.arange(nk + 6), indexing="ij")
+    x, y, z = i * h, j * h, (k - (nk + 2)) * h
+    rng = np.random.default_rng(5)
+    base = rng.integers([4, 4, 4], [ni + 1, nj + 1, nk + 1], size=(240, 3)).astype(np.float64)
+    pos = (base + rng.integers(0, 2, size=(240, 3)) * 0.5) * h  # half-way on some axes
+    pos[:, 2] -= (nk + 2) * h
+    loc, posz = cgfd.locate_points(x, y, z, pos, hyper_height=1e9)
+    vx, vy, vz = (a[3:-3, 3:-3, 3:-3].ravel() for a in (x, y, z))
+    for q in range(len(pos)):
+        d = (vx - pos[q, 0]) ** 2 + (vy - pos[q, 1]) ** 2 + (vz - pos[q, 2]) ** 2
+        t = int(np.argmin(d))  # first minimum in C (i, j, k) order
+        want = np.array(np.unravel_index(t, (ni, nj, nk))) + 3
+        assert np.array_equal(loc[q], want), q
+    assert np.array_equal(posz, pos[:, 2])
