@@ -102,7 +102,9 @@ int cgfd_upload_metric(cgfd_solver *h, const double *zeta_x, const double *zeta_
                        const double *zeta_z, const double *jac);
 
 /* Media: P velocity (alpha), S velocity (beta), density (rho); full arrays.
- * Replaces H_mpa + ParH2D (src/typedata.h:149, src/calculate.cu:2105-2113). */
+ * Replaces H_mpa + ParH2D (src/typedata.h:149, src/calculate.cu:2105-2113).
+ * The density of every valid cell must be positive; an upload refused for
+ * that (CGFD_ERR_ARG) leaves the solver without media until one succeeds. */
 int cgfd_upload_media(cgfd_solver *h, const float *alpha, const float *beta,
                       const float *rho);
 
