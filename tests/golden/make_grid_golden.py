@@ -1,7 +1,10 @@
 """Generates the vmap-grid fixtures (tests/golden/grid_vmap_*.npz): vmap
 descriptions run through the reference's own gridmesh (oracle/_ref/ref_grid,
 built by oracle/ref/Makefile from the reference's sources in its
-double-precision configuration), inputs and outputs saved together.
+double-precision configuration), inputs and outputs saved together: the
+node coordinates and ConIndex (read_vmapnew), the metric of that grid
+(calmetric: xi, eta, zeta derivatives and the Jacobian, steph 100) and its
+ADE CFS-PML profiles (absorb::CalCFSfactors: APD, B, DB per axis).
 
 Run from the repository root after `make -C oracle/ref`:
     python tests/golden/make_grid_golden.py
@@ -52,6 +55,11 @@ CASES = {
 }
 
 
+# CFS-PML parameters for absorb::CalCFSfactors on each grid (small layers:
+# the grids are 6-9 nodes wide)
+PML = dict(nabs=(3, 2, 2, 2, 4, 0), velabs=6000.0, bmax=2.5, amax=5.0, stept=0.008)
+
+
 def run_reference(ni, nj, nk, gp, eq, a, hybrid, depth):
     with tempfile.TemporaryDirectory(prefix="g", dir="/tmp") as d:
         with open(os.path.join(d, "grid.dat"), "w") as f:
@@ -63,25 +71,37 @@ def run_reference(ni, nj, nk, gp, eq, a, hybrid, depth):
             for i in range(ni):
                 for j in range(nj):
                     f.write(" ".join(f"{v:.17g}" for v in a[i, j]) + "\n")
-        out = os.path.join(d, "out.bin")
-        subprocess.run([REF, d, str(ni), str(nj), str(nk), str(hybrid), repr(float(depth)), out],
+        out, met, pml = (os.path.join(d, f) for f in ("out.bin", "met.bin", "pml.bin"))
+        subprocess.run([REF, d, str(ni), str(nj), str(nk), str(hybrid), repr(float(depth)), out,
+                        met, pml, *map(str, PML["nabs"]), repr(PML["velabs"]),
+                        repr(PML["bmax"]), repr(PML["amax"]), repr(PML["stept"])],
                        check=True, stdout=subprocess.DEVNULL)
         raw = open(out, "rb").read()
+        metric = np.fromfile(met, np.float64).reshape(10, ni + 6, nj + 6, nk + 6)
+        p = np.fromfile(pml, np.float64)
+        n3 = (ni + 6, nj + 6, nk + 6)
+        cfs, o = [], 0
+        for ax in range(3):
+            cfs.append(p[o:o + 3 * n3[ax]].reshape(3, n3[ax]))  # APD, B, DB
+            o += 3 * n3[ax]
     con = int(np.frombuffer(raw[:4], np.int32)[0])
     xyz = np.frombuffer(raw[4:], np.float64).reshape(3, ni + 6, nj + 6, nk + 6)
-    return con, xyz
+    return con, xyz, metric, cfs
 
 
 def main():
     for name, c in CASES.items():
         a = anchors(c["ni"], c["nj"], c["tops"], c["seed"])
         nk = sum(c["gp"]) + 1
-        con, xyz = run_reference(c["ni"], c["nj"], nk, c["gp"], c["eq"], a, c["hybrid"], c["depth"])
+        con, xyz, metric, cfs = run_reference(c["ni"], c["nj"], nk, c["gp"], c["eq"], a,
+                                              c["hybrid"], c["depth"])
         np.savez_compressed(os.path.join(OUT, name + ".npz"), ni=c["ni"], nj=c["nj"], nk=nk,
                             gridpoints=np.array(c["gp"], np.int32),
                             equalspacing=np.array(c["eq"], np.int32), anchor=a,
                             hybrid=c["hybrid"], depth=c["depth"], con_index=con, x=xyz[0],
-                            y=xyz[1], z=xyz[2])
+                            y=xyz[1], z=xyz[2], metric=metric, pml_nabs=np.array(PML["nabs"]),
+                            pml_velabs=PML["velabs"], pml_bmax=PML["bmax"],
+                            pml_amax=PML["amax"], pml_x=cfs[0], pml_y=cfs[1], pml_z=cfs[2])
         print(name, "ConIndex", con)
 
 
