@@ -3,24 +3,31 @@
 // SrcSmooth and TypeDouble options) and its point location
 // (common::reposition, src/common.cpp:225-270, as seisplot::locpoint calls it
 // for receivers), built unmodified from the sources, for the parity fixtures
-// of cgfd_locate_points and cgfd_source_smoothing.
+// of cgfd_locate_points, cgfd_source_smoothing, cgfd_stf and
+// cgfd_angle2moment.
 //
 // TEST INFRASTRUCTURE ONLY (oracle/ref): never linked into the product.
 //
-// usage: ref_source <dir> <in> <out>
+// usage: ref_source <dir> <in> <out> [<ftype> <ft0> <ff0> <mtype> <mt0> <mf0> <mech> <start>]
 //   <in> (binary, native endian): int32 ni nj nk nf nm np nt; float64 hyp,
 //   stept; x, y, z, rho, vs as float64 full arrays (ni+6)(nj+6)(nk+6), z
 //   fastest; nf force rows (x y z fx fy fz), nm moment rows (x y z mxx myy
 //   mzz mxy mxz myz), np receiver rows (x y z), all float64.
 //   The driver writes the par files the reference reads into <dir> (keep it
-//   short: the reference keeps paths in 128-byte buffers); the source time
-//   functions are Ricker, t0 = 0.6 s, f0 = 2 Hz, start 0.
-//   <out>: per force: int32 loc[3], float64 posz, dnorm[343], stf[2(nt+1)];
-//   per moment the same; per receiver: int32 loc[3], float64 posz.
+//   short: the reference keeps paths in 128-byte buffers).  Source time
+//   functions: force_stf_type <ftype> with time factor <ft0> and frequency
+//   factor <ff0>, moment_stf_type likewise, every source starting at
+//   <start>; moment_mech_input <mech> ("moment", or "angle": the first three
+//   of a moment row's six values are strike, dip, rake).  Default: Ricker,
+//   t0 = 0.6 s, f0 = 2 Hz, "moment", start 0.
+//   <out>: per force: int32 loc[3], float64 posz, dnorm[343], stf[2(nt+1)],
+//   fx fy fz; per moment the same with mxx myy mzz mxy mxz myz (x mu for
+//   "angle"); per receiver: int32 loc[3], float64 posz.
 #include "typenew.h"
 
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 using namespace defstruct;
@@ -47,10 +54,17 @@ bool get(FILE *f, T *p, size_t n) {
 }  // namespace
 
 int main(int argc, char **argv) {
-  if (argc != 4) {
-    std::fprintf(stderr, "usage: ref_source <dir> <in> <out>\n");
+  if (argc != 4 && argc != 12) {
+    std::fprintf(stderr, "usage: ref_source <dir> <in> <out> [ftype ft0 ff0 mtype mt0 mf0 mech "
+                         "start]\n");
     return 2;
   }
+  const bool opt = argc == 12;
+  const char *ftype = opt ? argv[4] : "Ricker", *ft0 = opt ? argv[5] : "0.6",
+             *ff0 = opt ? argv[6] : "2.0", *mtype = opt ? argv[7] : "Ricker",
+             *mt0 = opt ? argv[8] : "0.6", *mf0 = opt ? argv[9] : "2.0",
+             *mech = opt ? argv[10] : "moment", *start = opt ? argv[11] : "0.0";
+  const bool angle = std::string(mech) == "angle";
   const char *dir = argv[1];
   FILE *in = std::fopen(argv[2], "rb");
   if (!in) return 3;
@@ -84,22 +98,26 @@ int main(int argc, char **argv) {
   std::fprintf(f, "source_type = 2\nnumber_of_force_source = %d\nnumber_of_moment_source = %d\n",
                nf, nm);
   std::fprintf(f, "distance2meter = 1.0\nsource_hyper_height = %.17g\n", hyp);
-  std::fprintf(f, "force_stf_window = 1\nforce_stf_type = Ricker\n");
-  std::fprintf(f, "force_stf_timefactor = 0.6\nforce_stf_freqfactor = 2.0\n");
-  std::fprintf(f, "moment_stf_window = 1\nmoment_mech_input = moment\n");
-  std::fprintf(f, "moment_stf_type = Ricker\nmoment_stf_timefactor = 0.6\n");
-  std::fprintf(f, "moment_stf_freqfactor = 2.0\nsimulate_damp = 1.0\n");
+  std::fprintf(f, "force_stf_window = 1\nforce_stf_type = %s\n", ftype);
+  std::fprintf(f, "force_stf_timefactor = %s\nforce_stf_freqfactor = %s\n", ft0, ff0);
+  std::fprintf(f, "moment_stf_window = 1\nmoment_mech_input = %s\n", mech);
+  std::fprintf(f, "moment_stf_type = %s\nmoment_stf_timefactor = %s\n", mtype, mt0);
+  std::fprintf(f, "moment_stf_freqfactor = %s\nsimulate_damp = 1.0\n", mf0);
   std::fprintf(f, "<anchor_force>\n");
   for (int q = 0; q < nf; ++q) {
     const double *r = &fr[(size_t)6 * q];
-    std::fprintf(f, "%.17g %.17g %.17g 0.0 1.0 %.17g %.17g %.17g\n", r[0], r[1], r[2], r[3],
-                 r[4], r[5]);
+    std::fprintf(f, "%.17g %.17g %.17g %s 1.0 %.17g %.17g %.17g\n", r[0], r[1], r[2], start,
+                 r[3], r[4], r[5]);
   }
   std::fprintf(f, "<anchor_moment>\n");
   for (int q = 0; q < nm; ++q) {
     const double *r = &mr[(size_t)9 * q];
-    std::fprintf(f, "%.17g %.17g %.17g 0.0 1.0 %.17g %.17g %.17g %.17g %.17g %.17g\n", r[0], r[1],
-                 r[2], r[3], r[4], r[5], r[6], r[7], r[8]);
+    if (angle)
+      std::fprintf(f, "%.17g %.17g %.17g %s 1.0 %.17g %.17g %.17g\n", r[0], r[1], r[2], start,
+                   r[3], r[4], r[5]);
+    else
+      std::fprintf(f, "%.17g %.17g %.17g %s 1.0 %.17g %.17g %.17g %.17g %.17g %.17g\n", r[0],
+                   r[1], r[2], start, r[3], r[4], r[5], r[6], r[7], r[8]);
   }
   std::fclose(f);
 
@@ -123,7 +141,8 @@ int main(int argc, char **argv) {
 
   FILE *o = std::fopen(argv[3], "wb");
   if (!o) return 4;
-  auto put_src = [&](int *lx, int *ly, int *lz, Real *pz, Real ****dn, Real **stf, int cnt) {
+  auto put_src = [&](int *lx, int *ly, int *lz, Real *pz, Real ****dn, Real **stf, int cnt,
+                     std::vector<Real *> coef) {
     for (int q = 0; q < cnt; ++q) {
       const int l[3] = {lx[q], ly[q], lz[q]};
       std::fwrite(l, sizeof(int), 3, o);
@@ -139,10 +158,18 @@ int main(int argc, char **argv) {
         const double s = (double)stf[q][t];
         std::fwrite(&s, sizeof s, 1, o);
       }
+      for (Real *c : coef) {
+        const double v = (double)c[q];
+        std::fwrite(&v, sizeof v, 1, o);
+      }
     }
   };
-  if (nf) put_src(sr.frc.locx, sr.frc.locy, sr.frc.locz, sr.frc.posz, sr.frc.dnorm, sr.frc.stf, nf);
-  if (nm) put_src(sr.mnt.locx, sr.mnt.locy, sr.mnt.locz, sr.mnt.posz, sr.mnt.dnorm, sr.mnt.stf, nm);
+  if (nf)
+    put_src(sr.frc.locx, sr.frc.locy, sr.frc.locz, sr.frc.posz, sr.frc.dnorm, sr.frc.stf, nf,
+            {sr.frc.fx, sr.frc.fy, sr.frc.fz});
+  if (nm)
+    put_src(sr.mnt.locx, sr.mnt.locy, sr.mnt.locz, sr.mnt.posz, sr.mnt.dnorm, sr.mnt.stf, nm,
+            {sr.mnt.mxx, sr.mnt.myy, sr.mnt.mzz, sr.mnt.mxy, sr.mnt.mxz, sr.mnt.myz});
   common com;
   for (int q = 0; q < np; ++q) {
     int l[3] = {0, 0, 0};

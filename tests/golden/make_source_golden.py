@@ -1,8 +1,10 @@
-"""Generates the source-location fixtures (tests/golden/source_locate_*.npz):
-node coordinates, source and receiver positions run through the reference's
-own source location and smoothing (oracle/_ref/ref_source, built by
+"""Generates the source fixtures: node coordinates, source and receiver
+positions run through the reference's own source location and smoothing
+(tests/golden/source_locate_*.npz), and its source time functions of every
+wavelet type and strike/dip/rake moment tensors (tests/golden/
+source_wavelets.npz), by oracle/_ref/ref_source, built by
 oracle/ref/Makefile from the reference's source.cpp, common.cpp and
-mathfunc.cpp with its SrcSmooth and TypeDouble options); inputs and outputs
+mathfunc.cpp with its SrcSmooth and TypeDouble options; inputs and outputs
 saved together.
 
 Run from the repository root after `make -C oracle/ref`:
@@ -75,7 +77,7 @@ def points(x, y, z, n, rng, margin, hyp=None, frac_above=0.0):
     return np.array(out, np.float64)
 
 
-def run_reference(x, y, z, rho, vs, hyp, stept, nt, forces, moments, recv):
+def run_reference(x, y, z, rho, vs, hyp, stept, nt, forces, moments, recv, opts=()):
     ni, nj, nk = (d - 6 for d in x.shape)
     with tempfile.TemporaryDirectory(prefix="s", dir="/tmp") as d:
         inp = os.path.join(d, "in.bin")
@@ -87,16 +89,18 @@ def run_reference(x, y, z, rho, vs, hyp, stept, nt, forces, moments, recv):
             for a in (forces, moments, recv):
                 np.ascontiguousarray(a, np.float64).tofile(f)
         out = os.path.join(d, "out.bin")
-        subprocess.run([REF, d, inp, out], check=True, stdout=subprocess.DEVNULL)
+        subprocess.run([REF, d, inp, out, *map(str, opts)], check=True, stdout=subprocess.DEVNULL)
         raw = open(out, "rb").read()
     nstf = 2 * (nt + 1)
-    rec_src = np.dtype([("loc", "<i4", 3), ("posz", "<f8"), ("dnorm", "<f8", 343),
-                        ("stf", "<f8", nstf)])
+    rec_frc = np.dtype([("loc", "<i4", 3), ("posz", "<f8"), ("dnorm", "<f8", 343),
+                        ("stf", "<f8", nstf), ("coef", "<f8", 3)])
+    rec_mnt = np.dtype([("loc", "<i4", 3), ("posz", "<f8"), ("dnorm", "<f8", 343),
+                        ("stf", "<f8", nstf), ("coef", "<f8", 6)])
     rec_pt = np.dtype([("loc", "<i4", 3), ("posz", "<f8")])
     o = 0
-    fr = np.frombuffer(raw, rec_src, len(forces), o)
+    fr = np.frombuffer(raw, rec_frc, len(forces), o)
     o += fr.nbytes
-    mr = np.frombuffer(raw, rec_src, len(moments), o)
+    mr = np.frombuffer(raw, rec_mnt, len(moments), o)
     o += mr.nbytes
     rr = np.frombuffer(raw, rec_pt, len(recv), o)
     assert o + rr.nbytes == len(raw)
@@ -125,6 +129,42 @@ def main():
                             moment_w=mr["dnorm"].reshape(-1, 7, 7, 7), moment_stf=mr["stf"],
                             recv_loc=rr["loc"], recv_posz=rr["posz"])
         print(name, "done")
+    wavelets()
+
+
+# wavelet types with (time factor t0, frequency factor f0) for each; start
+# times 0 and 0.05 s
+WAVELETS = {"Gauss": (0.3, 0.08), "gauss": (0.3, 0.08), "Ricker": (0.6, 2.0),
+            "ricker": (0.6, 2.0), "Bell": (0.1, 0.4), "bell": (0.1, 0.4), "BELL": (0.1, 0.4),
+            "Step": (0.0, 1.0)}
+ANGLES = [(30.0, 60.0, 90.0), (0.0, 90.0, 0.0), (123.0, 35.0, -71.0), (270.0, 10.0, 180.0)]
+
+
+def wavelets():
+    """One force and the ANGLES moments (moment_mech_input = angle) on a
+    small flat grid, once per wavelet type and start time: the reference's
+    sampled force and moment STFs and its moment tensors (x mu)."""
+    x, y, z = hill_grid(8, 8, 8, 100.0, 0.0, 1)
+    z = z - z[3:-3, 3:-3, -4].max()  # highest surface node at z = 0
+    rho = np.full(x.shape, 2500.0)
+    vs = np.full(x.shape, 3000.0)
+    nt, stept = 80, 0.01
+    c = [float(x[6, 6, 6]), float(y[6, 6, 6]), float(z[6, 6, 6])]
+    forces = np.array([c + [1.0, -2.0, 0.5]])
+    moments = np.array([c + list(a) + [0.0, 0.0, 0.0] for a in ANGLES])
+    out = dict(nt=nt, stept=stept, angles=np.array(ANGLES), mu=2500.0 * 3000.0 ** 2)
+    for start in (0.0, 0.05):
+        for name, (t0, f0) in WAVELETS.items():
+            fr, mr, _ = run_reference(x, y, z, rho, vs, 1e9, stept, nt, forces, moments,
+                                      np.zeros((0, 3)),
+                                      (name, t0, f0, name, t0, f0, "angle", start))
+            key = f"{name}_{start:g}"
+            out["force_" + key] = fr["stf"][0]
+            out["moment_" + key] = mr["stf"][0]
+            out["t0f0_" + name] = np.array([t0, f0])
+            out["m6"] = mr["coef"]
+    np.savez_compressed(os.path.join(OUT, "source_wavelets.npz"), **out)
+    print("source_wavelets done")
 
 
 if __name__ == "__main__":

@@ -16,10 +16,10 @@ TOL = 1e-5
 
 
 def _golden_names():
-    # the stepping fixtures (the vmap-grid and source-location fixtures,
-    # grid_vmap_* and source_locate_*, have their own tests)
+    # the stepping fixtures (the vmap-grid and source fixtures, grid_vmap_*
+    # and source_*, have their own tests)
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith(("grid_vmap_", "source_locate_")))
+                  if not os.path.basename(p).startswith(("grid_vmap_", "source_")))
 
 
 def test_golden_set_is_complete():

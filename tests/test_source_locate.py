@@ -157,3 +157,35 @@ def test_threaded_search_breaks_ties_in_scan_order():
         want = np.array(np.unravel_index(t, (ni, nj, nk))) + 3
         assert np.array_equal(loc[q], want), q
     assert np.array_equal(posz, pos[:, 2])
+
+
+WAVELET_NAMES = ("Gauss", "gauss", "Ricker", "ricker", "Bell", "bell", "BELL", "Step")
+
+
+@pytest.mark.parametrize("name", WAVELET_NAMES)
+def test_wavelets_match_reference(name):
+    """cgfd_stf (FP32 out) and the oracle's (FP64) against the reference's
+    cal_stf_force / cal_stf_moment samples of every wavelet type, at start
+    times 0 and 0.05 s (tests/golden/source_wavelets.npz)."""
+    g = np.load(os.path.join(GOLDEN, "source_wavelets.npz"))
+    n, dt = 2 * (int(g["nt"]) + 1), float(g["stept"]) / 2.0
+    t0, f0 = (float(v) for v in g["t0f0_" + name])
+    for start in (0.0, 0.05):
+        got32 = cgfd.stf(name, start, t0, f0, n, dt)
+        got64 = pyoracle.stf(cgfd.STF_TYPES[name], start, t0, f0, n, dt)
+        for kind in ("force", "moment"):
+            ref = g[f"{kind}_{name}_{start:g}"]
+            scale = np.abs(ref).max()
+            assert scale > 0
+            assert np.abs(got32 - ref).max() <= 1e-6 * scale, (kind, start)
+            assert np.abs(got64 - ref).max() <= 1e-12 * scale, (kind, start)
+
+
+def test_angle2moment_matches_reference():
+    """Strike/dip/rake to a moment tensor as the reference's source::
+    angle2moment, times mu at the source as its cal_index applies it."""
+    g = np.load(os.path.join(GOLDEN, "source_wavelets.npz"))
+    mu = float(g["mu"])
+    for fn in (cgfd.angle2moment, pyoracle.angle2moment):
+        m6 = np.array([fn(*a) for a in g["angles"]]) * mu
+        assert np.abs(m6 - g["m6"]).max() <= 1e-12 * np.abs(g["m6"]).max()
