@@ -1,18 +1,21 @@
 #!/usr/bin/env python
 """Benchmark of the CGFD time-stepping path: Gcell-updates/s per RK4 step.
 
-Workload (default): the 400x400x200 Gaussian-hill model (hybrid curvilinear
-grid, vertical spacing 50->150 m, 3 perturbed layers, double-couple source,
-20-cell CFS-PML, 400 surface receivers) on one B200, FP32.  A "step" is one
-full RK4 time step (4 fused RHS+update stage kernels, source injection and the
-receiver record, replayed as a CUDA graph).
+Workload (default, --config hill600): the 600x600x250 Gaussian-hill model
+(hybrid curvilinear grid, vertical spacing 50->150 m, 8 random layers with vp
+2500..7000 m/s, double-couple source, 20-cell CFS-PML, 400 surface
+receivers) on one B200, FP32.  --config hill400 is the 400x400x200 hill with
+3 perturbed layers.  A "step" is one full RK4 time step (4 fused RHS+update
+stages, source injection and the receiver record, replayed as a CUDA graph).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Multi-GPU runs are independent replicas (one model per GPU, no exchange);
 value is the sum over ranks of cells*K divided by the slowest rank's time.
 --impl reference runs the reference's own device runtime (src/calculate.cu,
-built from its sources into oracle/_ref/) on the same model.
+built from its sources into oracle/_ref/) on the same model; that process
+builds the model with the CPU oracle's pre-processing and never loads the
+solver library.
 """
 from __future__ import annotations
 
@@ -40,8 +43,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--kernel", choices=("fused", "simple", "scalar"), default="fused")
-    p.add_argument("--config", choices=("hill400", "flat160", "hill256", "batch64"),
-                   default="hill400")
+    p.add_argument("--config", choices=("hill600", "hill400", "flat160", "hill256", "batch64"),
+                   default="hill600")
     p.add_argument("--autotune", action="store_true",
                    help="tune the work list before timing (state unchanged)")
     p.add_argument("--storage", choices=("f32", "f16", "bf16"), default="f32",
@@ -54,6 +57,8 @@ def parse():
 
 def build_model(cfg, nt):
     import models
+    if cfg == "hill600":
+        return models.config_c5(nt=nt)
     if cfg == "hill400":
         return models.config_c2(nt=nt)
     if cfg == "hill256":
@@ -62,10 +67,29 @@ def build_model(cfg, nt):
 
 
 def workload_name(cfg):
-    return {"hill400": "gaussian_hill_400x400x200_pml20",
+    return {"hill600": "gaussian_hill_600x600x250_random_layers_pml20",
+            "hill400": "gaussian_hill_400x400x200_pml20",
             "flat160": "flat_halfspace_160x160x80_pml12",
             "hill256": "gaussian_hill_256x256x128_pml20",
             "batch64": "batch_64_hill_models_96-256_pml12"}[cfg]
+
+
+def config_dict(cfg, m, storage="f32"):
+    """The workload description both arms print (same keys, same values)."""
+    return {"workload": workload_name(cfg), "cells": m.cells,
+            "grid": [m.ni, m.nj, m.nk], "pml_cells": list(m.nabs), "storage": storage,
+            "receivers": int(len(m.rcv_loc)),
+            "l2": "state >> L2 (126 MB), no flush needed"}
+
+
+def product_library_mapped() -> bool:
+    """True when this process has mapped one of the solver's own shared
+    libraries (copara-cgfd3d_b200/*.so)."""
+    try:
+        with open("/proc/self/maps") as f:
+            return any("copara-cgfd3d_b200" in line for line in f)
+    except OSError:
+        return False
 
 
 def run_batch(args, dist, rank, world, local):
@@ -218,12 +242,22 @@ def committed_traffic(workload, kernel):
     return None if e is None else float(e["dram_bytes_per_launch"])
 
 
+def cpu_sample_model(cfg, nt):
+    """The model the CPU oracle is timed on: the workload itself, except for
+    the 600x600x250 hill, whose FP64 state (~45 GB) is cut to a 200x200x250
+    window of the same generator (layers, grid spacing, PML, dt)."""
+    import models
+    if cfg == "hill600":
+        return models.config_c5(nt=nt, ni=200, nj=200, name="gaussian_hill_200x200x250_window")
+    return build_model(cfg, nt)
+
+
 def cpu_baseline(cfg, seconds):
     """FP64 C++/OpenMP oracle (the CPU restatement of the reference path) on
     the same model, for a bounded number of steps."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    m = build_model(cfg, nt=64)
+    m = cpu_sample_model(cfg, nt=64)
     o = pyoracle.OracleSolver(m.desc(), 0)
     m.load(o)
     o.step(1)  # warm caches, first touch
@@ -236,8 +270,8 @@ def cpu_baseline(cfg, seconds):
     el = time.perf_counter() - t0
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return {"value": m.cells * steps / el / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{workload_name(cfg)}, {steps} RK4 steps after 1 warm-up step, "
-                      f"FP64 oracle, {el:.1f} s"}
+            "sample": f"{m.name} ({m.ni}x{m.nj}x{m.nk}, of {workload_name(cfg)}), {steps} RK4 "
+                      f"steps after 1 warm-up step, FP64 oracle, {el:.1f} s"}
 
 
 def dist_init(n, backend=None):
@@ -287,6 +321,9 @@ def replica_value(world, cells, steps, ms):
 
 
 def run_reference(args):
+    """The reference's own runtime (oracle/_ref/ref_wavesim: src/calculate.cu
+    built from its sources) on the same model.  The model is built with the
+    CPU oracle's pre-processing, so this process never maps libcgfd.so."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import refio
     rank = int(os.environ.get("RANK", "0"))
@@ -296,9 +333,14 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable":
                           "reference parity driver oracle/_ref/ref_wavesim not built"}))
         return
+    import models
+    models.use_preprocessing("oracle")
     nt = args.warmup + args.steps + 2
     m = build_model(args.config, nt)
-    r = refio.run(m, args.warmup + args.steps, timeout=3600)
+    r = refio.run(m, args.warmup + args.steps, timeout=3600, fields=False)
+    mapped = product_library_mapped()
+    if mapped:
+        raise RuntimeError("the reference arm mapped the solver library")
     secs = float(np.sum(r["step_secs"][args.warmup:args.warmup + args.steps]))
     value = m.cells * args.steps / secs / 1e9
     line = {
@@ -306,8 +348,10 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded model generator)", "impl": "reference",
-        "config": {"workload": workload_name(args.config), "cells": m.cells,
-                   "l2": "state >> L2 (126 MB), no flush needed"},
+        "config": config_dict(args.config, m),
+        "product_library_mapped": mapped,
+        "preprocessing": "CPU oracle (FP64 restatement of calmetric / CalCFSfactors / "
+                         "wavelets / angle2moment)",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                          "sample": f"{workload_name(args.config)}, {args.steps} steps after "
                                    f"{args.warmup} warm-up; the reference's own calculate.cu "
@@ -380,18 +424,19 @@ def main():
     traffic = committed_traffic(workload_name(args.config),
                                 args.kernel if args.storage == "f32" else
                                 f"{args.kernel}_{args.storage}")
+    traffic_src = ("profiles/stage_traffic.json: ncu dram__bytes of an earlier capture of "
+                   "this workload, per stage, not measured in this run") if traffic else None
     n_src = 1 if (len(m.mnt_loc) + len(m.frc_loc)) else 0
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
         "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded model generator)",
-        "config": {"workload": workload_name(args.config), "cells": m.cells,
-                   "kernel": args.kernel, "storage": args.storage, "replicas": world,
-                   "autotuned_ms_per_step": tuned,
-                   "l2": "state >> L2 (126 MB), no flush needed",
-                   "parallelism": "replicas" if world > 1 else "single"},
+        "config": config_dict(args.config, m, args.storage),
+        "kernel": args.kernel, "replicas": world, "autotuned_ms_per_step": tuned,
+        "parallelism": "replicas" if world > 1 else "single",
+        "product_library_mapped": product_library_mapped(),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
+                     "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_step": bps, "stage_kernel_ms": stage_ms},
         "clocks": clk.summary(),

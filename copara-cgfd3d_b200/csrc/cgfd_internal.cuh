@@ -198,6 +198,11 @@ struct WorkParams {
 };
 bool pair_supported(const Geom &g);
 bool pair_set_work(void *plan, const WorkParams &wp);
+// test hook (cgfd_test_withhold_copy): every wait of the plan's kernels gives
+// up after wait_s, and with withhold >= 0 the velocity part's CTA 0 does not
+// issue the halo copy of entry `withhold` of its first item; withhold < 0
+// restores the defaults
+bool pair_set_wait_test(void *plan, double wait_s, int withhold);
 WorkParams pair_get_work(const void *plan);
 void *pair_create_plan(const Geom &g, int elem, void *const sets[4], const float *media,
                        const float *metric, float *const aux[3]);

@@ -18,10 +18,12 @@
 // rejects larger sizes with CGFD_ERR_ARG before touching the device.
 //
 // In host code the array's name is only a host-side stand-in, not a device
-// address; the device address is looked up with cudaGetSymbolAddress once
-// per device, with that device current, on the first call that uses the
-// device.  That first call therefore does set-up work and should come before
-// any stream capture.  Every call shares the one array and leaves its last
+// address; every call looks the device address up with cudaGetSymbolAddress,
+// with the array's device current (cheap once the module is loaded, and
+// never stale: a cudaDeviceReset by the host program reloads the module and
+// may move the array).  The first call on a device loads the module there,
+// which is set-up work, so it should come before any stream capture.  Every
+// call shares the one array and leaves its last
 // contents there: each slot a call reads is written by the same call first,
 // so nothing needs clearing, but calls that overlap on the GPU (on different
 // streams, or from different host threads) race on it and must be serialised
@@ -33,7 +35,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
-#include <mutex>
 
 using namespace cgfd;
 using namespace cgfd::nf;
@@ -42,13 +43,11 @@ namespace {
 
 constexpr int NOALLOC_MAX_BLOCKS = 16384;
 constexpr size_t NOALLOC_MAX_VALUES = (size_t)NOALLOC_MAX_BLOCKS * NF_CHUNK;
-constexpr int MAX_DEVICES = 64;
+static_assert(NOALLOC_MAX_VALUES == (size_t)CGFD_NOALLOC_MAX_VALUES,
+              "the header's limit is the scratch array's");
 
 // partial counts [0, NOALLOC_MAX_BLOCKS) and the total at [nblocks]
 static __device__ __align__(256) unsigned long long g_nonfinite_scratch[NOALLOC_MAX_BLOCKS + 1];
-
-std::mutex g_lock;
-unsigned long long *g_scratch_addr[MAX_DEVICES] = {};
 
 }  // namespace
 
@@ -71,7 +70,7 @@ extern "C" int cgfd_count_nonfinite_noalloc(const float *d_values, size_t n, lon
   cudaPointerAttributes attr;
   cudaError_t e = cudaPointerGetAttributes(&attr, d_values);
   if (e != cudaSuccess || (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged) ||
-      attr.device < 0 || attr.device >= MAX_DEVICES) {
+      attr.device < 0) {
     cudaGetLastError();
     set_global_error("cgfd_count_nonfinite_noalloc: d_values is not device memory");
     return CGFD_ERR_ARG;
@@ -82,13 +81,9 @@ extern "C" int cgfd_count_nonfinite_noalloc(const float *d_values, size_t n, lon
   int status = CGFD_OK;
   unsigned long long *scratch = nullptr;
   {
-    std::lock_guard<std::mutex> lk(g_lock);
-    if (!g_scratch_addr[attr.device]) {
-      void *p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_nonfinite_scratch);
-      if (e == cudaSuccess) g_scratch_addr[attr.device] = (unsigned long long *)p;
-    }
-    scratch = g_scratch_addr[attr.device];
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_nonfinite_scratch);
+    if (e == cudaSuccess) scratch = (unsigned long long *)p;
   }
   if (!scratch) {
     char buf[160];

@@ -9,8 +9,8 @@
 namespace cgfd {
 namespace ptx {
 
-// every mbarrier wait gives up after this much %globaltimer time
-constexpr unsigned long long WAIT_NS = 2000000000ull;
+// every mbarrier wait gives up after this much %globaltimer time (microseconds)
+constexpr unsigned WAIT_US = 2000000u;
 
 __device__ __forceinline__ uint32_t su32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -38,12 +38,14 @@ __device__ __forceinline__ unsigned long long gtime() {
   asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
   return t;
 }
-// bounded wait on the phase of the given parity; false on expiry
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
+// bounded wait on the phase of the given parity; false after limit_us of
+// %globaltimer time
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity,
+                                          unsigned limit_us = WAIT_US) {
   if (mbar_try_wait(b, parity)) return true;
-  const unsigned long long t0 = gtime();
+  const unsigned long long t0 = gtime(), lim = 1000ull * limit_us;
   while (!mbar_try_wait(b, parity))
-    if (gtime() - t0 > WAIT_NS) return false;
+    if (gtime() - t0 > lim) return false;
   return true;
 }
 // box at (x, y, z, c) of a 4-D tensor map into shared memory, completing on

@@ -31,7 +31,9 @@ using namespace cgfd::nf;
 
 namespace {
 
-std::string g_last_create_error;
+// the last error of a call without a handle, per host thread (cgfd_last_error
+// with NULL reads the calling thread's)
+thread_local std::string g_last_create_error;
 
 // RK4 coefficients (src/calculate.cu:12-13).
 constexpr double RKA[3] = {0.5, 0.5, 1.0};
@@ -1893,6 +1895,20 @@ int cgfd_autotune(cgfd_solver *h, int steps, float *best_ms) {
   if (!st) st = build_graphs(h);
   if (best_ms) *best_ms = best / steps;
   return st;
+}
+
+int cgfd_test_withhold_copy(cgfd_solver *h, double wait_limit_s, int withhold) {
+  if (!h) return arg_fail(h, "null handle");
+  if (h->d.kernel != CGFD_KERNEL_FUSED || !h->plan)
+    return arg_fail(h, "the wait test needs the default kernel");
+  if (!(wait_limit_s > 0.0) || wait_limit_s > 60.0) return arg_fail(h, "wait limit out of range");
+  if (!pair_set_wait_test(h->plan, wait_limit_s, withhold))
+    return arg_fail(h, "wait test rejected");
+  // the step graphs hold the kernels' parameters by value
+  h->graphs_ok = false;
+  if (!h->prepared) return CGFD_OK;  // cgfd_prepare builds them
+  DevGuard guard(h->d.device);
+  return build_graphs(h);
 }
 
 }  // extern "C"

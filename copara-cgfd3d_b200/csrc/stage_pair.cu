@@ -319,6 +319,14 @@ bool pair_set_work(void *plan, const WorkParams &wp) {
   return true;
 }
 
+bool pair_set_wait_test(void *plan, double wait_s, int withhold) {
+  Plan *pl = reinterpret_cast<Plan *>(plan);
+  if (!pl || !(wait_s > 0.0) || wait_s > 60.0) return false;
+  pl->wk.wait_us = withhold >= 0 ? (unsigned)(wait_s * 1e6) : ptx::WAIT_US;
+  pl->wk.withhold = withhold >= 0 ? withhold : -1;
+  return true;
+}
+
 void pair_destroy_plan(void *plan) {
   Plan *pl = reinterpret_cast<Plan *>(plan);
   if (!pl) return;

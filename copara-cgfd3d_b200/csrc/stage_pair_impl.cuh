@@ -146,6 +146,11 @@ struct Work {
   int has_aux[3];     // direction has a PML (aux maps valid; single model)
   const StageArgs *bargs;
   const Maps *bmaps;
+  // bound of every mbarrier wait, and the test hook of cgfd_test_withhold_copy:
+  // with withhold >= 0 the velocity part's CTA 0 does not issue the halo copy
+  // of entry `withhold` of its first item, so its wait for that plane expires
+  unsigned wait_us = WAIT_US;
+  int withhold = -1;
 };
 
 // ---------------------------- float2 helpers ------------------------------
@@ -775,7 +780,9 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
       const bool met = compute && met_tile(p);
       mbar_expect_tx(&bars[s], S::HALO_B + (compute ? pw_bytes : 0u) +
                                    (met ? (uint32_t)(PWT * 4) * 3u : 0u));
-      tma_load(slot, &M.halo, XO + i0 - HOFF, j0, p, C0, &bars[s]);
+      const bool withheld = PART == PART_VEL && wk.withhold == q && base == 0 &&
+                            blockIdx.x == 0;
+      if (!withheld) tma_load(slot, &M.halo, XO + i0 - HOFF, j0, p, C0, &bars[s]);
       if (compute) {
         const int cx = XO + i0, cy = LFD + j0;
         tma_load(slot + S::U0, &M.u0, cx, cy, p, S0, &bars[s]);
@@ -807,7 +814,7 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
       for (int q = 0; q < NSLOT; ++q) issue(it, q, (base + q) & (NSLOT - 1));
     auto wait = [&](int q) -> bool {  // every thread, in march order
       const int s = (base + q) & (NSLOT - 1);
-      const bool ok = mbar_wait(&bars[s], (ph >> s) & 1u);
+      const bool ok = mbar_wait(&bars[s], (ph >> s) & 1u, wk.wait_us);
       if (ok) {  // an expired wait leaves the copy pending for the drain
         ph ^= 1u << s;
         if (tid == 0) pend &= ~(1u << s);
@@ -930,7 +937,7 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
     // drain: wait (bounded) for copies still in flight before the CTA's
     // shared memory goes away
     for (int s = 0; s < NSLOT; ++s)
-      if (pend & (1u << s)) mbar_wait(&bars[s], (ph >> s) & 1u);
+      if (pend & (1u << s)) mbar_wait(&bars[s], (ph >> s) & 1u, wk.wait_us);
   }
 }
 

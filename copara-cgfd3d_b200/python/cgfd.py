@@ -68,6 +68,7 @@ _SIGS = {
     "cgfd_check_finite": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "cgfd_set_field_scales": (C.c_int, [_P, _ip]),
     "cgfd_autotune": (C.c_int, [_P, C.c_int, _fp]),
+    "cgfd_test_withhold_copy": (C.c_int, [_P, C.c_double, C.c_int]),
     "cgfd_set_boundary_mlp": (C.c_int, [_P, C.c_int, C.c_void_p]),
     "cgfd_set_boundary_mlp_gains": (C.c_int, [_P, _fp]),
     "cgfd_upload_focal": (C.c_int, [_P, C.c_int, _ip, C.c_int, C.c_double, _fp]),
@@ -255,6 +256,12 @@ class Solver:
         ms = C.c_float()
         self._chk(_lib.cgfd_autotune(self._h, steps, C.byref(ms)))
         return ms.value
+
+    def test_withhold_copy(self, wait_limit_s: float, withhold: int):
+        """Test hook of the bounded device waits (cgfd_test_withhold_copy):
+        the first velocity CTA withholds one tensor copy and every wait gives
+        up after wait_limit_s; withhold < 0 restores normal operation."""
+        self._chk(_lib.cgfd_test_withhold_copy(self._h, float(wait_limit_s), int(withhold)))
 
     def __del__(self):
         self.close()

@@ -17,8 +17,14 @@ directly from seeded parameters:
 
 Grid coordinates are extended into the ghost cells by linear extrapolation
 (common::interpolated_extend, src/common.cpp:67-95); the metric, CFS-PML
-factors and source time functions come from the solver library's FP64
-pre-processing (cgfd.metric_from_coords / cfs_factors / stf).
+factors, source time functions and moment tensors come from an FP64
+pre-processing backend: by default the solver library's
+(cgfd.metric_from_coords / cfs_factors / stf / angle2moment); with
+use_preprocessing("oracle") the CPU oracle's restatement of the same
+reference functions, so that a process which must not load the solver
+library (the timing of the reference's own runtime) can still build every
+model.  The solver library is imported only when its backend is used or a
+solver description is made.
 """
 from __future__ import annotations
 
@@ -27,9 +33,43 @@ import math
 
 import numpy as np
 
-import cgfd
-
 LFD = 3
+
+# wavelet names of the reference's source.dat (src/source.cpp:723-775)
+STF_TYPES = {"Gauss": 0, "gauss": 1, "Ricker": 2, "ricker": 3, "Bell": 4,
+             "bell": 5, "BELL": 6, "Step": 7}
+
+_PREP = "product"
+
+
+def use_preprocessing(backend: str) -> None:
+    """Selects the FP64 pre-processing: "product" (libcgfd.so) or "oracle"
+    (the CPU oracle's restatement, which never loads libcgfd.so)."""
+    global _PREP
+    if backend not in ("product", "oracle"):
+        raise ValueError(backend)
+    _PREP = backend
+
+
+def _prep():
+    if _PREP == "oracle":
+        import pyoracle
+        return pyoracle
+    import cgfd
+    return cgfd
+
+
+def _metric_from_coords(ni, nj, nk, h, x, y, z):
+    return _prep().metric_from_coords(ni, nj, nk, h, x, y, z)
+
+
+def _stf(kind, start, t0, f0, n, dt):
+    k = STF_TYPES[kind] if isinstance(kind, str) else int(kind)
+    return np.asarray(_prep().stf(k, start, t0, f0, n, dt), np.float32)
+
+
+def _angle2moment(strike, dip, rake):
+    return np.asarray(_prep().angle2moment(strike, dip, rake), np.float64)
 
 
 @dataclasses.dataclass
@@ -43,7 +83,7 @@ class Model:
     nt: int
     con_index: int
     nabs: tuple
-    metric: dict            # zeta_x zeta_y zeta_z jac (+ xi/eta), float64 full arrays
+    metric: dict            # zeta_x zeta_y zeta_z jac, float64 full arrays
     alpha: np.ndarray       # float32 full arrays
     beta: np.ndarray
     rho: np.ndarray
@@ -75,7 +115,8 @@ class Model:
     def shape(self):
         return (self.ni + 6, self.nj + 6, self.nk + 6)
 
-    def desc(self, **kw) -> cgfd.Desc:
+    def desc(self, **kw):
+        import cgfd
         return cgfd.make_desc(self.ni, self.nj, self.nk, self.steph, self.stept,
                               self.nt, self.con_index, self.nabs, **kw)
 
@@ -161,8 +202,14 @@ def _pml(ni, nj, nk, steph, metric, nabs, velabs, bmax, amax):
     dlx = norm(m["xi_x"][:, LFD, LFD], m["xi_y"][:, LFD, LFD], m["xi_z"][:, LFD, LFD])
     dly = norm(m["eta_x"][LFD, :, LFD], m["eta_y"][LFD, :, LFD], m["eta_z"][LFD, :, LFD])
     dlz = norm(m["zeta_x"][LFD, LFD, :], m["zeta_y"][LFD, LFD, :], m["zeta_z"][LFD, LFD, :])
-    return cgfd.cfs_factors(ni, nj, nk, nabs, [velabs] * 6, [bmax] * 6, [amax] * 6,
+    return _prep().cfs_factors(ni, nj, nk, nabs, [velabs] * 6, [bmax] * 6, [amax] * 6,
                             dlx, dly, dlz)
+
+
+def _solver_metric(metric):
+    """The four metric arrays the solver consumes (the rest of calmetric's
+    output, xi and eta, is only needed for the PML thicknesses)."""
+    return {k: metric[k] for k in ("zeta_x", "zeta_y", "zeta_z", "jac")}
 
 
 def _surface_grid(ni, nj, n_side, spacing_cells):
@@ -182,17 +229,18 @@ def flat_halfspace(ni=160, nj=160, nk=80, h=100.0, dt=0.008, nt=500, vp=6000.0,
     surface receivers on an n_side x n_side grid."""
     con_index = max(LFD, nk + LFD - 1 - int(round(con_depth / h)))
     x, y, z = _coords(ni, nj, nk, h, h, h, 0.0, 1.0, con_index)
-    metric = cgfd.metric_from_coords(ni, nj, nk, h, x, y, z)
+    metric = _metric_from_coords(ni, nj, nk, h, x, y, z)
     shape = (ni + 6, nj + 6, nk + 6)
     alpha = np.full(shape, vp, np.float32)
     beta = np.full(shape, vs, np.float32)
     dens = np.full(shape, rho, np.float32)
     pml = _pml(ni, nj, nk, h, metric, nabs, velabs, bmax, amax)
+    metric = _solver_metric(metric)
     top = nk + LFD - 1
     sk = top - int(round(src_depth / h))
     src = np.array([[LFD + ni // 2, LFD + nj // 2, sk]], np.int32)
     nstf = 2 * (nt + 1)
-    wave = cgfd.stf("Ricker", 0.0, t0, f0, nstf, dt / 2.0)[None, :]
+    wave = _stf("Ricker", 0.0, t0, f0, nstf, dt / 2.0)[None, :]
     m6 = np.array([[1e16, 1e16, 1e16, 0, 0, 0]], np.float32)
     ij = _surface_grid(ni, nj, n_side, rcv_spacing / h)
     rcv = np.concatenate([ij, np.full((len(ij), 1), top, np.int32)], axis=1)
@@ -235,7 +283,7 @@ def gaussian_hill(ni=400, nj=400, nk=200, h=100.0, dt=0.006, nt=2000,
     top = nk + LFD - 1
     con_index = int(np.clip(np.searchsorted(zf[LFD:top + 1], -con_depth) + LFD, LFD, top - 3))
     x, y, z = _coords(ni, nj, nk, h, dz_top, dz_bot, hill_h, hill_w, con_index)
-    metric = cgfd.metric_from_coords(ni, nj, nk, h, x, y, z)
+    metric = _metric_from_coords(ni, nj, nk, h, x, y, z)
     shape = (ni + 6, nj + 6, nk + 6)
     vp = np.empty(shape, np.float32)
     dens = np.empty(shape, np.float32)
@@ -255,19 +303,20 @@ def gaussian_hill(ni=400, nj=400, nk=200, h=100.0, dt=0.006, nt=2000,
         del pert
     vs = (vp / np.float32(math.sqrt(3.0))).astype(np.float32)
     pml = _pml(ni, nj, nk, h, metric, nabs, velabs, bmax, amax)
+    metric = _solver_metric(metric)
     ci, cj = LFD + ni // 2, LFD + nj // 2
     sk = int(np.clip(np.searchsorted(zf[LFD:top + 1], -src_depth) + LFD, LFD, top))
     src = np.array([[ci, cj, sk]], np.int32)
     nstf = 2 * (nt + 1)
-    wave = cgfd.stf(stf_kind, 0.0, t0, f0, nstf, dt / 2.0)[None, :]
+    wave = _stf(stf_kind, 0.0, t0, f0, nstf, dt / 2.0)[None, :]
     mu = float(dens[ci, cj, sk]) * float(vs[ci, cj, sk]) ** 2
-    m6 = (cgfd.angle2moment(*sdr) * m0 * mu).astype(np.float32)[None, :]
+    m6 = (_angle2moment(*sdr) * m0 * mu).astype(np.float32)[None, :]
     ij = _surface_grid(ni, nj, n_side, rcv_spacing / h)
     rcv = np.concatenate([ij, np.full((len(ij), 1), top, np.int32)], axis=1)
     if force:
         frc_loc = np.array([[ci + 2, cj - 1, top]], np.int32)
         frc_f3 = np.array([[3e14, -2e14, 1e15]], np.float32)
-        frc_stf = cgfd.stf("Ricker", 0.0, t0, force_f0, nstf, dt / 2.0)[None, :]
+        frc_stf = _stf("Ricker", 0.0, t0, force_f0, nstf, dt / 2.0)[None, :]
     else:
         frc_loc = np.zeros((0, 3), np.int32)
         frc_f3 = np.zeros((0, 3), np.float32)
@@ -292,6 +341,38 @@ def config_c2(nt=2000) -> Model:
     50 -> 150 m, 3 layers with 5% perturbation (seed 12345), double couple
     (30/60/90) with a Gaussian STF, 20-cell PML, 400 surface receivers."""
     return gaussian_hill(nt=nt, name="gaussian_hill_400x400x200")
+
+
+def random_layers(n_layers, depth, vp_range=(2500.0, 7000.0), seed=5):
+    """Seeded layered medium for gaussian_hill: n_layers layers with tops at
+    sorted uniform depths in (0, 0.9 depth) and vp drawn uniformly from
+    vp_range, increasing with depth; density from Gardner's relation
+    310 vp^0.25 (kg/m^3, vp in m/s).  Returns ((z_bottom, vp, rho), ...)
+    from the top down, the last layer unbounded."""
+    rng = np.random.default_rng(seed)
+    tops = np.sort(rng.uniform(0.0, 0.9 * depth, n_layers - 1))
+    vps = np.sort(rng.uniform(vp_range[0], vp_range[1], n_layers))
+    vps[0], vps[-1] = vp_range[0], vp_range[1]
+    out = []
+    for q in range(n_layers):
+        zbot = -float(tops[q]) if q < n_layers - 1 else -1e30
+        out.append((zbot, float(vps[q]), float(310.0 * vps[q] ** 0.25)))
+    return tuple(out)
+
+
+def config_c5(nt=3000, nabs=(20, 20, 20, 20, 20, 0), ni=600, nj=600, nk=250,
+              name="gaussian_hill_600x600x250") -> Model:
+    """600x600x250 Gaussian hill (the 400x400x200 model's topography: 1500 m,
+    width 3000 m, vertical spacing 50 -> 150 m) over a seeded random-layered
+    medium (8 layers, vp 2500..7000 increasing with depth, vs = vp/sqrt(3),
+    Gardner density), double couple (30/60/90) with a Gaussian STF at 5 km,
+    20-cell CFS-PML on the 5 absorbing faces, 400 surface receivers (20 x 20
+    at 1.5 km); dt = 7 ms, 0.75 of the reference's bound 1.3 dmin / vp_max
+    (src/mediaparas.cpp:2263) with dmin = 50 m and vp_max = 7000 m/s."""
+    depth = float(np.sum(np.linspace(50.0, 150.0, nk - 1)))
+    return gaussian_hill(ni=ni, nj=nj, nk=nk, dt=0.007, nt=nt,
+                         layers=random_layers(8, depth), perturb=0.0, nabs=nabs,
+                         velabs=7000.0, name=name)
 
 
 def hill_256(nt=40, nabs=(20, 20, 20, 20, 20, 0)) -> Model:
@@ -398,7 +479,7 @@ def with_finite_fault(m: Model, center, length=8, width=5, strike=30.0, dip=60.0
     rng = np.random.default_rng(seed)
     h = m.steph
     fdt = fdt or 1.7 * m.stept
-    m6 = np.asarray(cgfd.angle2moment(strike, dip, rake), np.float64)
+    m6 = np.asarray(_angle2moment(strike, dip, rake), np.float64)
     st, dp = math.radians(strike), math.radians(dip)
     sv = np.array([math.sin(st), math.cos(st), 0.0])              # along strike (x east, y north)
     dv = np.array([math.cos(dp) * math.cos(st), -math.cos(dp) * math.sin(st), -math.sin(dp)])

@@ -91,8 +91,11 @@ int cgfd_create(const cgfd_desc *desc, cgfd_solver **out);
 /* Replaces ChildProcs::~ChildProcs (src/calculate.cu:1007-1334). NULL is a no-op. */
 int cgfd_destroy(cgfd_solver *h);
 
-/* Copies the text of the last error of h (or of the last failed cgfd_create
- * when h is NULL) into buf.  Replaces the reference's printf diagnostics. */
+/* Copies the text of the last error of h into buf; with h NULL, the last
+ * error of a call without a handle (a failed cgfd_create, the host
+ * pre-processing, cgfd_count_nonfinite_noalloc) made by the calling host
+ * thread (kept per thread, so concurrent callers do not mix their texts).
+ * Replaces the reference's printf diagnostics. */
 int cgfd_last_error(const cgfd_solver *h, char *buf, size_t len);
 
 /* Grid metric, FP64, full arrays (nx*ny*nz, reference layout).  Replaces the
@@ -222,13 +225,16 @@ int cgfd_get_field_scales(cgfd_solver *h, int *exp2);
  * No reference counterpart (the reference has no NaN/Inf check).
  * It allocates nothing: its scratch is a fixed array in the library's device
  * image, so n is limited to 134,217,728 values per call (larger n returns
- * CGFD_ERR_ARG).  The first call on a device looks that array up (set-up)
- * and should come before any stream capture.  All calls share the array:
+ * CGFD_ERR_ARG).  Every call looks up the array's device address (the
+ * first call on a device loads the library's device code there, which is
+ * set-up work, so it should come before any stream capture).  All calls share the array:
  * calls that overlap on the GPU race and must be serialised by the caller.
  * Runs on `stream` (a cudaStream_t, NULL = default stream) and waits for it;
  * returns CGFD_ERR_NONFINITE when *n_bad is not zero. */
 int cgfd_count_nonfinite_noalloc(const float *d_values, size_t n, long long *n_bad,
                                  void *stream);
+/* The most values cgfd_count_nonfinite_noalloc takes per call (16384 x 8192). */
+#define CGFD_NOALLOC_MAX_VALUES 134217728ull
 
 /* -------------------------------- outputs --------------------------------- */
 
@@ -298,6 +304,19 @@ int cgfd_mlp_gradient(const void *weights_fp16, const float *x, const float *t, 
  * No reference counterpart (the reference reads BlockPerGrid/ThreadPerBlock
  * from its configuration file). */
 int cgfd_autotune(cgfd_solver *h, int steps, float *ms_per_step);
+
+/* Test hook of the bounded device waits (no reference counterpart: the
+ * reference's waits are cudaDeviceSynchronize calls that abort on error,
+ * src/calculate.cu:17-41).  Every mbarrier wait of the default kernel gives
+ * up after wait_limit_s (0 < wait_limit_s <= 60) instead of about 2 s, and
+ * the velocity part's first CTA does not issue the halo tensor copy of entry
+ * `withhold` of its first work item, so its wait for that plane runs out:
+ * the CTA records the expiry, drains its own copies (bounded) and returns,
+ * and cgfd_sync reports CGFD_ERR_TIMEOUT.  The solver's state is then
+ * invalid (destroy it); other solvers are unaffected.  withhold < 0 restores
+ * normal operation.  Needs CGFD_KERNEL_FUSED; takes effect from the next
+ * step (the step graphs are rebuilt). */
+int cgfd_test_withhold_copy(cgfd_solver *h, double wait_limit_s, int withhold);
 
 /* ---------------------- batches of models (one GPU) ----------------------- */
 

@@ -6,15 +6,21 @@
 //   * builds the cindx exactly as get_conf does (src/simulation.cc:798-835);
 //   * writes the par file and device.dat that ChildProcs::GpuAbility reads
 //     (src/calculate.cu:2832-2950) into a scratch directory;
-//   * fills the public host buffers H_drv, H_mpa, H_apr, H_mnt, H_frc, Hpt
-//     (src/typedata.h:148-160), then C2DPointPick, ParH2D, VelCoeff;
+//   * fills the public host buffers H_drv, H_mpa, H_apr, H_mnt, H_frc, Hpt,
+//     and for the optional outputs and sources HSpt (snapshot points), HFpt
+//     and H_Rmnt (focal points and their moment series) (src/typedata.h:
+//     148-162), then calls C2DPointPick, C2DSnapPick, C2DFocalPick, ParH2D
+//     and VelCoeff in the order of src/simulation.cc:208-228;
 //   * runs the time loop of src/simulation.cc:252-700 with the same
-//     wavesyn/abssyn/RKite/PWpick sequence and direction table.  ShareData,
-//     IntraBoundGS and BoundGS are not called: with one child rank and one
-//     device they only move never-written zeros into the x ghost planes.
-// Input and output are flat binary files (see oracle/refio.py).  Built with
-// the reference's SrcSmooth option (ref_wavesim_smooth) it also reads the
-// sources' smoothing blocks (H_mnt.dnorm, H_frc.dnorm) after the input.
+//     wavesyn/abssyn/RKite/PWpick/SWpick sequence and direction table.
+//     ShareData, IntraBoundGS and BoundGS are not called: with one child rank
+//     and one device they only move never-written zeros into the x ghost
+//     planes.  With PVflag set, the last stage runs IterationFinalPV and the
+//     peak velocities are read from the device buffer Dpv it keeps.
+// Input and output are flat binary files (format version 2, see
+// oracle/refio.py).  Built with the reference's SrcSmooth option
+// (ref_wavesim_smooth) it also reads the sources' smoothing blocks
+// (H_mnt.dnorm, H_frc.dnorm) after the input.
 #include "typedata.h"
 
 #include <cuda_runtime.h>
@@ -62,18 +68,21 @@ int main(int argc, char **argv) {
   }
   FILE *fi = fopen(argv[1], "rb");
   if (!fi) { perror("input"); return 3; }
-  int32_t hdr[20];
-  rd(fi, hdr, 20);
-  if (hdr[0] != 0x52464743 || hdr[1] != 1) { fprintf(stderr, "bad input header\n"); return 4; }
+  int32_t hdr[28];
+  rd(fi, hdr, 28);
+  if (hdr[0] != 0x52464743 || hdr[1] != 2) { fprintf(stderr, "bad input header\n"); return 4; }
   const int ni = hdr[2], nj = hdr[3], nk = hdr[4], nt = hdr[5], nsteps = hdr[6];
   const int con = hdr[7];
   int nabs[6];
   for (int q = 0; q < 6; ++q) nabs[q] = hdr[8 + q];
   const int nmnt = hdr[14], nfrc = hdr[15], nstf = hdr[16], nrecv = hdr[17];
   const int has_init = hdr[18], nstages = hdr[19];
-  double hd[2];
-  rd(fi, hd, 2);
-  const Real steph = (Real)hd[0], stept = (Real)hd[1];
+  const int write_fields = hdr[20] & 1;
+  const int nfoc = hdr[21], fnt = hdr[22], pvflag = hdr[23];
+  const int nsnp = hdr[24], snap_tinv = hdr[25] > 0 ? hdr[25] : 1;
+  double hd[3];
+  rd(fi, hd, 3);
+  const Real steph = (Real)hd[0], stept = (Real)hd[1], fdt = (Real)hd[2];
 
   cindx cdx;
   cdx.ni = ni; cdx.nj = nj; cdx.nk = nk;
@@ -100,9 +109,9 @@ int main(int argc, char **argv) {
     fclose(fd);
   }
 
-  int CSpn[1] = {0};
+  int CSpn[1] = {nsnp};
   ChildProcs cp(conf.c_str(), cdx, steph, stept, nfrc, nmnt, nstf, cdx.nx, ni, 0, con, 1, nabs,
-                nrecv, nt, CSpn, 0, 0, 0, (Real)0, 0, 0, 1, 1);
+                nrecv, nt, CSpn, nsnp ? 1 : 0, nfoc, nfoc ? fnt : 0, fdt, pvflag, 0, 1, 1);
 
   rd(fi, cp.H_drv.zetax, N);
   rd(fi, cp.H_drv.zetay, N);
@@ -151,6 +160,29 @@ int main(int argc, char **argv) {
     init.resize(9 * N);
     rd(fi, init.data(), init.size());
   }
+  {  // focal points: locations, then the moment series [6][nfoc][fnt]
+    std::vector<int32_t> loc(3 * nfoc);
+    rd(fi, loc.data(), loc.size());
+    for (int q = 0; q < nfoc; ++q) {
+      cp.HFpt.Rsn[q] = q; cp.HFpt.Gsn[q] = q;
+      cp.HFpt.locx[q] = loc[3 * q]; cp.HFpt.locy[q] = loc[3 * q + 1]; cp.HFpt.locz[q] = loc[3 * q + 2];
+      cp.H_Rmnt.locx[q] = loc[3 * q]; cp.H_Rmnt.locy[q] = loc[3 * q + 1]; cp.H_Rmnt.locz[q] = loc[3 * q + 2];
+    }
+    Real *mom[6] = {cp.H_Rmnt.mxx, cp.H_Rmnt.myy, cp.H_Rmnt.mzz,
+                    cp.H_Rmnt.mxy, cp.H_Rmnt.mxz, cp.H_Rmnt.myz};
+    for (int c = 0; c < 6 && nfoc; ++c) rd(fi, mom[c], (size_t)nfoc * fnt);
+  }
+  if (nsnp) {  // snapshot points, all nine components every snap_tinv steps
+    std::vector<int32_t> loc(3 * nsnp);
+    rd(fi, loc.data(), loc.size());
+    for (int q = 0; q < nsnp; ++q) {
+      cp.HSpt[0].Rsn[q] = q; cp.HSpt[0].Gsn[q] = q;
+      cp.HSpt[0].locx[q] = loc[3 * q]; cp.HSpt[0].locy[q] = loc[3 * q + 1];
+      cp.HSpt[0].locz[q] = loc[3 * q + 2];
+    }
+    cp.HSpt[0].tinv = snap_tinv;
+    cp.HSpt[0].cmp = 3;
+  }
 #ifdef SrcSmooth
   // the smoothing blocks of the moments, then of the forces (7^3 each)
   if (nmnt) rd(fi, cp.H_mnt.dnorm, (size_t)nmnt * LenNorm * LenNorm * LenNorm);
@@ -159,6 +191,8 @@ int main(int argc, char **argv) {
   fclose(fi);
 
   cp.C2DPointPick();
+  if (nsnp) cp.C2DSnapPick();
+  if (nfoc) cp.C2DFocalPick();
   cp.ParH2D();
   cp.VelCoeff();
   if (has_init) {
@@ -188,6 +222,7 @@ int main(int argc, char **argv) {
     cp.wavesyn(cp.FW, cp.W);
     cp.abssyn(3);
     cp.PWpick(cp.FW, t);
+    if (nsnp) cp.SWpick(cp.FW, t);
     cudaDeviceSynchronize();
     step_secs[t] = std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
   }
@@ -216,13 +251,29 @@ int main(int argc, char **argv) {
                  cp.HPW.Tzz, cp.HPW.Txy, cp.HPW.Txz, cp.HPW.Tyz};
   for (int c = 0; c < 9; ++c) wr(fo, hp[c], (size_t)nrecv * nt);
   std::vector<float> buf;
-  wfield sets[2] = {cp.FW[0], cp.W[0]};
-  for (auto &w : sets) {
-    Real *p[9] = {w.Vx, w.Vy, w.Vz, w.Txx, w.Tyy, w.Tzz, w.Txy, w.Txz, w.Tyz};
-    for (int c = 0; c < 9; ++c) {
-      dl(p[c], buf, N);
-      wr(fo, buf.data(), N);
+  if (write_fields) {
+    wfield sets[2] = {cp.FW[0], cp.W[0]};
+    for (auto &w : sets) {
+      Real *p[9] = {w.Vx, w.Vy, w.Vz, w.Txx, w.Tyy, w.Tzz, w.Txy, w.Txz, w.Tyz};
+      for (int c = 0; c < 9; ++c) {
+        dl(p[c], buf, N);
+        wr(fo, buf.data(), N);
+      }
     }
+  }
+  if (pvflag) {  // Dpv[0]: [nx][ny], the top valid layer's max |V| per component
+    const size_t n2 = (size_t)cdx.nx * cdx.ny;
+    Real *pv[3] = {cp.Dpv[0].Vx, cp.Dpv[0].Vy, cp.Dpv[0].Vz};
+    for (int c = 0; c < 3; ++c) {
+      dl(pv[c], buf, n2);
+      wr(fo, buf.data(), n2);
+    }
+  }
+  if (nsnp) {  // HSW[0]: [component][point][time index]
+    const size_t ntime = (size_t)((nt + snap_tinv - 1) / snap_tinv);
+    wfield &w = cp.HSW[0];
+    Real *p[9] = {w.Vx, w.Vy, w.Vz, w.Txx, w.Tyy, w.Tzz, w.Txy, w.Txz, w.Tyz};
+    for (int c = 0; c < 9; ++c) wr(fo, p[c], (size_t)nsnp * ntime);
   }
   fclose(fo);
   fflush(stdout);

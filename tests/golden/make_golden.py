@@ -8,7 +8,9 @@ tests/cases.py.  Needs a GPU; run as
 (default: tests/golden/ itself, every case).  Cases whose model spreads its
 sources (SrcSmooth) run on oracle/_ref/ref_wavesim_smooth.  Each file holds the reference's
 seismograms (full steps) and the stage output W on the valid cells (partial
-steps), plus the digest of the inputs it was made from.
+steps), plus the digest of the inputs it was made from.  The case
+cases.OUTPUT_CASE also holds the reference's peak velocities and snapshot
+samples of a run with a finite fault.
 """
 import os
 import sys
@@ -25,9 +27,28 @@ import cases  # noqa: E402
 import refio  # noqa: E402
 
 
+def outputs_case(out_dir):
+    """The reference's focal source (C2DFocalPick / InterpFocus / LoadRmom),
+    peak velocity (IterationFinalPV) and snapshots (C2DSnapPick / SWpick) in
+    one run of cases.OUTPUT_CASE."""
+    m = cases.build_outputs_case()
+    pts = cases.snap_points()
+    r = refio.run(m, m.nt, fields=False, focal=True, peak_velocity=True, snap_points=pts,
+                  snap_tinv=cases.SNAP_TINV)
+    np.savez_compressed(os.path.join(out_dir, f"{cases.OUTPUT_CASE}.npz"),
+                        digest=np.array(cases.model_digest(m)), nsteps=m.nt,
+                        ref_secs=r["secs"], seis=r["seis"], pv=r["pv"][:, 3:-3, 3:-3],
+                        snap=r["snap"], snap_points=pts)
+    print(cases.OUTPUT_CASE, "done", f"{r['secs']:.3f}s")
+
+
 def main(out_dir, names=None):
     os.makedirs(out_dir, exist_ok=True)
+    if not names or cases.OUTPUT_CASE in names:
+        outputs_case(out_dir)
     for name in names or cases.CASES:
+        if name == cases.OUTPUT_CASE:
+            continue
         m, nsteps, nstages, init = cases.build(name)
         r = refio.run(m, nsteps, init, nstages)
         payload = dict(digest=np.array(cases.model_digest(m, init)), nsteps=nsteps,

@@ -78,3 +78,47 @@ def test_16bit_storage_needs_the_default_kernel(kernel):
         cgfd.Solver(d)
     assert e.value.status == cgfd.ERR_ARG
     assert "16-bit" in cgfd.last_error(None)
+
+
+def test_noalloc_limit_is_the_header_limit():
+    """cgfd_count_nonfinite_noalloc refuses more than CGFD_NOALLOC_MAX_VALUES
+    values before touching the device, and takes the size itself: on a host
+    pointer the limit passes the size check and fails the device-memory one
+    (no GPU needed).  The binding's constant is the header's."""
+    import ctypes as C
+
+    import cgfd
+    hdr = open(HEADER).read()
+    lim = int(re.search(r"#define\s+CGFD_NOALLOC_MAX_VALUES\s+(\d+)", hdr).group(1))
+    assert cgfd.NOALLOC_MAX_VALUES == lim
+    host = (C.c_float * 4)()
+    for n, text in ((lim + 1, "exceed the fixed scratch"), (lim, "not device memory")):
+        out = C.c_longlong(-1)
+        st = cgfd._lib.cgfd_count_nonfinite_noalloc(C.cast(host, C.c_void_p), n, C.byref(out),
+                                                    None)
+        assert st == cgfd.ERR_ARG and text in cgfd.last_error(None), (n, cgfd.last_error(None))
+
+
+def test_handle_less_errors_are_per_thread():
+    """The last error of a call without a handle is kept per host thread."""
+    import threading
+
+    import cgfd
+    d = cgfd.make_desc(20, 20, 20, 100.0, 0.005, 10, 10, (4, 4, 4, 4, 4, 2))
+    with pytest.raises(cgfd.CgfdError):
+        cgfd.Solver(d)
+    mine = cgfd.last_error(None)
+    seen = []
+
+    def other():
+        seen.append(cgfd.last_error(None))
+        bad = cgfd.make_desc(0, 20, 20, 100.0, 0.005, 10, 10, (4, 4, 4, 4, 4, 0))
+        with pytest.raises(cgfd.CgfdError):
+            cgfd.Solver(bad)
+        seen.append(cgfd.last_error(None))
+
+    t = threading.Thread(target=other)
+    t.start()
+    t.join()
+    assert seen[0] == "" and seen[1] and seen[1] != mine
+    assert cgfd.last_error(None) == mine

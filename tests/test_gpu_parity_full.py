@@ -1,0 +1,68 @@
+"""Full-size parity on the benchmark models: the B200 solver against the
+reference's own CUDA runtime (oracle/_ref/ref_wavesim: src/calculate.cu built
+from its sources) on the 400x400x200 hill (3 perturbed layers) and the
+600x600x250 hill (8 random layers), each with a 20-cell CFS-PML on five faces
+and 400 surface receivers.
+
+The runs are long enough for the P wave of the Gaussian source pulse (centre
+1.0 s, 5 km deep) to reach every surface receiver: 400 steps of 6 ms on the
+400-cell model, 500 steps of 7 ms on the 600-cell one (its top 6 km are
+2500-2700 m/s).  Bar: 1e-5 relative L2 over all receivers and samples, the
+velocity seismograms strictly per component, the stresses on their group's
+scale (tests/helpers.py: comp_errors); on the 400-cell model also the final
+wavefield (every third column in x and y, all depths).
+"""
+import numpy as np
+import pytest
+
+import cgfd
+import models
+import refio
+from helpers import comp_errors, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _check_seismograms(got, ref, what):
+    # the surface signal must be the physical arrival, not numerical
+    # precursors: the largest |V| over the receivers peaks well inside the
+    # window
+    env = np.abs(ref[:3]).max(axis=(0, 1))
+    assert env.max() > 0 and np.argmax(env) > 0.4 * len(env), f"{what}: no arrival"
+    for c in range(3):
+        e = rel_l2(got[c], ref[c])
+        assert e < TOL, f"{what} {cgfd.COMPONENTS[c]} rel L2 {e:.3e}"
+    for c, e in enumerate(comp_errors(got, ref)):
+        assert e < TOL, f"{what} {cgfd.COMPONENTS[c]} rel L2 {e:.3e}"
+
+
+def _run_product(m, nsteps, fields=False):
+    s = cgfd.Solver(m.desc(kernel=cgfd.KERNEL_FUSED))
+    m.load(s)
+    s.step(nsteps)
+    seis = s.seismograms()
+    fw = None
+    if fields:
+        fw = np.stack([s.get_field(c)[3:-3:3, 3:-3:3, 3:-3] for c in range(9)])
+    s.close()
+    return seis, fw
+
+
+def test_hill_400x400x200_400_steps_matches_reference():
+    m = models.config_c2(nt=400)
+    r = refio.run(m, m.nt, fields=True, timeout=1800)
+    seis, fw = _run_product(m, m.nt, fields=True)
+    _check_seismograms(seis, r["seis"], "400x400x200")
+    ref_fw = r["fw"][:, 3:-3:3, 3:-3:3, 3:-3]
+    del r
+    for c, e in enumerate(comp_errors(fw, ref_fw)):
+        assert e < TOL, f"final FW {cgfd.COMPONENTS[c]} rel L2 {e:.3e}"
+
+
+def test_hill_600x600x250_500_steps_matches_reference():
+    m = models.config_c5(nt=500)
+    r = refio.run(m, m.nt, fields=False, timeout=2400)
+    seis, _ = _run_product(m, m.nt)
+    _check_seismograms(seis, r["seis"], "600x600x250")
