@@ -248,7 +248,8 @@ def cpu_sample_model(cfg, nt):
     window of the same generator (layers, grid spacing, PML, dt)."""
     import models
     if cfg == "hill600":
-        return models.config_c5(nt=nt, ni=200, nj=200, name="gaussian_hill_200x200x250_window")
+        return models.config_c5(nt=nt, ni=200, nj=200, n_side=5, rcv_spacing=1000.0,
+                                name="gaussian_hill_200x200x250_window")
     return build_model(cfg, nt)
 
 

@@ -361,7 +361,7 @@ def random_layers(n_layers, depth, vp_range=(2500.0, 7000.0), seed=5):
 
 
 def config_c5(nt=3000, nabs=(20, 20, 20, 20, 20, 0), ni=600, nj=600, nk=250,
-              name="gaussian_hill_600x600x250") -> Model:
+              name="gaussian_hill_600x600x250", **kw) -> Model:
     """600x600x250 Gaussian hill (the 400x400x200 model's topography: 1500 m,
     width 3000 m, vertical spacing 50 -> 150 m) over a seeded random-layered
     medium (8 layers, vp 2500..7000 increasing with depth, vs = vp/sqrt(3),
@@ -372,7 +372,7 @@ def config_c5(nt=3000, nabs=(20, 20, 20, 20, 20, 0), ni=600, nj=600, nk=250,
     depth = float(np.sum(np.linspace(50.0, 150.0, nk - 1)))
     return gaussian_hill(ni=ni, nj=nj, nk=nk, dt=0.007, nt=nt,
                          layers=random_layers(8, depth), perturb=0.0, nabs=nabs,
-                         velabs=7000.0, name=name)
+                         velabs=7000.0, name=name, **kw)
 
 
 def hill_256(nt=40, nabs=(20, 20, 20, 20, 20, 0)) -> Model:

@@ -123,9 +123,34 @@ struct Solver {
   std::vector<double> seis;
   int steps = 0;
   bool have_metric = false, have_media = false, have_pml = false, prepared = false;
+  // emulated reduced-precision storage of the field sets (orc_set_storage_emulation)
+  struct Emul {
+    int ebits = 0, mbits = 0;  // 0: off
+    int mask = 0;              // 1: W, 2: tW, 4: FW
+    int flags = 0;             // 1: tW kept as tW - FW, 2: W kept as W - FW
+    int adapt = -1;            // >= 0: scales re-chosen every step, max at 2^adapt
+    double scale[9] = {1, 1, 1, 1, 1, 1, 1, 1, 1};
+  } em;
 
   long gi(int i, int j, int k) const { return ((long)i * ny + j) * nz + k; }
 };
+
+// Round x to a binary format of ebits exponent bits and mbits mantissa bits
+// (IEEE layout: bias 2^(ebits-1)-1, subnormals, round to nearest even,
+// saturating), e.g. (5, 10) is FP16 and (8, 7) BF16.
+double quant_fmt(double x, int ebits, int mbits) {
+  if (x == 0.0 || ebits <= 0) return x;
+  const int emax = (1 << (ebits - 1)) - 1, emin = 1 - emax;
+  int e;
+  std::frexp(x, &e);
+  const int ex = (e - 1 < emin) ? emin : e - 1;
+  const double ulp = std::ldexp(1.0, ex - mbits);
+  double q = std::nearbyint(x / ulp) * ulp;
+  const double mx = std::ldexp(2.0 - std::ldexp(1.0, -mbits), emax);
+  if (q > mx) q = mx;
+  if (q < -mx) q = -mx;
+  return q;
+}
 
 struct Handle {
   int prec;  // 0 = double, 1 = float
@@ -524,6 +549,43 @@ void sources(Solver<R> &S, int tindex, double time) {
 
 // IterationBegin / Inner / Final (src/calculate.cu:6330-6734) for the
 // wavefield (valid cells) and the ADE auxiliaries.
+// The same update with the stored sets rounded as the 16-bit storage of
+// the solver keeps them (test infrastructure: localises the storage error).
+// The first stage writes no tW; the second rebuilds it from the rounded
+// stage output, tW = FW + (b0/a0)(W - FW) + b1 dt H, as the solver does.
+template <class R>
+void update_emulated(Solver<R> &S, int rk) {
+  const auto &E = S.em;
+  const double a = (rk < 3) ? RKA[rk] * S.d.stept : 0.0;
+  const double b = RKB[rk] * S.d.stept;
+  const int ni = S.d.ni, nj = S.d.nj, nk = S.d.nk;
+  auto q = [&](double v, int c, int set) {
+    if (!(E.mask & set)) return v;
+    return quant_fmt(v / E.scale[c], E.ebits, E.mbits) * E.scale[c];
+  };
+#pragma omp parallel for schedule(static)
+  for (int i = LFD; i < ni + LFD; ++i)
+    for (int j = LFD; j < nj + LFD; ++j)
+      for (int k = LFD; k < nk + LFD; ++k) {
+        const long p = S.gi(i, j, k);
+        for (int c = 0; c < 9; ++c) {
+          const double f = S.FW[c][p], h = S.hW[c][p], w = S.W[c][p];
+          const double dtw = (E.flags & 1) ? 1.0 : 0.0, dw = (E.flags & 2) ? 1.0 : 0.0;
+          if (rk == 0) {
+            S.W[c][p] = (R)(dw * f + q(f * (1 - dw) + a * h, c, 1));
+          } else if (rk < 3) {
+            double t;
+            if (rk == 1) t = (RKB[0] / RKA[0]) * (w - f) + b * h + (1 - dtw) * f;
+            else t = S.tW[c][p] - dtw * f + b * h;
+            S.tW[c][p] = (R)(dtw * f + q(t, c, 2));
+            S.W[c][p] = (R)(dw * f + q(f * (1 - dw) + a * h, c, 1));
+          } else {
+            S.W[c][p] = (R)q(S.tW[c][p] + b * h, c, 4);
+          }
+        }
+      }
+}
+
 template <class R>
 void update(Solver<R> &S, int rk) {
   const R a = (rk < 3) ? (R)(RKA[rk] * S.d.stept) : R(0);
@@ -544,10 +606,13 @@ void update(Solver<R> &S, int rk) {
       }
     }
   };
+  if (S.em.ebits > 0) update_emulated(S, rk);
+  else {
 #pragma omp parallel for schedule(static)
   for (int i = LFD; i < ni + LFD; ++i)
     for (int j = LFD; j < nj + LFD; ++j)
       for (int k = LFD; k < nk + LFD; ++k) upd(S.FW, S.W, S.hW, S.tW, S.gi(i, j, k));
+  }
 #pragma omp parallel for schedule(static)
   for (int xa = 0; xa < S.nab[0]; ++xa)
     for (int j = LFD; j < nj + LFD; ++j)
@@ -590,6 +655,17 @@ int rk_stage(Solver<R> &S, int rk, int curr_t, int X, int Y, int Z, std::string 
     for (int c = 0; c < 9; ++c) S.FW[c] = S.W[c];
     for (int a = 0; a < 3; ++a)
       for (int c = 0; c < 9; ++c) S.FA[a][c] = S.A[a][c];
+    if (S.em.ebits > 0 && S.em.adapt >= 0) {  // emulation: scales from this step's maxima
+      for (int c = 0; c < 9; ++c) {
+        double mx = 0;
+        for (long p = 0; p < S.N; ++p) mx = std::max(mx, (double)std::fabs(S.FW[c][p]));
+        if (mx > 0) {
+          int e;
+          std::frexp(mx, &e);
+          S.em.scale[c] = std::ldexp(1.0, e - S.em.adapt);
+        }
+      }
+    }
   }
   return CGFD_OK;
 }
@@ -862,6 +938,27 @@ int orc_get_aux(void *h, int dir, int set, int comp, double *out, long *n) {
 }
 
 // VelPDcoeff matrices (nx*ny*9 each, reference index (i*ny+j)*9+m).
+// Test infrastructure: rounds the stored field sets (mask 1 W, 2 tW, 4 FW) to
+// a binary format of ebits/mbits bits with per-component scales (a stored s
+// stands for s * scale[c]); flags 1: tW kept as its difference from FW, 2: W
+// kept as its difference from FW; adapt >= 0: after every step each scale
+// becomes the power of two that puts the component's maximum just below
+// 2^adapt.  ebits = 0 turns it off.  FP64 oracle only.
+int orc_set_storage_emulation(void *h, int ebits, int mbits, const double *scale, int mask,
+                              int flags, int adapt) {
+  Handle *H = (Handle *)h;
+  if (!H || H->prec != 0 || ebits < 0 || ebits > 11 || mbits < 1 || mbits > 52)
+    return CGFD_ERR_ARG;
+  auto &S = *(Solver<double> *)H->s;
+  S.em.ebits = ebits;
+  S.em.mbits = mbits;
+  S.em.mask = mask;
+  S.em.flags = flags;
+  S.em.adapt = adapt;
+  for (int c = 0; c < 9; ++c) S.em.scale[c] = scale ? scale[c] : 1.0;
+  return CGFD_OK;
+}
+
 int orc_get_matv(void *h, double *mx, double *my) {
   Handle *H = (Handle *)h;
   auto f = [&](auto &S) {

@@ -48,6 +48,8 @@ _SIGS = {
     "orc_set_field": (C.c_int, [_P, C.c_int, C.c_int, _dp]),
     "orc_get_aux": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _dp, C.POINTER(C.c_long)]),
     "orc_get_matv": (C.c_int, [_P, _dp, _dp]),
+    "orc_set_storage_emulation": (C.c_int, [_P, C.c_int, C.c_int, _dp, C.c_int, C.c_int,
+                                            C.c_int]),
     "orc_metric_from_coords": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double,
                                          _dp, _dp, _dp, C.POINTER(_dp)]),
     "orc_cfs_factors": (C.c_int, [C.c_int, C.c_int, C.c_int, _ip, _dp, _dp, _dp,
@@ -184,6 +186,14 @@ class OracleSolver:
         out = np.zeros(n.value, np.float64)
         self._chk(_lib.orc_get_aux(self._h, direction, aset, comp, _d(out), C.byref(n)))
         return out
+
+    def set_storage_emulation(self, ebits, mbits, scale=None, mask=7, flags=0, adapt=-1):
+        """Rounds the stored field sets to an (ebits, mbits) binary format with
+        per-component scales (orc_set_storage_emulation); ebits 0 = off."""
+        sc = None if scale is None else np.ascontiguousarray(scale, np.float64)
+        self._chk(_lib.orc_set_storage_emulation(self._h, ebits, mbits,
+                                                 None if sc is None else _d(sc), mask, flags,
+                                                 adapt))
 
     def matv(self):
         nx, ny = self.shape[0], self.shape[1]

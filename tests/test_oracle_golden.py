@@ -19,7 +19,7 @@ def _golden_names():
     # the stepping fixtures (the vmap-grid and source fixtures, grid_vmap_*
     # and source_*, have their own tests)
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith(("grid_vmap_", "source_")))
+                  if not os.path.basename(p).startswith(("grid_vmap_", "source_", "outputs_")))
 
 
 def test_golden_set_is_complete():
@@ -52,3 +52,24 @@ def test_oracle_fp32_and_fp64_agree():
     b = cases.run_oracle(m, nsteps, nstages, init, prec=1)[0]
     for e in comp_errors(b, a):
         assert e < 1e-5
+
+
+def test_oracle_matches_reference_focal_pv_snapshot_golden():
+    """The reference's finite fault (InterpFocus / LoadRmom), peak velocity
+    (IterationFinalPV) and snapshots (SWpick) against the oracle's."""
+    path = os.path.join(GOLDEN, f"{cases.OUTPUT_CASE}.npz")
+    if not os.path.exists(path):
+        pytest.fail(f"missing golden file {path}")
+    g = np.load(path)
+    m = cases.build_outputs_case()
+    assert str(g["digest"]) == cases.model_digest(m), "inputs changed since the golden run"
+    assert np.array_equal(g["snap_points"], cases.snap_points())
+    seis, pv, snap = cases.run_oracle_outputs(m, int(g["nsteps"]))
+    assert np.abs(g["seis"][:3]).max() > 0 and g["pv"].max() > 0
+    for c in range(3):
+        assert rel_l2(seis[c], g["seis"][c]) < TOL, c
+        assert rel_l2(pv[c], g["pv"][c]) < TOL, c
+    for c, e in enumerate(comp_errors(seis, g["seis"])):
+        assert e < TOL, (c, e)
+    for c, e in enumerate(comp_errors(snap, g["snap"])):
+        assert e < TOL, (c, e)
