@@ -102,6 +102,9 @@ _SIGS = {
     "cgfd_get_field_scales": (C.c_int, [_P, _ip]),
     "cgfd_count_nonfinite_noalloc": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_longlong),
                                                C.c_void_p]),
+    "cgfd_read_media_volume_nc": (C.c_int, [C.c_char_p, _ip, _ip, _ip, _dp, _dp, _dp, _fp, _fp,
+                                            _fp]),
+    "cgfd_read_focal_nc": (C.c_int, [C.c_char_p, _ip, _ip, _dp, _dp, _dp, _dp, _fp]),
     "cgfd_metric_from_coords": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double,
                                           _dp, _dp, _dp, C.POINTER(_dp)]),
     "cgfd_cfs_factors": (C.c_int, [C.c_int, C.c_int, C.c_int, _ip, _dp, _dp, _dp,
@@ -587,6 +590,43 @@ def source_smoothing(x, y, z, kind, pos, loc):
     if st:
         raise CgfdError(st, last_error(None))
     return loc, w
+
+
+def read_media_volume_nc(path):
+    """(vx, vy, vz, vp, vs, rho) of a volume media file in NetCDF classic
+    format (cgfd_read_media_volume_nc); vp, vs, rho [nvx][nvy][nvz]."""
+    n = [C.c_int() for _ in range(3)]
+    b = path.encode()
+    st = _lib.cgfd_read_media_volume_nc(b, *[C.byref(x) for x in n], None, None, None, None,
+                                        None, None)
+    if st:
+        raise CgfdError(st, last_error(None))
+    nv = [x.value for x in n]
+    ax = [np.zeros(k) for k in nv]
+    vol = [np.zeros(nv, np.float32) for _ in range(3)]
+    st = _lib.cgfd_read_media_volume_nc(b, *[C.byref(x) for x in n], *[_d(a) for a in ax],
+                                        *[_f(v) for v in vol])
+    if st:
+        raise CgfdError(st, last_error(None))
+    return (*ax, *vol)
+
+
+def read_focal_nc(path):
+    """(dt, pos (np, 3), mom [6][np][nt]) of a finite-fault series file in
+    NetCDF classic format (cgfd_read_focal_nc)."""
+    npt, nt, dt = C.c_int(), C.c_int(), C.c_double()
+    b = path.encode()
+    st = _lib.cgfd_read_focal_nc(b, C.byref(npt), C.byref(nt), C.byref(dt), None, None, None,
+                                 None)
+    if st:
+        raise CgfdError(st, last_error(None))
+    pos = [np.zeros(npt.value) for _ in range(3)]
+    mom = np.zeros((6, npt.value, nt.value), np.float32)
+    st = _lib.cgfd_read_focal_nc(b, C.byref(npt), C.byref(nt), C.byref(dt), *[_d(p) for p in pos],
+                                 _f(mom))
+    if st:
+        raise CgfdError(st, last_error(None))
+    return dt.value, np.stack(pos, axis=1), mom
 
 
 def angle2moment(strike, dip, rake) -> np.ndarray:

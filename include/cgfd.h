@@ -383,6 +383,27 @@ int cgfd_media_volume(int ni, int nj, int nk, const double *x, const double *y, 
                       double crit_value, double crit_perc, int samp_x, int samp_y, int samp_z,
                       float *alpha, float *beta, float *dens);
 
+/* Volume media model file (the reference's media_filename for media_type
+ * = volume, e.g. Vsim_gpu.nc; mediapar::read_volume_new,
+ * src/mediaparas.cpp:1273-1425) in NetCDF classic format (CDF-1, -2 or -5;
+ * a NetCDF-4 file needs `nccopy -k classic` first): 1-D x, y, depth (or z)
+ * axes and Vp, Vs, rho over [x][y][depth], the input of cgfd_media_volume.
+ * With vx NULL only *nvx, *nvy, *nvz are set; then vx, vy, vz (n each) and
+ * vp, vs, rho (nvx*nvy*nvz each) receive the data. */
+int cgfd_read_media_volume_nc(const char *path, int *nvx, int *nvy, int *nvz,
+                              double *vx, double *vy, double *vz,
+                              float *vp, float *vs, float *rho);
+
+/* Finite-fault series file (the reference's focal_process_NC_file,
+ * stf-GPU.nc; source::source / readdata, src/source.cpp:43-56, 796-840) in
+ * NetCDF classic format: dimensions NP, NT, global attribute DT (s),
+ * Mxx Myy Mzz Mxy Mxz Myz [NP][NT] and posx, posy, posz [NP] (m).  With mom
+ * NULL only *np, *nt and *dt are set; then mom receives [6][np][nt] (the
+ * layout cgfd_upload_focal takes) and posx/posy/posz the positions.  The
+ * reference's simulate_damp factor is not applied. */
+int cgfd_read_focal_nc(const char *path, int *np, int *nt, double *dt,
+                       double *posx, double *posy, double *posz, float *mom);
+
 /* Grid metric from node coordinates (full arrays, reference layout), by
  * 2-point central differences and cross products, then mirrored into the
  * ghost cells: gridmesh::calmetric (src/gridmesh.cpp:1476-1627).

@@ -559,8 +559,9 @@ void update_emulated(Solver<R> &S, int rk) {
   const double a = (rk < 3) ? RKA[rk] * S.d.stept : 0.0;
   const double b = RKB[rk] * S.d.stept;
   const int ni = S.d.ni, nj = S.d.nj, nk = S.d.nk;
+  const bool block = E.ebits >= 100;  // block floating point: rounded below, per block
   auto q = [&](double v, int c, int set) {
-    if (!(E.mask & set)) return v;
+    if (!(E.mask & set) || block) return v;
     return quant_fmt(v / E.scale[c], E.ebits, E.mbits) * E.scale[c];
   };
 #pragma omp parallel for schedule(static)
@@ -584,6 +585,41 @@ void update_emulated(Solver<R> &S, int rk) {
           }
         }
       }
+  if (!block) return;
+  // block floating point: every run of B x-adjacent valid cells shares one
+  // exponent, each value keeps a sign and mbits magnitude bits below it
+  const int B = E.ebits - 100;
+  auto qblock = [&](std::vector<R> *set, std::vector<R> *base, bool delta) {
+#pragma omp parallel for schedule(static)
+    for (int j = LFD; j < nj + LFD; ++j)
+      for (int k = LFD; k < nk + LFD; ++k)
+        for (int c = 0; c < 9; ++c)
+          for (int i0 = 0; i0 < ni; i0 += B) {
+            const int i1 = std::min(i0 + B, ni);
+            double mx = 0;
+            for (int i = i0; i < i1; ++i) {
+              const long p = S.gi(i + LFD, j, k);
+              const double v = set[c][p] - (delta ? (double)base[c][p] : 0.0);
+              mx = std::max(mx, std::fabs(v));
+            }
+            if (mx == 0) continue;
+            int e;
+            std::frexp(mx, &e);  // mx < 2^e
+            const double ulp = std::ldexp(1.0, e - E.mbits);
+            for (int i = i0; i < i1; ++i) {
+              const long p = S.gi(i + LFD, j, k);
+              const double bv = delta ? (double)base[c][p] : 0.0;
+              const double v = set[c][p] - bv;
+              set[c][p] = (R)(bv + std::nearbyint(v / ulp) * ulp);
+            }
+          }
+  };
+  if (rk < 3) {
+    if (E.mask & 1) qblock(S.W, S.FW, (E.flags & 2) != 0);
+    if ((E.mask & 2) && rk > 0) qblock(S.tW, S.FW, (E.flags & 1) != 0);
+  } else if (E.mask & 4) {
+    qblock(S.W, S.FW, false);
+  }
 }
 
 template <class R>
@@ -943,11 +979,14 @@ int orc_get_aux(void *h, int dir, int set, int comp, double *out, long *n) {
 // stands for s * scale[c]); flags 1: tW kept as its difference from FW, 2: W
 // kept as its difference from FW; adapt >= 0: after every step each scale
 // becomes the power of two that puts the component's maximum just below
-// 2^adapt.  ebits = 0 turns it off.  FP64 oracle only.
+// 2^adapt.  ebits = 0 turns it off; ebits = 100 + B: block floating point,
+// B x-adjacent cells sharing an exponent, mbits magnitude bits each (plus a
+// sign).  FP64 oracle only.
 int orc_set_storage_emulation(void *h, int ebits, int mbits, const double *scale, int mask,
                               int flags, int adapt) {
   Handle *H = (Handle *)h;
-  if (!H || H->prec != 0 || ebits < 0 || ebits > 11 || mbits < 1 || mbits > 52)
+  if (!H || H->prec != 0 || ebits < 0 || (ebits > 11 && ebits < 101) || ebits > 164 ||
+      mbits < 1 || mbits > 52)
     return CGFD_ERR_ARG;
   auto &S = *(Solver<double> *)H->s;
   S.em.ebits = ebits;

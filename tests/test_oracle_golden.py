@@ -19,7 +19,7 @@ def _golden_names():
     # the stepping fixtures (the vmap-grid and source fixtures, grid_vmap_*
     # and source_*, have their own tests)
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith(("grid_vmap_", "source_", "outputs_")))
+                  if not os.path.basename(p).startswith(("grid_vmap_", "source_", "outputs_", "parfiles_")))
 
 
 def test_golden_set_is_complete():
