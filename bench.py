@@ -52,18 +52,27 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-target", action="store_true",
+                   help="skip the batched FP16 learned-thin-layer timing on the same model")
+    p.add_argument("--target-accuracy", type=int, default=0, metavar="STEPS",
+                   help="instead of the benchmark: reflected energy and 16-bit error of the "
+                        "thin-layer configurations over STEPS steps (one JSON line)")
     return p.parse_args()
 
 
-def build_model(cfg, nt):
+def build_model(cfg, nt, nabs=None):
+    """The workload's model; nabs replaces its CFS-PML widths (the same grid,
+    media and sources with another absorbing layer)."""
     import models
+    kw = {} if nabs is None else {"nabs": tuple(nabs)}
     if cfg == "hill600":
-        return models.config_c5(nt=nt)
+        return models.config_c5(nt=nt, **kw)
     if cfg == "hill400":
-        return models.config_c2(nt=nt)
+        return models.gaussian_hill(nt=nt, name="gaussian_hill_400x400x200", **kw)
     if cfg == "hill256":
-        return models.hill_256(nt=nt)
-    return models.config_c1(nt=nt)
+        return models.hill_256(nt=nt, **kw)
+    return models.flat_halfspace(nt=nt, name="flat_halfspace_160x160x80",
+                                 **({"nabs": tuple(nabs)} if nabs else {}))
 
 
 def workload_name(cfg):
@@ -363,10 +372,106 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+MLP_WEIGHTS = os.path.join(ROOT, "copara-cgfd3d_b200", "data", "layer_mlp_w4.npz")
+THIN = (4, 4, 4, 4, 4, 0)  # the learned layer's CFS-PML widths
+
+
+def thin_members(m, n=2):
+    """n members of the same model with a 4-cell CFS-PML for the learned
+    layer: the model's own source, then the source moved by (+60, -40)
+    cells with the mechanism rotated (independent shots on one model)."""
+    import dataclasses
+    out = [m]
+    for q in range(1, n):
+        loc = m.mnt_loc.copy()
+        loc[:, 0] += 60 * q
+        loc[:, 1] -= 40 * q
+        out.append(dataclasses.replace(m, mnt_loc=loc, mnt_m6=np.roll(m.mnt_m6, q, axis=1)))
+    return out
+
+
+def thin_batch(ms, storage, device, mlp=True):
+    import cgfd
+    b = cgfd.Batch([mm.desc(storage=storage, device=device) for mm in ms])
+    d = np.load(MLP_WEIGHTS)
+    for mm, s in zip(ms, b.models):
+        mm.load(s)
+        if mlp:
+            s.set_boundary_mlp(4, d["weights"].astype(np.float16))
+            s.set_boundary_mlp_gains(d["gains"].astype(np.float32))
+    b.prepare()
+    return b
+
+
+def run_target(args, plain_value, plain_ms, local):
+    """The batched FP16-storage learned-thin-layer solver on the same model:
+    two shots of the model with a 4-cell CFS-PML and the learned layer
+    stepped as one batch with FP16 field storage, timed like the plain run."""
+    import cgfd
+    K, W = args.steps, args.warmup
+    m4 = build_model(args.config, W + K + 2, nabs=THIN)
+    ms = thin_members(m4)
+    b = thin_batch(ms, cgfd.STORE_F16, local)
+    b.step(W)
+    b.sync()
+    ms_b = b.step_timed(K)
+    nbad = sum(s.check_finite() for s in b.models)
+    b.close()
+    value = len(ms) * m4.cells * K / (ms_b / 1e3) / 1e9
+    return {"what": "batched FP16-storage learned-thin-layer solver (4-cell CFS-PML + boundary "
+                    "MLP, committed weights) on the same model, 2 shots in one batch",
+            "value": value, "unit": UNIT, "ms_per_step": ms_b / K, "members": len(ms),
+            "plain_fp32_pml20_value": plain_value, "plain_fp32_pml20_ms_per_step": plain_ms,
+            "speedup_vs_plain_fp32_pml20": value / plain_value, "nonfinite": nbad,
+            "accuracy": "bench.py --target-accuracy STEPS (reflected energy against the "
+                        "20-cell PML, FP16 against FP32 storage)"}
+
+
+def run_target_accuracy(args, local):
+    """Reflected-energy fraction of the thin-layer configurations against the
+    plain 20-cell CFS-PML run, and the seismogram error of FP16 storage
+    against FP32 storage, over args.target_accuracy steps of the workload
+    (surface receivers)."""
+    import cgfd
+    n = args.target_accuracy
+    m20 = build_model(args.config, n + 2)
+    s = cgfd.Solver(m20.desc(device=local))
+    m20.load(s)
+    s.step(n)
+    u20 = s.seismograms()[:3, :, :n].astype(np.float64)
+    s.close()
+    m4 = build_model(args.config, n + 2, nabs=THIN)
+    out = {}
+
+    def refl(u):
+        return float(((u - u20) ** 2).sum() / (u20 ** 2).sum())
+
+    runs = {}
+    for name, storage, mlp in (("pml4_f32", cgfd.STORE_F32, False),
+                               ("pml4_mlp_f32", cgfd.STORE_F32, True),
+                               ("pml4_mlp_f16_batched", cgfd.STORE_F16, True)):
+        b = thin_batch([m4] if storage == cgfd.STORE_F32 else thin_members(m4), storage, local, mlp)
+        b.step(n)
+        b.sync()
+        runs[name] = b.models[0].seismograms()[:3, :, :n].astype(np.float64)
+        b.close()
+        out["reflected_energy_" + name] = refl(runs[name])
+    f16, f32 = runs["pml4_mlp_f16_batched"], runs["pml4_mlp_f32"]
+    out["seismogram_rel_l2_f16_vs_f32"] = [float(np.linalg.norm(f16[c] - f32[c]) /
+                                                 np.linalg.norm(f32[c])) for c in range(3)]
+    line = {"mode": "target accuracy", "workload": workload_name(args.config), "steps": n,
+            "reference": "plain FP32 run with the 20-cell CFS-PML, same grid, surface receivers",
+            **out}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.target_accuracy > 0:
+        run_target_accuracy(args, 0)
         return
     dist, rank, world, local = dist_init(args.gpus)
     if args.config == "batch64":
@@ -446,6 +551,8 @@ def main():
     }
     if e2e:
         line["e2e"] = e2e
+    if not args.no_target and world == 1 and args.storage == "f32" and args.kernel == "fused":
+        line["target"] = run_target(args, value, ms / K, local)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.config, args.cpu_seconds)
     print(json.dumps(line))

@@ -220,10 +220,11 @@ struct SideStream {
 void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *err, void *stream,
                        const SideStream *side = nullptr);
 int pair_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str);
-// A batch of models (FP32 storage) in one persistent launch per stage part:
-// per-model buffers as n x 4 sets, n media, n metrics, n x 3 auxiliaries.
+// A batch of models (one storage type) in one persistent launch per stage
+// part: per-model buffers as n x 4 sets, n media, n metrics, n x 3
+// auxiliaries.
 void *pair_create_batch_plan(int n, const Geom *gs, void *const *sets, const float *const *media,
-                             const float *const *metric, float *const *aux);
+                             const float *const *metric, float *const *aux, int elem);
 // the models' stage arguments, [pattern * 4 + stage][model]
 bool pair_batch_set_args(void *plan, const StageArgs *args);
 // both parts and the traction image of stage rep.rk (step pattern `pattern`)
@@ -233,14 +234,21 @@ void launch_stage_pair_batch(const void *plan, int pattern, const StageArgs &rep
 // learned absorbing layer (mlp.cu): the correction of every layer cell
 // (gain: [depth][9]; delta: 9 x n scratch), and the training features of
 // the layer's cells
+// fw: FW of element type elem, sc: its per-component scales (stored value
+// times sc is the value)
+struct ScaleSet {
+  float sc[NCOMP];
+};
 size_t mlp_delta_smem();
-void launch_mlp_step(const float *fw, size_t fs, const float *lam2mu, const float *irho,
-                     const int4 *cells, int n, const void *w, const float *gain, float *delta,
-                     void *stream);
-void launch_mlp_features(const float *fw, size_t fs, const float *lam2mu, const float *irho,
-                         const int4 *cells, int n, float *xs, float *scales, float *zs,
-                         void *stream);
+void mlp_set_attrs();
+void launch_mlp_step(const void *fw, int elem, size_t fs, const ScaleSet &sc, const float *lam2mu,
+                     const float *irho, const int4 *cells, int n, const void *w, const float *gain,
+                     float *delta, void *stream);
+void launch_mlp_features(const void *fw, int elem, size_t fs, const ScaleSet &sc,
+                         const float *lam2mu, const float *irho, const int4 *cells, int n,
+                         float *xs, float *scales, float *zs, void *stream);
 // the traction image of n models (args: device array, one per model)
-void launch_timg_batch(const StageArgs *args, int n, int max_ni, int max_nj, void *stream);
+void launch_timg_batch(const StageArgs *args, int n, int max_ni, int max_nj, int elem,
+                       void *stream);
 
 }  // namespace cgfd

@@ -1,5 +1,6 @@
 // pair_hv0.cu -- instantiates the paired velocity kernels of RK stage kind
-// 0 (first stage) with FP16 storage for the 8 stencil directions.
+// 0 (first stage) with FP16 storage for the 8 stencil directions,
+// single-model and batched.
 #include "stage_pair_impl.cuh"
 
 namespace cgfd {
@@ -11,5 +12,11 @@ void launch_hv0(const Plan &pl, const Maps &m, const StageArgs &a, int *err, cud
 
 void attrs_hv0() { set_attrs<__half, PART_VEL, 0>(); }
 
+void launch_hv0_b(const Plan &pl, const StageArgs &a, const Work &wk, int *err,
+                 cudaStream_t s) {
+  launch_dirs<__half, PART_VEL, 0, true>(pl, Maps{}, a, wk, err, s);
+}
+
+void attrs_hv0_b() { set_attrs<__half, PART_VEL, 0, true>(); }
 }  // namespace pair
 }  // namespace cgfd

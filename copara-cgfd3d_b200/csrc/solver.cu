@@ -137,9 +137,10 @@ template <typename T>
 __global__ void inject_sources_kernel(SourceArgs s) {
   if (threadIdx.x == 0 && blockIdx.x == 0) inject_sources_body<T>(s);
 }
-// a batch of models (FP32 storage): block b injects model b's sources
+// a batch of models (one storage type): block b injects model b's sources
+template <typename T>
 __global__ void inject_sources_batch_kernel(const SourceArgs *sa) {
-  if (threadIdx.x == 0) inject_sources_body<float>(sa[blockIdx.x]);
+  if (threadIdx.x == 0) inject_sources_body<T>(sa[blockIdx.x]);
 }
 // Focal points (LoadRmom without SrcSmooth, src/calculate.cu:6257-6319):
 // each adds -M(t) / (h^3 J) to its cell's stress RHS; M(t) as the
@@ -193,10 +194,11 @@ template <typename T>
 __global__ void inject_focal_kernel(SourceArgs s) {
   inject_focal_body<T>(s, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
-// a batch of models (FP32 storage): blockIdx.y = model
+// a batch of models (one storage type): blockIdx.y = model
+template <typename T>
 __global__ void inject_focal_batch_kernel(const SourceArgs *sa) {
-  inject_focal_body<float>(sa[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x,
-                           gridDim.x * blockDim.x);
+  inject_focal_body<T>(sa[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x,
+                       gridDim.x * blockDim.x);
 }
 // Smoothed sources (the SrcSmooth forms of LoadMoment, LoadForce and
 // LoadRmom, src/calculate.cu:6147-6175, 6210-6232, 6275-6296): one thread
@@ -243,10 +245,11 @@ template <typename T>
 __global__ void inject_spread_kernel(SourceArgs s) {
   inject_spread_body<T>(s, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
-// a batch of models (FP32 storage): blockIdx.y = model
+// a batch of models (one storage type): blockIdx.y = model
+template <typename T>
 __global__ void inject_spread_batch_kernel(const SourceArgs *sa) {
-  inject_spread_body<float>(sa[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x,
-                            gridDim.x * blockDim.x);
+  inject_spread_body<T>(sa[blockIdx.y], blockIdx.x * blockDim.x + threadIdx.x,
+                        gridDim.x * blockDim.x);
 }
 int spread_blocks(int nsp) { return nsp <= 0 ? 1 : ((nsp + 127) / 128 < 296 ? (nsp + 127) / 128 : 296); }
 void launch_spread(const SourceArgs &s, cudaStream_t st) {
@@ -271,13 +274,10 @@ void launch_sources(const SourceArgs &s, cudaStream_t st) {
 
 // Receiver recording (PWpick, src/calculate.cu:2780-2830) from FW after a
 // step, into seis[(c*nrecv + r)*nt + t]; then advances the step counter.
-struct Scales {
-  float sc[NCOMP];
-};
 template <typename T>
 __device__ void record_body(const T *__restrict__ fw, size_t fstride,
                             const int *__restrict__ cells, int nrecv, int nt,
-                            float *__restrict__ seis, int *step, const Scales &s) {
+                            float *__restrict__ seis, int *step, const ScaleSet &s) {
   const int t = *step;
   for (int q = threadIdx.x; q < 9 * nrecv; q += blockDim.x) {
     const int c = q / nrecv, r = q % nrecv;
@@ -291,22 +291,24 @@ __device__ void record_body(const T *__restrict__ fw, size_t fstride,
 template <typename T>
 __global__ void record_kernel(const T *__restrict__ fw, size_t fstride,
                               const int *__restrict__ cells, int nrecv, int nt,
-                              float *__restrict__ seis, int *step, Scales s) {
+                              float *__restrict__ seis, int *step, ScaleSet s) {
   record_body<T>(fw, fstride, cells, nrecv, nt, seis, step, s);
 }
-// receiver record of one model of a batch (FP32 storage)
+// receiver record of one model of a batch (storage type of the batch)
 struct RecordArgs {
-  const float *fw;
+  const void *fw;
   size_t fstride;
   const int *cells;
   int nrecv, nt;
   float *seis;
   int *step;
-  Scales s;
+  ScaleSet s;
 };
+template <typename T>
 __global__ void record_batch_kernel(const RecordArgs *ra) {
   const RecordArgs &r = ra[blockIdx.x];
-  record_body<float>(r.fw, r.fstride, r.cells, r.nrecv, r.nt, r.seis, r.step, r.s);
+  record_body<T>(static_cast<const T *>(r.fw), r.fstride, r.cells, r.nrecv, r.nt, r.seis, r.step,
+                 r.s);
 }
 
 // multiplies component comp of the four field sets by factor (a power of two:
@@ -344,7 +346,7 @@ __global__ void pgv_kernel(const T *__restrict__ fw, Geom g, float *__restrict__
 // start + n*stride.
 template <typename T>
 __global__ void snapshot_kernel(const T *__restrict__ set, Geom g, int mask, int3 st, int3 cnt,
-                                int3 sd, Scales s, float *__restrict__ out) {
+                                int3 sd, ScaleSet s, float *__restrict__ out) {
   const long per = (long)cnt.x * cnt.y * cnt.z;
   int slot = 0;
   for (int c = 0; c < NCOMP; ++c) {
@@ -695,7 +697,7 @@ void surface_matrices(const cgfd_solver *h, std::vector<float> &out) {
 
 // the receiver record of one step (after its four stages)
 void launch_record(cgfd_solver *h) {
-  Scales s;
+  ScaleSet s;
   for (int c = 0; c < NCOMP; ++c) s.sc[c] = std::ldexp(1.f, h->sexp[c]);
   if (h->elem == ELEM_F16)
     record_kernel<<<1, 256, 0, h->st>>>((const __half *)h->set[0], h->g.fstride, h->d_rcell,
@@ -708,11 +710,18 @@ void launch_record(cgfd_solver *h) {
                                         h->nrecv, h->d.nt, h->d_seis, h->d_step, s);
 }
 
+// the per-component scales of the field sets (1 for FP32 storage)
+ScaleSet field_scales(const cgfd_solver *h) {
+  ScaleSet s;
+  for (int c = 0; c < NCOMP; ++c) s.sc[c] = std::ldexp(1.f, h->sexp[c]);
+  return s;
+}
+
 // the learned layer's correction of FW after a step
-void launch_mlp(cgfd_solver *h) {
+void launch_mlp(cgfd_solver *h, cudaStream_t st) {
   const size_t fs = h->g.fstride;
-  launch_mlp_step((const float *)h->set[0], fs, h->media, h->media + 2 * fs, h->d_mlp_cells,
-                  h->mlp_n, h->d_mlp_w, h->d_mlp_gain, h->d_mlp_delta, h->st);
+  launch_mlp_step(h->set[0], h->elem, fs, field_scales(h), h->media, h->media + 2 * fs,
+                  h->d_mlp_cells, h->mlp_n, h->d_mlp_w, h->d_mlp_gain, h->d_mlp_delta, st);
 }
 
 // the peak-velocity update of one step
@@ -847,7 +856,7 @@ int enqueue_step(cgfd_solver *h, int p) {
     if (st) return st;
   }
   if (h->mlp_n) {
-    launch_mlp(h);
+    launch_mlp(h, h->st);
     CK(h, cudaGetLastError());
   }
   launch_record(h);
@@ -1639,7 +1648,7 @@ int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms) {
         if (sst) return sst;
       }
       if (h->mlp_n) {
-        launch_mlp(h);
+        launch_mlp(h, h->st);
         CK(h, cudaGetLastError());
       }
       launch_record(h);
@@ -1916,6 +1925,7 @@ int cgfd_test_withhold_copy(cgfd_solver *h, double wait_limit_s, int withhold) {
 struct cgfd_batch {
   std::vector<cgfd_solver *> m;
   int device = 0;
+  int elem = ELEM_F32;           // the members' storage type
   cudaStream_t st = nullptr;
   void *plan = nullptr;
   int *d_err = nullptr;
@@ -1957,27 +1967,36 @@ static void batch_free(cgfd_batch *b) {
 
 // the batched step of pattern p: per stage one launch per part over every
 // model, the traction image, the sources; then the receiver record
+template <typename T>
+static void batch_sources(cgfd_batch *b, int rk) {
+  const int n = (int)b->m.size();
+  if (b->any_src)
+    inject_sources_batch_kernel<T><<<n, 32, 0, b->st>>>(b->d_src + (size_t)rk * n);
+  if (b->max_foc > 0)  // after the point sources (both may touch a cell)
+    inject_focal_batch_kernel<T><<<dim3(focal_blocks(b->max_foc), n), 128, 0, b->st>>>(
+        b->d_src + (size_t)rk * n);
+  if (b->max_sp > 0)  // the smoothed sources last
+    inject_spread_batch_kernel<T><<<dim3(spread_blocks(b->max_sp), n), 128, 0, b->st>>>(
+        b->d_src + (size_t)rk * n);
+}
+
 static int batch_enqueue(cgfd_batch *b, int p, const std::vector<StageArgs> &args) {
   const int n = (int)b->m.size();
   for (int rk = 0; rk < 4; ++rk) {
     launch_stage_pair_batch(b->plan, p, args[(size_t)(p * 4 + rk) * n], b->d_err, b->st);
     BCK(b, cudaGetLastError());
-    if (b->any_src) {
-      inject_sources_batch_kernel<<<n, 32, 0, b->st>>>(b->d_src + (size_t)rk * n);
-      BCK(b, cudaGetLastError());
-    }
-    if (b->max_foc > 0) {  // after the point sources (both may touch a cell)
-      inject_focal_batch_kernel<<<dim3(focal_blocks(b->max_foc), n), 128, 0, b->st>>>(
-          b->d_src + (size_t)rk * n);
-      BCK(b, cudaGetLastError());
-    }
-    if (b->max_sp > 0) {  // the smoothed sources last
-      inject_spread_batch_kernel<<<dim3(spread_blocks(b->max_sp), n), 128, 0, b->st>>>(
-          b->d_src + (size_t)rk * n);
-      BCK(b, cudaGetLastError());
-    }
+    if (b->elem == ELEM_F16) batch_sources<__half>(b, rk);
+    else if (b->elem == ELEM_BF16) batch_sources<__nv_bfloat16>(b, rk);
+    else batch_sources<float>(b, rk);
+    BCK(b, cudaGetLastError());
   }
-  record_batch_kernel<<<n, 256, 0, b->st>>>(b->d_rec);
+  // the learned layers of the members that have one, after the step
+  for (cgfd_solver *h : b->m)
+    if (h->mlp_n) launch_mlp(h, b->st);
+  BCK(b, cudaGetLastError());
+  if (b->elem == ELEM_F16) record_batch_kernel<__half><<<n, 256, 0, b->st>>>(b->d_rec);
+  else if (b->elem == ELEM_BF16) record_batch_kernel<__nv_bfloat16><<<n, 256, 0, b->st>>>(b->d_rec);
+  else record_batch_kernel<float><<<n, 256, 0, b->st>>>(b->d_rec);
   BCK(b, cudaGetLastError());
   return CGFD_OK;
 }
@@ -2006,14 +2025,14 @@ static int batch_build(cgfd_batch *b) {
     if (h->nfoc > b->max_foc) b->max_foc = h->nfoc;
     if (h->sp_n > b->max_sp) b->max_sp = h->sp_n;
     RecordArgs &r = rec[i];
-    r.fw = (const float *)h->set[0];
+    r.fw = h->set[0];
     r.fstride = h->g.fstride;
     r.cells = h->d_rcell;
     r.nrecv = h->nrecv;
     r.nt = h->d.nt;
     r.seis = h->d_seis;
     r.step = h->d_step;
-    for (int c = 0; c < NCOMP; ++c) r.s.sc[c] = 1.f;
+    r.s = field_scales(h);
   }
   if (!b->plan) {
     std::vector<Geom> gs(n);
@@ -2029,7 +2048,7 @@ static int batch_build(cgfd_batch *b) {
       for (int d = 0; d < 3; ++d) aux[(size_t)3 * i + d] = h->aux[d];
     }
     b->plan = pair_create_batch_plan(n, gs.data(), sets.data(), media.data(), metric.data(),
-                                     aux.data());
+                                     aux.data(), b->elem);
     if (!b->plan) return batch_fail(b, CGFD_ERR_CUDA, "batch plan (tensor maps or work list)");
   }
   if (!pair_batch_set_args(b->plan, args.data()))
@@ -2062,8 +2081,8 @@ int cgfd_batch_create(const cgfd_desc *descs, int n, cgfd_batch **out) {
   if (!descs || !out || n < 1) return batch_fail(nullptr, CGFD_ERR_ARG, "bad batch arguments");
   *out = nullptr;
   for (int i = 0; i < n; ++i) {
-    if (descs[i].storage != CGFD_STORE_F32)
-      return batch_fail(nullptr, CGFD_ERR_ARG, "batched models use FP32 storage");
+    if (descs[i].storage != descs[0].storage)
+      return batch_fail(nullptr, CGFD_ERR_ARG, "batched models share one storage type");
     if (descs[i].kernel != CGFD_KERNEL_FUSED)
       return batch_fail(nullptr, CGFD_ERR_ARG, "batched models use the default kernel family");
     if (descs[i].device != descs[0].device)
@@ -2071,6 +2090,9 @@ int cgfd_batch_create(const cgfd_desc *descs, int n, cgfd_batch **out) {
   }
   cgfd_batch *b = new cgfd_batch();
   b->device = descs[0].device;
+  b->elem = descs[0].storage == CGFD_STORE_F16    ? ELEM_F16
+            : descs[0].storage == CGFD_STORE_BF16 ? ELEM_BF16
+                                                  : ELEM_F32;
   for (int i = 0; i < n; ++i) {
     cgfd_solver *h = nullptr;
     int st = cgfd_create(&descs[i], &h);
@@ -2302,7 +2324,7 @@ int cgfd_get_snapshot(cgfd_solver *h, int set, const int *start, const int *coun
   CK(h, cudaStreamSynchronize(h->st));
   float *tmp = nullptr;
   CK(h, cudaMalloc(&tmp, n * sizeof(float)));
-  Scales sc;
+  ScaleSet sc;
   for (int c = 0; c < NCOMP; ++c) sc.sc[c] = std::ldexp(1.f, h->sexp[c]);
   const int3 st3 = make_int3(start[0], start[1], start[2]);
   const int3 cn3 = make_int3(count[0], count[1], count[2]);
@@ -2407,7 +2429,6 @@ int cgfd_set_boundary_mlp(cgfd_solver *h, int width, const void *weights_fp16) {
   h->mlp_ijk.clear();
   invalidate(h);
   if (!weights_fp16) return CGFD_OK;
-  if (h->elem != ELEM_F32) return arg_fail(h, "the learned layer needs FP32 storage");
   const int ni = h->d.ni, nj = h->d.nj, nk = h->d.nk;
   if (width < 1 || width > 16 || ni < width + 5 || nj < width + 5 || nk < width + 5)
     return arg_fail(h, "bad layer width for this grid");
@@ -2441,6 +2462,7 @@ int cgfd_set_boundary_mlp(cgfd_solver *h, int width, const void *weights_fp16) {
   CK(h, cudaMalloc(&h->d_mlp_cells, cells.size() * sizeof(int4)));
   CK(h, cudaMemcpy(h->d_mlp_cells, cells.data(), cells.size() * sizeof(int4),
                    cudaMemcpyHostToDevice));
+  mlp_set_attrs();
   CK(h, cudaMalloc(&h->d_mlp_w, CGFD_MLP_PARAMS * 2));
   CK(h, cudaMemcpy(h->d_mlp_w, weights_fp16, CGFD_MLP_PARAMS * 2, cudaMemcpyHostToDevice));
   CK(h, cudaMalloc(&h->d_mlp_delta, (size_t)9 * h->mlp_n * sizeof(float)));
@@ -2480,7 +2502,8 @@ int cgfd_boundary_mlp_features(cgfd_solver *h, float *x, float *scale, float *rh
   const size_t n = h->mlp_n, fs = h->g.fstride;
   float *d = nullptr;
   CK(h, cudaMalloc(&d, n * (45 + 2) * sizeof(float)));
-  launch_mlp_features((const float *)h->set[0], fs, h->media, h->media + 2 * fs, h->d_mlp_cells,
+  launch_mlp_features(h->set[0], h->elem, fs, field_scales(h), h->media, h->media + 2 * fs,
+                      h->d_mlp_cells,
                       h->mlp_n, d, d + n * 45, d + n * 46, h->st);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(x, d, n * 45 * sizeof(float), cudaMemcpyDeviceToHost, h->st);

@@ -83,6 +83,8 @@ void set_all_attrs() {
   attrs_hv0(); attrs_hv1(); attrs_hv2(); attrs_hs0(); attrs_hs1(); attrs_hs2();
   attrs_bv0(); attrs_bv1(); attrs_bv2(); attrs_bs0(); attrs_bs1(); attrs_bs2();
   attrs_fv0_b(); attrs_fv1_b(); attrs_fv2_b(); attrs_fs0_b(); attrs_fs1_b(); attrs_fs2_b();
+  attrs_hv0_b(); attrs_hv1_b(); attrs_hv2_b(); attrs_hs0_b(); attrs_hs1_b(); attrs_hs2_b();
+  attrs_bv0_b(); attrs_bv1_b(); attrs_bv2_b(); attrs_bs0_b(); attrs_bs1_b(); attrs_bs2_b();
   done = true;
 }
 
@@ -277,8 +279,8 @@ bool upload_items(Plan *pl, const std::vector<int4> &hv, int rv, int rs) {
 
 void resident(int elem, bool batch, int *rv, int *rs) {
   if (batch) {
-    *rv = resident_fv_b();
-    *rs = resident_fs_b();
+    *rv = elem == ELEM_F16 ? resident_hv_b() : elem == ELEM_BF16 ? resident_bv_b() : resident_fv_b();
+    *rs = elem == ELEM_F16 ? resident_hs_b() : elem == ELEM_BF16 ? resident_bs_b() : resident_fs_b();
   } else {
     *rv = elem == ELEM_F16 ? resident_hv() : elem == ELEM_BF16 ? resident_bv() : resident_fv();
     *rs = elem == ELEM_F16 ? resident_hs() : elem == ELEM_BF16 ? resident_bs() : resident_fs();
@@ -383,18 +385,18 @@ void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *er
 // ---------------------------- batched models ------------------------------
 
 void *pair_create_batch_plan(int n, const Geom *gs, void *const *sets, const float *const *media,
-                             const float *const *metric, float *const *aux) {
+                             const float *const *metric, float *const *aux, int elem) {
   set_all_attrs();
   Plan *pl = new (std::nothrow) Plan();
   if (!pl) return nullptr;
-  pl->elem = ELEM_F32;
+  pl->elem = elem;
   pl->nmodels = n;
   pl->geoms.assign(gs, gs + n);
   pl->mm.resize(n);
   bool ok = true;
   for (int i = 0; i < n && ok; ++i) {
     int ha[3];
-    ok = model_maps(&pl->mm[i], ha, gs[i], ELEM_F32, sets + 4 * i, media[i], metric[i],
+    ok = model_maps(&pl->mm[i], ha, gs[i], elem, sets + 4 * i, media[i], metric[i],
                     aux + 3 * i);
   }
   // per stage, part and model: the maps of that stage (input set per stage
@@ -433,17 +435,22 @@ void launch_stage_pair_batch(const void *plan, int pattern, const StageArgs &rep
   wv.bmaps = pl.d_bmaps + (size_t)(rk * 2) * n;
   ws.bmaps = pl.d_bmaps + (size_t)(rk * 2 + 1) * n;
   typedef void (*LaunchFn)(const Plan &, const StageArgs &, const Work &, int *, cudaStream_t);
-  static const LaunchFn fv[3] = {launch_fv0_b, launch_fv1_b, launch_fv2_b};
-  static const LaunchFn fs[3] = {launch_fs0_b, launch_fs1_b, launch_fs2_b};
+  static const LaunchFn fv[3][3] = {{launch_fv0_b, launch_fv1_b, launch_fv2_b},
+                                    {launch_hv0_b, launch_hv1_b, launch_hv2_b},
+                                    {launch_bv0_b, launch_bv1_b, launch_bv2_b}};
+  static const LaunchFn fs[3][3] = {{launch_fs0_b, launch_fs1_b, launch_fs2_b},
+                                    {launch_hs0_b, launch_hs1_b, launch_hs2_b},
+                                    {launch_bs0_b, launch_bs1_b, launch_bs2_b}};
+  const int e = pl.elem == ELEM_F16 ? 1 : pl.elem == ELEM_BF16 ? 2 : 0;
   cudaMemsetAsync(pl.wk.counter, 0, 2 * sizeof(int), s);
-  fv[kind](pl, rep, wv, err, s);
-  fs[kind](pl, rep, ws, err, s);
+  fv[e][kind](pl, rep, wv, err, s);
+  fs[e][kind](pl, rep, ws, err, s);
   int mi = 0, mj = 0;
   for (const Geom &g : pl.geoms) {
     mi = g.ni > mi ? g.ni : mi;
     mj = g.nj > mj ? g.nj : mj;
   }
-  launch_timg_batch(wv.bargs, n, mi, mj, s);
+  launch_timg_batch(wv.bargs, n, mi, mj, pl.elem, s);
 }
 
 int pair_plan_info(const void *plan, int *zchunk, int *grid_vel, int *grid_str) {

@@ -1020,16 +1020,16 @@ int resident_ctas() {
 }
 
 // per-(storage, part, kind) entry points, one translation unit each
-// (pair_{f,h,b}{v,s}{0,1,2}.cu; f: FP32, h: FP16, b: BF16 storage); the
-// FP32 units also hold the batched kernels (suffix _b)
+// (pair_{f,h,b}{v,s}{0,1,2}.cu; f: FP32, h: FP16, b: BF16 storage), each
+// with its batched kernels (suffix _b)
 #define CGFD_PAIR_DECL(E, P, K)                                                          \
   void launch_##E##P##K(const Plan &pl, const Maps &m, const StageArgs &a, int *err,   \
                         cudaStream_t s);                                                \
   void attrs_##E##P##K();
-#define CGFD_PAIR_DECL_B(P, K)                                                           \
-  void launch_f##P##K##_b(const Plan &pl, const StageArgs &a, const Work &wk, int *err, \
-                          cudaStream_t s);                                              \
-  void attrs_f##P##K##_b();
+#define CGFD_PAIR_DECL_B(E, P, K)                                                        \
+  void launch_##E##P##K##_b(const Plan &pl, const StageArgs &a, const Work &wk, int *err, \
+                            cudaStream_t s);                                            \
+  void attrs_##E##P##K##_b();
 #define CGFD_PAIR_DECL_E(E)                                                   \
   CGFD_PAIR_DECL(E, v, 0) CGFD_PAIR_DECL(E, v, 1) CGFD_PAIR_DECL(E, v, 2)     \
   CGFD_PAIR_DECL(E, s, 0) CGFD_PAIR_DECL(E, s, 1) CGFD_PAIR_DECL(E, s, 2)     \
@@ -1038,10 +1038,15 @@ int resident_ctas() {
 CGFD_PAIR_DECL_E(f)
 CGFD_PAIR_DECL_E(h)
 CGFD_PAIR_DECL_E(b)
-CGFD_PAIR_DECL_B(v, 0) CGFD_PAIR_DECL_B(v, 1) CGFD_PAIR_DECL_B(v, 2)
-CGFD_PAIR_DECL_B(s, 0) CGFD_PAIR_DECL_B(s, 1) CGFD_PAIR_DECL_B(s, 2)
-int resident_fv_b();
-int resident_fs_b();
+#define CGFD_PAIR_DECL_BE(E)                                                         \
+  CGFD_PAIR_DECL_B(E, v, 0) CGFD_PAIR_DECL_B(E, v, 1) CGFD_PAIR_DECL_B(E, v, 2)          \
+  CGFD_PAIR_DECL_B(E, s, 0) CGFD_PAIR_DECL_B(E, s, 1) CGFD_PAIR_DECL_B(E, s, 2)          \
+  int resident_##E##v_b();                                                            \
+  int resident_##E##s_b();
+CGFD_PAIR_DECL_BE(f)
+CGFD_PAIR_DECL_BE(h)
+CGFD_PAIR_DECL_BE(b)
+#undef CGFD_PAIR_DECL_BE
 #undef CGFD_PAIR_DECL_B
 #undef CGFD_PAIR_DECL_E
 #undef CGFD_PAIR_DECL

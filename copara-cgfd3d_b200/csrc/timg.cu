@@ -135,18 +135,23 @@ __global__ void __launch_bounds__(128) timg_kernel(StageArgs a) {
 }
 
 // n models: blockIdx.z = model * 3 + layer; the grid covers the largest model
+template <typename T>
 __global__ void __launch_bounds__(128) timg_batch_kernel(const StageArgs *args) {
   const StageArgs &a = args[blockIdx.z / 3];
-  timg_cell<float>(a, blockIdx.x * 32 + threadIdx.x, blockIdx.y * 4 + threadIdx.y,
-                   a.g.top - 2 + (int)(blockIdx.z % 3));
+  timg_cell<T>(a, blockIdx.x * 32 + threadIdx.x, blockIdx.y * 4 + threadIdx.y,
+               a.g.top - 2 + (int)(blockIdx.z % 3));
 }
 
 }  // namespace
 
-void launch_timg_batch(const StageArgs *args, int n, int max_ni, int max_nj, void *stream) {
+void launch_timg_batch(const StageArgs *args, int n, int max_ni, int max_nj, int elem,
+                       void *stream) {
   dim3 block(32, 4, 1);
   dim3 grid((max_ni + 31) / 32, (max_nj + 3) / 4, 3 * n);
-  timg_batch_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(args);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (elem == ELEM_F16) timg_batch_kernel<__half><<<grid, block, 0, s>>>(args);
+  else if (elem == ELEM_BF16) timg_batch_kernel<__nv_bfloat16><<<grid, block, 0, s>>>(args);
+  else timg_batch_kernel<float><<<grid, block, 0, s>>>(args);
 }
 
 void launch_timg(const StageArgs &a, void *stream) {

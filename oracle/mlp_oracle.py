@@ -96,3 +96,66 @@ def init_weights(seed=0, scale=1.0):
     w[OW2:OB2] = rng.standard_normal(NH * NH) * scale / np.sqrt(NH)
     w[OW3:OB3] = rng.standard_normal(NOUT * NH) * scale / np.sqrt(NH)
     return w.astype(np.float16)
+
+
+def forward_fp16(w, x):
+    """forward() with the device inference's roundings: the features and
+    both hidden layers' SiLU outputs rounded to FP16 (the tensor-core
+    operands), sums in float64."""
+    W1, b1, W2, b2, W3, b3 = unpack(w)
+    x = np.asarray(x, np.float32).astype(np.float16).astype(np.float64)
+    h1 = silu(x @ W1.T + b1).astype(np.float16).astype(np.float64)
+    h2 = silu(h1 @ W2.T + b2).astype(np.float16).astype(np.float64)
+    return h2 @ W3.T + b3
+
+
+def layer_cells(ni, nj, nk, nabs, width):
+    """The layer cells of the solver's learned layer (csrc/solver.cu:
+    cgfd_set_boundary_mlp), in its order (i, then j, then k): valid cells
+    within `width` of an absorbing face (never the free surface), each with
+    the inward unit step of its nearest face (ties x-, x+, y-, y+, z-) and
+    its depth in the layer.  Returns (ijk (n, 3) in reference indices,
+    step (n, 3), depth (n,))."""
+    ijk, step, depth = [], [], []
+    dirs = [(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1)]
+    for i in range(ni):
+        for j in range(nj):
+            for k in range(nk):
+                dist = [i if nabs[0] > 0 else 1 << 30, ni - 1 - i if nabs[1] > 0 else 1 << 30,
+                        j if nabs[2] > 0 else 1 << 30, nj - 1 - j if nabs[3] > 0 else 1 << 30,
+                        k if nabs[4] > 0 else 1 << 30]
+                best, bd = -1, width
+                for f in range(5):
+                    if dist[f] < bd:
+                        bd, best = dist[f], f
+                if best < 0:
+                    continue
+                ijk.append((i + 3, j + 3, k + 3))
+                step.append(dirs[best])
+                depth.append(bd)
+    return np.array(ijk), np.array(step), np.array(depth)
+
+
+def apply_layer(fields, rho, vp, cells, w, gains, fp16=True):
+    """The learned layer's correction of FW (fields [9][nx][ny][nz], float64,
+    changed in place) after a step: features of every layer cell from the
+    uncorrected fields, then all corrections added (csrc/mlp.cu)."""
+    ijk, step, depth = cells
+    n = len(ijk)
+    z = np.array([rho[tuple(p)] * vp[tuple(p)] for p in ijk], np.float64)
+    x = np.zeros((n, NIN))
+    for s in range(5):
+        p = ijk + s * step
+        for c in range(NOUT):
+            v = fields[c][p[:, 0], p[:, 1], p[:, 2]]
+            x[:, s * NOUT + c] = v / z if c >= 3 else v
+    scale = np.abs(x).max(axis=1)
+    on = scale > 1e-30
+    x[on] /= scale[on, None]
+    y = forward_fp16(w, x) if fp16 else forward(w, x)[0]
+    d = correction(y, x[:, :9], np.asarray(gains)[depth]) * scale[:, None]
+    d[:, 3:] *= z[:, None]
+    d[~on] = 0.0
+    for c in range(NOUT):
+        fields[c][ijk[:, 0], ijk[:, 1], ijk[:, 2]] += d[:, c]
+    return fields
