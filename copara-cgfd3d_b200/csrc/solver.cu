@@ -2447,10 +2447,13 @@ int cgfd_set_boundary_mlp(cgfd_solver *h, int width, const void *weights_fp16) {
     return best;
   };
   const long step[5] = {1, -1, (long)h->g.px, -(long)h->g.px, (long)h->g.plane};
+  // cells in the order of the field layout (x fastest): neighbouring cells of
+  // the list are neighbours in memory, so the correction kernels' gathers of
+  // 16 consecutive cells are coalesced
   std::vector<int4> cells;
-  for (int i = 0; i < ni; ++i)
+  for (int k = 0; k < nk; ++k)
     for (int j = 0; j < nj; ++j)
-      for (int k = 0; k < nk; ++k) {
+      for (int i = 0; i < ni; ++i) {
         const int f = face(i, j, k);
         if (f < 0) continue;
         cells.push_back(

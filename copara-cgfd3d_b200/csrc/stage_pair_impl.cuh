@@ -49,6 +49,7 @@
 #include <cudaTypedefs.h>
 
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 namespace cgfd {
@@ -687,6 +688,7 @@ __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, cons
 }
 
 // ------------------------------ the march ---------------------------------
+static_assert(sizeof(StageArgs) % 4 == 0, "stage arguments are copied in 4-byte words");
 // items: tile index fastest, so the CTAs resident at one time work on
 // neighbouring tiles of the same z-chunk and share halo rows in L2
 template <typename T, int PART, int X, int Y, int Z, int KIND, bool B>
@@ -743,9 +745,15 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
     const int4 it4 = wk.items[cur];
     const int model = B ? it4.w : 0;
     if (B) {  // this item's model: its stage arguments into shared memory
-      const uint32_t *src = reinterpret_cast<const uint32_t *>(wk.bargs + model);
-      uint32_t *dst = reinterpret_cast<uint32_t *>(&s_args);
-      for (int w = tid; w < (int)(sizeof(StageArgs) / 4); w += TT) dst[w] = src[w];
+      // Copied as bytes (memcpy may alias any type).  A copy through
+      // uint32_t lvalues let the compiler treat the float fields read later
+      // (the 16-bit scales sc / isc) as unwritten inside the item loop and
+      // hoist their loads above the first copy: every batched 16-bit stage
+      // then ran with zero scales.
+      const unsigned char *src = reinterpret_cast<const unsigned char *>(wk.bargs + model);
+      unsigned char *dst = reinterpret_cast<unsigned char *>(&s_args);
+      for (int w = tid; w < (int)(sizeof(StageArgs) / 4); w += TT)
+        memcpy(dst + 4 * w, src + 4 * w, 4);
       __syncthreads();
     }
     const StageArgs &A = B ? s_args : a;

@@ -384,8 +384,9 @@ def hill_256(nt=40, nabs=(20, 20, 20, 20, 20, 0)) -> Model:
 
 def small_flat(nt=40, ni=28, nj=24, nk=20, **kw) -> Model:
     kw.setdefault("nabs", (5, 5, 5, 5, 5, 0))
+    kw.setdefault("src_depth", 600.0)
     return flat_halfspace(ni=ni, nj=nj, nk=nk, h=100.0, dt=0.008, nt=nt,
-                          src_depth=600.0, f0=4.0, t0=0.3, n_side=3,
+                          f0=4.0, t0=0.3, n_side=3,
                           rcv_spacing=400.0, con_depth=800.0, name="small_flat", **kw)
 
 
@@ -406,8 +407,9 @@ def batch_models(n=64, seed=7, nt=1000, side=(96, 256), nabs_cells=12, h=100.0,
     (nz = side/2), Gaussian hill height U(0, 2000) m and width U(1, 5) km,
     two layers with vp U(3000, 7000) and vs = vp/1.73 (density 2600/2800), a
     random point moment source (M_ij ~ N(0, 1) x 1e15) with a Ricker STF of
-    f0 U(1, 4) Hz, 5 x 5 surface receivers, 12-cell CFS-PML, dt from a CFL
-    number of 0.8 (vp_max dt / min spacing); seeded."""
+    f0 U(1, 4) Hz, 5 x 5 surface receivers, 12-cell CFS-PML, dt at 0.8 of
+    the reference's stability bound 1.3 dmin / vp_max (src/mediaparas.cpp:2263;
+    dmin = the top vertical spacing, the smallest of the grid); seeded."""
     rng = np.random.default_rng(seed)
     out = []
     for q in range(n):
@@ -417,7 +419,7 @@ def batch_models(n=64, seed=7, nt=1000, side=(96, 256), nabs_cells=12, h=100.0,
         hill_w = float(rng.uniform(1000.0, 5000.0))
         vp1, vp2 = sorted(rng.uniform(3000.0, 7000.0, 2))
         dz_top, dz_bot = 0.5 * h, 1.5 * h
-        dt = 0.8 * dz_top / max(vp1, vp2)
+        dt = 0.8 * 1.3 * min(dz_top, h) / max(vp1, vp2)
         f0 = float(rng.uniform(1.0, 4.0))
         depth = nk * h
         m = gaussian_hill(ni=s, nj=s, nk=nk, h=h, dt=dt, nt=nt, dz_top=dz_top, dz_bot=dz_bot,

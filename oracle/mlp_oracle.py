@@ -111,16 +111,17 @@ def forward_fp16(w, x):
 
 def layer_cells(ni, nj, nk, nabs, width):
     """The layer cells of the solver's learned layer (csrc/solver.cu:
-    cgfd_set_boundary_mlp), in its order (i, then j, then k): valid cells
+    cgfd_set_boundary_mlp), in its order (k, then j, then i: i fastest, as
+    the solver's field layout): valid cells
     within `width` of an absorbing face (never the free surface), each with
     the inward unit step of its nearest face (ties x-, x+, y-, y+, z-) and
     its depth in the layer.  Returns (ijk (n, 3) in reference indices,
     step (n, 3), depth (n,))."""
     ijk, step, depth = [], [], []
     dirs = [(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1)]
-    for i in range(ni):
+    for k in range(nk):
         for j in range(nj):
-            for k in range(nk):
+            for i in range(ni):
                 dist = [i if nabs[0] > 0 else 1 << 30, ni - 1 - i if nabs[1] > 0 else 1 << 30,
                         j if nabs[2] > 0 else 1 << 30, nj - 1 - j if nabs[3] > 0 else 1 << 30,
                         k if nabs[4] > 0 else 1 << 30]

@@ -1,15 +1,21 @@
 """16-bit field storage (FP16 with per-component power-of-two scales, BF16):
 the nine wavefields and the RK registers are stored at 16 bits, the
 arithmetic stays FP32.  There is no reference counterpart to match bit for
-bit; the checks are accuracy bounds against the solver's own FP32 storage
-(which matches the reference within 1e-5) on the same inputs, plus exact
-properties of the storage conversions and scales.
+bit; the checks are accuracy bounds against the FP64 oracle's seismograms
+(tests/golden/c1_fp64_seismograms.npz, made by make_c1_fp64.py) and
+against the solver's own FP32 storage (which matches the reference within
+1e-5) on the same inputs, plus exact properties of the storage conversions
+and scales.
 
-Measured on a B200 (seismogram relative L2 of Vx..Vz against FP32 storage):
-small flat 60 steps FP16 1.7e-3 / BF16 1.5e-2; small hill FP16 2.8e-3 / BF16
-9.3e-3; the 160x160x80 flat half-space, 500 steps, FP16 7.0e-3 / BF16 6.3e-2.
-The bounds below leave about 3x margin.
+Measured on a B200 (seismogram relative L2 of Vx..Vz): small flat 60 steps
+FP16 1.7e-3 / BF16 1.5e-2 against FP32 storage; small hill FP16 2.8e-3 /
+BF16 9.3e-3; the 160x160x80 flat half-space, 500 steps, against the FP64
+oracle: FP16 7.0e-3, BF16 6.3e-2 (peak amplitude 0.14% / 2.9%).  The bounds
+sit 10-25% above these: a regression shows.  Where the FP16 error comes
+from (which stored set) is measured on the CPU in test_storage_emulation.py.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -31,8 +37,8 @@ def _run(m, steps, storage):
     return seis, nbad, scales
 
 
-@pytest.mark.parametrize("name,bound", [("small_flat", {"f16": 6e-3, "bf16": 5e-2}),
-                                        ("small_hill", {"f16": 1e-2, "bf16": 3e-2})])
+@pytest.mark.parametrize("name,bound", [("small_flat", {"f16": 2.2e-3, "bf16": 1.9e-2}),
+                                        ("small_hill", {"f16": 3.5e-3, "bf16": 1.2e-2})])
 @pytest.mark.parametrize("store", list(STORES))
 def test_16bit_storage_tracks_fp32_storage(name, bound, store):
     m = getattr(models, name)(nt=60)
@@ -43,15 +49,19 @@ def test_16bit_storage_tracks_fp32_storage(name, bound, store):
     assert e < bound[store], (name, store, e, scales)
 
 
-@pytest.mark.parametrize("store,bound,peak", [("f16", 2e-2, 1e-2), ("bf16", 0.2, 0.1)])
+@pytest.mark.parametrize("store,bound,peak", [("f16", 8e-3, 2e-3), ("bf16", 7e-2, 3.5e-2)])
 def test_flat_halfspace_160x160x80_500_steps_16bit(store, bound, peak):
-    """The FP16/BF16 variant of the 160x160x80 flat half-space model."""
+    """The FP16/BF16 variant of the 160x160x80 flat half-space model against
+    the FP64 oracle's seismograms (and FP32 storage against the same, 1e-5)."""
     m = models.config_c1()
+    gold = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                "c1_fp64_seismograms.npz"))["seis"]
     ref, _, _ = _run(m, m.nt, cgfd.STORE_F32)
     seis, nbad, scales = _run(m, m.nt, STORES[store])
     assert nbad == 0
-    assert rel_l2(seis[:3], ref[:3]) < bound
-    pk, pk_ref = np.abs(seis[:3]).max(), np.abs(ref[:3]).max()
+    assert rel_l2(ref[:3], gold) < 1e-5
+    assert rel_l2(seis[:3], gold) < bound
+    pk, pk_ref = np.abs(seis[:3]).max(), np.abs(gold).max()
     assert abs(pk - pk_ref) / pk_ref < peak
     if store == "f16":
         assert scales[0] != 0 or scales[3] != 0  # the automatic scales were set

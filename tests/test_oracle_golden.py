@@ -16,10 +16,12 @@ TOL = 1e-5
 
 
 def _golden_names():
-    # the stepping fixtures (the vmap-grid and source fixtures, grid_vmap_*
-    # and source_*, have their own tests)
+    # the stepping fixtures of the reference's runtime (the vmap-grid, source,
+    # output and par-file fixtures and the FP64 oracle's c1_fp64_* have their
+    # own tests)
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith(("grid_vmap_", "source_", "outputs_", "parfiles_")))
+                  if not os.path.basename(p).startswith(("grid_vmap_", "source_", "outputs_",
+                                                         "parfiles_", "c1_fp64_")))
 
 
 def test_golden_set_is_complete():

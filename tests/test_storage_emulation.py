@@ -1,0 +1,70 @@
+"""Where the error of 16-bit field storage comes from (CPU, FP64 oracle).
+
+The FP64 oracle can round any of the stored field sets -- the stage outputs
+W, the RK accumulator tW, the step state FW -- to an IEEE format after every
+write, as the solver's 16-bit storage does (orc_set_storage_emulation;
+per-component power-of-two scales putting each component's maximum at 2^12,
+as the solver's automatic FP16 scales do).  Rounding one set at a time
+localises the seismogram error of FP16 storage: on the small flat model the
+RK accumulator tW contributes most (it is rounded twice a step and carries
+the whole state), then FW, then W; keeping tW as its difference from FW
+(small, so rounded far more finely) removes most of it.  The same
+measurements on the 160x160x80 flat half-space over 500 steps (a few minutes
+each, not run here) give 7.1e-3 for all sets (the GPU's FP16 storage: 7.0e-3),
+5.8e-3 for tW alone, 3.5e-3 for FW alone and 1.9e-3 for W alone: FP16's
+11-bit significand bounds the error of any one set well above 1e-3 there.
+"""
+import numpy as np
+import pytest
+
+import models
+import pyoracle
+
+
+@pytest.fixture(scope="module")
+def runs():
+    prev = models._PREP
+    models.use_preprocessing("oracle")
+    try:
+        m = models.small_flat(nt=60)
+        out = {}
+
+        def run(key, **em):
+            o = pyoracle.OracleSolver(m.desc(), 0)
+            m.load(o)
+            if em:
+                o.set_storage_emulation(**em)
+            o.step(60)
+            out[key] = o.seismograms()[:3].astype(np.float64)
+            o.close()
+
+        fp16 = dict(ebits=5, mbits=10, adapt=12)
+        run("fp64")
+        run("all", **fp16)
+        run("W", mask=1, **fp16)
+        run("tW", mask=2, **fp16)
+        run("FW", mask=4, **fp16)
+        run("all_tw_delta", flags=1, **fp16)
+        run("bf16", ebits=8, mbits=7)
+    finally:
+        models.use_preprocessing(prev)
+    ref = out.pop("fp64")
+    return {k: float(np.linalg.norm(v - ref) / np.linalg.norm(ref)) for k, v in out.items()}
+
+
+def test_fp16_storage_error_is_localised_by_set(runs):
+    e = runs
+    # measured: all 2.1e-3, tW 1.2e-3, FW 7.5e-4, W 2.9e-4
+    assert 1.5e-3 < e["all"] < 3e-3
+    assert e["tW"] > e["FW"] > e["W"] > 0
+    # the three sets' errors together make up the total (within correlation)
+    q = np.sqrt(e["tW"] ** 2 + e["FW"] ** 2 + e["W"] ** 2)
+    assert 0.5 * e["all"] < q < 1.2 * e["all"]
+
+
+def test_accumulator_as_difference_and_bf16(runs):
+    e = runs
+    # tW kept as tW - FW: 8.8e-4 against 2.1e-3
+    assert e["all_tw_delta"] < 0.5 * e["all"]
+    # BF16's 8-bit significand: 1.4e-2, several times FP16's error
+    assert e["bf16"] > 4 * e["all"]
