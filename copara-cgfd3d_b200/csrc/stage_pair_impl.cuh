@@ -49,7 +49,6 @@
 #include <cudaTypedefs.h>
 
 #include <cstdint>
-#include <cstring>
 #include <vector>
 
 namespace cgfd {
@@ -262,13 +261,21 @@ __device__ __forceinline__ void rk_store2(const StageArgs &a, T *out, T *tw, int
 }
 
 // ADE auxiliaries of one pair and direction: the stage input ai (FA in the
-// first stage, A after) is loaded early (it enters the RHS); the RK update
-// then reads FA and tA of one direction together right before writing A (FA
-// in the final stage) and tA, so that only one direction's values are live.
+// first stage, A after) enters the RHS and is loaded before the stencil
+// arithmetic.  EARLY (FP32 storage, which has the registers): the RK
+// registers of the update (FA and tA in the inner stages, tA in the final
+// one) are loaded with it, so the boundary path pays one memory round trip
+// per plane, hidden behind the stencil.  Otherwise (16-bit storage, three
+// CTAs per SM at 168 registers) the update reads FA and tA of one direction
+// right before writing A (FA in the final stage) and tA, so only one
+// direction's values are live; loading them early there doubled the spills.
 // o0/o1: the cells' indices, m: the cells' mask.
-template <int KIND, int N>
+template <int KIND, int N, bool EARLY>
 struct Aux2 {
+  static constexpr int NU = (KIND == 0 || !EARLY) ? 1 : N, NV = (KIND == 1 && EARLY) ? N : 1;
   f2 ai[N];
+  f2 u[NU];  // EARLY: FA (inner stages) or tA (final stage)
+  f2 v[NV];  // EARLY: tA (inner stages)
   __device__ __forceinline__ void load(const StageArgs &a, int d, size_t o0, size_t o1, int m,
                                        int c0) {
     const size_t as = a.g.astride[d];
@@ -276,46 +283,65 @@ struct Aux2 {
     for (int q = 0; q < N; ++q) {
       const float *b = a.ain[d] + (c0 + q) * as;
       ai[q] = ld2(b + o0, b + o1, m);
+      if constexpr (EARLY && KIND == 1) {
+        const float *f = a.afw[d] + (c0 + q) * as, *t = a.ta[d] + (c0 + q) * as;
+        u[q] = ld2(f + o0, f + o1, m);
+        v[q] = ld2(t + o0, t + o1, m);
+      } else if constexpr (EARLY && KIND == 2) {
+        const float *t = a.ta[d] + (c0 + q) * as;
+        u[q] = ld2(t + o0, t + o1, m);
+      }
     }
   }
   __device__ __forceinline__ void update(const StageArgs &a, int d, size_t o0, size_t o1, int m,
                                          int c0, const f2 *hh) const {
     const size_t as = a.g.astride[d];
-    if (KIND == 0) {
+    if constexpr (KIND == 0) {
 #pragma unroll
       for (int q = 0; q < N; ++q) {
         float *po = a.aout[d] + (c0 + q) * as, *pt = a.ta[d] + (c0 + q) * as;
         st2(po + o0, po + o1, m, fma2(S2(a.adt), hh[q], ai[q]));
         st2(pt + o0, pt + o1, m, fma2(S2(a.bdt), hh[q], ai[q]));
       }
-    } else if (KIND == 1) {
+    } else if constexpr (EARLY) {
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        float *po = a.aout[d] + (c0 + q) * as, *pt = a.ta[d] + (c0 + q) * as;
+        if (KIND == 1) {
+          st2(po + o0, po + o1, m, fma2(S2(a.adt), hh[q], u[q]));
+          st2(pt + o0, pt + o1, m, fma2(S2(a.bdt), hh[q], v[q]));
+        } else {
+          st2(po + o0, po + o1, m, fma2(S2(a.bdt), hh[q], u[q]));
+        }
+      }
+    } else if constexpr (KIND == 1) {
       // FA and tA together: one memory round trip per direction
-      f2 u[N], v[N];
+      f2 fu[N], tv[N];
 #pragma unroll
       for (int q = 0; q < N; ++q) {
         const float *b = a.afw[d] + (c0 + q) * as;
         const float *t = a.ta[d] + (c0 + q) * as;
-        u[q] = ld2(b + o0, b + o1, m);
-        v[q] = ld2(t + o0, t + o1, m);
+        fu[q] = ld2(b + o0, b + o1, m);
+        tv[q] = ld2(t + o0, t + o1, m);
       }
 #pragma unroll
       for (int q = 0; q < N; ++q) {
         float *po = a.aout[d] + (c0 + q) * as;
         float *pt = a.ta[d] + (c0 + q) * as;
-        st2(po + o0, po + o1, m, fma2(S2(a.adt), hh[q], u[q]));
-        st2(pt + o0, pt + o1, m, fma2(S2(a.bdt), hh[q], v[q]));
+        st2(po + o0, po + o1, m, fma2(S2(a.adt), hh[q], fu[q]));
+        st2(pt + o0, pt + o1, m, fma2(S2(a.bdt), hh[q], tv[q]));
       }
     } else {
-      f2 u[N];
+      f2 tu[N];
 #pragma unroll
       for (int q = 0; q < N; ++q) {
         const float *b = a.ta[d] + (c0 + q) * as;
-        u[q] = ld2(b + o0, b + o1, m);
+        tu[q] = ld2(b + o0, b + o1, m);
       }
 #pragma unroll
       for (int q = 0; q < N; ++q) {
         float *po = a.aout[d] + (c0 + q) * as;
-        st2(po + o0, po + o1, m, fma2(S2(a.bdt), hh[q], u[q]));
+        st2(po + o0, po + o1, m, fma2(S2(a.bdt), hh[q], tu[q]));
       }
     }
   }
@@ -428,7 +454,7 @@ __device__ __forceinline__ void vel_pair(const StageArgs &a, const Pair &e, cons
   // general path: issue every auxiliary load before the stencil arithmetic
   const AuxIdx ix(a, e, pl);
   const int mx = e.mx, my = e.ypml ? e.m : 0, mz = pl.zpml ? e.m : 0;
-  Aux2<KIND, 3> ax, ay, az;
+  Aux2<KIND, 3, sizeof(T) == 4> ax, ay, az;
   if (mx) ax.load(a, 0, ix.x0, ix.x1, mx, 0);
   if (my) ay.load(a, 1, ix.y, ix.y + 1, my, 0);
   if (mz) az.load(a, 2, ix.z, ix.z + 1, mz, 0);
@@ -530,7 +556,7 @@ __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, cons
   const bool gen = !pl.lean;
   int mx = 0, my = 0, mz = 0;
   AuxIdx ix;
-  Aux2<KIND, 3> ax, ay, az;
+  Aux2<KIND, 3, sizeof(T) == 4> ax, ay, az;
   if (gen) {
     ix = AuxIdx(a, e, pl);
     mx = e.mx;
@@ -744,19 +770,22 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
     if (cur >= wk.nitems || abort_flag) break;  // CTA-uniform
     const int4 it4 = wk.items[cur];
     const int model = B ? it4.w : 0;
-    if (B) {  // this item's model: its stage arguments into shared memory
-      // Copied as bytes (memcpy may alias any type).  A copy through
-      // uint32_t lvalues let the compiler treat the float fields read later
-      // (the 16-bit scales sc / isc) as unwritten inside the item loop and
-      // hoist their loads above the first copy: every batched 16-bit stage
-      // then ran with zero scales.
-      const unsigned char *src = reinterpret_cast<const unsigned char *>(wk.bargs + model);
-      unsigned char *dst = reinterpret_cast<unsigned char *>(&s_args);
-      for (int w = tid; w < (int)(sizeof(StageArgs) / 4); w += TT)
-        memcpy(dst + 4 * w, src + 4 * w, 4);
+    // a batched launch copies the item's model's stage arguments into shared
+    // memory and reads them through a pointer the compiler cannot trace to
+    // that variable (generic loads).  Read through the __shared__ variable
+    // itself, the 16-bit batched stages behaved as if every scale were zero
+    // (measured; FP32 was unaffected); read from global memory in place,
+    // they were correct but a third slower.
+    const StageArgs *Ap = &a;
+    if (B) {
+      const uint32_t *src = reinterpret_cast<const uint32_t *>(wk.bargs + model);
+      uint32_t *dst = reinterpret_cast<uint32_t *>(&s_args);
+      for (int w = tid; w < (int)(sizeof(StageArgs) / 4); w += TT) dst[w] = src[w];
       __syncthreads();
+      Ap = &s_args;
+      asm volatile("" : "+l"(Ap)::"memory");
     }
-    const StageArgs &A = B ? s_args : a;
+    const StageArgs &A = *Ap;
     const Maps &M = B ? wk.bmaps[model] : maps;
     const Geom &g = A.g;
     const size_t fs = g.fstride;

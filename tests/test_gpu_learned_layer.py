@@ -129,10 +129,17 @@ def _oracle_with_layer(m, steps, w, gains, width=4):
 
 def test_batched_fp16_learned_layer_matches_oracle_and_single_runs():
     """Two members with FP16 storage and the committed 4-cell layer weights,
-    stepped as one batch: equal to the same members run alone (1e-5), and
-    within the FP16 storage error of the FP64 oracle stepped with the
-    restated layer (2e-2 over 30 steps, seismograms and final fields; FP16
-    storage alone measures 1.7e-3 on this model, tests/test_gpu_storage16)."""
+    stepped as one batch: within the FP16 storage error of the FP64 oracle
+    stepped with the restated layer (2e-2 over 30 steps, final fields; FP16
+    storage alone measures 1.7e-3 on this model, tests/test_gpu_storage16),
+    and close to the same members run alone.  Alone and batched runs are
+    not bit-equal with 16-bit storage: the batched kernels are compiled
+    separately, their FP32 results differ from the single-model kernels' in
+    the last bit now and then (<= 1e-6 with FP32 storage), and such a
+    difference flips an FP16 rounding, after which the two runs carry
+    independent FP16 rounding errors.  Measured after 30 steps: the first
+    member bit-equal, the second 7.7e-3 apart, where its FP16 run alone is
+    1.0e-2 from its FP32 run; the bound is 1.5e-2."""
     path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
                         "copara-cgfd3d_b200", "data", "layer_mlp_w4.npz")
     d = np.load(path)
@@ -161,7 +168,7 @@ def test_batched_fp16_learned_layer_matches_oracle_and_single_runs():
         seis = s.seismograms()
         fw = np.stack([s.get_field(c) for c in range(9)])
         for c, e in enumerate(comp_errors(seis, alone[q][0])):
-            assert e < 1e-5, ("batch vs alone", q, cgfd.COMPONENTS[c], e)
+            assert e < 1.5e-2, ("batch vs alone", q, cgfd.COMPONENTS[c], e)
         o, cells = _oracle_with_layer(m, steps, w, gains)
         ofw = np.stack([o.get_field(c) for c in range(9)])
         o.close()
