@@ -106,14 +106,15 @@ def run_batch(args, dist, rank, world, local):
     import cgfd
     import models
     K, W = args.steps, args.warmup
-    ms_models = models.batch_models(n=64, seed=7, nt=W + K + 2 + (4 if args.autotune else 0))
-    b = cgfd.Batch([m.desc(device=local) for m in ms_models])
+    ms_models = models.batch_models(n=64, seed=7, nt=W + K + 2 + (6 if args.autotune else 0))
+    storage = {"f32": cgfd.STORE_F32, "f16": cgfd.STORE_F16, "bf16": cgfd.STORE_BF16}[args.storage]
+    b = cgfd.Batch([m.desc(device=local, storage=storage) for m in ms_models])
     for m, s in zip(ms_models, b.models):
         m.load(s)
     b.prepare()
     tuned = None
     if args.autotune:
-        tuned = b.autotune(steps=1)
+        tuned = b.autotune(steps=3)
     b.step(W)
     b.sync()
     barrier(dist)
@@ -122,11 +123,12 @@ def run_batch(args, dist, rank, world, local):
     ms = allmax(dist, ms)
     cells = sum(m.cells for m in ms_models)
     nbad = sum(s.check_finite() for s in b.models)
+    shape = "members" if b.launch == cgfd.BATCH_MEMBERS else "persistent"
     b.close()
     if rank != 0:
         return
     value = world * cells * K / (ms / 1e3) / 1e9
-    bps = sum(algorithmic_bytes_per_step(m) for m in ms_models)
+    bps = sum(algorithmic_bytes_per_step(m, 4 if args.storage == "f32" else 2) for m in ms_models)
     achieved = bps / (ms / K / 1e3) / 1e9
     peak, peak_kind = measured_peak()
     n_src = sum(1 for m in ms_models if len(m.mnt_loc) + len(m.frc_loc))
@@ -135,8 +137,8 @@ def run_batch(args, dist, rank, world, local):
         "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded model generator)",
         "config": {"workload": workload_name(args.config), "models": len(ms_models),
-                   "cells": cells, "kernel": "fused", "storage": "f32", "replicas": world,
-                   "autotuned_ms_per_step": tuned,
+                   "cells": cells, "kernel": "fused", "storage": args.storage, "replicas": world,
+                   "autotuned_ms_per_step": tuned, "launch_shape": shape,
                    "l2": "state >> L2 (126 MB), no flush needed",
                    "parallelism": "replicas" if world > 1 else "single"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -409,9 +411,11 @@ def run_target(args, plain_value, plain_ms, local):
     stepped as one batch with FP16 field storage, timed like the plain run."""
     import cgfd
     K, W = args.steps, args.warmup
-    m4 = build_model(args.config, W + K + 2, nabs=THIN)
+    m4 = build_model(args.config, W + K + 2 + 6, nabs=THIN)
     ms = thin_members(m4)
     b = thin_batch(ms, cgfd.STORE_F16, local)
+    tuned = b.autotune(steps=2)  # work list and launch shape; state restored
+    shape = "members" if b.launch == cgfd.BATCH_MEMBERS else "persistent"
     b.step(W)
     b.sync()
     ms_b = b.step_timed(K)
@@ -421,6 +425,7 @@ def run_target(args, plain_value, plain_ms, local):
     return {"what": "batched FP16-storage learned-thin-layer solver (4-cell CFS-PML + boundary "
                     "MLP, committed weights) on the same model, 2 shots in one batch",
             "value": value, "unit": UNIT, "ms_per_step": ms_b / K, "members": len(ms),
+            "launch_shape": shape, "autotuned_ms_per_step": tuned,
             "plain_fp32_pml20_value": plain_value, "plain_fp32_pml20_ms_per_step": plain_ms,
             "speedup_vs_plain_fp32_pml20": value / plain_value, "nonfinite": nbad,
             "accuracy": "bench.py --target-accuracy STEPS (reflected energy against the "

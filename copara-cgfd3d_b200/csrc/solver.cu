@@ -1935,6 +1935,12 @@ struct cgfd_batch {
   int max_foc = 0;  // most focal points of any member
   int max_sp = 0;   // longest spread list (smoothed sources) of any member
   cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+  // launch shape: false, one persistent launch per stage part over every
+  // member's items (uneven, small members share the GPU without tails);
+  // true, every member's own step graphs on its own stream (members large
+  // enough to fill the GPU alone run the single-model kernels, whose stage
+  // arguments are kernel parameters).  cgfd_batch_autotune times both.
+  bool member_launch = false;
   cudaEvent_t ev = nullptr;      // orders the batch's and the members' streams
   bool ready = false;
   int steps = 0;
@@ -2160,6 +2166,24 @@ int cgfd_batch_step(cgfd_batch *b, int n_steps) {
     BCK(b, cudaEventRecord(b->ev, h->st));
     BCK(b, cudaStreamWaitEvent(b->st, b->ev, 0));
   }
+  if (b->member_launch) {
+    // each member's own step graphs on its stream (the members' step counters
+    // were set above, ordered on the batch's stream, which they now follow)
+    BCK(b, cudaEventRecord(b->ev, b->st));
+    for (cgfd_solver *h : b->m) {
+      BCK(b, cudaStreamWaitEvent(h->st, b->ev, 0));
+      for (int s = 0; s < n_steps; ++s)
+        BCK(b, cudaGraphLaunch(h->graph[(h->steps + s) % 4], h->st));
+    }
+    // the batch's stream follows every member's last step
+    for (cgfd_solver *h : b->m) {
+      BCK(b, cudaEventRecord(b->ev, h->st));
+      BCK(b, cudaStreamWaitEvent(b->st, b->ev, 0));
+      h->steps += n_steps;
+      h->wcur = 0;
+    }
+    return CGFD_OK;
+  }
   const int s0 = b->m[0]->steps;
   for (int s = 0; s < n_steps; ++s) BCK(b, cudaGraphLaunch(b->graph[(s0 + s) % 4], b->st));
   BCK(b, cudaEventRecord(b->ev, b->st));
@@ -2180,6 +2204,12 @@ int cgfd_batch_sync(cgfd_batch *b, double timeout_s) {
     if (e == cudaSuccess) {
       int flag = 0;
       BCK(b, cudaMemcpy(&flag, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+      for (cgfd_solver *h : b->m) {  // member launches record into the members' flags
+        int f = 0;
+        if (flag || !h->d_err) break;
+        BCK(b, cudaMemcpy(&f, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        flag = f;
+      }
       if (flag)
         return batch_fail(b, flag == 2 ? CGFD_ERR_CUDA : CGFD_ERR_TIMEOUT,
                           flag == 2 ? "stage kernel alignment self-check failed"
@@ -2238,15 +2268,40 @@ int cgfd_batch_autotune(cgfd_batch *b, int steps, float *best_ms) {
     if (st) break;
     if (ms < best) { best = ms; bestp = wp; }
   }
+  // the other launch shape: every member's own step graphs
+  bool members_best = false;
+  if (!st) {
+    b->member_launch = true;
+    for (size_t i = 0; i < b->m.size(); ++i) b->m[i]->steps = sn[i].steps;
+    float ms = 0;
+    st = cgfd_batch_step(b, 1);  // warm-up
+    if (!st) st = cgfd_batch_step_timed(b, steps, &ms);
+    if (!st && ms < best) { best = ms; members_best = true; }
+    b->member_launch = false;
+  }
   for (size_t i = 0; i < b->m.size(); ++i) {
     int st2 = snapshot_restore(b->m[i], sn[i]);
     if (!st) st = st2;
   }
+  b->member_launch = members_best;
   if (!pair_set_work(b->plan, bestp) && !st) st = batch_fail(b, CGFD_ERR_CUDA, "work list");
   b->ready = false;
   if (!st) st = batch_build(b);
   if (best_ms) *best_ms = best / steps;
   return st;
+}
+
+int cgfd_batch_set_launch(cgfd_batch *b, int shape) {
+  if (!b || (shape != CGFD_BATCH_PERSISTENT && shape != CGFD_BATCH_MEMBERS))
+    return batch_fail(b, CGFD_ERR_ARG, "bad launch shape");
+  b->member_launch = shape == CGFD_BATCH_MEMBERS;
+  return CGFD_OK;
+}
+
+int cgfd_batch_get_launch(cgfd_batch *b, int *shape) {
+  if (!b || !shape) return batch_fail(b, CGFD_ERR_ARG, "null argument");
+  *shape = b->member_launch ? CGFD_BATCH_MEMBERS : CGFD_BATCH_PERSISTENT;
+  return CGFD_OK;
 }
 
 int cgfd_batch_last_error(cgfd_batch *b, char *buf, size_t len) {

@@ -714,7 +714,6 @@ __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, cons
 }
 
 // ------------------------------ the march ---------------------------------
-static_assert(sizeof(StageArgs) % 4 == 0, "stage arguments are copied in 4-byte words");
 // items: tile index fastest, so the CTAs resident at one time work on
 // neighbouring tiles of the same z-chunk and share halo rows in L2
 template <typename T, int PART, int X, int Y, int Z, int KIND, bool B>
@@ -759,7 +758,6 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
   const int kinda = (KIND == 1) ? 3 : (KIND == 2 ? 2 : 1);        // aux sets read
 
   __shared__ int s_next;
-  __shared__ StageArgs s_args;  // batched launch: the current item's model
   int base = 0;  // stream position of the current item's entry 0
   for (;;) {
     // the next item, taken only when this CTA is free (a CTA never holds a
@@ -770,22 +768,14 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
     if (cur >= wk.nitems || abort_flag) break;  // CTA-uniform
     const int4 it4 = wk.items[cur];
     const int model = B ? it4.w : 0;
-    // a batched launch copies the item's model's stage arguments into shared
-    // memory and reads them through a pointer the compiler cannot trace to
-    // that variable (generic loads).  Read through the __shared__ variable
-    // itself, the 16-bit batched stages behaved as if every scale were zero
-    // (measured; FP32 was unaffected); read from global memory in place,
-    // they were correct but a third slower.
-    const StageArgs *Ap = &a;
-    if (B) {
-      const uint32_t *src = reinterpret_cast<const uint32_t *>(wk.bargs + model);
-      uint32_t *dst = reinterpret_cast<uint32_t *>(&s_args);
-      for (int w = tid; w < (int)(sizeof(StageArgs) / 4); w += TT) dst[w] = src[w];
-      __syncthreads();
-      Ap = &s_args;
-      asm volatile("" : "+l"(Ap)::"memory");
-    }
-    const StageArgs &A = *Ap;
+    // a batched launch reads the item's model's stage arguments in place
+    // (global memory, read-only during the launch).  Copied per item into a
+    // __shared__ StageArgs and read from there, the 16-bit batched stages
+    // behaved as if every component scale were zero (FP32, whose kernels
+    // never read the scales, was unaffected); read through a pointer to the
+    // copy hidden from the compiler they were correct but 15% slower than
+    // in place.
+    const StageArgs &A = B ? wk.bargs[model] : a;
     const Maps &M = B ? wk.bmaps[model] : maps;
     const Geom &g = A.g;
     const size_t fs = g.fstride;

@@ -27,6 +27,7 @@ _lib = C.CDLL(LIB_PATH)
 OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_TIMEOUT, ERR_NONFINITE, ERR_NODEVICE = range(8)
 STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
 KERNEL_FUSED, KERNEL_SIMPLE, KERNEL_SCALAR = 0, 1, 2
+BATCH_PERSISTENT, BATCH_MEMBERS = 0, 1  # cgfd_batch_set_launch
 SET_FW, SET_W, SET_TW = 0, 1, 2
 COMPONENTS = ("Vx", "Vy", "Vz", "Txx", "Tyy", "Tzz", "Txy", "Txz", "Tyz")
 STF_TYPES = {"Gauss": 0, "gauss": 1, "Ricker": 2, "ricker": 3, "Bell": 4,
@@ -97,6 +98,8 @@ _SIGS = {
     "cgfd_batch_step_timed": (C.c_int, [_P, C.c_int, _fp]),
     "cgfd_batch_sync": (C.c_int, [_P, C.c_double]),
     "cgfd_batch_autotune": (C.c_int, [_P, C.c_int, _fp]),
+    "cgfd_batch_set_launch": (C.c_int, [_P, C.c_int]),
+    "cgfd_batch_get_launch": (C.c_int, [_P, _ip]),
     "cgfd_batch_last_error": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
     "cgfd_batch_destroy": (C.c_int, [_P]),
     "cgfd_get_field_scales": (C.c_int, [_P, _ip]),
@@ -449,6 +452,17 @@ class Batch:
         ms = C.c_float()
         self._chk(_lib.cgfd_batch_autotune(self._h, steps, C.byref(ms)))
         return ms.value
+
+    @property
+    def launch(self) -> int:
+        """BATCH_PERSISTENT or BATCH_MEMBERS (cgfd_batch_get_launch)."""
+        v = C.c_int()
+        self._chk(_lib.cgfd_batch_get_launch(self._h, C.byref(v)))
+        return v.value
+
+    @launch.setter
+    def launch(self, shape: int):
+        self._chk(_lib.cgfd_batch_set_launch(self._h, shape))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -321,9 +321,14 @@ int cgfd_test_withhold_copy(cgfd_solver *h, double wait_limit_s, int withhold);
 /* ---------------------- batches of models (one GPU) ----------------------- */
 
 /* A batch steps n independent models (each its own grid, medium, PML,
- * sources, receivers and dt; FP32 storage, default kernel family) together
- * through one persistent launch per stage part, so that uneven models share
- * the GPU without per-model launch tails.  Each model is a member solver:
+ * sources, receivers, dt and learned layer; one storage type for all, default
+ * kernel family) together.  Launch shape CGFD_BATCH_PERSISTENT (the default):
+ * one persistent launch per stage part over every member's work items, so
+ * that uneven, small models share the GPU without per-model launch tails.
+ * CGFD_BATCH_MEMBERS: every member's own step graphs, each member on its own
+ * stream (members that fill the GPU alone run at the single-model kernels'
+ * speed).  cgfd_batch_autotune times both shapes (and the work-list shapes of
+ * the persistent one) and keeps the fastest.  Each model is a member solver:
  * fill it through the usual upload calls on the handle cgfd_batch_solver
  * returns, read its seismograms and fields there.  All members must be at the
  * same step when the batch steps.
@@ -337,8 +342,13 @@ int cgfd_batch_step(cgfd_batch *b, int n_steps);
 /* n_steps steps timed with CUDA events on the batch's stream (whole batch) */
 int cgfd_batch_step_timed(cgfd_batch *b, int n_steps, float *ms);
 int cgfd_batch_sync(cgfd_batch *b, double timeout_s);
-/* cgfd_autotune for the batch's shared work list */
+/* cgfd_autotune for the batch: the shared work list's shapes and the launch
+ * shape; the state and the seismograms are restored afterwards */
 int cgfd_batch_autotune(cgfd_batch *b, int steps, float *ms_per_step);
+#define CGFD_BATCH_PERSISTENT 0
+#define CGFD_BATCH_MEMBERS 1
+int cgfd_batch_set_launch(cgfd_batch *b, int shape);
+int cgfd_batch_get_launch(cgfd_batch *b, int *shape);
 int cgfd_batch_last_error(cgfd_batch *b, char *buf, size_t len);
 int cgfd_batch_destroy(cgfd_batch *b);
 

@@ -5,9 +5,10 @@ stage part; its per-cell arithmetic is the single-model kernel's source, so
 every member's seismograms and fields must equal those of the same model run
 alone up to FP32 rounding (the batched instantiation is a separate
 compilation; measured <= 9.3e-7 relative L2 per component over 24 steps, held
-to the 1e-5 parity bar).  The autotuner only changes
-the work list (tile order and z-chunking) of the same kernels, so it must
-leave the state unchanged and the results bit-identical.
+to the 1e-5 parity bar).  The autotuner changes the work list (tile order
+and z-chunking) of the same kernels and the launch shape (one persistent
+launch, or every member's own single-model step graphs), so it must leave
+the state unchanged and the results within that bar.
 """
 import numpy as np
 import pytest
@@ -98,4 +99,38 @@ def test_batch_autotune_keeps_results():
         seis, _ = _alone(m, 15)
         for c, e in enumerate(comp_errors(s.seismograms()[:, :, :15], seis[:, :, :15])):
             assert e < 1e-5, (cgfd.COMPONENTS[c], e)
+    b.close()
+
+
+@pytest.mark.parametrize("storage", [cgfd.STORE_F32, cgfd.STORE_F16])
+def test_member_launch_equals_single_model_runs_bit_for_bit(storage):
+    """The member launch shape runs every member's own step graphs (the
+    single-model kernels), so members equal the same models run alone bit
+    for bit, 16-bit storage included, over steps taken in several calls."""
+    ms = _small_batch(n=2)
+    steps = 12
+
+    def alone(m):
+        s = cgfd.Solver(m.desc(storage=storage))
+        m.load(s)
+        s.step(steps)
+        out = (s.seismograms(), np.stack([s.get_field(c) for c in range(9)]))
+        s.close()
+        return out
+
+    ref = [alone(m) for m in ms]
+    b = cgfd.Batch([m.desc(storage=storage) for m in ms])
+    for m, s in zip(ms, b.models):
+        m.load(s)
+    assert b.launch == cgfd.BATCH_PERSISTENT
+    b.launch = cgfd.BATCH_MEMBERS
+    assert b.launch == cgfd.BATCH_MEMBERS
+    b.step(steps // 2)
+    b.step(steps - steps // 2)
+    b.sync()
+    for q, s in enumerate(b.models):
+        assert np.array_equal(s.seismograms(), ref[q][0]), q
+        assert np.array_equal(np.stack([s.get_field(c) for c in range(9)]), ref[q][1]), q
+    with pytest.raises(cgfd.CgfdError):
+        b.launch = 7
     b.close()
