@@ -117,10 +117,13 @@ __device__ void inject_sources_body(const SourceArgs &s) {
 // tW elision, single-stage driving: after a first stage run alone, tW (valid
 // cells) is written as the reference's first stage leaves it,
 // tW = FW + r * (W - FW), so the state between stages matches the
-// reference's; the next stage rebuilds it the same way anyway.
+// reference's; the next stage rebuilds it the same way anyway.  16-bit
+// storage keeps tW as its difference from FW (the stage kernels' form):
+// r * (W - FW).
 template <typename T>
 __global__ void rebuild_tw_kernel(Geom g, const T *fw, const T *w, T *tw, float r) {
   using E = Elem<T>;
+  constexpr bool D = sizeof(T) != 4;
   const long n = (long)g.ni * g.nj * g.nk;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
        t += (long)gridDim.x * blockDim.x) {
@@ -129,7 +132,7 @@ __global__ void rebuild_tw_kernel(Geom g, const T *fw, const T *w, T *tw, float 
     for (int c = 0; c < NCOMP; ++c) {
       const size_t q = (size_t)c * g.fstride + o;
       const float f = E::ld(fw + q);
-      E::st(tw + q, f + r * (E::ld(w + q) - f));
+      E::st(tw + q, D ? r * (E::ld(w + q) - f) : f + r * (E::ld(w + q) - f));
     }
   }
 }
@@ -1776,7 +1779,15 @@ int cgfd_get_field(cgfd_solver *h, int set, int comp, float *out) {
   if (!p) return arg_fail(h, "bad set or component");
   DevGuard guard(h->d.device);
   CK(h, cudaStreamSynchronize(h->st));
-  return download_ref(h, p, out, h->elem, std::ldexp(1.f, h->sexp[comp]));
+  const float sc = std::ldexp(1.f, h->sexp[comp]);
+  int st = download_ref(h, p, out, h->elem, sc);
+  if (st || set != CGFD_SET_TW || h->elem == ELEM_F32) return st;
+  // 16-bit storage keeps tW - FW: add FW back
+  std::vector<float> f(ref_n(h));
+  st = download_ref(h, set_ptr(h, CGFD_SET_FW, comp), f.data(), h->elem, sc);
+  if (st) return st;
+  for (size_t t = 0; t < f.size(); ++t) out[t] += f[t];
+  return CGFD_OK;
 }
 
 int cgfd_set_field(cgfd_solver *h, int set, int comp, const float *in) {
@@ -1789,11 +1800,19 @@ int cgfd_set_field(cgfd_solver *h, int set, int comp, const float *in) {
   const long n = ref_n(h);
   const int nx = h->d.ni + 6, ny = h->d.nj + 6, nz = h->d.nk + 6;
   std::vector<float> v(n, 0.f);
+  // 16-bit storage keeps tW - FW: subtract the stored FW
+  std::vector<float> f;
+  if (set == CGFD_SET_TW && h->elem != ELEM_F32) {
+    f.resize(n);
+    int st = download_ref(h, set_ptr(h, CGFD_SET_FW, comp), f.data(), h->elem,
+                          std::ldexp(1.f, h->sexp[comp]));
+    if (st) return st;
+  }
   for (int i = LFD; i < nx - LFD; ++i)
     for (int j = LFD; j < ny - LFD; ++j)
       for (int k = LFD; k < nz - LFD; ++k) {
         const long t = ((long)i * ny + j) * nz + k;
-        v[t] = in[t];
+        v[t] = f.empty() ? in[t] : in[t] - f[t];
       }
   return upload_ref(h, v.data(), p, h->elem, std::ldexp(1.f, -h->sexp[comp]));
 }
@@ -2377,28 +2396,39 @@ int cgfd_get_snapshot(cgfd_solver *h, int set, const int *start, const int *coun
   const size_t n = (size_t)nc * count[0] * count[1] * count[2];
   DevGuard guard(h->d.device);
   CK(h, cudaStreamSynchronize(h->st));
+  // 16-bit storage keeps tW - FW: gather FW too and add it back
+  const bool add_fw = set == CGFD_SET_TW && h->elem != ELEM_F32;
+  const int parts = add_fw ? 2 : 1;
   float *tmp = nullptr;
-  CK(h, cudaMalloc(&tmp, n * sizeof(float)));
+  CK(h, cudaMalloc(&tmp, parts * n * sizeof(float)));
   ScaleSet sc;
   for (int c = 0; c < NCOMP; ++c) sc.sc[c] = std::ldexp(1.f, h->sexp[c]);
   const int3 st3 = make_int3(start[0], start[1], start[2]);
   const int3 cn3 = make_int3(count[0], count[1], count[2]);
   const int3 sd3 = make_int3(stride[0], stride[1], stride[2]);
-  if (h->elem == ELEM_F16)
-    snapshot_kernel<<<592, 256, 0, h->st>>>((const __half *)base, h->g, comp_mask, st3, cn3, sd3,
-                                            sc, tmp);
-  else if (h->elem == ELEM_BF16)
-    snapshot_kernel<<<592, 256, 0, h->st>>>((const __nv_bfloat16 *)base, h->g, comp_mask, st3,
-                                            cn3, sd3, sc, tmp);
-  else
-    snapshot_kernel<<<592, 256, 0, h->st>>>((const float *)base, h->g, comp_mask, st3, cn3, sd3,
-                                            sc, tmp);
+  for (int q = 0; q < parts; ++q) {
+    const void *src = q == 0 ? base : set_ptr(h, CGFD_SET_FW, 0);
+    float *dst = tmp + (size_t)q * n;
+    if (h->elem == ELEM_F16)
+      snapshot_kernel<<<592, 256, 0, h->st>>>((const __half *)src, h->g, comp_mask, st3, cn3,
+                                              sd3, sc, dst);
+    else if (h->elem == ELEM_BF16)
+      snapshot_kernel<<<592, 256, 0, h->st>>>((const __nv_bfloat16 *)src, h->g, comp_mask, st3,
+                                              cn3, sd3, sc, dst);
+    else
+      snapshot_kernel<<<592, 256, 0, h->st>>>((const float *)src, h->g, comp_mask, st3, cn3, sd3,
+                                              sc, dst);
+  }
+  std::vector<float> fw(add_fw ? n : 0);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(out, tmp, n * sizeof(float), cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess && add_fw)
+    e = cudaMemcpyAsync(fw.data(), tmp + n, n * sizeof(float), cudaMemcpyDeviceToHost, h->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
   cudaFree(tmp);
   if (e != cudaSuccess) return cuda_fail(h, e, "snapshot");
+  for (size_t t = 0; t < fw.size(); ++t) out[t] += fw[t];
   return CGFD_OK;
 }
 

@@ -118,15 +118,19 @@ bool model_maps(ModelMaps *pl, int *has_aux, const Geom &g, int elem, void *cons
 // the maps of one stage (stage input set, RK kind, stage index) for the
 // velocity (mv) and stress (ms) parts
 // (rebuild: the second stage under tW elision, whose u1 is the stage input)
-void stage_maps(const ModelMaps &pl, int rk, int in_set, bool rebuild, Maps &mv, Maps &ms) {
+// (tw_delta: 16-bit storage, tW kept as tW - FW; the final stage reads FW as
+// its first register set and the difference as its second)
+void stage_maps(const ModelMaps &pl, int rk, int in_set, bool rebuild, bool tw_delta, Maps &mv,
+                Maps &ms) {
   const int kind = rk == 0 ? 0 : (rk < 3 ? 1 : 2);
+  const bool fw_first = kind != 2 || tw_delta;
   mv.halo = pl.haloV[in_set];
-  mv.u0 = kind == 2 ? pl.ctrV[3] : pl.ctrV[0];
+  mv.u0 = fw_first ? pl.ctrV[0] : pl.ctrV[3];
   mv.u1 = rebuild ? pl.ctrV[in_set] : pl.ctrV[3];
   mv.coef = pl.coefV;
   mv.met = pl.met;
   ms.halo = pl.haloS[in_set];
-  ms.u0 = kind == 2 ? pl.ctrT[3] : pl.ctrT[0];
+  ms.u0 = fw_first ? pl.ctrT[0] : pl.ctrT[3];
   ms.u1 = rebuild ? pl.ctrT[in_set] : pl.ctrT[3];
   ms.coef = pl.coefS;
   ms.met = pl.met;
@@ -345,7 +349,7 @@ void launch_stage_pair(const void *plan, const StageArgs &a, int in_set, int *er
   cudaStream_t s = (cudaStream_t)stream;
   const int kind = a.rk == 0 ? 0 : (a.rk < 3 ? 1 : 2);
   Maps mv, ms;
-  stage_maps(pl.mm[0], a.rk, in_set, a.tw_skip && a.rk == 1, mv, ms);
+  stage_maps(pl.mm[0], a.rk, in_set, a.tw_skip && a.rk == 1, pl.elem != ELEM_F32, mv, ms);
   // the traction image needs only the stage input and writes what the two
   // parts neither write nor use (the top three layers' V, their tW and x/y
   // auxiliaries): with a side stream it runs beside them, joined at the end
@@ -406,7 +410,7 @@ void *pair_create_batch_plan(int n, const Geom *gs, void *const *sets, const flo
   std::vector<Maps> hm((size_t)8 * n);
   for (int rk = 0; rk < 4 && ok; ++rk)
     for (int i = 0; i < n; ++i)
-      stage_maps(pl->mm[i], rk, ins[rk], rk == 1, hm[(size_t)(rk * 2) * n + i],
+      stage_maps(pl->mm[i], rk, ins[rk], rk == 1, elem != ELEM_F32, hm[(size_t)(rk * 2) * n + i],
                  hm[(size_t)(rk * 2 + 1) * n + i]);
   ok = ok && cudaMalloc(&pl->d_bmaps, hm.size() * sizeof(Maps)) == cudaSuccess &&
        cudaMemcpy(pl->d_bmaps, hm.data(), hm.size() * sizeof(Maps), cudaMemcpyHostToDevice) ==

@@ -239,24 +239,40 @@ __device__ __forceinline__ void stt2(T *p, int m, f2 v) {
   }
 }
 
+// 16-bit storage keeps the RK accumulator as its difference from the step
+// state, tW - FW: the difference is about a time step's change of the field,
+// an order of magnitude below the field, so its FP16/BF16 rounding is that
+// much finer (the accumulator's rounding was the largest share of the 16-bit
+// storage error).  The final stage then reads FW besides it.
+template <typename T> struct TwDelta { static constexpr bool value = sizeof(T) != 4; };
+// the second pointwise register set is loaded: inner stages (tW, or the stage
+// input under tW elision), and the final stage with the difference form (tW)
+template <int KIND, typename T> struct TwoRegs {
+  static constexpr bool value = KIND == 1 || (KIND == 2 && TwDelta<T>::value);
+};
+
 // RK update of one pair (Iteration*): KIND 0 first stage (u0 = FW; no tW
 // under tW elision), 1 inner (u0 = FW, u1 = tW; in the second stage under
 // elision u1 = the stage input W and tW = FW + rtw*(W - FW) + bdt*h),
-// 2 final (u0 = tW).  u0, u1 and the outputs are in stored units; adt, bdt
-// carry the component's inverse scale (every set of a component shares its
-// scale, so the rebuild is the same in stored units).
+// 2 final (u0 = tW; with the difference form u0 = FW and u1 = tW - FW).
+// u0, u1 and the outputs are in stored units; adt, bdt carry the component's
+// inverse scale (every set of a component shares its scale, so the rebuild
+// and the difference are the same in stored units).
 template <int KIND, typename T>
 __device__ __forceinline__ void rk_store2(const StageArgs &a, T *out, T *tw, int m, f2 u0, f2 u1,
                                           f2 hh, float adt, float bdt) {
+  constexpr bool D = TwDelta<T>::value;
   if (KIND == 0) {
     stt2(out, m, fma2(S2(adt), hh, u0));
-    if (!a.tw_skip) stt2(tw, m, fma2(S2(bdt), hh, u0));
+    if (!a.tw_skip) stt2(tw, m, D ? mul2(S2(bdt), hh) : fma2(S2(bdt), hh, u0));
   } else if (KIND == 1) {
     stt2(out, m, fma2(S2(adt), hh, u0));
-    const f2 base = (a.tw_skip && a.rk == 1) ? fma2(S2(a.rtw), add2(u1, neg2(u0)), u0) : u1;
+    f2 base = u1;
+    if (a.tw_skip && a.rk == 1)
+      base = D ? mul2(S2(a.rtw), add2(u1, neg2(u0))) : fma2(S2(a.rtw), add2(u1, neg2(u0)), u0);
     stt2(tw, m, fma2(S2(bdt), hh, base));
   } else {
-    stt2(out, m, fma2(S2(bdt), hh, u0));
+    stt2(out, m, fma2(S2(bdt), hh, D ? add2(u0, u1) : u0));
   }
 }
 
@@ -447,7 +463,7 @@ __device__ __forceinline__ void vel_pair(const StageArgs &a, const Pair &e, cons
 #pragma unroll
     for (int q = 0; q < 3; ++q)
       rk_store2<KIND>(a, out + (VX + q) * fs + pl.c, tw + (VX + q) * fs + pl.c, 3, pw.U0(q),
-                      KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], adt(VX + q), bdt(VX + q));
+                      TwoRegs<KIND, T>::value ? pw.U1(q) : S2(0.f), hw[q], adt(VX + q), bdt(VX + q));
     return;
   }
 
@@ -516,7 +532,7 @@ __device__ __forceinline__ void vel_pair(const StageArgs &a, const Pair &e, cons
 #pragma unroll
   for (int q = 0; q < 3; ++q)
     rk_store2<KIND>(a, out + (VX + q) * fs + pl.c, tw + (VX + q) * fs + pl.c, e.m, pw.U0(q),
-                    KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], adt(VX + q), bdt(VX + q));
+                    TwoRegs<KIND, T>::value ? pw.U1(q) : S2(0.f), hw[q], adt(VX + q), bdt(VX + q));
 }
 
 // --------------------------- stress part ----------------------------------
@@ -709,7 +725,7 @@ __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, cons
 #pragma unroll
   for (int q = 0; q < 6; ++q)
     rk_store2<KIND>(a, out + (TXX + q) * fs + pl.c, tw + (TXX + q) * fs + pl.c, m, pw.U0(q),
-                    KIND == 1 ? pw.U1(q) : S2(0.f), hw[q], scaled<T>(a.adt, a.isc[TXX + q]),
+                    TwoRegs<KIND, T>::value ? pw.U1(q) : S2(0.f), hw[q], scaled<T>(a.adt, a.isc[TXX + q]),
                     scaled<T>(a.bdt, a.isc[TXX + q]));
 }
 
@@ -782,7 +798,8 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
     const bool flat = A.flat;
     // bytes one plane delivers: halo always, pointwise only for computed
     // planes, the metric tile only where the plane's metric is not uniform
-    const uint32_t pw_bytes = S::U_B * (KIND == 1 ? 2u : 1u) + (uint32_t)(PWT * 4) * NCOEF;
+    const uint32_t pw_bytes =
+        S::U_B * (TwoRegs<KIND, T>::value ? 2u : 1u) + (uint32_t)(PWT * 4) * NCOEF;
     auto met_tile = [&](int p) { return !flat && p >= A.zu_end; };
     // zeta_z of a plane without a metric tile (loaded one plane ahead)
     auto zz_of = [&](int p) { return flat ? 1.f : (p < A.zu_end ? A.zzp[p] : 0.f); };
@@ -813,7 +830,7 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
       if (compute) {
         const int cx = XO + i0, cy = LFD + j0;
         tma_load(slot + S::U0, &M.u0, cx, cy, p, S0, &bars[s]);
-        if (KIND == 1) tma_load(slot + S::U1, &M.u1, cx, cy, p, S0, &bars[s]);
+        if (TwoRegs<KIND, T>::value) tma_load(slot + S::U1, &M.u1, cx, cy, p, S0, &bars[s]);
         tma_load(slot + S::COEF, &M.coef, cx, cy, p, COEF0, &bars[s]);
         if (met) tma_load(slot + S::MET, &M.met, cx, cy, p, 0, &bars[s]);
         // the plane's PML auxiliaries into L2 (tile- and plane-uniform presence)

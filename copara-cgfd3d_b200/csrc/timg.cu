@@ -113,17 +113,22 @@ __device__ __forceinline__ void timg_cell(const StageArgs &a, int i, int j, int 
     // RK update in stored units (every set of a component shares its scale)
     const size_t o = (size_t)(VX + q) * fs + c;
     const float adt = a.adt * a.isc[VX + q], bdt = a.bdt * a.isc[VX + q];
+    // 16-bit storage keeps tW as tW - FW (the paired kernels' form)
+    constexpr bool D = sizeof(T) != 4;
     if (kind == 0) {
       const float u0 = E::ld(in + o);
       E::st(out + o, u0 + adt * hv);
-      if (!a.tw_skip) E::st(tw + o, u0 + bdt * hv);
+      if (!a.tw_skip) E::st(tw + o, D ? bdt * hv : u0 + bdt * hv);
     } else if (kind == 1) {
       const float u0 = E::ld(fw + o);
-      const float u1 = rebuild ? u0 + a.rtw * (E::ld(in + o) - u0) : E::ld(tw + o);
+      float u1;
+      if (rebuild) u1 = D ? a.rtw * (E::ld(in + o) - u0) : u0 + a.rtw * (E::ld(in + o) - u0);
+      else u1 = E::ld(tw + o);
       E::st(out + o, u0 + adt * hv);
       E::st(tw + o, u1 + bdt * hv);
     } else {
-      E::st(out + o, E::ld(tw + o) + bdt * hv);
+      const float t = D ? E::ld(fw + o) + E::ld(tw + o) : E::ld(tw + o);
+      E::st(out + o, t + bdt * hv);
     }
   }
 }

@@ -43,7 +43,10 @@ typedef enum cgfd_status {
 } cgfd_status;
 
 /* Storage type of the 9 wavefields and the RK registers.  Arithmetic is FP32
- * in every case; 16-bit storage keeps one power-of-two scale per field. */
+ * in every case; 16-bit storage keeps one power-of-two scale per field and
+ * holds the RK accumulator as its difference from the step state, tW - FW
+ * (rounded far more finely than tW itself); cgfd_get_field, cgfd_set_field
+ * and cgfd_get_snapshot of CGFD_SET_TW convert, so callers see tW. */
 typedef enum cgfd_storage {
     CGFD_STORE_F32  = 0,
     CGFD_STORE_F16  = 1,
