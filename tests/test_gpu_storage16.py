@@ -7,12 +7,15 @@ against the solver's own FP32 storage (which matches the reference within
 1e-5) on the same inputs, plus exact properties of the storage conversions
 and scales.
 
-Measured on a B200 (seismogram relative L2 of Vx..Vz): small flat 60 steps
-FP16 1.7e-3 / BF16 1.5e-2 against FP32 storage; small hill FP16 2.8e-3 /
-BF16 9.3e-3; the 160x160x80 flat half-space, 500 steps, against the FP64
-oracle: FP16 7.0e-3, BF16 6.3e-2 (peak amplitude 0.50% / 2.9%).  The bounds
-sit 10-25% above these: a regression shows.  Where the FP16 error comes
-from (which stored set) is measured on the CPU in test_storage_emulation.py.
+Measured on a B200 (seismogram relative L2 of Vx..Vz), with the RK
+accumulator stored as its difference from FW: small flat 60 steps FP16
+1.10e-3 / BF16 8.9e-3 against FP32 storage; small hill FP16 1.39e-3 / BF16
+2.9e-3; the 160x160x80 flat half-space, 500 steps, against the FP64 oracle:
+FP16 3.7e-3, BF16 2.8e-2 (peak amplitude 0.23% / 0.03%).  (Storing tW
+itself they were 1.7e-3 / 1.5e-2, 2.8e-3 / 9.3e-3 and 7.0e-3 / 6.3e-2.)
+The bounds sit about 25% above the measurements: a regression shows.  Where
+the FP16 error comes from (which stored set) is measured on the CPU in
+test_storage_emulation.py.
 """
 import os
 
@@ -37,8 +40,8 @@ def _run(m, steps, storage):
     return seis, nbad, scales
 
 
-@pytest.mark.parametrize("name,bound", [("small_flat", {"f16": 2.2e-3, "bf16": 1.9e-2}),
-                                        ("small_hill", {"f16": 3.5e-3, "bf16": 1.2e-2})])
+@pytest.mark.parametrize("name,bound", [("small_flat", {"f16": 1.4e-3, "bf16": 1.1e-2}),
+                                        ("small_hill", {"f16": 1.75e-3, "bf16": 3.6e-3})])
 @pytest.mark.parametrize("store", list(STORES))
 def test_16bit_storage_tracks_fp32_storage(name, bound, store):
     m = getattr(models, name)(nt=60)
@@ -49,7 +52,7 @@ def test_16bit_storage_tracks_fp32_storage(name, bound, store):
     assert e < bound[store], (name, store, e, scales)
 
 
-@pytest.mark.parametrize("store,bound,peak", [("f16", 8e-3, 6e-3), ("bf16", 7e-2, 3.5e-2)])
+@pytest.mark.parametrize("store,bound,peak", [("f16", 4.6e-3, 3e-3), ("bf16", 3.5e-2, 1e-3)])
 def test_flat_halfspace_160x160x80_500_steps_16bit(store, bound, peak):
     """The FP16/BF16 variant of the 160x160x80 flat half-space model against
     the FP64 oracle's seismograms (and FP32 storage against the same, 1e-5)."""
@@ -90,3 +93,28 @@ def test_field_round_trip_and_rescale_are_exact(store, ulp):
     assert s.field_scales() == e2
     assert np.array_equal(s.get_field(4), g)
     s.close()
+
+
+def test_accumulator_read_back_through_the_difference_form():
+    """16-bit storage holds tW - FW; get_field / set_field of the tW set
+    convert, so after single stages the accumulator a caller sees follows
+    FP32 storage's within FP16 precision (measured <= 5.6e-4 per component
+    after two stages), and a tW written by the caller reads back."""
+    m = models.small_hill(nt=8)
+    res = {}
+    for k, st in (("f32", cgfd.STORE_F32), ("f16", cgfd.STORE_F16)):
+        s = cgfd.Solver(m.desc(storage=st))
+        m.load(s)
+        s.step(3)
+        s.rk_stage(0, 3, 1, 1, 1)
+        s.rk_stage(1, 3, 1, 1, 1)
+        res[k] = np.stack([s.get_field(c, cgfd.SET_TW) for c in range(9)])
+        if k == "f16":
+            t = res[k][4] * 0.5
+            s.set_field(4, t, cgfd.SET_TW)
+            back = s.get_field(4, cgfd.SET_TW)
+            v = (slice(3, -3),) * 3
+            assert rel_l2(back[v], t[v]) < 2e-3
+        s.close()
+    for c in range(9):
+        assert rel_l2(res["f16"][c], res["f32"][c]) < 1.5e-3, (cgfd.COMPONENTS[c],)
