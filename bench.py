@@ -45,8 +45,12 @@ def parse():
     p.add_argument("--kernel", choices=("fused", "simple", "scalar"), default="fused")
     p.add_argument("--config", choices=("hill600", "hill400", "flat160", "hill256", "batch64"),
                    default="hill600")
-    p.add_argument("--autotune", action="store_true",
-                   help="tune the work list before timing (state unchanged)")
+    p.add_argument("--autotune", dest="autotune", action="store_true", default=True,
+                   help="tune the work list before timing (state unchanged; the default for "
+                        "single models; batch64 tunes only when asked)")
+    p.add_argument("--no-autotune", dest="autotune", action="store_false")
+    p.add_argument("--tune-batch", action="store_true",
+                   help="batch64: tune the work list and launch shape before timing")
     p.add_argument("--storage", choices=("f32", "f16", "bf16"), default="f32",
                    help="storage type of the field sets (arithmetic is FP32)")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -106,14 +110,14 @@ def run_batch(args, dist, rank, world, local):
     import cgfd
     import models
     K, W = args.steps, args.warmup
-    ms_models = models.batch_models(n=64, seed=7, nt=W + K + 2 + (6 if args.autotune else 0))
+    ms_models = models.batch_models(n=64, seed=7, nt=W + K + 2 + (6 if args.tune_batch else 0))
     storage = {"f32": cgfd.STORE_F32, "f16": cgfd.STORE_F16, "bf16": cgfd.STORE_BF16}[args.storage]
     b = cgfd.Batch([m.desc(device=local, storage=storage) for m in ms_models])
     for m, s in zip(ms_models, b.models):
         m.load(s)
     b.prepare()
     tuned = None
-    if args.autotune:
+    if args.tune_batch:
         tuned = b.autotune(steps=3)
     b.step(W)
     b.sync()
@@ -489,13 +493,14 @@ def main():
               "scalar": cgfd.KERNEL_SCALAR}[args.kernel]
     K, W = args.steps, args.warmup
     K2 = min(K, 20)
-    nt = W + K + K2 + 2
+    nt = W + K + K2 + 2 + (4 if args.autotune else 0)
     m = build_model(args.config, nt)
     storage = {"f32": cgfd.STORE_F32, "f16": cgfd.STORE_F16, "bf16": cgfd.STORE_BF16}[args.storage]
     s = cgfd.Solver(m.desc(kernel=kernel, device=local, storage=storage))
     m.load(s)
     s.prepare()
-    tuned = s.autotune(steps=2) if args.autotune else None
+    tuned = s.autotune(steps=2) if args.autotune and args.kernel == "fused" else None
+    work_shape = list(s.work_shape) if args.kernel == "fused" else None
     s.step(W)
     s.sync()
     barrier(dist)
@@ -515,6 +520,9 @@ def main():
         t0 = time.perf_counter()
         s2 = cgfd.Solver(m.desc(kernel=kernel, device=local, storage=storage))
         m.load(s2)
+        if work_shape is not None:  # the shape the autotuner chose, as a user reuses it
+            s2.prepare()
+            s2.work_shape = work_shape
         s2.step(K)
         seis = s2.seismograms()
         s2.sync()
@@ -544,6 +552,7 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded model generator)",
         "config": config_dict(args.config, m, args.storage),
         "kernel": args.kernel, "replicas": world, "autotuned_ms_per_step": tuned,
+        "work_shape": work_shape,
         "parallelism": "replicas" if world > 1 else "single",
         "product_library_mapped": product_library_mapped(),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -1883,11 +1883,18 @@ static int snapshot_restore(cgfd_solver *h, Snapshot &sn) {
   return CGFD_OK;
 }
 // the work-list shapes the autotuner tries
-static std::vector<WorkParams> tuning_candidates() {
-  std::vector<WorkParams> v;
+// (the plan's current shape first, so the autotuner never ends on a worse
+// one than it started from)
+static std::vector<WorkParams> tuning_candidates(const WorkParams &current) {
+  std::vector<WorkParams> v{current};
   for (int ipc : {3, 6, 12})
-    for (int mc : {12, 24})
-      for (double pw : {1.0, 2.0}) v.push_back(WorkParams{ipc, mc, pw});
+    for (int mc : {12, 16, 24, 32})
+      for (double pw : {1.0, 2.0}) {
+        const WorkParams w{ipc, mc, pw};
+        if (w.items_per_cta != current.items_per_cta || w.min_chunk != current.min_chunk ||
+            w.pml_weight != current.pml_weight)
+          v.push_back(w);
+      }
   return v;
 }
 
@@ -1904,7 +1911,7 @@ int cgfd_autotune(cgfd_solver *h, int steps, float *best_ms) {
   if (st) return st;
   float best = 1e30f;
   WorkParams bestp = pair_get_work(h->plan);
-  for (const WorkParams &wp : tuning_candidates()) {
+  for (const WorkParams &wp : tuning_candidates(bestp)) {
     if (!pair_set_work(h->plan, wp)) continue;
     h->graphs_ok = false;
     st = build_graphs(h);
@@ -1923,6 +1930,35 @@ int cgfd_autotune(cgfd_solver *h, int steps, float *best_ms) {
   if (!st) st = build_graphs(h);
   if (best_ms) *best_ms = best / steps;
   return st;
+}
+
+int cgfd_get_work_shape(cgfd_solver *h, int *items_per_cta, int *min_chunk, double *pml_weight) {
+  if (!h || !items_per_cta || !min_chunk || !pml_weight) return arg_fail(h, "null argument");
+  if (h->d.kernel != CGFD_KERNEL_FUSED || !h->plan)
+    return arg_fail(h, "work shapes belong to the default kernel after cgfd_prepare");
+  const WorkParams w = pair_get_work(h->plan);
+  *items_per_cta = w.items_per_cta;
+  *min_chunk = w.min_chunk;
+  *pml_weight = w.pml_weight;
+  return CGFD_OK;
+}
+
+int cgfd_set_work_shape(cgfd_solver *h, int items_per_cta, int min_chunk, double pml_weight) {
+  if (!h) return arg_fail(h, "null handle");
+  if (h->d.kernel != CGFD_KERNEL_FUSED || !h->plan)
+    return arg_fail(h, "work shapes belong to the default kernel after cgfd_prepare");
+  if (items_per_cta < 1 || items_per_cta > 64 || min_chunk < 4 || min_chunk > 1024 ||
+      !(pml_weight >= 0.0 && pml_weight <= 16.0))
+    return arg_fail(h, "bad work shape");
+  DevGuard guard(h->d.device);
+  CK(h, cudaStreamSynchronize(h->st));
+  WorkParams w = pair_get_work(h->plan);
+  w.items_per_cta = items_per_cta;
+  w.min_chunk = min_chunk;
+  w.pml_weight = pml_weight;
+  if (!pair_set_work(h->plan, w)) return arg_fail(h, "work list rejected for this model");
+  h->graphs_ok = false;  // the step graphs hold the launch configuration
+  return build_graphs(h);
 }
 
 int cgfd_test_withhold_copy(cgfd_solver *h, double wait_limit_s, int withhold) {
@@ -2275,7 +2311,7 @@ int cgfd_batch_autotune(cgfd_batch *b, int steps, float *best_ms) {
   }
   float best = 1e30f;
   WorkParams bestp = pair_get_work(b->plan);
-  for (const WorkParams &wp : tuning_candidates()) {
+  for (const WorkParams &wp : tuning_candidates(bestp)) {
     if (!pair_set_work(b->plan, wp)) continue;
     b->ready = false;
     st = batch_build(b);

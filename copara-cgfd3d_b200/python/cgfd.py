@@ -99,6 +99,8 @@ _SIGS = {
     "cgfd_batch_sync": (C.c_int, [_P, C.c_double]),
     "cgfd_batch_autotune": (C.c_int, [_P, C.c_int, _fp]),
     "cgfd_batch_set_launch": (C.c_int, [_P, C.c_int]),
+    "cgfd_get_work_shape": (C.c_int, [_P, _ip, _ip, C.POINTER(C.c_double)]),
+    "cgfd_set_work_shape": (C.c_int, [_P, C.c_int, C.c_int, C.c_double]),
     "cgfd_batch_get_launch": (C.c_int, [_P, _ip]),
     "cgfd_batch_last_error": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
     "cgfd_batch_destroy": (C.c_int, [_P]),
@@ -262,6 +264,19 @@ class Solver:
         ms = C.c_float()
         self._chk(_lib.cgfd_autotune(self._h, steps, C.byref(ms)))
         return ms.value
+
+    @property
+    def work_shape(self) -> tuple:
+        """(items per resident CTA, shortest z-chunk, PML cost weight) of the
+        work list in use (cgfd_get_work_shape; after prepare)."""
+        a, b, c = C.c_int(), C.c_int(), C.c_double()
+        self._chk(_lib.cgfd_get_work_shape(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return (a.value, b.value, c.value)
+
+    @work_shape.setter
+    def work_shape(self, shape):
+        self._chk(_lib.cgfd_set_work_shape(self._h, int(shape[0]), int(shape[1]),
+                                           float(shape[2])))
 
     def test_withhold_copy(self, wait_limit_s: float, withhold: int):
         """Test hook of the bounded device waits (cgfd_test_withhold_copy):

@@ -298,8 +298,9 @@ int cgfd_mlp_gradient(const void *weights_fp16, const float *x, const float *t, 
 /* ------------------------------ autotuning ------------------------------- */
 
 /* Tries the work-list shapes of the default kernel family (items per
- * resident CTA, z-chunk length, PML cost weight), times `steps` steps of
- * each (after one warm-up step), keeps the fastest and reports its time per
+ * resident CTA 3/6/12, shortest z-chunk 12/16/24/32 planes, PML cost weight
+ * 1/2, and the shape in use), times `steps` steps of each (after one
+ * warm-up step), keeps the fastest and reports its time per
  * step in *ms_per_step.  The wavefields, auxiliaries, seismograms and step
  * count are saved before and restored after, so the simulation is
  * unchanged; the run needs steps + 1 steps of room in nt and the source time
@@ -307,6 +308,12 @@ int cgfd_mlp_gradient(const void *weights_fp16, const float *x, const float *t, 
  * No reference counterpart (the reference reads BlockPerGrid/ThreadPerBlock
  * from its configuration file). */
 int cgfd_autotune(cgfd_solver *h, int steps, float *ms_per_step);
+/* The work-list shape in use (after cgfd_prepare, default kernel family):
+ * items per resident CTA, shortest z-chunk in planes, PML cost weight of the
+ * item order; the autotuner's choice can be read and set on another solver
+ * of the same model without tuning again.  No reference counterpart. */
+int cgfd_get_work_shape(cgfd_solver *h, int *items_per_cta, int *min_chunk, double *pml_weight);
+int cgfd_set_work_shape(cgfd_solver *h, int items_per_cta, int min_chunk, double pml_weight);
 
 /* Test hook of the bounded device waits (no reference counterpart: the
  * reference's waits are cudaDeviceSynchronize calls that abort on error,

@@ -87,6 +87,27 @@ def test_autotune_keeps_state_and_results():
     ref.close()
 
 
+def test_work_shape_is_readable_settable_and_leaves_results_bit_equal():
+    """The work-list shape (cgfd_get/set_work_shape) changes only which CTA
+    computes which (tile, z-chunk) item: the results stay bit-equal."""
+    m = models.small_hill(nt=40)
+    a = cgfd.Solver(m.desc())
+    m.load(a)
+    a.prepare()
+    assert a.work_shape == (6, 16, 1.0)  # the default
+    a.work_shape = (3, 12, 2.0)
+    assert a.work_shape == (3, 12, 2.0)
+    with pytest.raises(cgfd.CgfdError):
+        a.work_shape = (0, 12, 1.0)
+    a.step(20)
+    b = cgfd.Solver(m.desc())
+    m.load(b)
+    b.step(20)
+    assert np.array_equal(a.seismograms(), b.seismograms())
+    a.close()
+    b.close()
+
+
 def test_batch_autotune_keeps_results():
     ms = _small_batch(n=2, nt=30)
     b = cgfd.Batch([m.desc() for m in ms])
