@@ -1887,9 +1887,9 @@ static int snapshot_restore(cgfd_solver *h, Snapshot &sn) {
 // one than it started from)
 static std::vector<WorkParams> tuning_candidates(const WorkParams &current) {
   std::vector<WorkParams> v{current};
-  for (int ipc : {3, 6, 12})
-    for (int mc : {12, 16, 24, 32})
-      for (double pw : {1.0, 2.0}) {
+  for (int ipc : {3, 6, 12, 24})
+    for (int mc : {12, 16, 24, 32, 48})
+      for (double pw : {1.0, 2.0, 3.0}) {
         const WorkParams w{ipc, mc, pw};
         if (w.items_per_cta != current.items_per_cta || w.min_chunk != current.min_chunk ||
             w.pml_weight != current.pml_weight)

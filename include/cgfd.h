@@ -298,8 +298,8 @@ int cgfd_mlp_gradient(const void *weights_fp16, const float *x, const float *t, 
 /* ------------------------------ autotuning ------------------------------- */
 
 /* Tries the work-list shapes of the default kernel family (items per
- * resident CTA 3/6/12, shortest z-chunk 12/16/24/32 planes, PML cost weight
- * 1/2, and the shape in use), times `steps` steps of each (after one
+ * resident CTA 3/6/12/24, shortest z-chunk 12/16/24/32/48 planes, PML cost
+ * weight 1/2/3, and the shape in use), times `steps` steps of each (after one
  * warm-up step), keeps the fastest and reports its time per
  * step in *ms_per_step.  The wavefields, auxiliaries, seismograms and step
  * count are saved before and restored after, so the simulation is
