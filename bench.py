@@ -53,6 +53,9 @@ def parse():
                    help="batch64: tune the work list and launch shape before timing")
     p.add_argument("--storage", choices=("f32", "f16", "bf16"), default="f32",
                    help="storage type of the field sets (arithmetic is FP32)")
+    p.add_argument("--ref-build", choices=("optimised", "shipped"), default="optimised",
+                   help="reference arm: the reference's calculate.cu built -O3 for sm_100a "
+                        "(default) or as it ships (-arch=sm_60 -G, PTX JIT on the B200)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -353,7 +356,9 @@ def run_reference(args):
     models.use_preprocessing("oracle")
     nt = args.warmup + args.steps + 2
     m = build_model(args.config, nt)
-    r = refio.run(m, args.warmup + args.steps, timeout=3600, fields=False)
+    shipped = args.ref_build == "shipped"
+    r = refio.run(m, args.warmup + args.steps, timeout=3600, fields=False,
+                  binary=refio.REF_BIN_SHIPPED if shipped else None)
     mapped = product_library_mapped()
     if mapped:
         raise RuntimeError("the reference arm mapped the solver library")
@@ -364,6 +369,7 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded model generator)", "impl": "reference",
+        "reference_build": args.ref_build,
         "config": config_dict(args.config, m),
         "product_library_mapped": mapped,
         "preprocessing": "CPU oracle (FP64 restatement of calmetric / CalCFSfactors / "
@@ -371,8 +377,10 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                          "sample": f"{workload_name(args.config)}, {args.steps} steps after "
                                    f"{args.warmup} warm-up; the reference's own calculate.cu "
-                                   "(CUDA-only path) built from its sources, driven by one host "
-                                   "thread on the B200"},
+                                   "(CUDA-only path) built from its sources "
+                                   + ("as it ships (-arch=sm_60 -G, PTX JIT)" if shipped else
+                                      "(-O3, sm_100a)")
+                                   + ", driven by one host thread on the B200"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))

@@ -19,6 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_BIN = os.path.join(HERE, "_ref", "ref_wavesim")
 # the same runtime built with the reference's SrcSmooth option
 REF_BIN_SMOOTH = os.path.join(HERE, "_ref", "ref_wavesim_smooth")
+# the same runtime built as the reference ships it (-arch=sm_60 -G)
+REF_BIN_SHIPPED = os.path.join(HERE, "_ref", "ref_wavesim_shipped")
 MAGIC = 0x52464743
 
 
@@ -108,7 +110,7 @@ def read_output(path, shape, fields=True, peak_velocity=False, nsnap=0, snap_tin
 
 
 def run(m, nsteps, init_fields=None, nstages=0, timeout=1800, fields=True, focal=False,
-        peak_velocity=False, snap_points=None, snap_tinv=1):
+        peak_velocity=False, snap_points=None, snap_tinv=1, binary=None):
     """Runs the reference on the GPU; returns read_output()'s dict: the
     seismograms (HPW), the step times, and as asked the final FW and W
     fields, the peak velocities (Dpv, [3][nx][ny]) and the snapshot samples
@@ -119,7 +121,10 @@ def run(m, nsteps, init_fields=None, nstages=0, timeout=1800, fields=True, focal
         raise ValueError("the SrcSmooth build spreads every moment and force")
     if focal and getattr(m, "foc_smooth", None) is not None:
         raise ValueError("the driver takes focal points without smoothing")
-    binary = REF_BIN_SMOOTH if smooth else REF_BIN
+    if binary is None:
+        binary = REF_BIN_SMOOTH if smooth else REF_BIN
+    elif smooth:
+        raise ValueError("smoothed sources need the SrcSmooth build")
     if not os.path.exists(binary):
         raise FileNotFoundError(f"{binary} not built (make -C {HERE}/ref)")
     nsnap = 0 if snap_points is None else len(np.asarray(snap_points).reshape(-1, 3))
