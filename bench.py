@@ -444,24 +444,50 @@ def run_target(args, plain_value, plain_ms, local):
                         "20-cell PML, FP16 against FP32 storage)"}
 
 
+def near_face_receivers(m, inset=30, spacing=25):
+    """Receivers inset cells inside the absorbing faces (outside a 20-cell
+    layer): on the surface along the four side faces, and on a grid inset
+    cells above the bottom; reference indices."""
+    LFD = 3
+    top = m.nk + LFD - 1
+    pts = set()
+    for i in range(inset, m.ni - inset, spacing):
+        pts.add((LFD + i, LFD + inset, top))
+        pts.add((LFD + i, LFD + m.nj - 1 - inset, top))
+    for j in range(inset, m.nj - inset, spacing):
+        pts.add((LFD + inset, LFD + j, top))
+        pts.add((LFD + m.ni - 1 - inset, LFD + j, top))
+    for i in range(inset, m.ni - inset, 4 * spacing):
+        for j in range(inset, m.nj - inset, 4 * spacing):
+            pts.add((LFD + i, LFD + j, LFD + inset))
+    return np.array(sorted(pts), np.int32)
+
+
 def run_target_accuracy(args, local):
     """Reflected-energy fraction of the thin-layer configurations against the
     plain 20-cell CFS-PML run, and the seismogram error of FP16 storage
-    against FP32 storage, over args.target_accuracy steps of the workload
-    (surface receivers)."""
+    against FP32 storage, over args.target_accuracy steps of the workload:
+    at the model's surface receivers and at receivers 30 cells inside the
+    absorbing faces (near_face_receivers)."""
+    import dataclasses
     import cgfd
     n = args.target_accuracy
-    m20 = build_model(args.config, n + 2)
+
+    def with_face_receivers(m):
+        return dataclasses.replace(m, rcv_loc=np.concatenate([m.rcv_loc, near_face_receivers(m)]))
+
+    m20 = with_face_receivers(build_model(args.config, n + 2))
+    nsurf = len(m20.rcv_loc) - len(near_face_receivers(m20))
     s = cgfd.Solver(m20.desc(device=local))
     m20.load(s)
     s.step(n)
     u20 = s.seismograms()[:3, :, :n].astype(np.float64)
     s.close()
-    m4 = build_model(args.config, n + 2, nabs=THIN)
-    out = {}
+    m4 = with_face_receivers(build_model(args.config, n + 2, nabs=THIN))
+    out = {"receivers_surface": nsurf, "receivers_near_faces": len(m20.rcv_loc) - nsurf}
 
-    def refl(u):
-        return float(((u - u20) ** 2).sum() / (u20 ** 2).sum())
+    def refl(u, sel):
+        return float(((u[:, sel] - u20[:, sel]) ** 2).sum() / (u20[:, sel] ** 2).sum())
 
     runs = {}
     for name, storage, mlp in (("pml4_f32", cgfd.STORE_F32, False),
@@ -472,12 +498,13 @@ def run_target_accuracy(args, local):
         b.sync()
         runs[name] = b.models[0].seismograms()[:3, :, :n].astype(np.float64)
         b.close()
-        out["reflected_energy_" + name] = refl(runs[name])
+        out["reflected_energy_" + name] = refl(runs[name], slice(0, nsurf))
+        out["reflected_energy_near_faces_" + name] = refl(runs[name], slice(nsurf, None))
     f16, f32 = runs["pml4_mlp_f16_batched"], runs["pml4_mlp_f32"]
     out["seismogram_rel_l2_f16_vs_f32"] = [float(np.linalg.norm(f16[c] - f32[c]) /
                                                  np.linalg.norm(f32[c])) for c in range(3)]
     line = {"mode": "target accuracy", "workload": workload_name(args.config), "steps": n,
-            "reference": "plain FP32 run with the 20-cell CFS-PML, same grid, surface receivers",
+            "reference": "plain FP32 run with the 20-cell CFS-PML, same grid",
             **out}
     print(json.dumps(line))
 
