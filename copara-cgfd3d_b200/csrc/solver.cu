@@ -2323,10 +2323,17 @@ int cgfd_batch_autotune(cgfd_batch *b, int steps, float *best_ms) {
     if (st) break;
     if (ms < best) { best = ms; bestp = wp; }
   }
-  // the other launch shape: every member's own step graphs
+  // the other launch shape: every member's own step graphs, each with its
+  // own work shape tuned first (cgfd_autotune restores the member's state)
   bool members_best = false;
   if (!st) {
     b->member_launch = true;
+    for (size_t i = 0; i < b->m.size() && !st; ++i) {
+      b->m[i]->steps = sn[i].steps;
+      float member_ms = 0;
+      st = cgfd_autotune(b->m[i], steps, &member_ms);
+      if (st) st = batch_fail(b, st, b->m[i]->err);
+    }
     for (size_t i = 0; i < b->m.size(); ++i) b->m[i]->steps = sn[i].steps;
     float ms = 0;
     st = cgfd_batch_step(b, 1);  // warm-up

@@ -353,7 +353,8 @@ int cgfd_batch_step(cgfd_batch *b, int n_steps);
 int cgfd_batch_step_timed(cgfd_batch *b, int n_steps, float *ms);
 int cgfd_batch_sync(cgfd_batch *b, double timeout_s);
 /* cgfd_autotune for the batch: the shared work list's shapes and the launch
- * shape; the state and the seismograms are restored afterwards */
+ * shape (for the members shape, every member's own work shape is tuned
+ * first); the state and the seismograms are restored afterwards */
 int cgfd_batch_autotune(cgfd_batch *b, int steps, float *ms_per_step);
 #define CGFD_BATCH_PERSISTENT 0
 #define CGFD_BATCH_MEMBERS 1
