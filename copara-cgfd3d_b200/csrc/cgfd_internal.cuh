@@ -243,7 +243,7 @@ size_t mlp_delta_smem();
 void mlp_set_attrs();
 void launch_mlp_step(const void *fw, int elem, size_t fs, const ScaleSet &sc, const float *lam2mu,
                      const float *irho, const int4 *cells, int n, const void *w, const float *gain,
-                     float *delta, void *stream);
+                     int width, float *delta, void *stream);
 void launch_mlp_features(const void *fw, int elem, size_t fs, const ScaleSet &sc,
                          const float *lam2mu, const float *irho, const int4 *cells, int n,
                          float *xs, float *scales, float *zs, void *stream);

@@ -69,6 +69,10 @@ constexpr int OW3 = OB2 + NH, OB3 = OW3 + NOUT * NH, NPAR = OB3 + NOUT;
 static_assert(NPAR == CGFD_MLP_PARAMS, "parameter count of the ABI");
 
 __device__ __forceinline__ float silu(float a) { return a / (1.f + __expf(-a)); }
+// the inference form: one fast reciprocal instead of an IEEE division (its
+// relative error, a few units in the last FP32 place, is far below the FP16
+// rounding of the activation that follows)
+__device__ __forceinline__ float silu_fast(float a) { return __fdividef(a, 1.f + __expf(-a)); }
 // d silu / da
 __device__ __forceinline__ float dsilu(float a) {
   const float s = 1.f / (1.f + __expf(-a));
@@ -91,9 +95,13 @@ struct TileSmem {
   __half x[16 * LDX];  // normalised features of the 16 cells, FP16
   float own[16 * NOUT];  // the cells' own 9 normalised values (FP32)
   float scale[16], z[16];
+  int depth[16];       // the cells' depths in the layer (gain rows)
 };
 constexpr int INF_WARPS = 4;
-constexpr size_t INF_SMEM = sizeof(WSmem) + INF_WARPS * sizeof(TileSmem);
+constexpr int MAX_WIDTH = 16;  // widest layer cgfd_set_boundary_mlp accepts
+// weights, the gain table [MAX_WIDTH][NOUT] and the warps' tiles
+constexpr size_t INF_SMEM =
+    sizeof(WSmem) + MAX_WIDTH * NOUT * sizeof(float) + INF_WARPS * sizeof(TileSmem);
 
 __device__ __forceinline__ uint32_t pack_h2(float a, float b) {
   const __half2 h = __floats2half2_rn(a, b);
@@ -136,49 +144,58 @@ __device__ void load_weights(const __half *w, WSmem &s) {
 
 // The features of the warp's 16 cells (cells[q0 .. q0+15], fewer at the
 // end) into the tile: lane & 15 is the cell, lanes 0-15 take stencil points
-// 0-2 and lanes 16-31 points 3-4.  Returns nothing; a cell without a
-// correction gets scale 0 and zero features.
+// 0-2 and lanes 16-31 points 3-4.  Every loop has a fixed trip count, so
+// the lane's 27 (18) field loads are all issued before the first use and
+// its values stay in registers.  A cell without a correction gets scale 0
+// and zero features.
 template <typename T>
-__device__ void stage_features(const T *fw, size_t fs, const float *sc, const float *lam2mu,
-                               const float *irho, const int4 *cells, int n, int q0,
-                               TileSmem &tl) {
+__device__ __forceinline__ void stage_features(const T *fw, size_t fs, const float *sc,
+                                               const float *lam2mu, const float *irho,
+                                               const int4 *cells, int n, int q0, TileSmem &tl) {
   const int lane = threadIdx.x & 31, r = lane & 15, half = lane >> 4;
   const int q = q0 + r;
   const bool live = q < n;
   int4 cell = make_int4(0, 0, 0, 0);
-  float z = 1.f;
-  if (live) {
-    cell = cells[q];
-    z = sqrtf(lam2mu[cell.x] / irho[cell.x]);  // rho vp
-  }
-  const int s0 = half ? 3 : 0, s1 = half ? 5 : 3;
+  if (live) cell = cells[q];
+  const int s0 = half ? 3 : 0, np = half ? 2 : 3;  // first stencil point, points taken
   float v[3][NOUT];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const bool on = live && k < np;
+    const size_t o = on ? (size_t)((long)cell.x + (long)(s0 + k) * cell.y) : 0;
+#pragma unroll
+    for (int c = 0; c < NOUT; ++c) v[k][c] = on ? Elem<T>::ld(fw + (size_t)c * fs + o) : 0.f;
+  }
+  const float z = live ? sqrtf(lam2mu[cell.x] / irho[cell.x]) : 1.f;  // rho vp
   float m = 0.f;
-  for (int s = s0; s < s1; ++s)
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
     for (int c = 0; c < NOUT; ++c) {
-      float x = 0.f;
-      if (live) {
-        x = Elem<T>::ld(fw + (size_t)c * fs + cell.x + (long)s * cell.y) * sc[c];
-        if (c >= 3) x /= z;
-      }
-      v[s - s0][c] = x;
+      float x = v[k][c] * sc[c];
+      if (c >= 3) x /= z;
+      v[k][c] = x;
       m = fmaxf(m, fabsf(x));
     }
   m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 16));
   const bool on = live && m > MIN_SCALE;
   const float rinv = on ? 1.f / m : 0.f;
-  __half *xr = tl.x + r * LDX;
-  for (int s = s0; s < s1; ++s)
+  __half *xr = tl.x + r * LDX + s0 * NOUT;
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
     for (int c = 0; c < NOUT; ++c) {
-      const float x = v[s - s0][c] * rinv;
-      xr[s * NOUT + c] = __float2half_rn(x);
-      if (s == 0) tl.own[r * NOUT + c] = x;
+      const float x = v[k][c] * rinv;
+      if (k < np) xr[k * NOUT + c] = __float2half_rn(x);
+      if (k == 0 && !half) tl.own[r * NOUT + c] = x;
     }
   if (half) {
-    for (int k = NIN; k < LDX; ++k) xr[k] = __float2half(0.f);
+#pragma unroll
+    for (int k = NIN; k < LDX; ++k) tl.x[r * LDX + k] = __float2half(0.f);
   } else {
     tl.scale[r] = on ? m : 0.f;
     tl.z[r] = z;
+    tl.depth[r] = cell.z;
   }
 }
 
@@ -209,10 +226,10 @@ __device__ void mlp_tile(const WSmem &w, const TileSmem &tl, float (&out)[2][4])
 #pragma unroll
   for (int ks = 0; ks < 4; ++ks) {
     const float *c0 = acc[2 * ks], *c1 = acc[2 * ks + 1];
-    ha[ks][0] = pack_h2(silu(c0[0]), silu(c0[1]));
-    ha[ks][1] = pack_h2(silu(c0[2]), silu(c0[3]));
-    ha[ks][2] = pack_h2(silu(c1[0]), silu(c1[1]));
-    ha[ks][3] = pack_h2(silu(c1[2]), silu(c1[3]));
+    ha[ks][0] = pack_h2(silu_fast(c0[0]), silu_fast(c0[1]));
+    ha[ks][1] = pack_h2(silu_fast(c0[2]), silu_fast(c0[3]));
+    ha[ks][2] = pack_h2(silu_fast(c1[0]), silu_fast(c1[1]));
+    ha[ks][3] = pack_h2(silu_fast(c1[2]), silu_fast(c1[3]));
   }
   // layer 2: [16 x 64] x [64 x 64]
 #pragma unroll
@@ -230,10 +247,10 @@ __device__ void mlp_tile(const WSmem &w, const TileSmem &tl, float (&out)[2][4])
 #pragma unroll
   for (int ks = 0; ks < 4; ++ks) {
     const float *c0 = acc[2 * ks], *c1 = acc[2 * ks + 1];
-    ha[ks][0] = pack_h2(silu(c0[0]), silu(c0[1]));
-    ha[ks][1] = pack_h2(silu(c0[2]), silu(c0[3]));
-    ha[ks][2] = pack_h2(silu(c1[0]), silu(c1[1]));
-    ha[ks][3] = pack_h2(silu(c1[2]), silu(c1[3]));
+    ha[ks][0] = pack_h2(silu_fast(c0[0]), silu_fast(c0[1]));
+    ha[ks][1] = pack_h2(silu_fast(c0[2]), silu_fast(c0[3]));
+    ha[ks][2] = pack_h2(silu_fast(c1[0]), silu_fast(c1[1]));
+    ha[ks][3] = pack_h2(silu_fast(c1[2]), silu_fast(c1[3]));
   }
   // layer 3: [16 x 64] x [64 x 16]
 #pragma unroll
@@ -250,17 +267,21 @@ __device__ void mlp_tile(const WSmem &w, const TileSmem &tl, float (&out)[2][4])
     }
 }
 
-// corrections of all layer cells into delta [9][n] (values, not stored units)
+// corrections of all layer cells into delta [9][n] (values, not stored units);
+// gain: [width][9], width <= MAX_WIDTH
 template <typename T>
 __global__ void __launch_bounds__(INF_WARPS * 32)
     delta_kernel(const T *__restrict__ fw, size_t fs, ScaleSet scs, const float *lam2mu,
                  const float *irho, const int4 *__restrict__ cells, int n,
-                 const __half *__restrict__ wts, const float *__restrict__ gain,
+                 const __half *__restrict__ wts, const float *__restrict__ gain, int width,
                  float *__restrict__ delta) {
   extern __shared__ __align__(16) unsigned char smem[];
   WSmem &w = *reinterpret_cast<WSmem *>(smem);
-  TileSmem &tl = reinterpret_cast<TileSmem *>(smem + sizeof(WSmem))[threadIdx.x >> 5];
-  load_weights(wts, w);
+  float *sgain = reinterpret_cast<float *>(smem + sizeof(WSmem));
+  TileSmem &tl = reinterpret_cast<TileSmem *>(smem + sizeof(WSmem) +
+                                               MAX_WIDTH * NOUT * sizeof(float))[threadIdx.x >> 5];
+  for (int q = threadIdx.x; q < width * NOUT; q += blockDim.x) sgain[q] = gain[q];
+  load_weights(wts, w);  // ends with a block barrier
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int warp = blockIdx.x * INF_WARPS + (threadIdx.x >> 5);
   const int nwarps = gridDim.x * INF_WARPS;
@@ -281,7 +302,7 @@ __global__ void __launch_bounds__(INF_WARPS * 32)
         float d = 0.f;
         if (s > 0.f) {
           const float u = tl.own[r * NOUT + c];
-          d = gain[cells[q].z * NOUT + c] * GAIN * tanhf(y[nt][e] / GAIN);
+          d = sgain[tl.depth[r] * NOUT + c] * GAIN * tanhf(y[nt][e] / GAIN);
           d = fminf(fmaxf(d, fminf(0.f, -u)), fmaxf(0.f, -u));
         }
         delta[(size_t)c * n + q] = d * s * (c < 3 ? 1.f : tl.z[r]);
@@ -290,16 +311,20 @@ __global__ void __launch_bounds__(INF_WARPS * 32)
   }
 }
 
+// one thread per layer cell: its 9 components read first, then written
 template <typename T>
-__global__ void apply_kernel(T *__restrict__ fw, size_t fs, ScaleSet scs,
-                             const int4 *__restrict__ cells, int n,
-                             const float *__restrict__ delta) {
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
-    for (int c = 0; c < NOUT; ++c) {
-      T *p = fw + (size_t)c * fs + cells[q].x;
-      // in stored units: the component's scale divides the correction
-      Elem<T>::st(p, Elem<T>::ld(p) + delta[(size_t)c * n + q] / scs.sc[c]);
-    }
+__global__ void __launch_bounds__(256)
+    apply_kernel(T *__restrict__ fw, size_t fs, ScaleSet scs, const int4 *__restrict__ cells,
+                 int n, const float *__restrict__ delta) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  T *p = fw + (size_t)cells[q].x;
+  float u[NOUT];
+#pragma unroll
+  for (int c = 0; c < NOUT; ++c)  // in stored units: the component's scale divides the correction
+    u[c] = Elem<T>::ld(p + (size_t)c * fs) + delta[(size_t)c * n + q] / scs.sc[c];
+#pragma unroll
+  for (int c = 0; c < NOUT; ++c) Elem<T>::st(p + (size_t)c * fs, u[c]);
 }
 
 // normalised features and scales of all layer cells (training samples):
@@ -459,14 +484,14 @@ int mlp_blocks(int n) {
 template <typename T>
 void mlp_step_t(const void *fw, size_t fs, const ScaleSet &sc, const float *lam2mu,
                 const float *irho, const int4 *cells, int n, const void *w, const float *gain,
-                float *delta, cudaStream_t s) {
+                int width, float *delta, cudaStream_t s) {
   // every 16 cells are one warp's tile
   int blocks = (n + 16 * mlp::INF_WARPS - 1) / (16 * mlp::INF_WARPS);
   blocks = blocks < 1 ? 1 : (blocks < 4 * 148 ? blocks : 4 * 148);
   mlp::delta_kernel<T><<<blocks, mlp::INF_WARPS * 32, mlp::INF_SMEM, s>>>(
-      (const T *)fw, fs, sc, lam2mu, irho, cells, n, (const __half *)w, gain, delta);
-  mlp::apply_kernel<T><<<mlp_blocks(n), 128, 0, s>>>((T *)const_cast<void *>(fw), fs, sc, cells,
-                                                     n, delta);
+      (const T *)fw, fs, sc, lam2mu, irho, cells, n, (const __half *)w, gain, width, delta);
+  mlp::apply_kernel<T><<<(n + 255) / 256, 256, 0, s>>>((T *)const_cast<void *>(fw), fs, sc,
+                                                       cells, n, delta);
 }
 }  // namespace
 
@@ -481,14 +506,15 @@ void mlp_set_attrs() {
 
 void launch_mlp_step(const void *fw, int elem, size_t fs, const ScaleSet &sc, const float *lam2mu,
                      const float *irho, const int4 *cells, int n, const void *w, const float *gain,
-                     float *delta, void *stream) {
+                     int width, float *delta, void *stream) {
   cudaStream_t s = (cudaStream_t)stream;
+  if (n <= 0 || width < 1 || width > mlp::MAX_WIDTH) return;  // the setter refuses such layers
   if (elem == ELEM_F16)
-    mlp_step_t<__half>(fw, fs, sc, lam2mu, irho, cells, n, w, gain, delta, s);
+    mlp_step_t<__half>(fw, fs, sc, lam2mu, irho, cells, n, w, gain, width, delta, s);
   else if (elem == ELEM_BF16)
-    mlp_step_t<__nv_bfloat16>(fw, fs, sc, lam2mu, irho, cells, n, w, gain, delta, s);
+    mlp_step_t<__nv_bfloat16>(fw, fs, sc, lam2mu, irho, cells, n, w, gain, width, delta, s);
   else
-    mlp_step_t<float>(fw, fs, sc, lam2mu, irho, cells, n, w, gain, delta, s);
+    mlp_step_t<float>(fw, fs, sc, lam2mu, irho, cells, n, w, gain, width, delta, s);
 }
 
 void launch_mlp_features(const void *fw, int elem, size_t fs, const ScaleSet &sc,

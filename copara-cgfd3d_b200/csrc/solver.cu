@@ -724,7 +724,8 @@ ScaleSet field_scales(const cgfd_solver *h) {
 void launch_mlp(cgfd_solver *h, cudaStream_t st) {
   const size_t fs = h->g.fstride;
   launch_mlp_step(h->set[0], h->elem, fs, field_scales(h), h->media, h->media + 2 * fs,
-                  h->d_mlp_cells, h->mlp_n, h->d_mlp_w, h->d_mlp_gain, h->d_mlp_delta, st);
+                  h->d_mlp_cells, h->mlp_n, h->d_mlp_w, h->d_mlp_gain, h->mlp_width,
+                  h->d_mlp_delta, st);
 }
 
 // the peak-velocity update of one step

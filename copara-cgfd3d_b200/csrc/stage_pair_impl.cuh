@@ -239,6 +239,49 @@ __device__ __forceinline__ void stt2(T *p, int m, f2 v) {
   }
 }
 
+// The per-thread register window of the z-stencil holds the staged
+// components as stored: a float2 for FP32, the raw 16-bit pair (one 32-bit
+// register) for FP16 / BF16, widened at use.  The widening is exact, so the
+// arithmetic is that of a widened window, at half its registers (the 16-bit
+// kernels run at 168 registers to fit three CTAs per SM).
+template <typename T> struct Win {
+  using type = f2;
+  __device__ __forceinline__ static f2 get(f2 v) { return v; }
+  __device__ __forceinline__ static type ld(const T *p) { return ldp(p); }
+  __device__ __forceinline__ static type ldm(const T *p, int m) { return ldt2(p, m); }
+  __device__ __forceinline__ static type zero() { return S2(0.f); }
+};
+template <> struct Win<__half> {
+  using type = __half2;
+  __device__ __forceinline__ static f2 get(__half2 v) { return __half22float2(v); }
+  __device__ __forceinline__ static type ld(const __half *p) {
+    return *reinterpret_cast<const __half2 *>(p);
+  }
+  __device__ __forceinline__ static type zero() { return __float2half2_rn(0.f); }
+  __device__ __forceinline__ static type ldm(const __half *p, int m) {
+    if (m == 3) return ld(p);
+    __half2 r = zero();
+    if (m & 1) r.x = p[0];
+    if (m & 2) r.y = p[1];
+    return r;
+  }
+};
+template <> struct Win<__nv_bfloat16> {
+  using type = __nv_bfloat162;
+  __device__ __forceinline__ static f2 get(__nv_bfloat162 v) { return __bfloat1622float2(v); }
+  __device__ __forceinline__ static type ld(const __nv_bfloat16 *p) {
+    return *reinterpret_cast<const __nv_bfloat162 *>(p);
+  }
+  __device__ __forceinline__ static type zero() { return __float2bfloat162_rn(0.f); }
+  __device__ __forceinline__ static type ldm(const __nv_bfloat16 *p, int m) {
+    if (m == 3) return ld(p);
+    __nv_bfloat162 r = zero();
+    if (m & 1) r.x = p[0];
+    if (m & 2) r.y = p[1];
+    return r;
+  }
+};
+
 // 16-bit storage keeps the RK accumulator as its difference from the step
 // state, tW - FW: the difference is about a time step's change of the field,
 // an order of magnitude below the field, so its FP16/BF16 rounding is that
@@ -427,15 +470,17 @@ struct AuxIdx {
 template <typename T, int X, int Y, int Z, int KIND>
 __device__ __forceinline__ void vel_pair(const StageArgs &a, const Pair &e, const Plane &pl,
                                          const T *H, int ry, int cb, const Pw2<T> &pw,
-                                         const f2 (&w)[6][5], float rx, float rys, float rz) {
+                                         const typename Win<T>::type (&w)[6][5], float rx,
+                                         float rys, float rz) {
   constexpr int HX = Halo<T>::HX, HPL = Halo<T>::HPL;
   const size_t fs = a.g.fstride;
+  auto W = [&](int s, int q) { return Win<T>::get(w[s][q]); };
   // 1/h factors carry the staged component's scale (stored units -> values)
   auto sr = [&](float r, int s) { return scaled<T>(r, a.sc[TXX + s]); };
-  auto dx = [&](int s) { return dx_pair<X>(H + s * HPL + ry * HX, cb, w[s][3], sr(rx, s)); };
-  auto dy = [&](int s) { return dy_pair<Y>(H + s * HPL, ry, cb, w[s][3], sr(rys, s)); };
+  auto dx = [&](int s) { return dx_pair<X>(H + s * HPL + ry * HX, cb, W(s, 3), sr(rx, s)); };
+  auto dy = [&](int s) { return dy_pair<Y>(H + s * HPL, ry, cb, W(s, 3), sr(rys, s)); };
   auto dz = [&](int s) {
-    return drp2(w[s][4], w[s][3], w[s][2], w[s][1], w[s][0], sr(rz, s));
+    return drp2(W(s, 4), W(s, 3), W(s, 2), W(s, 1), W(s, 0), sr(rz, s));
   };
   T *out = static_cast<T *>(a.out), *tw = static_cast<T *>(a.tw);
   auto adt = [&](int c) { return scaled<T>(a.adt, a.isc[c]); };
@@ -550,16 +595,18 @@ __device__ __forceinline__ f2 mat_row(const float *mv, size_t plane, int r, f2 u
 template <typename T, int X, int Y, int Z, int KIND>
 __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, const Plane &pl,
                                          const T *H, int ry, int cb, const Pw2<T> &pw,
-                                         const f2 (&w)[3][5], float rx, float rys, float rz) {
+                                         const typename Win<T>::type (&w)[3][5], float rx,
+                                         float rys, float rz) {
   constexpr int HX = Halo<T>::HX, HPL = Halo<T>::HPL;
   const Geom &g = a.g;
+  auto W = [&](int s, int q) { return Win<T>::get(w[s][q]); };
   const size_t fs = g.fstride;
   // 1/h factors carry the staged component's scale (stored units -> values)
   auto sr = [&](float r, int s) { return scaled<T>(r, a.sc[VX + s]); };
-  auto dx = [&](int s) { return dx_pair<X>(H + s * HPL + ry * HX, cb, w[s][3], sr(rx, s)); };
-  auto dy = [&](int s) { return dy_pair<Y>(H + s * HPL, ry, cb, w[s][3], sr(rys, s)); };
+  auto dx = [&](int s) { return dx_pair<X>(H + s * HPL + ry * HX, cb, W(s, 3), sr(rx, s)); };
+  auto dy = [&](int s) { return dy_pair<Y>(H + s * HPL, ry, cb, W(s, 3), sr(rys, s)); };
   auto dz = [&](int s) {
-    return drp2(w[s][4], w[s][3], w[s][2], w[s][1], w[s][0], sr(rz, s));
+    return drp2(W(s, 4), W(s, 3), W(s, 2), W(s, 1), W(s, 0), sr(rz, s));
   };
   T *out = static_cast<T *>(a.out), *tw = static_cast<T *>(a.tw);
 
@@ -595,13 +642,13 @@ __device__ __forceinline__ void str_pair(const StageArgs &a, const Pair &e, cons
     DzVz = add2(mat_row(mv + 9 * g.plane, g.plane, 6, DyVx, DyVy, DyVz),
                 mat_row(mv, g.plane, 6, DxVx, DxVy, DxVz));
   } else if (pl.iz == g.top - 1) {  // 2-point (M22)
-    DzVx = mul2(add2(w[0][2], neg2(w[0][3])), S2(sr(rz, 0)));
-    DzVy = mul2(add2(w[1][2], neg2(w[1][3])), S2(sr(rz, 1)));
-    DzVz = mul2(add2(w[2][2], neg2(w[2][3])), S2(sr(rz, 2)));
+    DzVx = mul2(add2(W(0, 2), neg2(W(0, 3))), S2(sr(rz, 0)));
+    DzVy = mul2(add2(W(1, 2), neg2(W(1, 3))), S2(sr(rz, 1)));
+    DzVz = mul2(add2(W(2, 2), neg2(W(2, 3))), S2(sr(rz, 2)));
   } else if (pl.iz == g.top - 2) {  // Gottlieb 2-4 (M24)
     auto m24 = [&](int s) {
-      return mul2(fma2(S2(CGFD_MA2), w[s][1], fma2(S2(CGFD_MA1), w[s][2],
-                                                  mul2(S2(CGFD_MA0), w[s][3]))), S2(sr(rz, s)));
+      return mul2(fma2(S2(CGFD_MA2), W(s, 1), fma2(S2(CGFD_MA1), W(s, 2),
+                                                  mul2(S2(CGFD_MA0), W(s, 3)))), S2(sr(rz, s)));
     };
     DzVx = m24(0);
     DzVy = m24(1);
@@ -903,18 +950,18 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
                           (j0 + TY <= g.nj - g.nabs[3]);
 
     // register window: w[c][q] = plane (current) + DIR * (q - 3)
-    f2 w[NC][5];
+    typename Win<T>::type w[NC][5];
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
-      for (int q = 0; q < 5; ++q) w[c][q] = S2(0.f);
+      for (int q = 0; q < 5; ++q) w[c][q] = Win<T>::zero();
     auto push_smem = [&](const unsigned char *slot) {
       const T *plane = reinterpret_cast<const T *>(slot);
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) w[c][q] = w[c][q + 1];
-        w[c][4] = ldp(plane + c * HPL + sc);
+        w[c][4] = Win<T>::ld(plane + c * HPL + sc);
       }
     };
     // the three planes behind the chunk come straight from global memory
@@ -925,7 +972,7 @@ __global__ void __launch_bounds__(TT, MinCtas<T>::value)
 #pragma unroll
         for (int q = 0; q < 4; ++q) w[c][q] = w[c][q + 1];
         const T *src = static_cast<const T *>(A.in) + (size_t)(C0 + c) * fs + o;
-        w[c][4] = e.m ? ldt2(src, e.m) : S2(0.f);
+        w[c][4] = e.m ? Win<T>::ldm(src, e.m) : Win<T>::zero();
       }
     }
     // A wait that expires sets the CTA-wide abort flag; the flag is read only
