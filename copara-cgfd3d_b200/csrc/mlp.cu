@@ -167,13 +167,14 @@ __device__ __forceinline__ void stage_features(const T *fw, size_t fs, const flo
     for (int c = 0; c < NOUT; ++c) v[k][c] = on ? Elem<T>::ld(fw + (size_t)c * fs + o) : 0.f;
   }
   const float z = live ? sqrtf(lam2mu[cell.x] / irho[cell.x]) : 1.f;  // rho vp
+  const float rz = 1.f / z;
   float m = 0.f;
 #pragma unroll
   for (int k = 0; k < 3; ++k)
 #pragma unroll
     for (int c = 0; c < NOUT; ++c) {
       float x = v[k][c] * sc[c];
-      if (c >= 3) x /= z;
+      if (c >= 3) x *= rz;
       v[k][c] = x;
       m = fmaxf(m, fabsf(x));
     }
@@ -336,12 +337,12 @@ __global__ void features_kernel(const T *__restrict__ fw, size_t fs, ScaleSet sc
                                 float *__restrict__ scales, float *__restrict__ zs) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
     const int4 cell = cells[q];
-    const float z = sqrtf(lam2mu[cell.x] / irho[cell.x]);
+    const float z = sqrtf(lam2mu[cell.x] / irho[cell.x]), rz = 1.f / z;
     float x[NIN], m = 0.f;
     for (int s = 0; s < 5; ++s)
       for (int c = 0; c < NOUT; ++c) {
         float v = Elem<T>::ld(fw + (size_t)c * fs + cell.x + (long)s * cell.y) * scs.sc[c];
-        if (c >= 3) v /= z;
+        if (c >= 3) v *= rz;
         x[s * NOUT + c] = v;
         m = fmaxf(m, fabsf(v));
       }
