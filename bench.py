@@ -59,6 +59,12 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--pml", type=int, default=0, metavar="N",
+                   help="single models: an N-cell CFS-PML on the five absorbing faces instead "
+                        "of the workload's own")
+    p.add_argument("--mlp", action="store_true",
+                   help="single models: the learned thin layer (committed weights, width 4) "
+                        "after every step; implies --pml 4 unless --pml is given")
     p.add_argument("--no-target", action="store_true",
                    help="skip the batched FP16 learned-thin-layer timing on the same model")
     p.add_argument("--target-accuracy", type=int, default=0, metavar="STEPS",
@@ -82,17 +88,22 @@ def build_model(cfg, nt, nabs=None):
                                  **({"nabs": tuple(nabs)} if nabs else {}))
 
 
-def workload_name(cfg):
-    return {"hill600": "gaussian_hill_600x600x250_random_layers_pml20",
+def workload_name(cfg, pml=0, mlp=False):
+    """The workload's name; pml replaces its CFS-PML width, mlp adds the
+    learned layer."""
+    name = {"hill600": "gaussian_hill_600x600x250_random_layers_pml20",
             "hill400": "gaussian_hill_400x400x200_pml20",
             "flat160": "flat_halfspace_160x160x80_pml12",
             "hill256": "gaussian_hill_256x256x128_pml20",
             "batch64": "batch_64_hill_models_96-256_pml12"}[cfg]
+    if pml:
+        name = name[:name.rindex("_pml")] + f"_pml{pml}"
+    return name + ("_mlp" if mlp else "")
 
 
-def config_dict(cfg, m, storage="f32"):
+def config_dict(cfg, m, storage="f32", pml=0, mlp=False):
     """The workload description both arms print (same keys, same values)."""
-    return {"workload": workload_name(cfg), "cells": m.cells,
+    return {"workload": workload_name(cfg, pml, mlp), "cells": m.cells,
             "grid": [m.ni, m.nj, m.nk], "pml_cells": list(m.nabs), "storage": storage,
             "receivers": int(len(m.rcv_loc)),
             "l2": "state >> L2 (126 MB), no flush needed"}
@@ -404,15 +415,20 @@ def thin_members(m, n=2):
     return out
 
 
+def set_layer(s):
+    """The learned thin layer with the committed weights and gains."""
+    d = np.load(MLP_WEIGHTS)
+    s.set_boundary_mlp(THIN[0], d["weights"].astype(np.float16))
+    s.set_boundary_mlp_gains(d["gains"].astype(np.float32))
+
+
 def thin_batch(ms, storage, device, mlp=True):
     import cgfd
     b = cgfd.Batch([mm.desc(storage=storage, device=device) for mm in ms])
-    d = np.load(MLP_WEIGHTS)
     for mm, s in zip(ms, b.models):
         mm.load(s)
         if mlp:
-            s.set_boundary_mlp(4, d["weights"].astype(np.float16))
-            s.set_boundary_mlp_gains(d["gains"].astype(np.float32))
+            set_layer(s)
     b.prepare()
     return b
 
@@ -529,10 +545,13 @@ def main():
     K, W = args.steps, args.warmup
     K2 = min(K, 20)
     nt = W + K + K2 + 2 + (4 if args.autotune else 0)
-    m = build_model(args.config, nt)
+    pml = args.pml or (THIN[0] if args.mlp else 0)
+    m = build_model(args.config, nt, nabs=(pml,) * 5 + (0,) if pml else None)
     storage = {"f32": cgfd.STORE_F32, "f16": cgfd.STORE_F16, "bf16": cgfd.STORE_BF16}[args.storage]
     s = cgfd.Solver(m.desc(kernel=kernel, device=local, storage=storage))
     m.load(s)
+    if args.mlp:
+        set_layer(s)
     s.prepare()
     tuned = s.autotune(steps=2) if args.autotune and args.kernel == "fused" else None
     work_shape = list(s.work_shape) if args.kernel == "fused" else None
@@ -555,6 +574,8 @@ def main():
         t0 = time.perf_counter()
         s2 = cgfd.Solver(m.desc(kernel=kernel, device=local, storage=storage))
         m.load(s2)
+        if args.mlp:
+            set_layer(s2)
         if work_shape is not None:  # the shape the autotuner chose, as a user reuses it
             s2.prepare()
             s2.work_shape = work_shape
@@ -575,7 +596,7 @@ def main():
     bps = algorithmic_bytes_per_step(m, 4 if args.storage == "f32" else 2)
     achieved = bps / 4 / (stage_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    traffic = committed_traffic(workload_name(args.config),
+    traffic = committed_traffic(workload_name(args.config, pml, args.mlp),
                                 args.kernel if args.storage == "f32" else
                                 f"{args.kernel}_{args.storage}")
     traffic_src = ("profiles/stage_traffic.json: ncu dram__bytes of an earlier capture of "
@@ -585,7 +606,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
         "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded model generator)",
-        "config": config_dict(args.config, m, args.storage),
+        "config": config_dict(args.config, m, args.storage, pml, args.mlp),
         "kernel": args.kernel, "replicas": world, "autotuned_ms_per_step": tuned,
         "work_shape": work_shape,
         "parallelism": "replicas" if world > 1 else "single",
@@ -595,12 +616,14 @@ def main():
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_step": bps, "stage_kernel_ms": stage_ms},
         "clocks": clk.summary(),
-        "gpu_launches": K * (4 * (1 if args.kernel == "simple" else 3) + 4 * n_src + 1),
+        "gpu_launches": K * (4 * (1 if args.kernel == "simple" else 3) + 4 * n_src + 1 +
+                             (2 if args.mlp else 0)),
         "nonfinite": nbad,
     }
     if e2e:
         line["e2e"] = e2e
-    if not args.no_target and world == 1 and args.storage == "f32" and args.kernel == "fused":
+    if (not args.no_target and world == 1 and args.storage == "f32" and args.kernel == "fused"
+            and not pml):
         line["target"] = run_target(args, value, ms / K, local)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.config, args.cpu_seconds)
