@@ -49,6 +49,9 @@ def parse():
                    help="tune the work list before timing (state unchanged; the default for "
                         "single models; batch64 tunes only when asked)")
     p.add_argument("--no-autotune", dest="autotune", action="store_false")
+    p.add_argument("--work-shape", default=None, metavar="ITEMS,CHUNK,PMLW",
+                   help="single models: use this work shape (items per resident CTA, minimum "
+                        "z-chunk, PML cost weight; a line's work_shape) instead of tuning")
     p.add_argument("--tune-batch", action="store_true",
                    help="batch64: tune the work list and launch shape before timing")
     p.add_argument("--storage", choices=("f32", "f16", "bf16"), default="f32",
@@ -261,14 +264,17 @@ def measured_peak():
 
 def committed_traffic(workload, kernel):
     """Per-launch DRAM bytes of the stage kernel from the committed ncu
-    summary (profiles/stage_traffic.json), or None."""
+    summary (profiles/stage_traffic.json) and the work shape it was captured
+    at (None where the summary does not name one), or (None, None)."""
     p = os.path.join(ROOT, "profiles", "stage_traffic.json")
     if not os.path.exists(p):
-        return None
+        return None, None
     with open(p) as f:
         d = json.load(f)
     e = d.get(workload, {}).get(kernel)
-    return None if e is None else float(e["dram_bytes_per_launch"])
+    if e is None:
+        return None, None
+    return float(e["dram_bytes_per_launch"]), e.get("work_shape")
 
 
 def cpu_sample_model(cfg, nt):
@@ -553,7 +559,12 @@ def main():
     if args.mlp:
         set_layer(s)
     s.prepare()
-    tuned = s.autotune(steps=2) if args.autotune and args.kernel == "fused" else None
+    tuned = None
+    if args.work_shape and args.kernel == "fused":
+        ws = args.work_shape.split(",")
+        s.work_shape = (int(ws[0]), int(ws[1]), float(ws[2]))
+    elif args.autotune and args.kernel == "fused":
+        tuned = s.autotune(steps=2)
     work_shape = list(s.work_shape) if args.kernel == "fused" else None
     s.step(W)
     s.sync()
@@ -596,11 +607,15 @@ def main():
     bps = algorithmic_bytes_per_step(m, 4 if args.storage == "f32" else 2)
     achieved = bps / 4 / (stage_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    traffic = committed_traffic(workload_name(args.config, pml, args.mlp),
-                                args.kernel if args.storage == "f32" else
-                                f"{args.kernel}_{args.storage}")
-    traffic_src = ("profiles/stage_traffic.json: ncu dram__bytes of an earlier capture of "
-                   "this workload, per stage, not measured in this run") if traffic else None
+    traffic, traffic_shape = committed_traffic(
+        workload_name(args.config, pml, args.mlp),
+        args.kernel if args.storage == "f32" else f"{args.kernel}_{args.storage}")
+    traffic_src = None
+    if traffic:
+        traffic_src = ("profiles/stage_traffic.json: ncu dram__bytes of an earlier capture of "
+                       "this workload, per stage, not measured in this run")
+        if traffic_shape is not None:
+            traffic_src += f" (captured at work shape {traffic_shape})"
     n_src = 1 if (len(m.mnt_loc) + len(m.frc_loc)) else 0
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
