@@ -48,6 +48,7 @@
 // sums across the block's chunks; per-block partial gradients are summed in
 // block order by a second kernel, so the result does not depend on timing.
 #include "../../include/cgfd.h"
+#include "abi_guard.h"
 #include "cgfd_internal.cuh"
 #include "elem.cuh"
 
@@ -555,6 +556,7 @@ std::vector<GradBuffers> g_grad;
 
 extern "C" int cgfd_mlp_gradient(const void *weights_fp16, const float *x, const float *t, int n,
                                  float *grad, float *loss) {
+  CGFD_ABI_BEGIN
   if (!weights_fp16 || !x || !t || n < 1 || !grad || !loss) {
     set_global_error("cgfd_mlp_gradient: bad arguments");
     return CGFD_ERR_ARG;
@@ -606,4 +608,5 @@ extern "C" int cgfd_mlp_gradient(const void *weights_fp16, const float *x, const
     return CGFD_ERR_CUDA;
   }
   return CGFD_OK;
+  CGFD_ABI_END(nullptr)
 }

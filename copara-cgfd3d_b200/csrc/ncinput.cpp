@@ -3,8 +3,10 @@
 // (focal) series file.  Two-call pattern: with the data pointers NULL the
 // functions return the sizes only.
 #include "../../include/cgfd.h"
+#include "abi_guard.h"
 #include "ncread.h"
 
+#include <climits>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -31,6 +33,7 @@ extern "C" {
 // with the grid's z coordinates as stored (the reference does the same).
 int cgfd_read_media_volume_nc(const char *path, int *nvx, int *nvy, int *nvz, double *vx,
                               double *vy, double *vz, float *vp, float *vs, float *rho) {
+  CGFD_ABI_BEGIN
   if (!path || !nvx || !nvy || !nvz) return fail("cgfd_read_media_volume_nc: null argument");
   nc::File f;
   if (!f.open(path)) return fail(f.err);
@@ -38,7 +41,11 @@ int cgfd_read_media_volume_nc(const char *path, int *nvx, int *nvy, int *nvz, do
   const long long n[3] = {f.dim("x"), f.dim("y"), f.dim(zname)};
   if (n[0] < 2 || n[1] < 2 || n[2] < 2)
     return fail(std::string(path) + ": dimensions x, y and depth (or z) of at least 2 needed");
-  const long long total = n[0] * n[1] * n[2];
+  if (n[0] > INT_MAX || n[1] > INT_MAX || n[2] > INT_MAX)
+    return fail(std::string(path) + ": a dimension exceeds the int range");
+  long long total = 0;
+  if (__builtin_mul_overflow(n[0], n[1], &total) || __builtin_mul_overflow(total, n[2], &total))
+    return fail(std::string(path) + ": the volume's size overflows");
   const bool query = !vx;
   if (!query && (*nvx != n[0] || *nvy != n[1] || *nvz != n[2]))
     return fail("cgfd_read_media_volume_nc: the arrays' sizes differ from the file's");
@@ -66,6 +73,7 @@ int cgfd_read_media_volume_nc(const char *path, int *nvx, int *nvy, int *nvz, do
     for (long long q = 0; q < total; ++q) outs[c][q] = (float)v[q];
   }
   return CGFD_OK;
+  CGFD_ABI_END(nullptr)
 }
 
 // source::source + readdata for source_type 1 (src/source.cpp:43-56,
@@ -75,11 +83,14 @@ int cgfd_read_media_volume_nc(const char *path, int *nvx, int *nvy, int *nvz, do
 // the reference's simulate_damp factor is the caller's to apply.
 int cgfd_read_focal_nc(const char *path, int *np, int *nt, double *dt, double *posx,
                        double *posy, double *posz, float *mom) {
+  CGFD_ABI_BEGIN
   if (!path || !np || !nt || !dt) return fail("cgfd_read_focal_nc: null argument");
   nc::File f;
   if (!f.open(path)) return fail(f.err);
   const long long p = f.dim("NP"), t = f.dim("NT");
   if (p < 1 || t < 1) return fail(std::string(path) + ": dimensions NP and NT needed");
+  if (p > INT_MAX || t > INT_MAX)
+    return fail(std::string(path) + ": NP or NT exceeds the int range");
   auto it = f.gatts.find("DT");
   if (it == f.gatts.end() || it->second.empty() || !(it->second[0] > 0.0))
     return fail(std::string(path) + ": a positive global attribute DT is needed");
@@ -109,6 +120,7 @@ int cgfd_read_focal_nc(const char *path, int *np, int *nt, double *dt, double *p
     for (long long q = 0; q < p; ++q) pos[a][q] = v[q];
   }
   return CGFD_OK;
+  CGFD_ABI_END(nullptr)
 }
 
 }  // extern "C"

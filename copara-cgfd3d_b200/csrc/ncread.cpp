@@ -127,6 +127,9 @@ bool File::open(const char *path) {
     return false;
   }
   r.version = magic[3];
+  if (fseeko(r.f, 0, SEEK_END) != 0) { err = std::string(path) + ": cannot seek"; return false; }
+  fsize = (uint64_t)ftello(r.f);
+  fseeko(r.f, 4, SEEK_SET);
   numrecs = r.count();
   // dimensions
   uint64_t tag = r.be(4), n = r.count();
@@ -208,10 +211,26 @@ bool File::shape(const std::string &name, std::vector<size_t> *out) const {
 bool File::read(const std::string &name, std::vector<double> *out) {
   const Var *v = var(name);
   if (!v) { err = path + ": no variable " + name; return false; }
-  const size_t sz = type_size(v->type);
-  size_t per = 1;  // values per record (or in all of a fixed variable)
-  for (size_t d = is_record(*v) ? 1 : 0; d < v->dims.size(); ++d) per *= dims[v->dims[d]].len;
+  const uint64_t sz = type_size(v->type);
+  // values per record (or in all of a fixed variable), and the extent of the
+  // data in the file, checked against the file's size before anything is
+  // allocated (a damaged header cannot ask for more memory than the file holds)
+  uint64_t per = 1;
+  bool bad = false;
+  for (size_t d = is_record(*v) ? 1 : 0; d < v->dims.size(); ++d)
+    bad |= __builtin_mul_overflow(per, (uint64_t)dims[v->dims[d]].len, &per);
   const uint64_t nrec = is_record(*v) ? numrecs : 1;
+  uint64_t bytes = 0, end = 0;
+  bad |= __builtin_mul_overflow(per, sz, &bytes);
+  bad |= nrec > 1 && recsize < bytes;  // records overlap
+  if (!bad && nrec > 0 && per > 0) {
+    uint64_t last = 0;
+    bad |= __builtin_mul_overflow(nrec - 1, recsize, &last);
+    bad |= __builtin_add_overflow(v->begin, last, &end);
+    bad |= __builtin_add_overflow(end, bytes, &end);
+    bad |= end > fsize;
+  }
+  if (bad) { err = path + ": data of " + name + " lies outside the file"; return false; }
   std::unique_ptr<FILE, int (*)(FILE *)> f(std::fopen(path.c_str(), "rb"), std::fclose);
   if (!f) { err = "cannot reopen " + path; return false; }
   out->assign(per * nrec, 0.0);

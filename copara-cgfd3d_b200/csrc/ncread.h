@@ -24,6 +24,7 @@ struct File {
   };
   std::string path, err;
   uint64_t numrecs = 0, recsize = 0;
+  uint64_t fsize = 0;  // bytes in the file: every variable's data must lie inside
   std::vector<Dim> dims;
   std::vector<Var> vars;
   std::map<std::string, std::vector<double>> gatts;  // numeric global attributes

@@ -29,6 +29,7 @@
 // streams, or from different host threads) race on it and must be serialised
 // by the caller.
 #include "../../include/cgfd.h"
+#include "abi_guard.h"
 #include "cgfd_internal.cuh"
 #include "nonfinite.cuh"
 
@@ -53,6 +54,7 @@ static __device__ __align__(256) unsigned long long g_nonfinite_scratch[NOALLOC_
 
 extern "C" int cgfd_count_nonfinite_noalloc(const float *d_values, size_t n, long long *n_bad,
                                             void *stream) {
+  CGFD_ABI_BEGIN
   if (!n_bad || (n > 0 && !d_values)) {
     set_global_error("cgfd_count_nonfinite_noalloc: null argument");
     return CGFD_ERR_ARG;
@@ -113,4 +115,5 @@ extern "C" int cgfd_count_nonfinite_noalloc(const float *d_values, size_t n, lon
   }
   if (prev >= 0 && prev != attr.device) cudaSetDevice(prev);
   return status;
+  CGFD_ABI_END(nullptr)
 }

@@ -19,6 +19,7 @@
 //   source smoothing         src/source.cpp:157-378 (MomentShiftPosition,
 //                            eighth_locate, cal_norm; the SrcSmooth build)
 #include "../../include/cgfd.h"
+#include "abi_guard.h"
 
 #include <algorithm>
 #include <cmath>
@@ -255,6 +256,7 @@ extern "C" {
 
 int cgfd_metric_from_coords(int ni, int nj, int nk, double steph, const double *x,
                             const double *y, const double *z, double *const out[10]) {
+  CGFD_ABI_BEGIN
   if (ni < 1 || nj < 1 || nk < 1 || !(steph > 0) || !x || !y || !z || !out)
     return CGFD_ERR_ARG;
   for (int q = 0; q < 10; ++q)
@@ -293,6 +295,7 @@ int cgfd_metric_from_coords(int ni, int nj, int nk, double steph, const double *
       }
   for (int q = 0; q < 10; ++q) mirror_ghosts(out[q], D, ni, nj, nk);
   return CGFD_OK;
+  CGFD_ABI_END(nullptr)
 }
 
 int cgfd_cfs_factors(int ni, int nj, int nk, const int nabs[6], const double velabs[6],
@@ -300,6 +303,7 @@ int cgfd_cfs_factors(int ni, int nj, int nk, const int nabs[6], const double vel
                      const double *dly, const double *dlz, double *apd_x, double *apd_y,
                      double *apd_z, double *b_x, double *b_y, double *b_z, double *db_x,
                      double *db_y, double *db_z) {
+  CGFD_ABI_BEGIN
   if (ni < 1 || nj < 1 || nk < 1 || !nabs || !velabs || !bmax || !amax || !dlx || !dly ||
       !dlz || !apd_x || !apd_y || !apd_z || !b_x || !b_y || !b_z || !db_x || !db_y || !db_z)
     return CGFD_ERR_ARG;
@@ -347,9 +351,11 @@ int cgfd_cfs_factors(int ni, int nj, int nk, const int nabs[6], const double vel
     }
   }
   return CGFD_OK;
+  CGFD_ABI_END(nullptr)
 }
 
 int cgfd_stf(int type, double start, double t0, double f0, int n, double dt, float *out) {
+  CGFD_ABI_BEGIN
   if (n < 0 || (n > 0 && !out)) return CGFD_ERR_ARG;
   if (type < CGFD_STF_GAUSS || type > CGFD_STF_STEP) return CGFD_ERR_ARG;
   for (int q = 0; q < n; ++q) {
@@ -379,9 +385,11 @@ int cgfd_stf(int type, double start, double t0, double f0, int n, double dt, flo
     out[q] = std::fabs(v) < 1e-20 ? 0.f : (float)v;
   }
   return CGFD_OK;
+  CGFD_ABI_END(nullptr)
 }
 
 int cgfd_angle2moment(double strike, double dip, double rake, double m6[6]) {
+  CGFD_ABI_BEGIN
   if (!m6) return CGFD_ERR_ARG;
   const double s = strike * kPi / 180.0, d = dip * kPi / 180.0, r = rake * kPi / 180.0;
   const double sd = std::sin(d), cd = std::cos(d), s2d = std::sin(2 * d), c2d = std::cos(2 * d);
@@ -397,11 +405,13 @@ int cgfd_angle2moment(double strike, double dip, double rake, double m6[6]) {
   m6[4] = -(cd * cr * cs + c2d * sr * ss);
   m6[5] = -(cd * cr * ss - c2d * sr * cs);
   return CGFD_OK;
+  CGFD_ABI_END(nullptr)
 }
 
 int cgfd_grid_vmap(int ni, int nj, int nk, int nsurf, const int *gridpoints,
                    const int *equalspacing, const double *anchor, int hybrid,
                    double convers_depth, double *x, double *y, double *z, int *con_index) {
+  CGFD_ABI_BEGIN
   if (ni < 1 || nj < 1 || nk < 2 || nsurf < 2 || !gridpoints || !equalspacing || !anchor || !x ||
       !y || !z || !con_index)
     return grid_fail("bad arguments");
@@ -518,6 +528,7 @@ int cgfd_grid_vmap(int ni, int nj, int nk, int nsurf, const int *gridpoints,
   extend_linear(y, D, ni, nj, nk);
   extend_linear(z, D, ni, nj, nk);
   return CGFD_OK;
+  CGFD_ABI_END(nullptr)
 }
 
 int cgfd_media_volume(int ni, int nj, int nk, const double *x, const double *y, const double *z,
@@ -525,6 +536,7 @@ int cgfd_media_volume(int ni, int nj, int nk, const double *x, const double *y, 
                       const double *vz, const float *vp, const float *vs, const float *rho,
                       double crit_value, double crit_perc, int sampx, int sampy, int sampz,
                       float *alpha, float *beta, float *dens) {
+  CGFD_ABI_BEGIN
   auto fail = [](const char *m) {
     cgfd::set_global_error((std::string("cgfd_media_volume: ") + m).c_str());
     return CGFD_ERR_ARG;
@@ -674,6 +686,7 @@ int cgfd_media_volume(int ni, int nj, int nk, const double *x, const double *y, 
     dens[g] = (float)out[2][g];
   }
   return CGFD_OK;
+  CGFD_ABI_END(nullptr)
 }
 
 }  // extern "C"
@@ -890,6 +903,7 @@ extern "C" {
 
 int cgfd_locate_points(int ni, int nj, int nk, const double *x, const double *y, const double *z,
                        double hyper_height, int n, const double *pos, int *loc, double *posz) {
+  CGFD_ABI_BEGIN
   if (ni < 1 || nj < 1 || nk < 1 || n < 0 || (n > 0 && (!x || !y || !z || !pos || !loc)))
     return locate_fail("bad arguments");
   const Dims D{ni + 6, nj + 6, nk + 6};
@@ -914,11 +928,13 @@ int cgfd_locate_points(int ni, int nj, int nk, const double *x, const double *y,
   if (!put(above, ba, true) || !put(below, bb, false))
     return locate_fail("no finite distance to any valid node");
   return CGFD_OK;
+  CGFD_ABI_END(nullptr)
 }
 
 int cgfd_source_smoothing(int ni, int nj, int nk, const double *x, const double *y,
                           const double *z, int kind, int n, const double *pos, int *loc,
                           double *weights) {
+  CGFD_ABI_BEGIN
   if (ni < 1 || nj < 1 || nk < 1 || n < 0 || (kind != 0 && kind != 1) ||
       (n > 0 && (!x || !y || !z || !pos || !loc || !weights)))
     return locate_fail("bad smoothing arguments");
@@ -939,6 +955,7 @@ int cgfd_source_smoothing(int ni, int nj, int nk, const double *x, const double 
       return locate_fail("smoothing weights sum to zero");
   }
   return CGFD_OK;
+  CGFD_ABI_END(nullptr)
 }
 
 }  // extern "C"

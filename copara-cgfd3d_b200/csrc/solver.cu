@@ -7,6 +7,7 @@
 // 1336-1353, RKite 1355-1600, wavesyn/abssyn 2956-3119, C2DPointPick/PWpick
 // 2678-2830), driven by the step loop of src/simulation.cc:252-711.
 #include "../../include/cgfd.h"
+#include "abi_guard.h"
 #include "cgfd_internal.cuh"
 #include "ncwrite.h"
 #include "nonfinite.cuh"
@@ -20,6 +21,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <limits>
 #include <memory>
 #include <string>
@@ -444,11 +446,35 @@ struct cgfd_solver {
   bool plain_interior = true;
 };
 
+void cgfd::set_global_error(const char *msg) { g_last_create_error = msg; }
+
 namespace {
+
+// "fn: host allocation or thread failure (what)" for the exception being
+// handled (called from inside a catch handler only)
+void exception_text(const char *fn, char *buf, size_t len) noexcept {
+  const char *what = "unknown C++ exception";
+  try {
+    throw;
+  } catch (const std::exception &e) {
+    what = e.what();
+  } catch (...) {
+  }
+  std::snprintf(buf, len, "%s: host allocation or thread failure (%s)", fn, what);
+}
 
 }  // namespace
 
-void cgfd::set_global_error(const char *msg) { g_last_create_error = msg; }
+int cgfd::abi_exception(const cgfd_solver *h, const char *fn) noexcept {
+  char buf[320];
+  exception_text(fn, buf, sizeof(buf));
+  try {
+    if (h) const_cast<cgfd_solver *>(h)->err = buf;
+    else g_last_create_error = buf;
+  } catch (...) {
+  }
+  return CGFD_ERR_NOMEM;
+}
 
 namespace {
 
@@ -895,6 +921,7 @@ int build_graphs(cgfd_solver *h) {
 extern "C" {
 
 int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
+  CGFD_ABI_BEGIN
   if (!d || !out) return arg_fail(nullptr, "null argument");
   *out = nullptr;
   if (d->ni < 1 || d->nj < 1 || d->nk < 4 || !(d->steph > 0) || !(d->stept > 0) || d->nt < 0)
@@ -1037,9 +1064,11 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
   h->wcur = 0;
   *out = h;
   return CGFD_OK;
+  CGFD_ABI_END(nullptr)
 }
 
 int cgfd_destroy(cgfd_solver *h) {
+  CGFD_ABI_BEGIN
   if (!h) return CGFD_OK;
   {
     DevGuard guard(h->d.device);
@@ -1048,16 +1077,20 @@ int cgfd_destroy(cgfd_solver *h) {
   }
   delete h;
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_last_error(const cgfd_solver *h, char *buf, size_t len) {
+  CGFD_ABI_BEGIN
   if (!buf || !len) return CGFD_ERR_ARG;
   std::snprintf(buf, len, "%s", h ? h->err.c_str() : g_last_create_error.c_str());
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_upload_metric(cgfd_solver *h, const double *zx, const double *zy, const double *zz,
                        const double *jac) {
+  CGFD_ABI_BEGIN
   if (!h || !zx || !zy || !zz || !jac) return arg_fail(h, "null argument");
   DevGuard guard(h->d.device);
   const long n = ref_n(h);
@@ -1133,9 +1166,11 @@ int cgfd_upload_metric(cgfd_solver *h, const double *zx, const double *zy, const
   h->have_metric = true;
   invalidate(h);
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_upload_media(cgfd_solver *h, const float *alpha, const float *beta, const float *rho) {
+  CGFD_ABI_BEGIN
   if (!h || !alpha || !beta || !rho) return arg_fail(h, "null argument");
   DevGuard guard(h->d.device);
   const long n = ref_n(h);
@@ -1191,11 +1226,13 @@ int cgfd_upload_media(cgfd_solver *h, const float *alpha, const float *beta, con
   h->have_media = true;
   invalidate(h);
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_upload_pml(cgfd_solver *h, const double *apdx, const double *apdy, const double *apdz,
                     const double *bx, const double *by, const double *bz, const double *dbx,
                     const double *dby, const double *dbz) {
+  CGFD_ABI_BEGIN
   if (!h || !apdx || !apdy || !apdz || !bx || !by || !bz || !dbx || !dby || !dbz)
     return arg_fail(h, "null argument");
   DevGuard guard(h->d.device);
@@ -1225,6 +1262,7 @@ int cgfd_upload_pml(cgfd_solver *h, const double *apdx, const double *apdy, cons
   h->have_pml = true;
   invalidate(h);
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 static int upload_points(cgfd_solver *h, int n, const int *loc, int ncoef, const float *coef,
@@ -1257,22 +1295,27 @@ static int upload_points(cgfd_solver *h, int n, const int *loc, int ncoef, const
 
 int cgfd_upload_moments(cgfd_solver *h, int n, const int *loc, const float *m6, int nstf,
                         const float *stf) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   h->smw[0].clear();
   return upload_points(h, n, loc, 6, m6, nstf, stf, h->mloc, h->m6, h->hmstf, h->d_mcell,
                        h->d_mstf, h->nmnt, h->nstfm);
+  CGFD_ABI_END(h)
 }
 
 int cgfd_upload_forces(cgfd_solver *h, int n, const int *loc, const float *f3, int nstf,
                        const float *stf) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   h->smw[1].clear();
   return upload_points(h, n, loc, 3, f3, nstf, stf, h->floc, h->f3, h->hfstf, h->d_fcell,
                        h->d_fstf, h->nfrc, h->nstff);
+  CGFD_ABI_END(h)
 }
 
 int cgfd_upload_focal(cgfd_solver *h, int n, const int *loc, int fnt, double fdt,
                       const float *mom) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   if (n < 0 || (n > 0 && (!loc || !mom || fnt < 1 || !(fdt > 0.0))))
     return arg_fail(h, "bad focal sources");
@@ -1302,9 +1345,11 @@ int cgfd_upload_focal(cgfd_solver *h, int n, const int *loc, int fnt, double fdt
   }
   invalidate(h);
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_set_source_smoothing(cgfd_solver *h, int kind, int n, const double *weights) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   if (kind < 0 || kind > 2) return arg_fail(h, "source smoothing: kind must be 0, 1 or 2");
   const int have = kind == 0 ? h->nmnt : (kind == 1 ? h->nfrc : h->nfoc);
@@ -1321,9 +1366,11 @@ int cgfd_set_source_smoothing(cgfd_solver *h, int kind, int n, const double *wei
   }
   invalidate(h);
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_set_receivers(cgfd_solver *h, int n, const int *loc) {
+  CGFD_ABI_BEGIN
   if (!h || n < 0 || (n > 0 && !loc)) return arg_fail(h, "bad receivers");
   for (int q = 0; q < n; ++q)
     if (!valid_loc(h, loc + 3 * q)) return arg_fail(h, "receiver outside the valid grid");
@@ -1342,6 +1389,7 @@ int cgfd_set_receivers(cgfd_solver *h, int n, const int *loc) {
   }
   invalidate(h);
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 // sets the per-component scale exponents of 16-bit storage, rescaling the
@@ -1362,6 +1410,7 @@ static int apply_scales(cgfd_solver *h, const int *e) {
 }
 
 int cgfd_set_field_scales(cgfd_solver *h, const int *exp2) {
+  CGFD_ABI_BEGIN
   if (!h || !exp2) return arg_fail(h, "null argument");
   for (int c = 0; c < NCOMP; ++c)
     if (exp2[c] < -60 || exp2[c] > 60) return arg_fail(h, "scale exponent out of range");
@@ -1377,12 +1426,15 @@ int cgfd_set_field_scales(cgfd_solver *h, const int *exp2) {
   h->user_scales = true;
   invalidate(h);
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_get_field_scales(cgfd_solver *h, int *exp2) {
+  CGFD_ABI_BEGIN
   if (!h || !exp2) return arg_fail(h, "null argument");
   for (int c = 0; c < NCOMP; ++c) exp2[c] = h->sexp[c];
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 }  // extern "C"
@@ -1469,6 +1521,7 @@ int build_spread(cgfd_solver *h) {
 extern "C" {
 
 int cgfd_prepare(cgfd_solver *h) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   if (!(h->have_metric && h->have_media && h->have_pml)) {
     h->err = "metric, media and PML must be uploaded before stepping";
@@ -1591,9 +1644,11 @@ int cgfd_prepare(cgfd_solver *h) {
   int st = build_graphs(h);
   if (st) return st;
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_step(cgfd_solver *h, int n_steps) {
+  CGFD_ABI_BEGIN
   if (!h || n_steps < 0) return arg_fail(h, "bad arguments");
   int st = cgfd_prepare(h);
   if (st) return st;
@@ -1612,9 +1667,11 @@ int cgfd_step(cgfd_solver *h, int n_steps) {
   }
   h->wcur = 0;
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms) {
+  CGFD_ABI_BEGIN
   if (!h || n_steps < 1 || !ms) return arg_fail(h, "bad arguments");
   int st = cgfd_prepare(h);
   if (st) return st;
@@ -1681,9 +1738,11 @@ int cgfd_step_timed(cgfd_solver *h, int n_steps, float *ms, float *stage_ms) {
   cudaEventDestroy(e1);
   h->wcur = 0;
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_rk_stage(cgfd_solver *h, int rk, int curr_t, int X, int Y, int Z) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   if (rk < 0 || rk > 3 || (X != 1 && X != -1) || (Y != 1 && Y != -1) || (Z != 1 && Z != -1) ||
       curr_t < 0)
@@ -1719,9 +1778,11 @@ int cgfd_rk_stage(cgfd_solver *h, int rk, int curr_t, int X, int Y, int Z) {
   }
   h->wcur = out;
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_sync(cgfd_solver *h, double timeout_s) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   DevGuard guard(h->d.device);
   const auto t0 = std::chrono::steady_clock::now();
@@ -1745,15 +1806,19 @@ int cgfd_sync(cgfd_solver *h, double timeout_s) {
     }
     std::this_thread::sleep_for(std::chrono::microseconds(50));
   }
+  CGFD_ABI_END(h)
 }
 
 int cgfd_steps_done(const cgfd_solver *h, int *n) {
+  CGFD_ABI_BEGIN
   if (!h || !n) return CGFD_ERR_ARG;
   *n = h->steps;
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_get_seismograms(cgfd_solver *h, float *out, int *nt_done) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   DevGuard guard(h->d.device);
   CK(h, cudaStreamSynchronize(h->st));
@@ -1762,6 +1827,7 @@ int cgfd_get_seismograms(cgfd_solver *h, float *out, int *nt_done) {
     CK(h, cudaMemcpy(out, h->d_seis, (size_t)9 * h->nrecv * h->d.nt * sizeof(float),
                      cudaMemcpyDeviceToHost));
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 static void *set_ptr(cgfd_solver *h, int set, int comp) {
@@ -1775,6 +1841,7 @@ static void *set_ptr(cgfd_solver *h, int set, int comp) {
 }
 
 int cgfd_get_field(cgfd_solver *h, int set, int comp, float *out) {
+  CGFD_ABI_BEGIN
   if (!h || !out) return arg_fail(h, "null argument");
   void *p = set_ptr(h, set, comp);
   if (!p) return arg_fail(h, "bad set or component");
@@ -1789,9 +1856,11 @@ int cgfd_get_field(cgfd_solver *h, int set, int comp, float *out) {
   if (st) return st;
   for (size_t t = 0; t < f.size(); ++t) out[t] += f[t];
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_set_field(cgfd_solver *h, int set, int comp, const float *in) {
+  CGFD_ABI_BEGIN
   if (!h || !in) return arg_fail(h, "null argument");
   void *p = set_ptr(h, set, comp);
   if (!p) return arg_fail(h, "bad set or component");
@@ -1816,9 +1885,11 @@ int cgfd_set_field(cgfd_solver *h, int set, int comp, const float *in) {
         v[t] = f.empty() ? in[t] : in[t] - f[t];
       }
   return upload_ref(h, v.data(), p, h->elem, std::ldexp(1.f, -h->sexp[comp]));
+  CGFD_ABI_END(h)
 }
 
 int cgfd_check_finite(cgfd_solver *h, long long *n_bad) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   DevGuard guard(h->d.device);
   if (h->elem == ELEM_F32)
@@ -1841,6 +1912,7 @@ int cgfd_check_finite(cgfd_solver *h, long long *n_bad) {
     return CGFD_ERR_NONFINITE;
   }
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 
@@ -1902,6 +1974,7 @@ static std::vector<WorkParams> tuning_candidates(const WorkParams &current) {
 extern "C" {
 
 int cgfd_autotune(cgfd_solver *h, int steps, float *best_ms) {
+  CGFD_ABI_BEGIN
   if (!h || steps < 1) return arg_fail(h, "bad arguments");
   if (h->d.kernel != CGFD_KERNEL_FUSED) return arg_fail(h, "autotuning needs the default kernel");
   int st = cgfd_prepare(h);
@@ -1931,9 +2004,11 @@ int cgfd_autotune(cgfd_solver *h, int steps, float *best_ms) {
   if (!st) st = build_graphs(h);
   if (best_ms) *best_ms = best / steps;
   return st;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_get_work_shape(cgfd_solver *h, int *items_per_cta, int *min_chunk, double *pml_weight) {
+  CGFD_ABI_BEGIN
   if (!h || !items_per_cta || !min_chunk || !pml_weight) return arg_fail(h, "null argument");
   if (h->d.kernel != CGFD_KERNEL_FUSED || !h->plan)
     return arg_fail(h, "work shapes belong to the default kernel after cgfd_prepare");
@@ -1942,9 +2017,11 @@ int cgfd_get_work_shape(cgfd_solver *h, int *items_per_cta, int *min_chunk, doub
   *min_chunk = w.min_chunk;
   *pml_weight = w.pml_weight;
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_set_work_shape(cgfd_solver *h, int items_per_cta, int min_chunk, double pml_weight) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   if (h->d.kernel != CGFD_KERNEL_FUSED || !h->plan)
     return arg_fail(h, "work shapes belong to the default kernel after cgfd_prepare");
@@ -1960,9 +2037,11 @@ int cgfd_set_work_shape(cgfd_solver *h, int items_per_cta, int min_chunk, double
   if (!pair_set_work(h->plan, w)) return arg_fail(h, "work list rejected for this model");
   h->graphs_ok = false;  // the step graphs hold the launch configuration
   return build_graphs(h);
+  CGFD_ABI_END(h)
 }
 
 int cgfd_test_withhold_copy(cgfd_solver *h, double wait_limit_s, int withhold) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   if (h->d.kernel != CGFD_KERNEL_FUSED || !h->plan)
     return arg_fail(h, "the wait test needs the default kernel");
@@ -1974,6 +2053,7 @@ int cgfd_test_withhold_copy(cgfd_solver *h, double wait_limit_s, int withhold) {
   if (!h->prepared) return CGFD_OK;  // cgfd_prepare builds them
   DevGuard guard(h->d.device);
   return build_graphs(h);
+  CGFD_ABI_END(h)
 }
 
 }  // extern "C"
@@ -2002,6 +2082,17 @@ struct cgfd_batch {
   int steps = 0;
   std::string err;
 };
+
+int cgfd::abi_exception(const cgfd_batch *b, const char *fn) noexcept {
+  char buf[320];
+  exception_text(fn, buf, sizeof(buf));
+  try {
+    if (b) const_cast<cgfd_batch *>(b)->err = buf;
+    else g_last_create_error = buf;
+  } catch (...) {
+  }
+  return CGFD_ERR_NOMEM;
+}
 
 static int batch_fail(cgfd_batch *b, int code, const std::string &msg) {
   if (b) b->err = msg;
@@ -2140,6 +2231,7 @@ static int batch_build(cgfd_batch *b) {
 extern "C" {
 
 int cgfd_batch_create(const cgfd_desc *descs, int n, cgfd_batch **out) {
+  CGFD_ABI_BEGIN
   if (!descs || !out || n < 1) return batch_fail(nullptr, CGFD_ERR_ARG, "bad batch arguments");
   *out = nullptr;
   for (int i = 0; i < n; ++i) {
@@ -2178,17 +2270,21 @@ int cgfd_batch_create(const cgfd_desc *descs, int n, cgfd_batch **out) {
   }
   *out = b;
   return CGFD_OK;
+  CGFD_ABI_END(nullptr)
 }
 
 int cgfd_batch_solver(cgfd_batch *b, int i, cgfd_solver **h) {
+  CGFD_ABI_BEGIN
   if (!b || !h || i < 0 || i >= (int)b->m.size())
     return batch_fail(b, CGFD_ERR_ARG, "bad model index");
   *h = b->m[i];
   b->ready = false;  // the caller may upload new inputs through it
   return CGFD_OK;
+  CGFD_ABI_END(b)
 }
 
 int cgfd_batch_prepare(cgfd_batch *b) {
+  CGFD_ABI_BEGIN
   if (!b) return batch_fail(b, CGFD_ERR_ARG, "null handle");
   for (cgfd_solver *h : b->m) {
     if (!h->prepared || !h->graphs_ok) b->ready = false;
@@ -2200,9 +2296,11 @@ int cgfd_batch_prepare(cgfd_batch *b) {
   if (b->ready) return CGFD_OK;
   DevGuard guard(b->device);
   return batch_build(b);
+  CGFD_ABI_END(b)
 }
 
 int cgfd_batch_step(cgfd_batch *b, int n_steps) {
+  CGFD_ABI_BEGIN
   if (!b || n_steps < 0) return batch_fail(b, CGFD_ERR_ARG, "bad arguments");
   int st = cgfd_batch_prepare(b);
   if (st) return st;
@@ -2249,9 +2347,11 @@ int cgfd_batch_step(cgfd_batch *b, int n_steps) {
     h->wcur = 0;
   }
   return CGFD_OK;
+  CGFD_ABI_END(b)
 }
 
 int cgfd_batch_sync(cgfd_batch *b, double timeout_s) {
+  CGFD_ABI_BEGIN
   if (!b) return batch_fail(b, CGFD_ERR_ARG, "null handle");
   DevGuard guard(b->device);
   const auto t0 = std::chrono::steady_clock::now();
@@ -2278,9 +2378,11 @@ int cgfd_batch_sync(cgfd_batch *b, double timeout_s) {
       return batch_fail(b, CGFD_ERR_TIMEOUT, "timeout waiting for the device");
     std::this_thread::sleep_for(std::chrono::microseconds(50));
   }
+  CGFD_ABI_END(b)
 }
 
 int cgfd_batch_step_timed(cgfd_batch *b, int n_steps, float *ms) {
+  CGFD_ABI_BEGIN
   if (!b || n_steps < 1 || !ms) return batch_fail(b, CGFD_ERR_ARG, "bad arguments");
   int st = cgfd_batch_prepare(b);
   if (st) return st;
@@ -2298,9 +2400,11 @@ int cgfd_batch_step_timed(cgfd_batch *b, int n_steps, float *ms) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return CGFD_OK;
+  CGFD_ABI_END(b)
 }
 
 int cgfd_batch_autotune(cgfd_batch *b, int steps, float *best_ms) {
+  CGFD_ABI_BEGIN
   if (!b || steps < 1) return batch_fail(b, CGFD_ERR_ARG, "bad arguments");
   int st = cgfd_batch_prepare(b);
   if (st) return st;
@@ -2352,29 +2456,37 @@ int cgfd_batch_autotune(cgfd_batch *b, int steps, float *best_ms) {
   if (!st) st = batch_build(b);
   if (best_ms) *best_ms = best / steps;
   return st;
+  CGFD_ABI_END(b)
 }
 
 int cgfd_batch_set_launch(cgfd_batch *b, int shape) {
+  CGFD_ABI_BEGIN
   if (!b || (shape != CGFD_BATCH_PERSISTENT && shape != CGFD_BATCH_MEMBERS))
     return batch_fail(b, CGFD_ERR_ARG, "bad launch shape");
   b->member_launch = shape == CGFD_BATCH_MEMBERS;
   return CGFD_OK;
+  CGFD_ABI_END(b)
 }
 
 int cgfd_batch_get_launch(cgfd_batch *b, int *shape) {
+  CGFD_ABI_BEGIN
   if (!b || !shape) return batch_fail(b, CGFD_ERR_ARG, "null argument");
   *shape = b->member_launch ? CGFD_BATCH_MEMBERS : CGFD_BATCH_PERSISTENT;
   return CGFD_OK;
+  CGFD_ABI_END(b)
 }
 
 int cgfd_batch_last_error(cgfd_batch *b, char *buf, size_t len) {
+  CGFD_ABI_BEGIN
   if (!buf || len == 0) return CGFD_ERR_ARG;
   const std::string &m = b ? b->err : std::string();
   std::snprintf(buf, len, "%s", m.c_str());
   return CGFD_OK;
+  CGFD_ABI_END(b)
 }
 
 int cgfd_batch_destroy(cgfd_batch *b) {
+  CGFD_ABI_BEGIN
   if (!b) return CGFD_OK;
   {
     DevGuard guard(b->device);
@@ -2384,12 +2496,14 @@ int cgfd_batch_destroy(cgfd_batch *b) {
   for (cgfd_solver *h : b->m) cgfd_destroy(h);
   delete b;
   return CGFD_OK;
+  CGFD_ABI_END(b)
 }
 
 
 // ------------------------------- outputs -----------------------------------
 
 int cgfd_enable_peak_velocity(cgfd_solver *h, int on) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   DevGuard guard(h->d.device);
   CK(h, cudaStreamSynchronize(h->st));
@@ -2402,9 +2516,11 @@ int cgfd_enable_peak_velocity(cgfd_solver *h, int on) {
   }
   invalidate(h);  // the step graphs gain or lose the update
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_get_peak_velocity(cgfd_solver *h, float *out) {
+  CGFD_ABI_BEGIN
   if (!h || !out) return arg_fail(h, "null argument");
   if (!h->d_pgv) {
     h->err = "peak velocity is not enabled";
@@ -2421,10 +2537,12 @@ int cgfd_get_peak_velocity(cgfd_solver *h, float *out) {
         out[((size_t)q * ni + i) * nj + j] =
             v[(size_t)q * h->g.plane + (size_t)(j + LFD) * h->g.px + i + XO];
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_get_snapshot(cgfd_solver *h, int set, const int *start, const int *count,
                       const int *stride, int comp_mask, float *out) {
+  CGFD_ABI_BEGIN
   if (!h || !start || !count || !stride || !out) return arg_fail(h, "null argument");
   if (comp_mask <= 0 || comp_mask >= (1 << NCOMP)) return arg_fail(h, "bad component mask");
   const int n3[3] = {h->d.ni + 6, h->d.nj + 6, h->d.nk + 6};
@@ -2474,12 +2592,14 @@ int cgfd_get_snapshot(cgfd_solver *h, int set, const int *start, const int *coun
   if (e != cudaSuccess) return cuda_fail(h, e, "snapshot");
   for (size_t t = 0; t < fw.size(); ++t) out[t] += fw[t];
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 // seismo.nc of the reference (src/seisnc.cpp:1229-1364) in NetCDF classic:
 // TimeNum (record) x PointNum; Vx..Tyz, currTime = (it+1)*stept, Pnum, Lnum,
 // posx/posy/posz
 int cgfd_write_seismograms_nc(cgfd_solver *h, const char *path, const float *pos) {
+  CGFD_ABI_BEGIN
   if (!h || !path) return arg_fail(h, "null argument");
   const int n = h->nrecv, nt = h->d.nt;
   int done = 0;
@@ -2520,12 +2640,14 @@ int cgfd_write_seismograms_nc(cgfd_solver *h, const char *path, const float *pos
     return CGFD_ERR_ARG;
   }
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 // peakvel.nc of the reference (src/seisnc.cpp:1671-1757) in NetCDF classic:
 // i x j; Vx, Vy, Vz (the reference's file holds Vy in its Vz variable; this
 // one holds Vz)
 int cgfd_write_peak_velocity_nc(cgfd_solver *h, const char *path) {
+  CGFD_ABI_BEGIN
   if (!h || !path) return arg_fail(h, "null argument");
   std::vector<float> pv((size_t)3 * h->d.ni * h->d.nj);
   int st = cgfd_get_peak_velocity(h, pv.data());
@@ -2541,12 +2663,14 @@ int cgfd_write_peak_velocity_nc(cgfd_solver *h, const char *path) {
     return CGFD_ERR_ARG;
   }
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 
 // ------------------------- learned absorbing layer -------------------------
 
 int cgfd_set_boundary_mlp(cgfd_solver *h, int width, const void *weights_fp16) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   DevGuard guard(h->d.device);
   CK(h, cudaStreamSynchronize(h->st));
@@ -2601,9 +2725,11 @@ int cgfd_set_boundary_mlp(cgfd_solver *h, int width, const void *weights_fp16) {
   CK(h, cudaMalloc(&h->d_mlp_gain, (size_t)9 * width * sizeof(float)));
   h->mlp_width = width;
   return cgfd_set_boundary_mlp_gains(h, nullptr);
+  CGFD_ABI_END(h)
 }
 
 int cgfd_set_boundary_mlp_gains(cgfd_solver *h, const float *gains) {
+  CGFD_ABI_BEGIN
   if (!h) return arg_fail(h, "null handle");
   if (!h->mlp_n) return arg_fail(h, "no learned layer set");
   DevGuard guard(h->d.device);
@@ -2615,18 +2741,22 @@ int cgfd_set_boundary_mlp_gains(cgfd_solver *h, const float *gains) {
   CK(h, cudaMemcpy(h->d_mlp_gain, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice));
   invalidate(h);
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_boundary_mlp_cells(cgfd_solver *h, int *ijk, int *n) {
+  CGFD_ABI_BEGIN
   if (!h || !n) return arg_fail(h, "null argument");
   const int cap = *n;
   *n = h->mlp_n;
   if (ijk && cap >= h->mlp_n)
     std::memcpy(ijk, h->mlp_ijk.data(), h->mlp_ijk.size() * sizeof(int));
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 int cgfd_boundary_mlp_features(cgfd_solver *h, float *x, float *scale, float *rho_vp) {
+  CGFD_ABI_BEGIN
   if (!h || !x || !scale || !rho_vp) return arg_fail(h, "null argument");
   if (!h->mlp_n) return arg_fail(h, "no learned layer set");
   DevGuard guard(h->d.device);
@@ -2647,6 +2777,7 @@ int cgfd_boundary_mlp_features(cgfd_solver *h, float *x, float *scale, float *rh
   cudaFree(d);
   if (e != cudaSuccess) return cuda_fail(h, e, "layer features");
   return CGFD_OK;
+  CGFD_ABI_END(h)
 }
 
 }  // extern "C"

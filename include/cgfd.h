@@ -36,7 +36,9 @@ typedef enum cgfd_status {
     CGFD_ERR_ARG       = 1,  /* bad argument, size or index                    */
     CGFD_ERR_CUDA      = 2,  /* CUDA runtime error (text in cgfd_last_error)    */
     CGFD_ERR_STATE     = 3,  /* call out of order (e.g. step before upload)     */
-    CGFD_ERR_NOMEM     = 4,  /* device or host allocation failed                */
+    CGFD_ERR_NOMEM     = 4,  /* device or host allocation failed, or a host     *
+                              * thread could not start (a C++ exception inside *
+                              * the library, caught at the entry point)        */
     CGFD_ERR_TIMEOUT   = 5,  /* a bounded wait on the device ran out            */
     CGFD_ERR_NONFINITE = 6,  /* NaN or Inf found in the wavefield               */
     CGFD_ERR_NODEVICE  = 7   /* no usable CUDA device                           */

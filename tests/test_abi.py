@@ -37,6 +37,34 @@ def test_binding_covers_every_declared_symbol():
     assert sorted(cgfd.EXPORTED) == declared()
 
 
+def test_every_entry_point_keeps_exceptions_inside():
+    """Every definition of a declared entry point runs its body between
+    CGFD_ABI_BEGIN and CGFD_ABI_END (csrc/abi_guard.h), so a host allocation
+    or thread failure returns CGFD_ERR_NOMEM instead of unwinding into the
+    caller; and every declared entry point is defined exactly once."""
+    csrc = os.path.join(ROOT, "copara-cgfd3d_b200", "csrc")
+    seen = {}
+    for fn in sorted(os.listdir(csrc)):
+        if not fn.endswith((".cu", ".cpp")):
+            continue
+        lines = open(os.path.join(csrc, fn)).read().split("\n")
+        for i, line in enumerate(lines):
+            m = re.match(r'^(?:extern "C" )?int (cgfd_\w+)\(', line)
+            if not m:
+                continue
+            j = i
+            while not lines[j].rstrip().endswith(("{", ";")):
+                j += 1
+            if lines[j].rstrip().endswith(";"):
+                continue
+            k = lines.index("}", j)
+            seen[m.group(1)] = seen.get(m.group(1), 0) + 1
+            assert lines[j + 1].strip() == "CGFD_ABI_BEGIN", (fn, m.group(1))
+            assert lines[k - 1].strip().startswith("CGFD_ABI_END("), (fn, m.group(1))
+    assert sorted(seen) == declared()
+    assert all(v == 1 for v in seen.values())
+
+
 def test_product_library_has_no_oracle_dependency():
     import cgfd
     out = subprocess.run(["nm", "-D", cgfd.LIB_PATH], capture_output=True, text=True).stdout

@@ -106,3 +106,47 @@ def test_readers_refuse_mismatched_sizes(tmp_path):
                                              *[cgfd._d(buf)] * 3, *[cgfd._f(f)] * 3)
     assert st == cgfd.ERR_ARG and "sizes differ" in cgfd.last_error(None)
     assert os.path.exists(p)
+
+
+def _damage_dims(raw, lens):
+    """raw with the lengths of the CDF-2 header's dimensions x and y replaced
+    (a dimension entry: name length, name padded to 4 bytes, length)."""
+    for (name, n), new in zip(((b"x", 5), (b"y", 4)), lens):
+        entry = (1).to_bytes(4, "big") + name + b"\0\0\0" + n.to_bytes(4, "big")
+        assert raw.count(entry) == 1
+        raw = raw.replace(entry, entry[:-4] + new.to_bytes(4, "big"))
+    return raw
+
+
+def test_readers_refuse_data_outside_the_file(tmp_path):
+    """A truncated file, and damaged headers whose dimensions claim more data
+    than the file holds, are refused before anything is allocated or
+    written: 2^31-1 x 2^31-1 x 6 values (a count that overflows 64 bits) at
+    the size query, 2^24 x 4 x 6 values when the variables are read."""
+    import ctypes as C
+    p = str(tmp_path / "v.nc")
+    _write_volume(p)
+    raw = open(p, "rb").read()
+    t = str(tmp_path / "truncated.nc")
+    with open(t, "wb") as f:
+        f.write(raw[:-100])
+    with pytest.raises(cgfd.CgfdError, match="outside the file"):
+        cgfd.read_media_volume_nc(t)
+    d = str(tmp_path / "overflow.nc")
+    with open(d, "wb") as f:
+        f.write(_damage_dims(raw, (0x7FFFFFFF, 0x7FFFFFFF)))
+    with pytest.raises(cgfd.CgfdError, match="overflows"):
+        cgfd.read_media_volume_nc(d)
+    d = str(tmp_path / "damaged.nc")
+    with open(d, "wb") as f:
+        f.write(_damage_dims(raw, (1 << 24, 4)))
+    n = [C.c_int(0) for _ in range(3)]
+    st = cgfd._lib.cgfd_read_media_volume_nc(d.encode(), *[C.byref(x) for x in n], None, None,
+                                             None, None, None, None)
+    assert st == 0 and [x.value for x in n] == [1 << 24, 4, 6]
+    small = [np.zeros(8) for _ in range(3)] + [np.zeros(8, np.float32) for _ in range(3)]
+    ptrs = [cgfd._d(a) for a in small[:3]] + [cgfd._f(a) for a in small[3:]]
+    st = cgfd._lib.cgfd_read_media_volume_nc(d.encode(), *[C.byref(x) for x in n], *ptrs)
+    assert st == cgfd.ERR_ARG
+    assert "outside the file" in cgfd.last_error(None)
+    assert all(not a.any() for a in small)
