@@ -41,6 +41,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -127,7 +128,9 @@ struct Solver {
   struct Emul {
     int ebits = 0, mbits = 0;  // 0: off
     int mask = 0;              // 1: W, 2: tW, 4: FW
-    int flags = 0;             // 1: tW kept as tW - FW, 2: W kept as W - FW
+    int flags = 0;             // 1: tW kept as tW - FW, 2: W kept as W - FW,
+                               // 4: FW's rounding residual carried in the tW set,
+                               // 8: stochastic rounding
     int adapt = -1;            // >= 0: scales re-chosen every step, max at 2^adapt
     double scale[9] = {1, 1, 1, 1, 1, 1, 1, 1, 1};
   } em;
@@ -150,6 +153,31 @@ double quant_fmt(double x, int ebits, int mbits) {
   if (q > mx) q = mx;
   if (q < -mx) q = -mx;
   return q;
+}
+
+// The same format, rounded stochastically: up with probability equal to the
+// fraction of an ulp above the lower neighbour (u uniform in [0, 1)).
+double quant_fmt_sr(double x, int ebits, int mbits, double u) {
+  if (x == 0.0 || ebits <= 0) return x;
+  const int emax = (1 << (ebits - 1)) - 1, emin = 1 - emax;
+  int e;
+  std::frexp(x, &e);
+  const int ex = (e - 1 < emin) ? emin : e - 1;
+  const double ulp = std::ldexp(1.0, ex - mbits);
+  double q = std::floor(x / ulp + u) * ulp;
+  const double mx = std::ldexp(2.0 - std::ldexp(1.0, -mbits), emax);
+  if (q > mx) q = mx;
+  if (q < -mx) q = -mx;
+  return q;
+}
+
+// uniform [0, 1) from a 64-bit key (splitmix64 finaliser)
+double hash_unit(uint64_t k) {
+  k += 0x9E3779B97F4A7C15ull;
+  k = (k ^ (k >> 30)) * 0xBF58476D1CE4E5B9ull;
+  k = (k ^ (k >> 27)) * 0x94D049BB133111EBull;
+  k ^= k >> 31;
+  return (double)(k >> 11) * 0x1.0p-53;
 }
 
 struct Handle {
@@ -560,8 +588,16 @@ void update_emulated(Solver<R> &S, int rk) {
   const double b = RKB[rk] * S.d.stept;
   const int ni = S.d.ni, nj = S.d.nj, nk = S.d.nk;
   const bool block = E.ebits >= 100;  // block floating point: rounded below, per block
-  auto q = [&](double v, int c, int set) {
+  const bool fb = (E.flags & 4) != 0;   // requires flags & 1 (checked at set-up)
+  const bool sr = (E.flags & 8) != 0;
+  const uint64_t stage_key = ((uint64_t)S.steps * 4 + (uint64_t)rk) << 40;
+  // v rounded as set `set` stores component c of cell p
+  auto qp = [&](double v, int c, int set, long p) {
     if (!(E.mask & set) || block) return v;
+    if (sr) {
+      const uint64_t key = stage_key ^ ((uint64_t)p * 64 + (uint64_t)c * 8 + (uint64_t)set);
+      return quant_fmt_sr(v / E.scale[c], E.ebits, E.mbits, hash_unit(key)) * E.scale[c];
+    }
     return quant_fmt(v / E.scale[c], E.ebits, E.mbits) * E.scale[c];
   };
 #pragma omp parallel for schedule(static)
@@ -569,6 +605,7 @@ void update_emulated(Solver<R> &S, int rk) {
     for (int j = LFD; j < nj + LFD; ++j)
       for (int k = LFD; k < nk + LFD; ++k) {
         const long p = S.gi(i, j, k);
+        auto q = [&](double v, int c, int set) { return qp(v, c, set, p); };
         for (int c = 0; c < 9; ++c) {
           const double f = S.FW[c][p], h = S.hW[c][p], w = S.W[c][p];
           const double dtw = (E.flags & 1) ? 1.0 : 0.0, dw = (E.flags & 2) ? 1.0 : 0.0;
@@ -576,12 +613,23 @@ void update_emulated(Solver<R> &S, int rk) {
             S.W[c][p] = (R)(dw * f + q(f * (1 - dw) + a * h, c, 1));
           } else if (rk < 3) {
             double t;
-            if (rk == 1) t = (RKB[0] / RKA[0]) * (w - f) + b * h + (1 - dtw) * f;
-            else t = S.tW[c][p] - dtw * f + b * h;
+            if (rk == 1) {
+              t = (RKB[0] / RKA[0]) * (w - f) + b * h + (1 - dtw) * f;
+              // error feedback: the tW set still holds FW + r, r the part of
+              // the last step's new state that FW's rounding dropped
+              if (fb) t += (double)S.tW[c][p] - f;
+            } else {
+              t = S.tW[c][p] - dtw * f + b * h;
+            }
             S.tW[c][p] = (R)(dtw * f + q(t, c, 2));
             S.W[c][p] = (R)(dw * f + q(f * (1 - dw) + a * h, c, 1));
           } else {
-            S.W[c][p] = (R)q(S.tW[c][p] + b * h, c, 4);
+            const double ex = S.tW[c][p] + b * h, wn = q(ex, c, 4);
+            S.W[c][p] = (R)wn;
+            // error feedback: keep the rounding residual as the tW set's
+            // difference from the new state (read back in the next step's
+            // second stage; the first stage does not touch the tW set)
+            if (fb) S.tW[c][p] = (R)(wn + q(ex - wn, c, 2));
           }
         }
       }
@@ -617,8 +665,10 @@ void update_emulated(Solver<R> &S, int rk) {
   if (rk < 3) {
     if (E.mask & 1) qblock(S.W, S.FW, (E.flags & 2) != 0);
     if ((E.mask & 2) && rk > 0) qblock(S.tW, S.FW, (E.flags & 1) != 0);
-  } else if (E.mask & 4) {
-    qblock(S.W, S.FW, false);
+  } else {
+    // the loop left the exact new state in W (and, with error feedback, in tW)
+    if (E.mask & 4) qblock(S.W, S.FW, false);
+    if (fb && (E.mask & 2)) qblock(S.tW, S.W, true);  // the residual, against the new FW
   }
 }
 
@@ -979,14 +1029,19 @@ int orc_get_aux(void *h, int dir, int set, int comp, double *out, long *n) {
 // stands for s * scale[c]); flags 1: tW kept as its difference from FW, 2: W
 // kept as its difference from FW; adapt >= 0: after every step each scale
 // becomes the power of two that puts the component's maximum just below
-// 2^adapt.  ebits = 0 turns it off; ebits = 100 + B: block floating point,
+// 2^adapt; flags 4 (with 1): error feedback -- the last stage keeps the part
+// of the new state that FW's rounding drops (r = exact - FW) in the tW set,
+// tW = FW + r, and the next step's second stage adds it to the accumulator,
+// so FW's roundings do not accumulate in the state; flags 8: every rounding
+// stochastic (keyed by step, stage, cell, component and set).  ebits = 0
+// turns it off; ebits = 100 + B: block floating point,
 // B x-adjacent cells sharing an exponent, mbits magnitude bits each (plus a
 // sign).  FP64 oracle only.
 int orc_set_storage_emulation(void *h, int ebits, int mbits, const double *scale, int mask,
                               int flags, int adapt) {
   Handle *H = (Handle *)h;
   if (!H || H->prec != 0 || ebits < 0 || (ebits > 11 && ebits < 101) || ebits > 164 ||
-      mbits < 1 || mbits > 52)
+      mbits < 1 || mbits > 52 || ((flags & 4) && !(flags & 1)) || ((flags & 8) && ebits >= 100))
     return CGFD_ERR_ARG;
   auto &S = *(Solver<double> *)H->s;
   S.em.ebits = ebits;
