@@ -308,6 +308,12 @@ int cgfd_cfs_factors(int ni, int nj, int nk, const int nabs[6], const double vel
       !dlz || !apd_x || !apd_y || !apd_z || !b_x || !b_y || !b_z || !db_x || !db_y || !db_z)
     return CGFD_ERR_ARG;
   const int nvalid[3] = {ni, nj, nk};
+  for (int face = 0; face < 6; ++face)
+    if (nabs[face] < 0 || nabs[face] > nvalid[face / 2]) {
+      cgfd::set_global_error(
+          "cgfd_cfs_factors: a layer is of negative width or wider than the grid along its axis");
+      return CGFD_ERR_ARG;
+    }
   const double *dl[3] = {dlx, dly, dlz};
   double *apd[3] = {apd_x, apd_y, apd_z}, *bb[3] = {b_x, b_y, b_z}, *db[3] = {db_x, db_y, db_z};
   // exponents of the d, beta and alpha profiles (Zhang 2010 ADE CFS-PML)

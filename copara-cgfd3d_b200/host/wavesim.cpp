@@ -115,6 +115,10 @@ struct Snap {
   int s[3], n[3], d[3], tinv, cmp;
 };
 
+// bounds on what a par file may ask for, far above any model that fits a GPU:
+// cells along one axis, time steps, receivers and sources of one kind
+constexpr int kMaxCells = 1 << 20, kMaxSteps = 1 << 28, kMaxPoints = 1 << 24;
+
 struct Model {
   int ni, nj, nk, nt, con = 0, nabs[6] = {0, 0, 0, 0, 0, 0};
   double steph, stept;
@@ -292,11 +296,13 @@ void read_sources(const Par &conf, const std::string &dir, Model &m) {
   }
   if (type != 2 && type != 3) die("source_type must be 1, 2 or 3");
   const int nfrc = s.i("number_of_force_source"), nmnt = s.i("number_of_moment_source");
+  if (nfrc < 0 || nmnt < 0 || nfrc > kMaxPoints || nmnt > kMaxPoints)
+    die("number_of_force_source or number_of_moment_source out of range");
   std::vector<double> stf(nstf);
   if (nfrc > 0) {
     const int nwin = s.i("force_stf_window");
     const std::vector<std::string> t = s.after("<anchor_force>");
-    if ((int)t.size() < 8 * nfrc) die("force block too short");
+    if (t.size() / 8 < (size_t)nfrc) die("force block too short");
     std::vector<double> pos(3 * nfrc), start(nfrc);
     m.f3.assign(3 * nfrc, 0.f);
     for (int q = 0; q < nfrc; ++q) {
@@ -324,7 +330,7 @@ void read_sources(const Par &conf, const std::string &dir, Model &m) {
     if (mech != "moment" && mech != "angle") die("moment_mech_input must be moment or angle");
     const int ncol = mech == "moment" ? 11 : 8;
     const std::vector<std::string> t = s.after("<anchor_moment>");
-    if ((int)t.size() < ncol * nmnt) die("moment block too short");
+    if (t.size() / ncol < (size_t)nmnt) die("moment block too short");
     std::vector<double> pos(3 * nmnt), start(nmnt);
     m.m6.assign(6 * nmnt, 0.f);
     for (int q = 0; q < nmnt; ++q) {
@@ -368,6 +374,9 @@ void read_stations(const Par &conf, const std::string &dir, Model &m) {
   if (m.seis_tinv < 1) die("tinv_of_seismo must be at least 1");
   const int nsnap = s.i("number_of_snap"), nline = s.i("number_of_inline");
   const int nrecv = s.i("number_of_recv");
+  if (nsnap < 0 || nline < 0 || nrecv < 0 || nsnap > 999 || nline > 999 || nrecv > kMaxPoints)
+    die("number_of_snap, number_of_inline or number_of_recv out of range");
+  const int last[3] = {m.ni + LFD - 1, m.nj + LFD - 1, m.nk + LFD - 1};
   char key[32];
   for (int q = 0; q < nsnap; ++q) {
     std::snprintf(key, sizeof(key), "snap_%3.3d", q + 1);
@@ -380,6 +389,10 @@ void read_stations(const Par &conf, const std::string &dir, Model &m) {
     sn.tinv = s.i(key, 12);
     sn.cmp = s.i(key, 13);
     if (sn.tinv < 1 || sn.cmp < 1 || sn.cmp > 3) die(std::string(key) + ": bad tinv or cmp");
+    for (int a = 0; a < 3; ++a)
+      if (sn.s[a] < LFD || sn.n[a] < 1 || sn.d[a] < 1 ||
+          sn.s[a] + (long long)(sn.n[a] - 1) * sn.d[a] > last[a])
+        die(std::string(key) + ": start, count and stride must stay inside the grid");
     m.snaps.push_back(sn);
   }
   for (int q = 0; q < nrecv; ++q) {
@@ -390,7 +403,10 @@ void read_stations(const Par &conf, const std::string &dir, Model &m) {
     std::snprintf(key, sizeof(key), "line_%3.3d", l + 1);
     const double x0 = s.d(key, 3), y0 = s.d(key, 4), z0 = s.d(key, 5);
     const double dx = s.d(key, 7), dy = s.d(key, 8), dz = s.d(key, 9);
-    const int num = (int)s.d(key, 11);
+    const double fnum = s.d(key, 11);
+    if (!(fnum >= 0 && fnum <= kMaxPoints)) die(std::string(key) + ": receiver count out of range");
+    const int num = (int)fnum;
+    if (m.recv.size() + (size_t)num > (size_t)kMaxPoints) die("too many receivers");
     for (int j = 0; j < num; ++j) m.recv.push_back({x0 + j * dx, y0 + j * dy, z0 + j * dz, j, l + 1});
   }
   std::vector<double> pos(3 * m.recv.size());
@@ -554,6 +570,8 @@ int main(int argc, char **argv) {
   m.steph = conf.d("steph");
   if (m.ni < 1 || m.nj < 1 || m.nk < 4 || m.nt < 1 || !(m.stept > 0) || !(m.steph > 0))
     die("bad ni/nj/nk/nt/stept/steph");
+  if (m.ni > kMaxCells || m.nj > kMaxCells || m.nk > kMaxCells || m.nt > kMaxSteps)
+    die("ni/nj/nk or nt out of range");
   m.N = (size_t)(m.ni + 6) * (m.nj + 6) * (m.nk + 6);
   read_grid(conf, dir, m);
   read_media(conf, dir, m);

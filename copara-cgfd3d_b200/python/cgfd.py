@@ -537,7 +537,7 @@ def cfs_factors(ni, nj, nk, nabs, velabs, bmax, amax, dlx, dly, dlz):
     st = _lib.cgfd_cfs_factors(ni, nj, nk, _i(nabs), _d(v), _d(bm), _d(am),
                                *[_d(a) for a in dl], *[_d(o) for o in outs])
     if st:
-        raise CgfdError(st, "cfs_factors")
+        raise CgfdError(st, last_error(None) or "cfs_factors")
     return tuple(outs[0:3]), tuple(outs[3:6]), tuple(outs[6:9])
 
 

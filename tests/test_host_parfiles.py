@@ -111,3 +111,29 @@ def test_host_reports_bad_par_files(tmp_path):
     open(conf, "w").write(txt.replace("absorb_filename = absorb.dat", "absorb_filename = no.dat"))
     with pytest.raises(RuntimeError, match="cannot open"):
         hostio.run(d, "--dump", "m.bin")
+
+
+@pytest.mark.parametrize("fname,old,new,match", [
+    ("source.dat", "number_of_force_source = 1", "number_of_force_source = 2147483647",
+     "out of range"),
+    ("source.dat", "number_of_moment_source = 2", "number_of_moment_source = 3",
+     "moment block too short"),
+    ("station.dat", "snap_002 = 24 1 1 1 20 16 1 2 2 20 3", "snap_002 = 24 1 1 1 21 16 1 2 2 20 3",
+     "inside the grid"),
+    ("station.dat", "line_001 = -1500 0 9e+06 | 500 0 0 | 7",
+     "line_001 = -1500 0 9e+06 | 500 0 0 | 1e12", "receiver count out of range"),
+    ("SeisFD3D.conf", "nj    = 40", "nj    = 2147483647", "out of range"),
+])
+def test_host_bounds_what_par_files_ask_for(tmp_path, fname, old, new, match):
+    """Counts and ranges read from the par files are checked before they size
+    an allocation or an index: source and receiver counts, the anchor blocks'
+    lengths, snapshot windows (start + (count - 1) * stride inside the grid)
+    and the grid's dimensions."""
+    d = str(tmp_path)
+    hostio.copy_parfiles(d)
+    p = os.path.join(d, fname)
+    txt = open(p).read()
+    assert old in txt
+    open(p, "w").write(txt.replace(old, new))
+    with pytest.raises(RuntimeError, match=match):
+        hostio.run(d, "--dump", "m.bin")

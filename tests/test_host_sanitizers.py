@@ -6,6 +6,8 @@ with AddressSanitizer and UndefinedBehaviorSanitizer on the CPU:
   wavelets, point location and smoothing, volume media, NetCDF round trips
   and errors) run with the binding's host entry points routed to the
   instrumented build (tests/sanitize/route_host.py);
+* the host program (wavesim_b200, host/wavesim.cpp, built the same way over
+  the instrumented host code) runs its par-file tests;
 * the NetCDF readers take 1500 damaged files (random header bytes and words,
   files cut short; tests/sanitize/fuzz_ncread.py).
 
@@ -69,3 +71,27 @@ def test_netcdf_readers_on_damaged_files_under_sanitizers(sanitized, tmp_path):
                        cwd=ROOT, env=env, capture_output=True, text=True, timeout=1200)
     assert r.returncode == 0, (r.stdout[-4000:], r.stderr[-4000:])
     assert "reads ok" in r.stdout
+
+
+def test_host_program_under_sanitizers(sanitized):
+    lib, env = sanitized
+    import cgfd
+    d = os.path.dirname(lib)
+    prog = os.path.join(d, "wavesim_sanitized")
+    subprocess.run(["g++", "-g", "-O1", "-std=c++17", "-pthread",
+                    "-fsanitize=address,undefined", "-fno-omit-frame-pointer",
+                    "-fno-sanitize-recover=undefined",
+                    os.path.join(ROOT, "copara-cgfd3d_b200", "host", "wavesim.cpp"),
+                    os.path.join(CSRC, "ncwrite.cpp"),
+                    "-L" + d, "-lcgfd_host_sanitized",
+                    "-L" + os.path.dirname(cgfd.LIB_PATH), "-lcgfd",
+                    "-Wl,-rpath," + d, "-Wl,-rpath," + os.path.dirname(cgfd.LIB_PATH),
+                    "-o", prog], check=True)
+    env = dict(env, CGFD_HOST_SANITIZED_PROGRAM=prog)
+    env.pop("LD_PRELOAD")  # the program links the sanitizer runtime itself
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-p", "route_host_program",
+                        "-p", "no:cacheprovider", "-m", "not gpu",
+                        os.path.join(HERE, "test_host_parfiles.py")],
+                       cwd=ROOT, env=env, capture_output=True, text=True, timeout=1200)
+    assert r.returncode == 0, (r.stdout[-4000:], r.stderr[-4000:])
+    assert " passed" in r.stdout

@@ -32,6 +32,16 @@ def test_flat_grid_has_trivial_metric():
     assert np.all(m["xi_x"][v] == 1) and np.all(m["eta_y"][v] == 1)
 
 
+@pytest.mark.parametrize("nabs", [(31, 0, 0, 0, 0, 0), (0, 0, 0, 28, 0, 0), (0, 0, 0, 0, -1, 0)])
+def test_cfs_factors_refuse_layers_wider_than_the_grid(nabs):
+    """A layer wider than the grid along its axis (or of negative width) is
+    an argument error, not a write before or past the profile arrays."""
+    ni, nj, nk = 30, 27, 25
+    dl = [np.full(n + 6, 100.0) for n in (ni, nj, nk)]
+    with pytest.raises(cgfd.CgfdError, match="wider than the grid"):
+        cgfd.cfs_factors(ni, nj, nk, nabs, [8500.0] * 6, [2.5] * 6, [5.0] * 6, *dl)
+
+
 @pytest.mark.parametrize("nabs", [(12, 12, 12, 12, 12, 0), (3, 5, 0, 7, 4, 0), (6, 4, 5, 5, 5, 0)])
 def test_cfs_factors_match_oracle(nabs):
     ni, nj, nk = 30, 27, 25
