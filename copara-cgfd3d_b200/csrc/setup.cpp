@@ -438,10 +438,13 @@ int cgfd_grid_vmap(int ni, int nj, int nk, int nsurf, const int *gridpoints,
       return grid_fail("two adjacent layers cannot both be graded");
   if (total + 1 != nk) return grid_fail("the layers' intervals + 1 must equal nk");
   for (int i = 0; i < ni; ++i)
-    for (int j = 0; j < nj; ++j)
+    for (int j = 0; j < nj; ++j) {
+      for (int q = 0; q < stride; ++q)
+        if (!std::isfinite(col(i, j)[q])) return grid_fail("anchor values must be finite");
       for (int q = 1; q < nsurf; ++q)
         if (col(i, j)[2 + q] > col(i, j)[1 + q])
           return grid_fail("interface depths must decrease from the top down");
+    }
 
   // the layer stack actually meshed: the given one, or (hybrid) its layers
   // above the conversion depth, the layer holding it cut there, and one flat
@@ -491,7 +494,10 @@ int cgfd_grid_vmap(int ni, int nj, int nk, int nsurf, const int *gridpoints,
     for (int l = 0; l < conv_iface; ++l) eq[l] = equalspacing[l];
     gp[conv_iface] = nk - 1;
     for (int l = 0; l < conv_iface; ++l) {
-      gp[l] = (int)(nk * (hi[l] - lo[l]) / total_len);
+      const double share = nk * (hi[l] - lo[l]) / total_len;  // truncated, as the reference
+      if (!(share >= 0.0 && share <= nk))
+        return grid_fail("the hybrid grid's layer thicknesses give no valid split");
+      gp[l] = (int)share;
       gp[conv_iface] -= gp[l];
     }
     for (int l = 0; l <= conv_iface; ++l)

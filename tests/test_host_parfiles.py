@@ -123,12 +123,14 @@ def test_host_reports_bad_par_files(tmp_path):
     ("station.dat", "line_001 = -1500 0 9e+06 | 500 0 0 | 7",
      "line_001 = -1500 0 9e+06 | 500 0 0 | 1e12", "receiver count out of range"),
     ("SeisFD3D.conf", "nj    = 40", "nj    = 2147483647", "out of range"),
+    ("grid_vmap.dat", "-2350.000000 -1950.000000 0.318052 -3100.000000",
+     "-2350.000000 -1950.000000 nan -3100.000000", "anchor values must be finite"),
 ])
 def test_host_bounds_what_par_files_ask_for(tmp_path, fname, old, new, match):
     """Counts and ranges read from the par files are checked before they size
     an allocation or an index: source and receiver counts, the anchor blocks'
-    lengths, snapshot windows (start + (count - 1) * stride inside the grid)
-    and the grid's dimensions."""
+    lengths, snapshot windows (start + (count - 1) * stride inside the grid),
+    the grid's dimensions and the vmap anchors (finite)."""
     d = str(tmp_path)
     hostio.copy_parfiles(d)
     p = os.path.join(d, fname)
