@@ -19,6 +19,7 @@
 #include "../../include/cgfd.h"
 #include "../csrc/ncwrite.h"
 
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -81,7 +82,14 @@ struct Par {
       die("no value at column " + std::to_string(col) + " for " + key + " in " + path);
     return v;
   }
-  int i(const std::string &key, int col = 3) const { return std::atoi(str(key, col).c_str()); }
+  // an integer (atoi's reading: leading digits, 0 for none), refused beyond
+  // half the int range so that index arithmetic on it cannot overflow
+  int i(const std::string &key, int col = 3) const {
+    const long long v = std::strtoll(str(key, col).c_str(), nullptr, 10);
+    if (v > INT_MAX / 2 || v < INT_MIN / 2)
+      die(key + " in " + path + ": integer out of range");
+    return (int)v;
+  }
   double d(const std::string &key, int col = 3) const { return std::atof(str(key, col).c_str()); }
   // whitespace tokens after the line whose first token is `anchor`
   std::vector<std::string> after(const std::string &anchor) const {
