@@ -8,6 +8,8 @@ with AddressSanitizer and UndefinedBehaviorSanitizer on the CPU:
   instrumented build (tests/sanitize/route_host.py);
 * the host program (wavesim_b200, host/wavesim.cpp, built the same way over
   the instrumented host code) runs its par-file tests;
+* the host program reads 120 damaged par-file sets in its --dump mode
+  (tests/sanitize/fuzz_parfiles.py);
 * the NetCDF readers take 1500 damaged files (random header bytes and words,
   files cut short; tests/sanitize/fuzz_ncread.py).
 
@@ -73,7 +75,8 @@ def test_netcdf_readers_on_damaged_files_under_sanitizers(sanitized, tmp_path):
     assert "reads ok" in r.stdout
 
 
-def test_host_program_under_sanitizers(sanitized):
+@pytest.fixture(scope="module")
+def sanitized_program(sanitized):
     lib, env = sanitized
     import cgfd
     d = os.path.dirname(lib)
@@ -89,9 +92,23 @@ def test_host_program_under_sanitizers(sanitized):
                     "-o", prog], check=True)
     env = dict(env, CGFD_HOST_SANITIZED_PROGRAM=prog)
     env.pop("LD_PRELOAD")  # the program links the sanitizer runtime itself
+    return prog, env
+
+
+def test_host_program_under_sanitizers(sanitized_program):
+    _, env = sanitized_program
     r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-p", "route_host_program",
                         "-p", "no:cacheprovider", "-m", "not gpu",
                         os.path.join(HERE, "test_host_parfiles.py")],
                        cwd=ROOT, env=env, capture_output=True, text=True, timeout=1200)
     assert r.returncode == 0, (r.stdout[-4000:], r.stderr[-4000:])
     assert " passed" in r.stdout
+
+
+def test_host_program_on_damaged_par_files_under_sanitizers(sanitized_program, tmp_path):
+    prog, env = sanitized_program
+    r = subprocess.run([sys.executable, os.path.join(HERE, "sanitize", "fuzz_parfiles.py"), prog,
+                        os.path.join(HERE, "golden", "parfiles"), "11", "120", str(tmp_path)],
+                       cwd=ROOT, env=env, capture_output=True, text=True, timeout=1200)
+    assert r.returncode == 0, (r.stdout[-4000:], r.stderr[-4000:])
+    assert "failed 0" in r.stdout
