@@ -65,6 +65,31 @@ def test_every_entry_point_keeps_exceptions_inside():
     assert all(v == 1 for v in seen.values())
 
 
+def test_a_c99_host_builds_and_calls_the_library(tmp_path):
+    """include/cgfd.h compiles as strict C99 (-pedantic, no warnings), a C
+    program links libcgfd.so and calls it: a host-side entry point returns
+    the reference's strike/dip/rake tensor, and cgfd_create refuses a zeroed
+    description with CGFD_ERR_ARG and its text, without touching a GPU."""
+    import shutil
+    import cgfd
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc needed")
+    exe = str(tmp_path / "abi_c_caller")
+    lib_dir = os.path.dirname(cgfd.LIB_PATH)
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                        "-I" + os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "abi_c_caller.c"), "-L" + lib_dir, "-lcgfd",
+                        "-Wl,-rpath," + lib_dir, "-o", exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, (out.stdout, out.stderr)
+    f = out.stdout.split()
+    assert f[0] == "abi" and f[2] == "m6"
+    ref = cgfd.angle2moment(30.0, 60.0, 90.0)
+    assert [float(v) for v in f[3:6]] == pytest.approx(list(ref[:3]), abs=1e-6)
+    assert f[6] == "create" and int(f[7]) == cgfd.ERR_ARG and "bad grid" in out.stdout
+
+
 def test_product_library_has_no_oracle_dependency():
     import cgfd
     out = subprocess.run(["nm", "-D", cgfd.LIB_PATH], capture_output=True, text=True).stdout
