@@ -30,6 +30,10 @@ CASES = {
 }
 
 
+QUOTED = ["fp16_tw_difference_feedback", "bfp8x14_tw_difference",
+          "bfp8x14_tw_difference_feedback"]
+
+
 def main(names):
     models.use_preprocessing("oracle")
     gold = np.load(os.path.join(HERE, "c1_fp64_seismograms.npz"))["seis"]
@@ -48,4 +52,4 @@ def main(names):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or list(CASES))
+    main(sys.argv[1:] or QUOTED)
