@@ -8,6 +8,9 @@ with AddressSanitizer and UndefinedBehaviorSanitizer on the CPU:
   instrumented build (tests/sanitize/route_host.py);
 * the host program (wavesim_b200, host/wavesim.cpp, built the same way over
   the instrumented host code) runs its par-file tests;
+* the host-side entry points take 2000 calls with odd arguments (nan, inf,
+  huge and subnormal coordinates and scalars, layers wider than the grid,
+  sources off the grid; tests/sanitize/fuzz_host_calls.py);
 * the host program reads 120 damaged par-file sets in its --dump mode
   (tests/sanitize/fuzz_parfiles.py);
 * the NetCDF readers take 1500 damaged files (random header bytes and words,
@@ -47,10 +50,12 @@ def sanitized(tmp_path_factory):
         pytest.skip("g++ with AddressSanitizer is needed")
     lib = str(tmp_path_factory.mktemp("sanitized") / "libcgfd_host_sanitized.so")
     subprocess.run(["g++", "-shared", "-fPIC", "-g", "-O1", "-std=c++17", "-pthread",
-                    "-fsanitize=address,undefined", "-fno-omit-frame-pointer",
-                    "-fno-sanitize-recover=undefined", *SOURCES, "-o", lib], check=True)
-    env = dict(os.environ, LD_PRELOAD=asan, ASAN_OPTIONS="detect_leaks=0:halt_on_error=1",
-               UBSAN_OPTIONS="print_stacktrace=1", CGFD_HOST_SANITIZED_LIB=lib,
+                    "-fsanitize=address,undefined,float-cast-overflow",
+                    "-fno-omit-frame-pointer", "-fno-sanitize-recover=all", *SOURCES,
+                    "-o", lib], check=True)
+    env = dict(os.environ, LD_PRELOAD=asan, UBSAN_OPTIONS="print_stacktrace=1",
+               ASAN_OPTIONS="detect_leaks=0:halt_on_error=1",
+               CGFD_HOST_SANITIZED_LIB=lib,
                PYTHONPATH=os.pathsep.join([os.path.join(HERE, "sanitize"),
                                            os.environ.get("PYTHONPATH", "")]))
     return lib, env
@@ -82,8 +87,8 @@ def sanitized_program(sanitized):
     d = os.path.dirname(lib)
     prog = os.path.join(d, "wavesim_sanitized")
     subprocess.run(["g++", "-g", "-O1", "-std=c++17", "-pthread",
-                    "-fsanitize=address,undefined", "-fno-omit-frame-pointer",
-                    "-fno-sanitize-recover=undefined",
+                    "-fsanitize=address,undefined,float-cast-overflow",
+                    "-fno-omit-frame-pointer", "-fno-sanitize-recover=all",
                     os.path.join(ROOT, "copara-cgfd3d_b200", "host", "wavesim.cpp"),
                     os.path.join(CSRC, "ncwrite.cpp"),
                     "-L" + d, "-lcgfd_host_sanitized",
@@ -112,3 +117,12 @@ def test_host_program_on_damaged_par_files_under_sanitizers(sanitized_program, t
                        cwd=ROOT, env=env, capture_output=True, text=True, timeout=1200)
     assert r.returncode == 0, (r.stdout[-4000:], r.stderr[-4000:])
     assert "failed 0" in r.stdout
+
+
+def test_host_entry_points_on_odd_arguments_under_sanitizers(sanitized):
+    lib, env = sanitized
+    r = subprocess.run([sys.executable, os.path.join(HERE, "sanitize", "fuzz_host_calls.py"),
+                        lib, "5", "2000"],
+                       cwd=ROOT, env=env, capture_output=True, text=True, timeout=1200)
+    assert r.returncode == 0, (r.stdout[-4000:], r.stderr[-4000:])
+    assert "calls" in r.stdout
