@@ -148,6 +148,15 @@ def _as(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
+def _sized(a, dtype, n, what):
+    """a as a contiguous flat array of n values: the C ABI reads exactly n
+    through the pointer, so a shorter array would be read past its end."""
+    v = np.ascontiguousarray(a, dtype=dtype).reshape(-1)
+    if v.size != n:
+        raise ValueError(f"{what}: {v.size} values, the model needs {n}")
+    return v
+
+
 def last_error(handle=None) -> str:
     buf = C.create_string_buffer(1024)
     _lib.cgfd_last_error(handle, buf, 1024)
@@ -200,8 +209,7 @@ class Solver:
         if weights is None:
             self._chk(_lib.cgfd_set_boundary_mlp(self._h, width, None))
             return
-        w = np.ascontiguousarray(weights, np.float16)
-        assert w.size == MLP_PARAMS
+        w = _sized(weights, np.float16, MLP_PARAMS, "MLP weights")
         self._chk(_lib.cgfd_set_boundary_mlp(self._h, width, w.ctypes.data_as(C.c_void_p)))
 
     def set_boundary_mlp_gains(self, gains=None):
@@ -294,15 +302,20 @@ class Solver:
         self.close()
 
     def upload_metric(self, zeta_x, zeta_y, zeta_z, jac):
-        arrs = [_as(a, np.float64).reshape(-1) for a in (zeta_x, zeta_y, zeta_z, jac)]
+        n = int(np.prod(self.shape))
+        arrs = [_sized(a, np.float64, n, "metric array") for a in (zeta_x, zeta_y, zeta_z, jac)]
         self._chk(_lib.cgfd_upload_metric(self._h, *[_d(a) for a in arrs]))
 
     def upload_media(self, alpha, beta, rho):
-        arrs = [_as(a, np.float32).reshape(-1) for a in (alpha, beta, rho)]
+        n = int(np.prod(self.shape))
+        arrs = [_sized(a, np.float32, n, "media array") for a in (alpha, beta, rho)]
         self._chk(_lib.cgfd_upload_media(self._h, *[_f(a) for a in arrs]))
 
     def upload_pml(self, apd, b, db):
-        arrs = [_as(a, np.float64) for a in (*apd, *b, *db)]
+        """CFS-PML profiles: apd, b and db each a triple of arrays over the
+        full x, y and z index ranges (CalCFSfactors' APD, B and DB)."""
+        arrs = [_sized(a, np.float64, self.shape[q % 3], "PML profile")
+                for q, a in enumerate((*apd, *b, *db))]
         self._chk(_lib.cgfd_upload_pml(self._h, *[_d(a) for a in arrs]))
 
     def upload_moments(self, loc, m6, stf):

@@ -90,6 +90,27 @@ def test_a_c99_host_builds_and_calls_the_library(tmp_path):
     assert f[6] == "create" and int(f[7]) == cgfd.ERR_ARG and "bad grid" in out.stdout
 
 
+def test_binding_refuses_arrays_of_the_wrong_size():
+    """The C ABI reads exactly the model's number of values through each
+    pointer; the binding checks the sizes first, so a short array is a
+    ValueError, never a read past its end (no GPU: the checks come before
+    any library call)."""
+    import numpy as np
+    import cgfd
+    s = object.__new__(cgfd.Solver)
+    s._h, s._owned, s.shape = None, False, (10, 9, 8)
+    n = 10 * 9 * 8
+    with pytest.raises(ValueError, match="metric array: 719 values, the model needs 720"):
+        s.upload_metric(*[np.zeros(n)] * 3, np.zeros(n - 1))
+    with pytest.raises(ValueError, match="media array"):
+        s.upload_media(np.zeros(n), np.zeros((10, 9, 7)), np.zeros(n))
+    prof = [np.zeros(k) for k in s.shape]
+    with pytest.raises(ValueError, match="PML profile: 10 values, the model needs 9"):
+        s.upload_pml(prof, (prof[0], prof[0], prof[2]), prof)
+    with pytest.raises(ValueError, match="MLP weights"):
+        s.set_boundary_mlp(4, np.zeros(cgfd.MLP_PARAMS - 1))
+
+
 def test_product_library_has_no_oracle_dependency():
     import cgfd
     out = subprocess.run(["nm", "-D", cgfd.LIB_PATH], capture_output=True, text=True).stdout
