@@ -208,16 +208,18 @@ class Solver:
         as FP16; None disables)."""
         if weights is None:
             self._chk(_lib.cgfd_set_boundary_mlp(self._h, width, None))
+            self._mlp_width = 0
             return
         w = _sized(weights, np.float16, MLP_PARAMS, "MLP weights")
         self._chk(_lib.cgfd_set_boundary_mlp(self._h, width, w.ctypes.data_as(C.c_void_p)))
+        self._mlp_width = int(width)
 
     def set_boundary_mlp_gains(self, gains=None):
         """Per (depth, component) gains of the correction, [width][9]; None: 1."""
         if gains is None:
             self._chk(_lib.cgfd_set_boundary_mlp_gains(self._h, None))
             return
-        g = np.ascontiguousarray(gains, np.float32)
+        g = _sized(gains, np.float32, 9 * getattr(self, "_mlp_width", 0), "layer gains")
         self._chk(_lib.cgfd_set_boundary_mlp_gains(self._h, _f(g)))
 
     def boundary_mlp_cells(self) -> np.ndarray:
@@ -320,14 +322,14 @@ class Solver:
 
     def upload_moments(self, loc, m6, stf):
         loc = _as(loc, np.int32).reshape(-1, 3)
-        m6 = _as(m6, np.float32).reshape(-1, 6)
+        m6 = _sized(m6, np.float32, 6 * len(loc), "moment tensors").reshape(-1, 6)
         stf = _as(stf, np.float32).reshape(len(loc), -1)
         self._chk(_lib.cgfd_upload_moments(self._h, len(loc), _i(loc), _f(m6),
                                            stf.shape[1], _f(stf)))
 
     def upload_forces(self, loc, f3, stf):
         loc = _as(loc, np.int32).reshape(-1, 3)
-        f3 = _as(f3, np.float32).reshape(-1, 3)
+        f3 = _sized(f3, np.float32, 3 * len(loc), "force vectors").reshape(-1, 3)
         stf = _as(stf, np.float32).reshape(len(loc), -1)
         self._chk(_lib.cgfd_upload_forces(self._h, len(loc), _i(loc), _f(f3),
                                           stf.shape[1], _f(stf)))

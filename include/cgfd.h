@@ -273,10 +273,13 @@ int cgfd_write_peak_velocity_nc(cgfd_solver *h, const char *path);
 
 /* Enables (weights != NULL) or disables the learned correction of the thin
  * absorbing layer: after every step, each valid cell within `width` cells of
- * an absorbing face gets FW += MLP(features), the features being the 9
- * components at the cell and the next 4 cells along its inward normal,
- * stresses over rho*vp, normalised by their largest magnitude (the output
- * is scaled back the same way).  FP32 storage only.
+ * an absorbing face (never the free surface) gets a correction of FW from
+ * MLP(features), the features being the 9 components at the cell and the
+ * next 4 cells along its inward normal, stresses over rho*vp, normalised by
+ * their largest magnitude.  The correction of component c at depth d is
+ * gains[d][c] * 0.25 * tanh(y_c / 0.25), scaled back the same way and
+ * clamped so that it only moves the value toward zero (a learned,
+ * state-dependent damping).  Any storage type; members of a batch too.
  * No reference counterpart (the reference has sponge and CFS-PML layers). */
 int cgfd_set_boundary_mlp(cgfd_solver *h, int width, const void *weights_fp16);
 /* Gains of the correction per depth in the layer (0: the cells next to the

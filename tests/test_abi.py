@@ -109,6 +109,13 @@ def test_binding_refuses_arrays_of_the_wrong_size():
         s.upload_pml(prof, (prof[0], prof[0], prof[2]), prof)
     with pytest.raises(ValueError, match="MLP weights"):
         s.set_boundary_mlp(4, np.zeros(cgfd.MLP_PARAMS - 1))
+    with pytest.raises(ValueError, match="moment tensors: 12 values, the model needs 6"):
+        s.upload_moments([[5, 5, 5]], np.zeros(12), np.zeros((1, 10)))
+    with pytest.raises(ValueError, match="force vectors"):
+        s.upload_forces([[5, 5, 5], [6, 6, 6]], np.zeros(3), np.zeros((2, 10)))
+    s._mlp_width = 4
+    with pytest.raises(ValueError, match="layer gains: 9 values, the model needs 36"):
+        s.set_boundary_mlp_gains(np.ones(9))
 
 
 def test_product_library_has_no_oracle_dependency():
