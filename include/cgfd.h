@@ -383,8 +383,9 @@ int cgfd_batch_destroy(cgfd_batch *b);
  * planes below, the layers above re-cut in proportion to their thickness as
  * the reference does.  Outputs x, y, z as full arrays (ni+6)(nj+6)(nk+6),
  * z fastest, and *con_index (ConIndex: the first node index of the
- * curvilinear part; 3 when not hybrid).  The reference's input checks apply
- * (the message is available from cgfd_last_error(NULL, ...)). */
+ * curvilinear part; 3 when not hybrid).  The reference's input checks apply,
+ * and the anchors must be finite (the message is available from
+ * cgfd_last_error(NULL, ...)). */
 int cgfd_grid_vmap(int ni, int nj, int nk, int nsurf, const int *gridpoints,
                    const int *equalspacing, const double *anchor, int hybrid,
                    double convers_depth, double *x, double *y, double *z, int *con_index);
@@ -440,7 +441,9 @@ int cgfd_metric_from_coords(int ni, int nj, int nk, double steph,
 
 /* ADE CFS-PML profiles: absorb::CalCFSfactors (src/absorb.cpp:346-805).
  * dlx[i] (dly[j], dlz[k]) is steph/|grad xi| at (i, nj1, nk1)
- * (resp. |grad eta| at (ni1, j, nk1), |grad zeta| at (ni1, nj1, k)). */
+ * (resp. |grad eta| at (ni1, j, nk1), |grad zeta| at (ni1, nj1, k)).
+ * Each layer width nabs[f] must lie in [0, n] of its axis (CGFD_ERR_ARG
+ * otherwise). */
 int cgfd_cfs_factors(int ni, int nj, int nk, const int nabs[6],
                      const double velabs[6], const double bmax[6],
                      const double amax[6], const double *dlx,
