@@ -640,7 +640,7 @@ def main():
     if (not args.no_target and world == 1 and args.storage == "f32" and args.kernel == "fused"
             and not pml):
         line["target"] = run_target(args, value, ms / K, local)
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:  # the host-core baseline: N = 1 only
         line["cpu_baseline"] = cpu_baseline(args.config, args.cpu_seconds)
     print(json.dumps(line))
     if dist is not None:
