@@ -926,12 +926,16 @@ int cgfd_create(const cgfd_desc *d, cgfd_solver **out) {
   *out = nullptr;
   if (d->ni < 1 || d->nj < 1 || d->nk < 4 || !(d->steph > 0) || !(d->stept > 0) || d->nt < 0)
     return arg_fail(nullptr, "bad grid or step sizes");
+  // far above any grid that fits one GPU; keeps every index product in range
+  constexpr int MAX_AXIS = 1 << 20;
+  if (d->ni > MAX_AXIS || d->nj > MAX_AXIS || d->nk > MAX_AXIS)
+    return arg_fail(nullptr, "grid dimension above 2^20 cells");
   if (d->hybrid_grid != 1) return arg_fail(nullptr, "only hybrid_grid=1 (SimpleCar) is supported");
   for (int q = 0; q < 6; ++q)
     if (d->nabs[q] < 0) return arg_fail(nullptr, "negative nabs");
   if (d->nabs[5] != 0) return arg_fail(nullptr, "nabs[5] (top) must be 0: free surface");
-  if (d->nabs[0] + d->nabs[1] > d->ni || d->nabs[2] + d->nabs[3] > d->nj ||
-      d->nabs[4] + d->nabs[5] > d->nk)
+  if (d->nabs[0] > d->ni || d->nabs[1] > d->ni - d->nabs[0] || d->nabs[2] > d->nj ||
+      d->nabs[3] > d->nj - d->nabs[2] || d->nabs[4] > d->nk || d->nabs[5] > d->nk - d->nabs[4])
     return arg_fail(nullptr, "PML wider than the grid");
   if (d->con_index < LFD || d->con_index > d->nk + LFD - 1)
     return arg_fail(nullptr, "con_index must lie in [3, nk+2]");

@@ -148,6 +148,14 @@ def test_create_rejects_pml_on_top_and_oversized_pml():
     d = cgfd.make_desc(20, 20, 20, 100.0, 0.005, 10, 10, (12, 12, 4, 4, 4, 0))
     with pytest.raises(cgfd.CgfdError):
         cgfd.Solver(d)
+    # widths whose sum overflows an int, and a grid beyond 2^20 cells a side
+    big = 2 ** 31 - 1
+    d = cgfd.make_desc(20, 20, 20, 100.0, 0.005, 10, 10, (big, big, 4, 4, 4, 0))
+    with pytest.raises(cgfd.CgfdError, match="PML wider than the grid"):
+        cgfd.Solver(d)
+    d = cgfd.make_desc(big - 6, 20, 20, 100.0, 0.005, 10, 10, (4, 4, 4, 4, 4, 0))
+    with pytest.raises(cgfd.CgfdError, match="above 2\\^20"):
+        cgfd.Solver(d)
 
 
 @pytest.mark.parametrize("kernel", [1, 2])
